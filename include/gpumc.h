@@ -1,0 +1,203 @@
+/*
+ * gpumc.h - C ABI of the B200 lattice Metropolis engine.
+ *
+ * The engine replaces the hot path of the scamper workspace's classical crate
+ * (cmc-rs): the single-site Metropolis sweep of Ising, q-state Potts and O(3)
+ * spins on periodic square and cubic lattices, the 64-replica multi-spin
+ * Ising variant, and the parallel-tempering exchange that carlo-rs schedules
+ * around the sweep.  Each entry point below names the reference interface it
+ * stands in for (paths within the scamper workspace).
+ *
+ * Conventions (mirroring the reference's contract, Carlo.rs/src/monte_carlo.rs
+ * and Carlo.rs/src/error.rs):
+ *   - every call returns an int status: 0 = ok, negative = GPUMC_E* code;
+ *     gpumc_last_error() gives the message of the calling thread's last error
+ *     (the reference's CarloError::InvalidConfig {field, reason} text);
+ *   - handles are opaque; a handle is not thread-safe (the reference's
+ *     `&mut self` ownership), distinct handles may be used from distinct host
+ *     threads;
+ *   - device memory is owned by the engine; host buffers passed in are
+ *     caller-owned and copied;
+ *   - there is no CPU fallback: without a usable CUDA device every call that
+ *     needs one returns GPUMC_ENODEV.
+ */
+#ifndef GPUMC_H
+#define GPUMC_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUMC_OK 0
+#define GPUMC_EINVAL -1   /* invalid configuration or argument          */
+#define GPUMC_ENODEV -2   /* no usable CUDA device                      */
+#define GPUMC_ECUDA -3    /* CUDA runtime error                         */
+#define GPUMC_ENOMEM -4   /* device memory exhausted                    */
+#define GPUMC_EAGAIN -5   /* server: job does not fit the HBM budget now */
+#define GPUMC_ESTATE -6   /* call not valid in the handle's current state */
+#define GPUMC_ENOTFOUND -7
+
+/* models (cmc-rs IsingModel, PottsModel, HeisenbergModel = ONModel<3>,
+ * MultiSpinIsing: CMC.rs/src/lattice/models.rs:29-595, CMC.rs/src/multi_spin.rs) */
+#define GPUMC_ISING 0
+#define GPUMC_POTTS 1
+#define GPUMC_O3 2
+#define GPUMC_ISING_MSC64 3
+
+#define GPUMC_INIT_HOT 0  /* "hot" / "random" initial_state */
+#define GPUMC_INIT_COLD 1 /* "cold" / "ordered" */
+
+/* run phases (Carlo.rs/src/phase.rs:11-35): proposal adaptation only while
+ * thermalizing, records only while measuring */
+#define GPUMC_PHASE_THERMALIZATION 1
+#define GPUMC_PHASE_MEASUREMENT 2
+
+typedef struct gpumc_engine gpumc_engine;
+typedef struct gpumc_sim gpumc_sim;
+typedef struct gpumc_server gpumc_server;
+
+/* Simulation spec: the reference's Params keys for this path
+ * (CMC.rs/src/classical_mc.rs:336-489: L|Lx,Ly,Lz, lattice_type
+ * square|cubic, pbc, J, q, beta, initial_state) plus the replica ladder of
+ * ParallelTemperingConfig (Carlo.rs/src/parallel_tempering.rs:53-60). */
+typedef struct {
+  int32_t model;            /* GPUMC_ISING / POTTS / O3 / ISING_MSC64          */
+  int32_t dims;             /* 2 = square, 3 = cubic                           */
+  int64_t lx, ly, lz;       /* even extents >= 4 (lz ignored for dims = 2)     */
+  int32_t pbc;              /* must be 1: periodic boundaries                  */
+  int32_t q;                /* Potts states, 2..8                              */
+  double J;                 /* coupling, finite                                */
+  int32_t n_replicas;       /* lattices in this handle (MSC: 64-bit words     */
+                            /* lattices, 64 bit-replicas each)                 */
+  int32_t n_temps;          /* entries in betas: 1 (shared) or n_replicas      */
+  const double* betas;      /* inverse temperatures, finite and >= 0           */
+  int32_t init;             /* GPUMC_INIT_HOT / GPUMC_INIT_COLD                */
+  double cone_half_angle;   /* O(3): initial cap half-angle (radians), (0, pi] */
+  int32_t record_capacity;  /* measured sweeps buffered on the device (>= 1)   */
+} gpumc_spec;
+
+/* One measured sweep of one replica (Context::measure of Energy, E2,
+ * Magnetization, M2, M4: CMC.rs/src/observables/common.rs:81-95).  Energy is
+ * the total physical energy, not per site.  For the multi-spin model there is
+ * one record per bit-replica (64 per word lattice). */
+typedef struct {
+  uint64_t sweep;        /* 0-based index of the sweep that produced it       */
+  int32_t replica;       /* lattice (or bit-replica) index                    */
+  int32_t temp_index;    /* parameter-chain index held during the sweep       */
+  double beta;
+  double energy;
+  double magnetization;  /* |M|/N (Ising, O(3)); Potts order parameter        */
+  double acceptance;     /* accepted / attempted in this sweep                */
+} gpumc_obs;
+
+/* ---- engine (device context, stream, batched launches) ---------------- */
+int gpumc_engine_create(int32_t device, gpumc_engine** out);
+int gpumc_engine_destroy(gpumc_engine* eng);
+/* One batched launch per sweep over every simulation in the engine (all
+ * sizes, all replicas): the batched form of Scheduler::run_parallel's
+ * independent chains (Carlo.rs/src/scheduler.rs:345-405).  measure != 0
+ * records observables of every simulation whose phase is MEASUREMENT.
+ * Sweeps are captured in CUDA graphs of up to 64 launches. */
+int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps);
+int gpumc_engine_synchronize(gpumc_engine* eng);
+/* The CUDA stream (cudaStream_t) the engine launches on, for callers that
+ * time or order work around the engine with their own events. */
+int gpumc_engine_stream(gpumc_engine* eng, void** stream);
+/* The engine a simulation handle runs on (its private one if created with
+ * eng = NULL). */
+int gpumc_sim_engine(gpumc_sim* sim, gpumc_engine** eng);
+/* Kernel launches one sweep of this handle issues (sweep kernel plus, for a
+ * measuring multi-spin handle, its measurement kernels). */
+int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n);
+
+/* ---- simulation handle: ClassicalMC<H, MetropolisCore, _> ------------- */
+/* FromParams::from_params (Carlo.rs/src/monte_carlo.rs:80-88;
+ * CMC.rs/src/classical_mc.rs:443-489).  eng may be NULL (private engine). */
+int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, gpumc_sim** out);
+/* FromParams::validate_params: checks a spec without allocating. */
+int gpumc_validate(const gpumc_spec* spec);
+int gpumc_destroy(gpumc_sim* sim);
+/* MonteCarlo::on_phase_start (Carlo.rs/src/monte_carlo.rs:31-77). */
+int gpumc_set_phase(gpumc_sim* sim, int32_t phase);
+/* MonteCarlo::sweep (+ measure after each sweep while measuring):
+ * n_sweeps full sweeps of every replica of this handle, launched alone
+ * (the plain single-simulation path). */
+int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps);
+/* Drains recorded measurements (oldest first); *n receives the count. */
+int gpumc_observables(gpumc_sim* sim, gpumc_obs* out, size_t cap, size_t* n);
+/* Spin state of one replica in the reference's site order (x fastest,
+ * CMC.rs/src/lattice/graph.rs:417-451): int8 (+-1 Ising, 0..q-1 Potts),
+ * float32[3] per site (O(3)), uint64 per site (multi-spin). */
+int gpumc_get_spins(gpumc_sim* sim, int32_t replica, void* host, size_t nbytes);
+int gpumc_set_spins(gpumc_sim* sim, int32_t replica, const void* host, size_t nbytes);
+/* Cached physical energies (System::energy, CMC.rs/src/lattice/state.rs:19-27)
+ * of every replica (multi-spin: joint energy of the 64 bit-replicas). */
+int gpumc_energy(gpumc_sim* sim, double* energies);
+/* Exact recomputation compared with the cache (audit_lattice_cache,
+ * CMC.rs/src/audit.rs:41-52); writes recomputed energies. */
+int gpumc_recompute_energy(gpumc_sim* sim, double* energies);
+/* Per-bit-replica energies and |M|/N of a multi-spin lattice
+ * (MultiSpinIsing::measure, CMC.rs/src/multi_spin.rs:220-286). */
+int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* energy64,
+                                  double* mag64);
+int gpumc_sweep_count(gpumc_sim* sim, uint64_t* out);
+int gpumc_acceptance(gpumc_sim* sim, int32_t replica, double* cone_half_angle);
+
+/* ---- ParallelTemperingCompatible (Carlo.rs/src/parallel_tempering.rs:71-84;
+ * CMC.rs/src/classical_mc.rs:203-229) ------------------------------------ */
+int gpumc_log_weight_ratio(gpumc_sim* sim, int32_t replica, double new_beta, double* out);
+int gpumc_change_parameter(gpumc_sim* sim, int32_t replica, double new_beta);
+/* Device-side exchange every `interval` sweeps between ladder neighbours
+ * (PtExchange::try_exchange, parallel_tempering.rs:362-419).  0 disables. */
+int gpumc_pt_configure(gpumc_sim* sim, uint32_t interval);
+/* labels[r] = ladder index held by replica r (always a permutation). */
+int gpumc_pt_labels(gpumc_sim* sim, int32_t* labels);
+int gpumc_pt_stats(gpumc_sim* sim, uint64_t* exchange_steps, uint64_t* accepted_swaps);
+
+/* ---- serving: continuous batching of simulation jobs ------------------ */
+typedef struct {
+  gpumc_spec spec;
+  uint64_t base_seed;
+  uint64_t n_sweeps;         /* measurement sweeps (each recorded)            */
+  uint64_t n_therm;          /* thermalization sweeps before them             */
+} gpumc_job;
+
+typedef struct {
+  uint64_t job_id;
+  int32_t status;            /* 0 done, GPUMC_E* on failure, 1 cancelled      */
+  int32_t n_replicas;
+  double submit_s, start_s, finish_s;  /* server clock (seconds)             */
+  double mean_energy;        /* per site, averaged over replicas and sweeps   */
+  double mean_abs_m;
+  double attempts;           /* spin-flip attempts performed                  */
+} gpumc_job_result;
+
+/* hbm_budget: bytes of device memory the server may hold for resident
+ * lattices; chunk: sweeps per batched launch group (admission granularity). */
+int gpumc_server_create(int32_t device, size_t hbm_budget, uint32_t chunk, gpumc_server** out);
+/* Admits the job if its footprint fits the free budget, else GPUMC_EAGAIN. */
+int gpumc_submit(gpumc_server* srv, const gpumc_job* job, uint64_t* job_id);
+/* Runs one scheduling round: packs admitted jobs into the running batch,
+ * launches `chunk` sweeps, retires finished jobs.  Returns the number of
+ * active jobs in *active. */
+int gpumc_server_step(gpumc_server* srv, int32_t* active);
+int gpumc_poll(gpumc_server* srv, gpumc_job_result* out, size_t cap, size_t* n);
+int gpumc_cancel(gpumc_server* srv, uint64_t job_id);
+/* Final spins of a finished job's replica (kept until polled). */
+int gpumc_job_spins(gpumc_server* srv, uint64_t job_id, int32_t replica, void* host, size_t nbytes);
+int gpumc_server_stats(gpumc_server* srv, double* attempts_total, double* busy_s, size_t* bytes_in_use);
+int gpumc_server_destroy(gpumc_server* srv);
+
+/* ---- diagnostics ------------------------------------------------------- */
+int gpumc_last_error(char* buf, size_t cap);
+/* Device Philox4x32-10 outputs for n (counter, key) pairs (4 + 2 words each). */
+int gpumc_philox_probe(const uint32_t* ctr4, const uint32_t* key2, uint32_t* out4, int32_t n);
+/* Bytes of device memory a spec needs (both ping-pong buffers, tables,
+ * records): the admission footprint. */
+int gpumc_footprint(const gpumc_spec* spec, size_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUMC_H */

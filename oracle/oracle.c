@@ -1,0 +1,621 @@
+/*
+ * CPU oracle, part 1: bit-exact replay of the engine's checkerboard method.
+ * TEST INFRASTRUCTURE ONLY (parity checker and CPU baseline), never shipped
+ * on a product path.  Compiled with -ffp-contract=off so that every float
+ * operation below is individually rounded, exactly like the device code.
+ *
+ * Reference anchors (paths relative to the scamper workspace):
+ *   stream keys      Carlo.rs/src/rng_stream.rs:126-154 (seed/fold/mix64)
+ *   acceptance       Carlo.rs/src/acceptance.rs:11-22
+ *   Ising dE / LUT   CMC.rs/src/lattice/interaction.rs:73-84, :149-181;
+ *                    CMC.rs/src/multi_spin.rs:84-91
+ *   Potts proposal   CMC.rs/src/lattice/models.rs:212-218, :271-273
+ *   site indexing    CMC.rs/src/lattice/graph.rs:417-451 (x fastest, +1 bonds)
+ *   PT exchange      Carlo.rs/src/parallel_tempering.rs:362-419
+ *   OPSS adaptation  CMC.rs/src/lattice/proposal.rs:156-167
+ * Third-party algorithms restated from their publications: Philox4x32-10
+ * (Salmon, Moraes, Dror, Shaw, SC'11); SplitMix64 and Xoshiro256++
+ * (Steele/Lea/Flood 2014; Blackman & Vigna 2018) as pinned by the reference's
+ * Cargo.lock (rand_core 0.10.0, rand_xoshiro 0.8.0).
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10                                                             */
+/* ------------------------------------------------------------------------ */
+void orc_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int round = 0; round < 10; ++round) {
+        if (round > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* ------------------------------------------------------------------------ */
+/* RngStreamKey::seed restated                                               */
+/* ------------------------------------------------------------------------ */
+static uint64_t mix64(uint64_t v) {
+    v += 0x9E3779B97F4A7C15ull;
+    v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+    v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+    return v ^ (v >> 31);
+}
+static uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+static uint64_t fold(uint64_t state, uint64_t domain, uint64_t value) {
+    return mix64(state ^ domain ^ mix64(value + rotl64(domain, 17)));
+}
+uint64_t orc_stream_seed(uint64_t base_seed, uint64_t task, uint64_t run, uint64_t chain,
+                         uint64_t replica, uint64_t thread, uint64_t phase, uint64_t substream) {
+    uint64_t s = mix64(base_seed ^ 0x53435554544C4552ull);
+    s = fold(s, 0x5441534Bull, task);
+    s = fold(s, 0x52554E00ull, run);
+    s = fold(s, 0x434841494E00ull, chain);
+    s = fold(s, 0x5245504C49434100ull, replica);
+    s = fold(s, 0x544852454144ull, thread);
+    s = fold(s, 0x504841534500ull, phase);
+    return fold(s, 0x535542535452ull, substream);
+}
+uint64_t orc_replica_key(uint64_t base_seed, uint64_t replica, uint64_t substream) {
+    return orc_stream_seed(base_seed, 0, 0, 0, replica, 0, 0, substream);
+}
+uint64_t orc_exchange_key(uint64_t base_seed) {
+    return orc_stream_seed(base_seed, 0, 0, 0, 0, 0, 3 /* RngPhase::Exchange */, 0);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Xoshiro256++                                                              */
+/* ------------------------------------------------------------------------ */
+void orc_xoshiro_seed(orc_xoshiro* g, uint64_t seed) {
+    uint64_t st = seed;
+    for (int i = 0; i < 4; ++i) {
+        st += 0x9E3779B97F4A7C15ull;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        g->s[i] = z ^ (z >> 31);
+    }
+}
+uint64_t orc_xoshiro_next(orc_xoshiro* g) {
+    uint64_t* s = g->s;
+    uint64_t result = rotl64(s[0] + s[3], 23) + s[0];
+    uint64_t t = s[1] << 17;
+    s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl64(s[3], 45);
+    return result;
+}
+
+/* ------------------------------------------------------------------------ */
+/* thresholds                                                                */
+/* ------------------------------------------------------------------------ */
+void orc_threshold(double p, uint32_t* head, uint64_t* tail) {
+    if (!(p > 0.0)) { *head = 0; *tail = 0; return; }        /* NaN or <= 0 */
+    if (p >= 1.0) { *head = 65536u; *tail = 0; return; }
+    double s = p * 65536.0;                                  /* exact scaling */
+    double h = floor(s);
+    double frac = s - h;                                     /* exact */
+    *head = (uint32_t)h;
+    *tail = (uint64_t)ldexp(frac, 64);                       /* exact, < 2^64 */
+}
+
+int orc_build_table(int model, int dims, double J, double beta, uint32_t* head, uint64_t* tail) {
+    int z = 2 * dims;
+    if (model == ORC_ISING || model == ORC_MSC) {
+        for (int k = 0; k <= z; ++k) {
+            double dE = 2.0 * J * (double)(z - 2 * k);
+            double logA = -beta * dE;
+            orc_threshold(logA >= 0.0 ? 1.0 : exp(logA), &head[k], &tail[k]);
+        }
+        return z + 1;
+    }
+    for (int d = -z; d <= z; ++d) {
+        double dE = -J * (double)d;
+        double logA = -beta * dE;
+        orc_threshold(logA >= 0.0 ? 1.0 : exp(logA), &head[d + z], &tail[d + z]);
+    }
+    return 2 * z + 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* geometry helpers                                                          */
+/* ------------------------------------------------------------------------ */
+typedef struct { int dims; int64_t lx, ly, lz; } geom;
+
+static inline int64_t site_of(const geom* g, int64_t x, int64_t y, int64_t z) {
+    return x + g->lx * (y + g->ly * z);
+}
+/* neighbours in the fixed order (x-1, x+1, y-1, y+1[, z-1, z+1]) */
+static inline int neighbours(const geom* g, int64_t x, int64_t y, int64_t z, int64_t nb[6]) {
+    int64_t xm = x ? x - 1 : g->lx - 1, xp = x + 1 < g->lx ? x + 1 : 0;
+    int64_t ym = y ? y - 1 : g->ly - 1, yp = y + 1 < g->ly ? y + 1 : 0;
+    nb[0] = site_of(g, xm, y, z);
+    nb[1] = site_of(g, xp, y, z);
+    nb[2] = site_of(g, x, ym, z);
+    nb[3] = site_of(g, x, yp, z);
+    if (g->dims == 2) return 4;
+    int64_t zm = z ? z - 1 : g->lz - 1, zp = z + 1 < g->lz ? z + 1 : 0;
+    nb[4] = site_of(g, x, y, zm);
+    nb[5] = site_of(g, x, y, zp);
+    return 6;
+}
+static inline void make_ctr(uint32_t ctr[4], uint64_t index, uint32_t colour, uint32_t tag,
+                            uint32_t plane_pair, uint64_t sweep) {
+    ctr[0] = (uint32_t)index;
+    ctr[1] = colour | (tag << 1) | (plane_pair << 8) | ((uint32_t)(index >> 32) << 16);
+    ctr[2] = (uint32_t)sweep;
+    ctr[3] = (uint32_t)(sweep >> 32);
+}
+static inline void key_of(uint64_t k64, uint32_t key[2]) {
+    key[0] = (uint32_t)k64;
+    key[1] = (uint32_t)(k64 >> 32);
+}
+
+/* 16-bit draw of a site from the 16-site chunk batch (x & 15 selects slot) */
+static uint32_t chunk_u16(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t colour,
+                          uint32_t tag, const uint32_t key[2], uint64_t sweep) {
+    int64_t pc = (g->lx + 15) / 16;
+    uint64_t chunk = (uint64_t)((y + g->ly * z) * pc + (x >> 4));
+    uint32_t ctr[4], out[4];
+    make_ctr(ctr, chunk, colour, tag, 0, sweep);
+    orc_philox4x32_10(ctr, key, out);
+    int slot = (int)((x & 15) >> 1);
+    return (out[slot >> 1] >> (16 * (slot & 1))) & 0xFFFFu;
+}
+
+static int accept_discrete(uint32_t u16, uint32_t head, uint64_t tail, uint64_t site,
+                           uint32_t colour, const uint32_t key[2], uint64_t sweep) {
+    if (u16 < head) return 1;
+    if (u16 > head) return 0;
+    uint32_t ctr[4], out[4];
+    make_ctr(ctr, site, colour, ORC_TAG_ACC_REFINE, 0, sweep);
+    orc_philox4x32_10(ctr, key, out);
+    uint64_t r = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
+    return r < tail;
+}
+
+/* uniform r in [0, n) for the Potts proposal, Lemire multiply-shift with
+ * exact rejection (16-bit first draw, 32-bit retries from a refine batch) */
+static uint32_t potts_draw(uint32_t u16, uint32_t n, uint64_t site, uint32_t colour,
+                           const uint32_t key[2], uint64_t sweep) {
+    uint32_t m = u16 * n;
+    uint32_t low = m & 0xFFFFu;
+    uint32_t reject16 = 65536u % n;
+    if (low >= reject16) return m >> 16;
+    uint32_t ctr[4], out[4];
+    make_ctr(ctr, site, colour, ORC_TAG_PROP_REFINE, 0, sweep);
+    orc_philox4x32_10(ctr, key, out);
+    uint32_t reject32 = (uint32_t)((0x100000000ull) % n);
+    uint64_t mm = 0;
+    for (int i = 0; i < 4; ++i) {
+        mm = (uint64_t)out[i] * n;
+        if ((uint32_t)mm >= reject32) return (uint32_t)(mm >> 32);
+    }
+    return (uint32_t)(mm >> 32);
+}
+
+/* ------------------------------------------------------------------------ */
+/* discrete models                                                           */
+/* ------------------------------------------------------------------------ */
+void orc_init_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
+                       uint64_t base_seed, uint64_t replica, int hot, int8_t* spins) {
+    int64_t n = lx * ly * (dims == 3 ? lz : 1);
+    if (!hot) {
+        memset(spins, model == ORC_ISING ? 1 : 0, (size_t)n);
+        return;
+    }
+    uint32_t key[2];
+    key_of(orc_replica_key(base_seed, replica, ORC_SUB_INIT), key);
+    for (int64_t s = 0; s < n; ++s) {
+        uint32_t ctr[4], out[4];
+        make_ctr(ctr, (uint64_t)s >> 2, 0, ORC_TAG_INIT, 0, 0);
+        orc_philox4x32_10(ctr, key, out);
+        uint32_t u = out[s & 3];
+        if (model == ORC_ISING)
+            spins[s] = (u >> 31) ? 1 : -1;
+        else
+            spins[s] = (int8_t)(((uint64_t)u * (uint64_t)q) >> 32);
+    }
+}
+
+int64_t orc_sweep_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
+                           const uint32_t* head, const uint64_t* tail, uint64_t key64,
+                           uint64_t sweep, int8_t* spins, int64_t* accepted) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    int zc = 2 * dims;
+    uint32_t key[2];
+    key_of(key64, key);
+    int64_t dE = 0, acc = 0;
+    for (uint32_t colour = 0; colour < 2; ++colour) {
+        for (int64_t z = 0; z < g.lz; ++z)
+            for (int64_t y = 0; y < g.ly; ++y)
+                for (int64_t x = 0; x < g.lx; ++x) {
+                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
+                    int64_t site = site_of(&g, x, y, z);
+                    int64_t nb[6];
+                    int nn = neighbours(&g, x, y, z, nb);
+                    int8_t s = spins[site];
+                    uint32_t u = chunk_u16(&g, x, y, z, colour, ORC_TAG_ACC, key, sweep);
+                    if (model == ORC_ISING) {
+                        int k = 0;
+                        for (int i = 0; i < nn; ++i) k += spins[nb[i]] != s;
+                        if (accept_discrete(u, head[k], tail[k], (uint64_t)site, colour, key,
+                                            sweep)) {
+                            spins[site] = (int8_t)-s;
+                            dE += 2 * (zc - 2 * k);
+                            ++acc;
+                        }
+                    } else {
+                        uint32_t pu = chunk_u16(&g, x, y, z, colour, ORC_TAG_PROP, key, sweep);
+                        uint32_t r = potts_draw(pu, (uint32_t)(q - 1), (uint64_t)site, colour, key,
+                                                sweep);
+                        int8_t t = (int8_t)((int)r < s ? (int)r : (int)r + 1);
+                        int nold = 0, nnew = 0;
+                        for (int i = 0; i < nn; ++i) {
+                            nold += spins[nb[i]] == s;
+                            nnew += spins[nb[i]] == t;
+                        }
+                        int d = nnew - nold;
+                        if (accept_discrete(u, head[d + zc], tail[d + zc], (uint64_t)site,
+                                            colour, key, sweep)) {
+                            spins[site] = t;
+                            dE += -d;
+                            ++acc;
+                        }
+                    }
+                }
+    }
+    if (accepted) *accepted = acc;
+    return dE;
+}
+
+int64_t orc_energy_int(int model, int dims, int64_t lx, int64_t ly, int64_t lz,
+                       const int8_t* spins) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    int64_t e = 0;
+    for (int64_t z = 0; z < g.lz; ++z)
+        for (int64_t y = 0; y < g.ly; ++y)
+            for (int64_t x = 0; x < g.lx; ++x) {
+                int64_t nb[6];
+                int nn = neighbours(&g, x, y, z, nb);
+                int8_t s = spins[site_of(&g, x, y, z)];
+                /* +1 bonds only: entries 1, 3, 5 of the neighbour list */
+                for (int i = 1; i < nn; i += 2) {
+                    int8_t t = spins[nb[i]];
+                    e -= (model == ORC_ISING) ? (int64_t)s * t : (int64_t)(s == t);
+                }
+            }
+    return e;
+}
+
+/* ------------------------------------------------------------------------ */
+/* O(3): engine arithmetic, one rounding per operation                       */
+/* ------------------------------------------------------------------------ */
+float orc_exp_neg(float x) {
+    if (!(x <= 0.0f)) return 1.0f;
+    if (x < -87.0f) return 0.0f;
+    float y = x * 0x1.715476p+0f;           /* log2(e) */
+    float n = floorf(y + 0.5f);
+    float f = y - n;
+    float t = f * 0x1.62e430p-1f;           /* ln 2 */
+    float p = 0x1.a01a02p-13f;              /* 1/7! */
+    p = p * t + 0x1.6c16c2p-10f;            /* 1/6! */
+    p = p * t + 0x1.111112p-7f;             /* 1/5! */
+    p = p * t + 0x1.555556p-5f;             /* 1/4! */
+    p = p * t + 0x1.555556p-3f;             /* 1/3! */
+    p = p * t + 0.5f;
+    p = p * t + 1.0f;
+    p = p * t + 1.0f;
+    int ni = (int)n;                        /* -126 <= ni <= 0 */
+    uint32_t bits = (uint32_t)(ni + 127) << 23;
+    float scale;
+    memcpy(&scale, &bits, 4);
+    return p * scale;
+}
+
+void orc_sincos_turn(uint32_t u, float* c, float* s) {
+    uint32_t octant = u >> 29;
+    float t = (float)((u >> 5) & 0xFFFFFFu) * 0x1p-24f;
+    if (octant & 1u) t = 1.0f - t;
+    float th = t * 0x1.921fb6p-1f;          /* pi / 4 */
+    float t2 = th * th;
+    float sp = 0x1.71de3ap-19f;             /* 1/9! */
+    sp = sp * t2 - 0x1.a01a02p-13f;         /* 1/7! */
+    sp = sp * t2 + 0x1.111112p-7f;          /* 1/5! */
+    sp = sp * t2 - 0x1.555556p-3f;          /* 1/3! */
+    sp = sp * t2 + 1.0f;
+    float sn = th * sp;
+    float cp = -0x1.27e4fcp-22f;            /* -1/10! */
+    cp = cp * t2 + 0x1.a01a02p-16f;         /* 1/8! */
+    cp = cp * t2 - 0x1.6c16c2p-10f;         /* 1/6! */
+    cp = cp * t2 + 0x1.555556p-5f;          /* 1/4! */
+    cp = cp * t2 - 0.5f;
+    float cs = cp * t2 + 1.0f;
+    float rc, rs;
+    switch (octant) {
+        case 0: rc = cs;  rs = sn;  break;
+        case 1: rc = sn;  rs = cs;  break;
+        case 2: rc = -sn; rs = cs;  break;
+        case 3: rc = -cs; rs = sn;  break;
+        case 4: rc = -cs; rs = -sn; break;
+        case 5: rc = -sn; rs = -cs; break;
+        case 6: rc = sn;  rs = -cs; break;
+        default: rc = cs; rs = -sn; break;
+    }
+    *c = rc;
+    *s = rs;
+}
+
+void orc_init_o3(int dims, int64_t lx, int64_t ly, int64_t lz, uint64_t base_seed,
+                 uint64_t replica, int hot, float* sx, float* sy, float* sz) {
+    int64_t n = lx * ly * (dims == 3 ? lz : 1);
+    uint32_t key[2];
+    key_of(orc_replica_key(base_seed, replica, ORC_SUB_INIT), key);
+    for (int64_t s = 0; s < n; ++s) {
+        if (!hot) { sx[s] = 1.0f; sy[s] = 0.0f; sz[s] = 0.0f; continue; }
+        uint32_t ctr[4], out[4];
+        make_ctr(ctr, (uint64_t)s, 0, ORC_TAG_INIT, 0, 0);
+        orc_philox4x32_10(ctr, key, out);
+        float t = (float)(out[0] >> 8) * 0x1p-24f;
+        float zz = 1.0f - 2.0f * t;
+        float r = sqrtf((1.0f - zz) * (1.0f + zz));
+        float c, sn;
+        orc_sincos_turn(out[1], &c, &sn);
+        sx[s] = r * c;
+        sy[s] = r * sn;
+        sz[s] = zz;
+    }
+}
+
+double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
+                    float omc, uint64_t key64, uint64_t sweep, float* sx, float* sy,
+                    float* sz, int64_t* accepted) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    uint32_t key[2];
+    key_of(key64, key);
+    double dEsum = 0.0;
+    int64_t acc = 0;
+    float mJ = -J;
+    for (uint32_t colour = 0; colour < 2; ++colour) {
+        for (int64_t z = 0; z < g.lz; ++z)
+            for (int64_t y = 0; y < g.ly; ++y)
+                for (int64_t x = 0; x < g.lx; ++x) {
+                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
+                    int64_t site = site_of(&g, x, y, z);
+                    int64_t nb[6];
+                    int nn = neighbours(&g, x, y, z, nb);
+                    float hx = sx[nb[0]], hy = sy[nb[0]], hz = sz[nb[0]];
+                    for (int i = 1; i < nn; ++i) {
+                        hx = hx + sx[nb[i]];
+                        hy = hy + sy[nb[i]];
+                        hz = hz + sz[nb[i]];
+                    }
+                    float ax = sx[site], ay = sy[site], az = sz[site];
+                    uint32_t ctr[4], o[4];
+                    make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_O3, 0, sweep);
+                    orc_philox4x32_10(ctr, key, o);
+                    float w = ((float)(o[0] >> 8) * 0x1p-24f) * omc;
+                    float ct = 1.0f - w;
+                    float st = sqrtf(w * (2.0f - w));
+                    float cp, sp;
+                    orc_sincos_turn(o[1], &cp, &sp);
+                    float e1x, e1y, e1z;
+                    if (fabsf(az) < 0.9f) {
+                        float a = sqrtf(ax * ax + ay * ay);
+                        e1x = ay / a; e1y = -ax / a; e1z = 0.0f;
+                    } else {
+                        float a = sqrtf(ay * ay + az * az);
+                        e1x = 0.0f; e1y = az / a; e1z = -ay / a;
+                    }
+                    float e2x = ay * e1z - az * e1y;
+                    float e2y = az * e1x - ax * e1z;
+                    float e2z = ax * e1y - ay * e1x;
+                    float nx = ct * ax + st * (cp * e1x + sp * e2x);
+                    float ny = ct * ay + st * (cp * e1y + sp * e2y);
+                    float nz = ct * az + st * (cp * e1z + sp * e2z);
+                    float r = sqrtf((nx * nx + ny * ny) + nz * nz);
+                    nx = nx / r; ny = ny / r; nz = nz / r;
+                    float dot = ((nx - ax) * hx + (ny - ay) * hy) + (nz - az) * hz;
+                    float dE = mJ * dot;
+                    int ok;
+                    if (dE <= 0.0f) {
+                        ok = 1;
+                    } else {
+                        float p = orc_exp_neg(-(beta * dE));
+                        float u = ((float)(o[2] >> 8) + 0.5f) * 0x1p-24f;
+                        ok = u < p;
+                    }
+                    if (ok) {
+                        /* energy cache: exact fp64 change of the fp32 configuration */
+                        double hxd = 0.0, hyd = 0.0, hzd = 0.0;
+                        for (int i = 0; i < nn; ++i) {
+                            hxd += (double)sx[nb[i]];
+                            hyd += (double)sy[nb[i]];
+                            hzd += (double)sz[nb[i]];
+                        }
+                        dEsum += -(double)J * (((double)nx - (double)ax) * hxd +
+                                               ((double)ny - (double)ay) * hyd +
+                                               ((double)nz - (double)az) * hzd);
+                        sx[site] = nx; sy[site] = ny; sz[site] = nz;
+                        ++acc;
+                    }
+                }
+    }
+    if (accepted) *accepted = acc;
+    return dEsum;
+}
+
+double orc_energy_o3(int dims, int64_t lx, int64_t ly, int64_t lz, double J, const float* sx,
+                     const float* sy, const float* sz) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    double e = 0.0;
+    for (int64_t z = 0; z < g.lz; ++z)
+        for (int64_t y = 0; y < g.ly; ++y)
+            for (int64_t x = 0; x < g.lx; ++x) {
+                int64_t nb[6];
+                int nn = neighbours(&g, x, y, z, nb);
+                int64_t s = site_of(&g, x, y, z);
+                for (int i = 1; i < nn; i += 2)
+                    e -= J * ((double)sx[s] * sx[nb[i]] + (double)sy[s] * sy[nb[i]] +
+                              (double)sz[s] * sz[nb[i]]);
+            }
+    return e;
+}
+
+float orc_o3_adapt(float omc, int64_t accepted, int64_t attempted) {
+    if (attempted <= 0) return omc;
+    float rate = (float)accepted / (float)attempted;
+    float f = 1.0f + 0.16f * (rate - 0.5f);
+    float w = omc * f;
+    const float lo = 5.0e-9f; /* 1 - cos(1e-4) */
+    if (w < lo) w = lo;
+    if (w > 2.0f) w = 2.0f;
+    return w;
+}
+
+/* ------------------------------------------------------------------------ */
+/* multi-spin coding                                                         */
+/* ------------------------------------------------------------------------ */
+void orc_init_msc(int dims, int64_t lx, int64_t ly, int64_t lz, uint64_t base_seed, int hot,
+                  uint64_t* words) {
+    int64_t n = lx * ly * (dims == 3 ? lz : 1);
+    if (!hot) {
+        for (int64_t s = 0; s < n; ++s) words[s] = ~0ull;
+        return;
+    }
+    memset(words, 0, (size_t)n * 8);
+    for (int r = 0; r < 64; ++r) {
+        uint32_t key[2];
+        key_of(orc_replica_key(base_seed, (uint64_t)r, ORC_SUB_INIT), key);
+        for (int64_t s = 0; s < n; ++s) {
+            uint32_t ctr[4], out[4];
+            make_ctr(ctr, (uint64_t)s >> 2, 0, ORC_TAG_INIT, 0, 0);
+            orc_philox4x32_10(ctr, key, out);
+            if (out[s & 3] >> 31) words[s] |= 1ull << r;
+        }
+    }
+}
+
+static int t_bit(uint32_t head, uint64_t tail, int j) {
+    return j < 16 ? (int)((head >> (15 - j)) & 1u) : (int)((tail >> (79 - j)) & 1u);
+}
+
+void orc_sweep_msc(int dims, int64_t lx, int64_t ly, int64_t lz, const uint32_t* head,
+                   const uint64_t* tail, uint64_t key64, uint64_t sweep, uint64_t* words,
+                   int64_t* accepted) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    uint32_t key[2];
+    key_of(key64, key);
+    int64_t acc = 0;
+    for (uint32_t colour = 0; colour < 2; ++colour)
+        for (int64_t z = 0; z < g.lz; ++z)
+            for (int64_t y = 0; y < g.ly; ++y)
+                for (int64_t x = 0; x < g.lx; ++x) {
+                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
+                    int64_t site = site_of(&g, x, y, z);
+                    int64_t nb[6];
+                    int nn = neighbours(&g, x, y, z, nb);
+                    uint64_t w = words[site];
+                    uint64_t planes[80];
+                    int have = 0;
+                    uint64_t flip = 0;
+                    for (int r = 0; r < 64; ++r) {
+                        int k = 0;
+                        for (int i = 0; i < nn; ++i) k += (int)(((w ^ words[nb[i]]) >> r) & 1u);
+                        if (head[k] >= 65536u) { flip |= 1ull << r; continue; }
+                        int decided = 0, less = 0;
+                        for (int j = 0; j < 80 && !decided; ++j) {
+                            while (have <= j) {
+                                uint32_t ctr[4], out[4];
+                                make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_MSC,
+                                         (uint32_t)(have >> 1), sweep);
+                                orc_philox4x32_10(ctr, key, out);
+                                planes[have] = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
+                                planes[have + 1] = (uint64_t)out[2] | ((uint64_t)out[3] << 32);
+                                have += 2;
+                            }
+                            int ub = (int)((planes[j] >> r) & 1u);
+                            int tb = t_bit(head[k], tail[k], j);
+                            if (ub != tb) { decided = 1; less = ub < tb; }
+                        }
+                        if (less) flip |= 1ull << r;
+                    }
+                    words[site] = w ^ flip;
+                    acc += __builtin_popcountll(flip);
+                }
+    if (accepted) *accepted = acc;
+}
+
+void orc_msc_observables(int dims, int64_t lx, int64_t ly, int64_t lz, const uint64_t* words,
+                         int64_t* e_int, int64_t* m_sum) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    for (int r = 0; r < 64; ++r) { e_int[r] = 0; m_sum[r] = 0; }
+    for (int64_t z = 0; z < g.lz; ++z)
+        for (int64_t y = 0; y < g.ly; ++y)
+            for (int64_t x = 0; x < g.lx; ++x) {
+                int64_t nb[6];
+                int nn = neighbours(&g, x, y, z, nb);
+                uint64_t w = words[site_of(&g, x, y, z)];
+                for (int r = 0; r < 64; ++r) m_sum[r] += ((w >> r) & 1u) ? 1 : -1;
+                for (int i = 1; i < nn; i += 2) {
+                    uint64_t a = w ^ words[nb[i]];
+                    for (int r = 0; r < 64; ++r) e_int[r] += ((a >> r) & 1u) ? 1 : -1;
+                }
+            }
+}
+
+/* ------------------------------------------------------------------------ */
+/* replica exchange                                                          */
+/* ------------------------------------------------------------------------ */
+int orc_accept_log(double logA, uint64_t u64) {
+    if (isnan(logA)) return 0;
+    if (logA >= 0.0) return 1;
+    if (isinf(logA)) return 0;
+    double u = (double)(u64 >> 11) * 0x1p-53;
+    if (u < 2.2250738585072014e-308) u = 2.2250738585072014e-308;
+    return log(u) < logA;
+}
+
+int orc_pt_exchange(int n, const double* betas, const double* energies, int32_t* label,
+                    uint64_t exchange_key, uint64_t exchange_step, int32_t* accepted_pairs) {
+    if (n < 2 || exchange_step == 0) return 0;
+    int32_t* at = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    for (int r = 0; r < n; ++r) at[label[r]] = r;
+    uint32_t key[2];
+    key_of(exchange_key, key);
+    int offset = (int)((exchange_step - 1) & 1u);
+    int count = 0;
+    for (int t = offset; t + 1 < n; t += 2) {
+        int a = at[t], b = at[t + 1];
+        double wa = (betas[t] - betas[t + 1]) * energies[a];
+        double wb = (betas[t + 1] - betas[t]) * energies[b];
+        uint32_t ctr[4], out[4];
+        make_ctr(ctr, (uint64_t)t, 0, ORC_TAG_PT, 0, exchange_step);
+        orc_philox4x32_10(ctr, key, out);
+        uint64_t u = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
+        int ok = orc_accept_log(wa + wb, u);
+        if (accepted_pairs) accepted_pairs[t] = ok;
+        if (ok) {
+            label[a] = t + 1;
+            label[b] = t;
+            at[t] = b;
+            at[t + 1] = a;
+            ++count;
+        }
+    }
+    free(at);
+    return count;
+}

@@ -1,0 +1,548 @@
+// Host side of the engine and the C ABI declared in include/gpumc.h.
+//
+// A gpumc_engine owns a CUDA stream and two device-resident descriptor pools
+// (lattices and groups).  A gpumc_sim takes one lattice slot per replica and
+// one group slot; its sweep kernels read the descriptors directly, and the
+// last CTA of every launch updates them (energy cache, records, sweep count,
+// PT labels), so a launch sequence can be captured once in a CUDA graph and
+// replayed without host involvement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/gpumc.h"
+#include "engine.h"
+#include "host_internal.h"
+
+namespace gpumc {
+
+template <int MODEL>
+__global__ void k_sweep_discrete_2d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int MODEL>
+__global__ void k_sweep_discrete_3d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM>
+__global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM>
+__global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM>
+__global__ void k_msc_measure(const LatDesc*, int, unsigned long long*);
+__global__ void k_msc_record(LatDesc*, GroupDesc*, int, unsigned long long*);
+__global__ void k_init_discrete(int8_t*, int, int, int, int, int, int, uint64_t, int);
+__global__ void k_init_o3(float*, int, int, int, int, uint64_t, int);
+__global__ void k_init_msc(unsigned long long*, int, int, int, int, const uint64_t*, int);
+__global__ void k_energy_int(const void*, int, int, int, int, int, unsigned long long*);
+__global__ void k_energy_o3(const float*, int, int, int, int, double, double*);
+__global__ void k_philox_probe(const uint4*, const uint2*, uint4*, int);
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+const std::string& last_error_ref() { return g_last_error; }
+size_t g_last_error_size() { return g_last_error.size(); }
+
+#define CUDA_TRY(expr)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? GPUMC_ENOMEM : GPUMC_ECUDA,   \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// stream keys: restatement of RngStreamKey::seed (Carlo.rs/src/rng_stream.rs:
+// 126-154): domain-separated SplitMix64 folding of the stream coordinates.
+// ---------------------------------------------------------------------------
+static uint64_t mix64(uint64_t v) {
+  v += 0x9E3779B97F4A7C15ull;
+  v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+  v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+  return v ^ (v >> 31);
+}
+static uint64_t fold(uint64_t state, uint64_t domain, uint64_t value) {
+  const uint64_t rot = (domain << 17) | (domain >> 47);
+  return mix64(state ^ domain ^ mix64(value + rot));
+}
+uint64_t stream_key(uint64_t base, uint64_t replica, uint64_t phase, uint64_t substream) {
+  uint64_t s = mix64(base ^ 0x53435554544C4552ull);  // "SCUTTLER"
+  s = fold(s, 0x5441534Bull, 0);                     // task
+  s = fold(s, 0x52554E00ull, 0);                     // run
+  s = fold(s, 0x434841494E00ull, 0);                 // chain
+  s = fold(s, 0x5245504C49434100ull, replica);       // replica
+  s = fold(s, 0x544852454144ull, 0);                 // thread
+  s = fold(s, 0x504841534500ull, phase);             // phase
+  return fold(s, 0x535542535452ull, substream);      // substream
+}
+
+// 80-bit acceptance threshold of probability p: head = floor(p 2^16) (65536
+// = always), tail = next 64 bits of p's binary expansion.
+void threshold80(double p, uint32_t& head, unsigned long long& tail) {
+  if (!(p > 0.0)) {
+    head = 0;
+    tail = 0;
+    return;
+  }
+  if (p >= 1.0) {
+    head = 65536u;
+    tail = 0;
+    return;
+  }
+  const double s = std::ldexp(p, 16);
+  const double h = std::floor(s);
+  head = (uint32_t)h;
+  tail = (unsigned long long)std::ldexp(s - h, 64);
+}
+
+// Class tables.  Ising / multi-spin: class k = anti-aligned neighbours,
+// dE = 2J(z - 2k) (multi_spin.rs:84-91 indexes by aligned count z - k).
+// Potts: class d + z with d = n(new) - n(old), dE = -J d.
+int n_classes(int model, int dims) {
+  const int z = 2 * dims;
+  return (model == POTTS) ? 2 * z + 1 : z + 1;
+}
+void build_table(int model, int dims, double J, double beta, uint32_t* head,
+                 unsigned long long* tail) {
+  const int z = 2 * dims;
+  const int n = n_classes(model, dims);
+  for (int c = 0; c < n; ++c) {
+    const double dE = (model == POTTS) ? -J * (double)(c - z) : 2.0 * J * (double)(z - 2 * c);
+    const double logA = -beta * dE;
+    threshold80(logA >= 0.0 ? 1.0 : std::exp(logA), head[c], tail[c]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// spec validation and layout planning
+// ---------------------------------------------------------------------------
+int validate_spec(const gpumc_spec* s) {
+  if (!s) return fail(GPUMC_EINVAL, "spec: null pointer");
+  if (s->model < GPUMC_ISING || s->model > GPUMC_ISING_MSC64)
+    return fail(GPUMC_EINVAL, "model: unknown model id");
+  if (s->dims != 2 && s->dims != 3)
+    return fail(GPUMC_EINVAL, "lattice_type: expected square (dims=2) or cubic (dims=3)");
+  if (!s->pbc) return fail(GPUMC_EINVAL, "pbc: the checkerboard engine requires periodic boundaries");
+  const int64_t lz = s->dims == 3 ? s->lz : 1;
+  const int64_t ext[3] = {s->lx, s->ly, lz};
+  for (int a = 0; a < s->dims; ++a) {
+    if (ext[a] < 4 || (ext[a] & 1))
+      return fail(GPUMC_EINVAL,
+                  "Lx/Ly/Lz: extents must be even and >= 4 (a periodic checkerboard needs a "
+                  "bipartite lattice)");
+    if (ext[a] > (1 << 20)) return fail(GPUMC_EINVAL, "Lx/Ly/Lz: extent too large");
+  }
+  if ((double)s->lx * (double)s->ly * (double)lz > 4.0e9)
+    return fail(GPUMC_EINVAL, "lattice: more than 4e9 sites");
+  if (!std::isfinite(s->J)) return fail(GPUMC_EINVAL, "J: must be finite");
+  if (s->model == GPUMC_POTTS && (s->q < 2 || s->q > kMaxPottsCounts))
+    return fail(GPUMC_EINVAL, "q: Potts q must be in 2..8");
+  if (s->n_replicas < 1 || s->n_replicas > 4096) return fail(GPUMC_EINVAL, "n_replicas: 1..4096");
+  if (s->n_temps != 1 && s->n_temps != s->n_replicas)
+    return fail(GPUMC_EINVAL, "n_temps: must be 1 or n_replicas");
+  if (!s->betas) return fail(GPUMC_EINVAL, "beta: missing");
+  for (int i = 0; i < s->n_temps; ++i)
+    if (!std::isfinite(s->betas[i]) || s->betas[i] < 0.0)
+      return fail(GPUMC_EINVAL, "beta: must be finite and non-negative");
+  if (s->init != GPUMC_INIT_HOT && s->init != GPUMC_INIT_COLD)
+    return fail(GPUMC_EINVAL, "initial_state: expected hot/random or cold/ordered");
+  if (s->model == GPUMC_O3 && !(s->cone_half_angle > 0.0 && s->cone_half_angle <= M_PI))
+    return fail(GPUMC_EINVAL, "cone_half_angle: must be in (0, pi]");
+  if (s->record_capacity < 1) return fail(GPUMC_EINVAL, "record_capacity: must be >= 1");
+  return GPUMC_OK;
+}
+
+Layout plan_layout(const gpumc_spec* s) {
+  Layout L;
+  L.model = s->model;
+  L.dims = s->dims;
+  L.lx = (int)s->lx;
+  L.ly = (int)s->ly;
+  L.lz = s->dims == 3 ? (int)s->lz : 1;
+  const int lx = L.lx, ly = L.ly, lz = L.lz;
+  L.n_sites = (int64_t)lx * ly * lz;
+  const size_t rows = (size_t)ly * lz;
+  if (L.model == ISING || L.model == POTTS) {
+    L.pitch = (lx + 15) / 16 * 16;
+    L.buf_bytes = (size_t)L.pitch * rows;
+    const int ncol = L.pitch / 16;
+    if (L.dims == 2) {
+      L.tile_cx = ncol <= 64 ? ncol : 32;
+      const int ty_max = std::min(1536 / L.tile_cx - 2, 120);
+      const int ty_target = std::max(8, 16384 / (16 * L.tile_cx));
+      L.tile_y = std::max(1, std::min(std::min(ty_target, ty_max), ly));
+      L.tile_z = 1;
+      L.smem = (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
+    } else {
+      L.tile_cx = ncol <= 16 ? ncol : 16;
+      const int ty_max = std::min(1024 / L.tile_cx - 2, 120);
+      L.tile_y = std::max(1, std::min(ty_max, ly));
+      L.tile_z = std::min(lz, 32);
+      L.smem = 4 * (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
+    }
+  } else if (L.model == O3) {
+    L.pitch = (lx + 3) / 4 * 4;
+    L.buf_bytes = 3 * sizeof(float) * (size_t)L.pitch * rows;
+    const int w = std::min(lx, 64);
+    L.tile_cx = (w + 3) / 4;
+    const int W = std::min(lx, L.tile_cx * 4);
+    if (L.dims == 2) {
+      const int ty_max = 2 * 6 * 256 / (W + 2) - 2;
+      L.tile_y = std::max(1, std::min(std::min(ty_max, 40), ly));
+      L.tile_z = 1;
+      L.smem = 3 * sizeof(float) * (size_t)(L.tile_y + 4) * (W + 4);
+    } else {
+      const int ty_max = 2 * 6 * 256 / (W + 2) - 2;
+      L.tile_y = std::max(1, std::min(std::min(ty_max, 16), ly));
+      L.tile_z = std::min(lz, 16);
+      L.smem = 4 * 3 * sizeof(float) * (size_t)(L.tile_y + 4) * (W + 4);
+    }
+  } else {  // MSC
+    L.pitch = (lx + 1) / 2 * 2;
+    L.buf_bytes = sizeof(unsigned long long) * (size_t)L.pitch * rows;
+    const int w = std::min(lx, L.dims == 2 ? 64 : 32);
+    L.tile_cx = (w + 1) / 2;
+    const int W = std::min(lx, L.tile_cx * 2);
+    const int ty_max = 2 * 4 * 256 / (W + 2) - 2;
+    if (L.dims == 2) {
+      L.tile_y = std::max(1, std::min(ty_max, ly));
+      L.tile_z = 1;
+      L.smem = 8 * (size_t)(L.tile_y + 4) * (W + 4);
+    } else {
+      L.tile_y = std::max(1, std::min(std::min(ty_max, 16), ly));
+      L.tile_z = std::min(lz, 16);
+      L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * (W + 4);
+    }
+  }
+  return L;
+}
+
+int tile_width_sites(const Layout& L) {
+  if (L.model == ISING || L.model == POTTS) return 16 * L.tile_cx;
+  if (L.model == O3) return 4 * L.tile_cx;
+  return 2 * L.tile_cx;
+}
+
+void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
+  const int tw = tile_width_sites(L);
+  for (int z0 = 0; z0 < L.lz; z0 += L.tile_z)
+    for (int y0 = 0; y0 < L.ly; y0 += L.tile_y)
+      for (int x0 = 0; x0 < L.lx; x0 += tw) out.push_back(TileItem{lat, x0, y0, z0});
+}
+
+int kernel_kind(int model, int dims) { return model * 2 + (dims - 2); }
+
+size_t footprint_bytes(const gpumc_spec* s) {
+  const Layout L = plan_layout(s);
+  const size_t per = 2 * L.buf_bytes;
+  const size_t rec_entries = (size_t)s->record_capacity * s->n_replicas * (L.model == MSC ? 64 : 1);
+  return per * s->n_replicas + rec_entries * sizeof(Record) +
+         (size_t)s->n_temps * kMaxClasses * 12 + 4096;
+}
+
+// ---------------------------------------------------------------------------
+// kernel launch table
+// ---------------------------------------------------------------------------
+typedef void (*SweepKernel)(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+static SweepKernel kernel_for(int kind) {
+  switch (kind) {
+    case 0: return k_sweep_discrete_2d<ISING>;
+    case 1: return k_sweep_discrete_3d<ISING>;
+    case 2: return k_sweep_discrete_2d<POTTS>;
+    case 3: return k_sweep_discrete_3d<POTTS>;
+    case 4: return k_sweep_o3<2>;
+    case 5: return k_sweep_o3<3>;
+    case 6: return k_sweep_msc<2>;
+    default: return k_sweep_msc<3>;
+  }
+}
+
+constexpr size_t kMaxDynSmem = 200 * 1024;
+
+static int prepare_kernels() {
+  static std::once_flag once;
+  static cudaError_t status = cudaSuccess;
+  std::call_once(once, [] {
+    for (int k = 0; k < 8; ++k) {
+      cudaError_t e = cudaFuncSetAttribute(kernel_for(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kMaxDynSmem);
+      if (e != cudaSuccess) status = e;
+    }
+  });
+  if (status != cudaSuccess)
+    return fail(GPUMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(status));
+  return GPUMC_OK;
+}
+
+int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
+                        LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem) {
+  if (n_tiles <= 0) return GPUMC_OK;
+  kernel_for(kind)<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  CUDA_TRY(cudaGetLastError());
+  return GPUMC_OK;
+}
+
+int launch_msc_measure(cudaStream_t st, const Layout& L, const LatDesc* lats, int lat,
+                       unsigned long long* counters) {
+  const int blocks = (int)std::min<int64_t>(1184, (L.n_sites + kThreads - 1) / kThreads);
+  if (L.dims == 2)
+    k_msc_measure<2><<<blocks, kThreads, 0, st>>>(lats, lat, counters);
+  else
+    k_msc_measure<3><<<blocks, kThreads, 0, st>>>(lats, lat, counters);
+  CUDA_TRY(cudaGetLastError());
+  return GPUMC_OK;
+}
+
+int launch_msc_record(cudaStream_t st, LatDesc* lats, GroupDesc* groups, int group,
+                      unsigned long long* counters) {
+  k_msc_record<<<1, 256, 0, st>>>(lats, groups, group, counters);
+  CUDA_TRY(cudaGetLastError());
+  return GPUMC_OK;
+}
+
+}  // namespace gpumc
+
+using namespace gpumc;
+
+// ===========================================================================
+// engine
+// ===========================================================================
+static int check_device(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(GPUMC_ENODEV, std::string("no usable CUDA device: ") +
+                                  (e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e)));
+  if (device < 0 || device >= n) return fail(GPUMC_ENODEV, "device index out of range");
+  return GPUMC_OK;
+}
+
+int gpumc_engine_create(int32_t device, gpumc_engine** out) {
+  if (!out) return fail(GPUMC_EINVAL, "out: null pointer");
+  int rc = check_device(device);
+  if (rc) return rc;
+  CUDA_TRY(cudaSetDevice(device));
+  rc = prepare_kernels();
+  if (rc) return rc;
+  gpumc_engine* e = new gpumc_engine();
+  e->device = device;
+  cudaError_t err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_lats, sizeof(LatDesc) * e->lat_cap);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_groups, sizeof(GroupDesc) * e->group_cap);
+  if (err == cudaSuccess) err = cudaMemset(e->d_lats, 0, sizeof(LatDesc) * e->lat_cap);
+  if (err == cudaSuccess) err = cudaMemset(e->d_groups, 0, sizeof(GroupDesc) * e->group_cap);
+  if (err != cudaSuccess) {
+    delete e;
+    return fail(GPUMC_ECUDA, std::string("engine allocation: ") + cudaGetErrorString(err));
+  }
+  e->lat_used.assign(e->lat_cap, false);
+  e->group_used.assign(e->group_cap, false);
+  *out = e;
+  return GPUMC_OK;
+}
+
+gpumc_engine::~gpumc_engine() {
+  cudaSetDevice(device);
+  drop_graphs();
+  for (auto& p : batch_plans) p.release();
+  if (d_lats) cudaFree(d_lats);
+  if (d_groups) cudaFree(d_groups);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void gpumc_engine::drop_graphs() {
+  for (auto& kv : batch_graphs) cudaGraphExecDestroy(kv.second);
+  batch_graphs.clear();
+}
+
+int gpumc_engine_destroy(gpumc_engine* eng) {
+  if (!eng) return GPUMC_OK;
+  if (!eng->sims.empty()) return fail(GPUMC_ESTATE, "engine still has simulations");
+  delete eng;
+  return GPUMC_OK;
+}
+
+int gpumc_engine_synchronize(gpumc_engine* eng) {
+  if (!eng) return fail(GPUMC_EINVAL, "engine: null");
+  CUDA_TRY(cudaSetDevice(eng->device));
+  CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return GPUMC_OK;
+}
+
+int gpumc_engine_stream(gpumc_engine* eng, void** stream) {
+  if (!eng || !stream) return fail(GPUMC_EINVAL, "null argument");
+  *stream = (void*)eng->stream;
+  return GPUMC_OK;
+}
+
+int gpumc_sim_engine(gpumc_sim* sim, gpumc_engine** eng) {
+  if (!sim || !eng) return fail(GPUMC_EINVAL, "null argument");
+  *eng = sim->eng;
+  return GPUMC_OK;
+}
+
+int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n) {
+  if (!sim || !n) return fail(GPUMC_EINVAL, "null argument");
+  *n = 1 + ((sim->lay.model == MSC && sim->phase == GPUMC_PHASE_MEASUREMENT) ? sim->n_rep + 1 : 0);
+  return GPUMC_OK;
+}
+
+void BatchPlan::release() {
+  if (d_tiles) cudaFree(d_tiles);
+  if (d_gids) cudaFree(d_gids);
+  if (d_ctl) cudaFree(d_ctl);
+  d_tiles = nullptr;
+  d_gids = nullptr;
+  d_ctl = nullptr;
+}
+
+int gpumc_engine::rebuild_batch() {
+  if (!batch_dirty) return GPUMC_OK;
+  drop_graphs();
+  for (auto& p : batch_plans) p.release();
+  batch_plans.clear();
+  std::map<int, BatchPlan> plans;
+  std::map<int, std::vector<TileItem>> tiles;
+  std::map<int, std::vector<int32_t>> gids;
+  for (gpumc_sim* s : sims) {
+    const int kind = kernel_kind(s->lay.model, s->lay.dims);
+    BatchPlan& p = plans[kind];
+    p.kind = kind;
+    p.smem = std::max(p.smem, s->lay.smem);
+    for (int r = 0; r < s->n_rep; ++r) enumerate_tiles(s->lay, s->lat0 + r, tiles[kind]);
+    gids[kind].push_back(s->group);
+  }
+  for (auto& kv : plans) {
+    BatchPlan p = kv.second;
+    auto& tv = tiles[kv.first];
+    auto& gv = gids[kv.first];
+    p.n_tiles = (int)tv.size();
+    p.n_groups = (int)gv.size();
+    CUDA_TRY(cudaMalloc(&p.d_tiles, sizeof(TileItem) * tv.size()));
+    CUDA_TRY(cudaMalloc(&p.d_gids, sizeof(int32_t) * gv.size()));
+    CUDA_TRY(cudaMalloc(&p.d_ctl, sizeof(LaunchCtl)));
+    CUDA_TRY(cudaMemcpy(p.d_tiles, tv.data(), sizeof(TileItem) * tv.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(p.d_gids, gv.data(), sizeof(int32_t) * gv.size(), cudaMemcpyHostToDevice));
+    LaunchCtl c;
+    c.done = 0;
+    c.n_groups = p.n_groups;
+    c.group_ids = p.d_gids;
+    CUDA_TRY(cudaMemcpy(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+    batch_plans.push_back(p);
+  }
+  batch_dirty = false;
+  return GPUMC_OK;
+}
+
+int gpumc_engine::launch_batch_sweep() {
+  for (auto& p : batch_plans) {
+    int rc = launch_sweep_kernel(stream, p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
+    if (rc) return rc;
+  }
+  for (gpumc_sim* s : sims) {
+    if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) {
+      int rc = s->launch_msc_measurement();
+      if (rc) return rc;
+    }
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
+  if (!eng) return fail(GPUMC_EINVAL, "engine: null");
+  CUDA_TRY(cudaSetDevice(eng->device));
+  int rc = eng->rebuild_batch();
+  if (rc) return rc;
+  if (eng->sims.empty() || n_sweeps == 0) return GPUMC_OK;
+  uint32_t left = n_sweeps;
+  while (left > 0) {
+    // never outrun the smallest free record space of a measuring simulation
+    uint32_t room = left;
+    for (gpumc_sim* s : eng->sims) {
+      if (s->phase != GPUMC_PHASE_MEASUREMENT || s->device_schedule) continue;
+      if (s->rec_used >= s->rec_cap) {
+        rc = s->drain_records();
+        if (rc) return rc;
+      }
+      room = std::min<uint32_t>(room, (uint32_t)(s->rec_cap - s->rec_used));
+    }
+    const uint32_t chunk = std::min<uint32_t>(room, 64);
+    if (eng->use_graphs) {
+      rc = eng->run_graph(chunk);
+    } else {
+      for (uint32_t i = 0; i < chunk && rc == GPUMC_OK; ++i) rc = eng->launch_batch_sweep();
+    }
+    if (rc) return rc;
+    for (gpumc_sim* s : eng->sims) {
+      s->sweeps = std::min<uint64_t>(s->sweeps + chunk, s->target);
+      if (s->phase == GPUMC_PHASE_MEASUREMENT && !s->device_schedule) s->rec_used += (int)chunk;
+    }
+    left -= chunk;
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_engine::run_graph(uint32_t n) {
+  auto it = batch_graphs.find(n);
+  if (it == batch_graphs.end()) {
+    cudaGraph_t g;
+    CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int rc = GPUMC_OK;
+    for (uint32_t i = 0; i < n && rc == GPUMC_OK; ++i) rc = launch_batch_sweep();
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    it = batch_graphs.emplace(n, ex).first;
+  }
+  CUDA_TRY(cudaGraphLaunch(it->second, stream));
+  return GPUMC_OK;
+}
+
+int gpumc_engine::alloc_slots(int n, int& first) {
+  // first fit of n consecutive free lattice slots
+  int run = 0;
+  for (int i = 0; i < lat_cap; ++i) {
+    run = lat_used[i] ? 0 : run + 1;
+    if (run == n) {
+      first = i - n + 1;
+      for (int j = first; j <= i; ++j) lat_used[j] = true;
+      return GPUMC_OK;
+    }
+  }
+  return fail(GPUMC_ENOMEM, "lattice descriptor pool exhausted");
+}
+
+int gpumc_engine::alloc_group(int& g) {
+  for (int i = 0; i < group_cap; ++i)
+    if (!group_used[i]) {
+      group_used[i] = true;
+      g = i;
+      return GPUMC_OK;
+    }
+  return fail(GPUMC_ENOMEM, "group descriptor pool exhausted");
+}
+
+int gpumc_last_error(char* buf, size_t cap) {
+  if (!buf || cap == 0) return (int)gpumc::g_last_error_size();
+  const std::string& m = gpumc::last_error_ref();
+  const size_t k = std::min(cap - 1, m.size());
+  std::memcpy(buf, m.data(), k);
+  buf[k] = 0;
+  return GPUMC_OK;
+}

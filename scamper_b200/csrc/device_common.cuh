@@ -1,0 +1,143 @@
+// Device helpers shared by the sweep kernels: Philox4x32-10 (Salmon, Moraes,
+// Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11), the
+// counter layout of the engine's random stream, and the exactly-rounded fp32
+// arithmetic the O(3) update is specified in.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "engine.h"
+
+namespace gpumc {
+
+__device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+  }
+  return c;
+}
+
+// Counter: word0 = index (chunk id or site id), word1 = colour | tag << 1 |
+// plane_pair << 8 | (index >> 32) << 16, words 2/3 = sweep.
+__device__ __forceinline__ uint4 draw(uint64_t key, uint64_t index, uint32_t colour, uint32_t tag,
+                                      uint32_t plane_pair, uint64_t sweep) {
+  uint4 c = make_uint4((uint32_t)index,
+                       colour | (tag << 1) | (plane_pair << 8) | ((uint32_t)(index >> 32) << 16),
+                       (uint32_t)sweep, (uint32_t)(sweep >> 32));
+  return philox10(c, (uint32_t)key, (uint32_t)(key >> 32));
+}
+
+__device__ __forceinline__ int wrapi(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
+// Exact decision u < T for the 80-bit threshold T = head:tail, given the
+// 16-bit head draw u16 that already tied with head.
+static __device__ __noinline__ bool refine_accept(uint64_t key, uint64_t site, uint32_t colour,
+                                           uint64_t sweep, unsigned long long tail) {
+  uint4 o = draw(key, site, colour, TAG_ACC_REFINE, 0, sweep);
+  unsigned long long r = (unsigned long long)o.x | ((unsigned long long)o.y << 32);
+  return r < tail;
+}
+
+// Potts proposal: uniform r in [0, n) from a 16-bit draw with Lemire's
+// multiply-shift and exact rejection; rejected draws retry with 32-bit values
+// from a per-site refine batch.
+static __device__ __noinline__ uint32_t potts_refine(uint64_t key, uint64_t site, uint32_t colour,
+                                              uint64_t sweep, uint32_t n) {
+  uint4 o = draw(key, site, colour, TAG_PROP_REFINE, 0, sweep);
+  const uint32_t rej = (uint32_t)(0x100000000ull % n);
+  uint32_t v[4] = {o.x, o.y, o.z, o.w};
+  unsigned long long m = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    m = (unsigned long long)v[i] * n;
+    if ((uint32_t)m >= rej) return (uint32_t)(m >> 32);
+  }
+  return (uint32_t)(m >> 32);
+}
+
+// ---- exactly rounded fp32 building blocks (no contraction into FMA) ------
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+
+// exp(x) for x <= 0: Cody-Waite split into 2^n * e^t with |t| <= ln2/2 and
+// the degree-7 Taylor polynomial of e^t (truncation error < 5e-9 relative).
+__device__ __forceinline__ float exp_neg(float x) {
+  if (!(x <= 0.0f)) return 1.0f;
+  if (x < -87.0f) return 0.0f;
+  const float y = fmul(x, 0x1.715476p+0f);
+  const float n = floorf(fadd(y, 0.5f));
+  const float f = fsub(y, n);
+  const float t = fmul(f, 0x1.62e430p-1f);
+  float p = 0x1.a01a02p-13f;
+  p = fadd(fmul(p, t), 0x1.6c16c2p-10f);
+  p = fadd(fmul(p, t), 0x1.111112p-7f);
+  p = fadd(fmul(p, t), 0x1.555556p-5f);
+  p = fadd(fmul(p, t), 0x1.555556p-3f);
+  p = fadd(fmul(p, t), 0.5f);
+  p = fadd(fmul(p, t), 1.0f);
+  p = fadd(fmul(p, t), 1.0f);
+  const int ni = (int)n;
+  const float scale = __int_as_float((ni + 127) << 23);
+  return fmul(p, scale);
+}
+
+// (cos, sin) of 2*pi*u/2^32: octant from the top 3 bits, the angle inside the
+// octant from the next 24 bits, Taylor polynomials on [0, pi/4].
+__device__ __forceinline__ void sincos_turn(uint32_t u, float& c, float& s) {
+  const uint32_t octant = u >> 29;
+  float t = fmul((float)((u >> 5) & 0xFFFFFFu), 0x1p-24f);
+  if (octant & 1u) t = fsub(1.0f, t);
+  const float th = fmul(t, 0x1.921fb6p-1f);
+  const float t2 = fmul(th, th);
+  float sp = 0x1.71de3ap-19f;
+  sp = fsub(fmul(sp, t2), 0x1.a01a02p-13f);
+  sp = fadd(fmul(sp, t2), 0x1.111112p-7f);
+  sp = fsub(fmul(sp, t2), 0x1.555556p-3f);
+  sp = fadd(fmul(sp, t2), 1.0f);
+  const float sn = fmul(th, sp);
+  float cp = -0x1.27e4fcp-22f;
+  cp = fadd(fmul(cp, t2), 0x1.a01a02p-16f);
+  cp = fsub(fmul(cp, t2), 0x1.6c16c2p-10f);
+  cp = fadd(fmul(cp, t2), 0x1.555556p-5f);
+  cp = fsub(fmul(cp, t2), 0.5f);
+  const float cs = fadd(fmul(cp, t2), 1.0f);
+  switch (octant) {
+    case 0: c = cs; s = sn; break;
+    case 1: c = sn; s = cs; break;
+    case 2: c = -sn; s = cs; break;
+    case 3: c = -cs; s = sn; break;
+    case 4: c = -cs; s = -sn; break;
+    case 5: c = -sn; s = -cs; break;
+    case 6: c = sn; s = -cs; break;
+    default: c = cs; s = -sn; break;
+  }
+}
+
+// log-space Metropolis decision of Carlo.rs/src/acceptance.rs:11-22 with u
+// built from the top 53 bits of a 64-bit draw.
+__device__ __forceinline__ bool accept_log(double logA, unsigned long long u64) {
+  if (isnan(logA)) return false;
+  if (logA >= 0.0) return true;
+  if (isinf(logA)) return false;
+  double u = (double)(u64 >> 11) * 0x1p-53;
+  if (u < 2.2250738585072014e-308) u = 2.2250738585072014e-308;
+  return log(u) < logA;
+}
+
+__device__ __forceinline__ void atomic_add_i64(unsigned long long* p, long long v) {
+  atomicAdd(p, (unsigned long long)v);
+}
+
+}  // namespace gpumc

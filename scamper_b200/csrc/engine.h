@@ -1,0 +1,110 @@
+// Shared host/device definitions of the lattice engine.
+//
+// A "lattice" is one spin configuration (one replica) resident in HBM.  Its
+// state lives in two ping-pong buffers: sweep t reads buf[t & 1] and writes
+// buf[(t + 1) & 1], so every tile of a sweep reads an immutable snapshot and
+// the two colour half-sweeps of the checkerboard can be fused in one pass
+// (2 bytes of compulsory HBM traffic per int8 attempt instead of 3-4).
+//
+// Layout in HBM:
+//   int8 models : rows of `pitch` = round_up(Lx, 16) bytes; row rho = y + Ly*z.
+//   O(3)        : three float planes (x, y, z components), each rows of
+//                 `pitch` = round_up(Lx, 4) floats.
+//   multi-spin  : rows of `pitch` = round_up(Lx, 2) uint64 words (bit r =
+//                 replica r, 1 = spin up), as in the reference's
+//                 MultiSpinIsing::packed_spins (CMC.rs/src/multi_spin.rs:28-43).
+#pragma once
+#include <stdint.h>
+
+namespace gpumc {
+
+enum Model : int32_t { ISING = 0, POTTS = 1, O3 = 2, MSC = 3 };
+
+// Stream tags (counter word 1, bits 1..7; bit 0 holds the colour).
+enum Tag : uint32_t {
+  TAG_ACC = 0, TAG_PROP = 1, TAG_ACC_REFINE = 2, TAG_PROP_REFINE = 3,
+  TAG_INIT = 4, TAG_O3 = 5, TAG_MSC = 6, TAG_PT = 7
+};
+
+constexpr int kMaxClasses = 13;    // 2z+1 for z = 6 (Potts on the cubic lattice)
+constexpr int kMaxPottsCounts = 8; // fused order-parameter histogram (q <= 8)
+constexpr int kThreads = 256;      // CTA size of the sweep kernels
+
+// Per-sweep accumulators, filled with atomics by the sweep kernels and
+// drained by the epilogue (last CTA of the launch).
+struct Accum {
+  unsigned long long dE;        // int64 energy change (units of J), two's complement
+  unsigned long long mag;       // int64 sum of spins (Ising)
+  unsigned long long accepted;  // accepted moves
+  unsigned long long counts[kMaxPottsCounts];
+  double dEf;                   // O(3): accumulated fp32 dE
+  double mx, my, mz;            // O(3): magnetisation components
+};
+
+// One measured sweep of one lattice, as recorded on the device.
+struct Record {
+  double energy;       // physical energy after the sweep
+  double m[3];         // Ising: {sum s}; Potts: {max count, -, -}; O(3): sum vector
+  double accepted;     // accepted moves in the sweep
+  int32_t label;       // temperature index held during the sweep
+  int32_t pad;
+  uint64_t sweep;      // sweep index (0-based) of this record
+};
+
+struct LatDesc {
+  // geometry / model (immutable after creation)
+  int32_t model, dims, lx, ly, lz, pitch, q, z;
+  int32_t tile_cx, tile_y, tile_z;  // tile shape: chunks (16 sites) x rows x planes
+  int32_t group;                    // index into the group array (PT / records)
+  int32_t replica;                  // replica index within its group
+  int32_t pad0;
+  int64_t n_sites;
+  void* buf[2];
+  uint64_t key;                     // Philox key of the sweep stream
+  // mutable device state
+  uint64_t sweep;                   // sweeps completed
+  uint64_t target;                  // stop once sweep reaches this count (serving)
+  long long e_int;                  // discrete: energy in units of J
+  double e_f;                       // O(3): running energy
+  float omc;                        // O(3): 1 - cos(cone half-angle)
+  int32_t adapt;                    // O(3): adapt omc during this sweep
+  Accum acc;
+};
+
+// A group is a set of lattices that share a temperature ladder and a record
+// stream: the replicas of one simulation handle (a PT ensemble, or independent
+// replicas with their own ladders).
+struct GroupDesc {
+  int32_t first_lat, n_rep, n_cls, pt_interval;  // pt_interval 0 = no exchange
+  int32_t measure;                // record every sweep of this launch
+  int32_t rec_cap, rec_count, overflow;
+  int32_t* label;                 // [n_rep] temperature index of each replica
+  int32_t* rep_at;                // [n_rep] scratch: replica holding each index
+  const uint32_t* head;           // [n_temps][n_cls] 17-bit threshold heads
+  const unsigned long long* tail; // [n_temps][n_cls] 64-bit threshold tails
+  const double* betas;            // [n_temps]
+  const float* betas_f;           // [n_temps] (O(3))
+  double J;
+  float Jf;
+  int32_t pad1;
+  uint64_t measure_from;          // record only sweeps with index >= this
+  uint64_t adapt_until;           // O(3): adapt the cone only below this sweep
+  uint64_t msc_recorded;          // multi-spin: sweep count of the last record
+  uint64_t pt_key;                // exchange stream key
+  uint64_t pt_step;               // exchanges attempted so far
+  unsigned long long pt_accepted; // accepted swaps (all pairs)
+  Record* records;                // [rec_cap][n_rep]
+};
+
+struct TileItem {
+  int32_t lat, x0, y0, z0;
+};
+
+// Device-side bookkeeping of one launch (last-CTA epilogue).
+struct LaunchCtl {
+  unsigned int done;
+  int32_t n_groups;
+  const int32_t* group_ids;  // [n_groups] indices into the group pool
+};
+
+}  // namespace gpumc

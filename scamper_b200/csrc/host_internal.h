@@ -1,0 +1,136 @@
+// Host-side structures of the engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/gpumc.h"
+#include "engine.h"
+
+namespace gpumc {
+
+struct Layout {
+  int model = 0, dims = 2, lx = 0, ly = 0, lz = 1, pitch = 0;
+  int64_t n_sites = 0;
+  size_t buf_bytes = 0;  // one ping-pong buffer
+  int tile_cx = 0, tile_y = 0, tile_z = 1;
+  size_t smem = 0;
+};
+
+int fail(int code, const std::string& msg);
+uint64_t stream_key(uint64_t base, uint64_t replica, uint64_t phase, uint64_t substream);
+void threshold80(double p, uint32_t& head, unsigned long long& tail);
+int n_classes(int model, int dims);
+void build_table(int model, int dims, double J, double beta, uint32_t* head,
+                 unsigned long long* tail);
+int validate_spec(const gpumc_spec* s);
+Layout plan_layout(const gpumc_spec* s);
+void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out);
+int kernel_kind(int model, int dims);
+size_t footprint_bytes(const gpumc_spec* s);
+int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
+                        LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem);
+int launch_msc_measure(cudaStream_t st, const Layout& L, const LatDesc* lats, int lat,
+                       unsigned long long* counters);
+const std::string& last_error_ref();
+size_t g_last_error_size();
+int launch_msc_record(cudaStream_t st, LatDesc* lats, GroupDesc* groups, int group,
+                      unsigned long long* counters);
+
+struct BatchPlan {
+  int kind = 0;
+  size_t smem = 0;
+  TileItem* d_tiles = nullptr;
+  int n_tiles = 0;
+  int32_t* d_gids = nullptr;
+  int n_groups = 0;
+  LaunchCtl* d_ctl = nullptr;
+  void release();
+};
+
+}  // namespace gpumc
+
+struct gpumc_sim;
+
+struct gpumc_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  gpumc::LatDesc* d_lats = nullptr;
+  gpumc::GroupDesc* d_groups = nullptr;
+  int lat_cap = 16384;
+  int group_cap = 8192;
+  std::vector<bool> lat_used, group_used;
+  std::set<gpumc_sim*> sims;
+  bool batch_dirty = true;
+  bool use_graphs = true;
+  std::vector<gpumc::BatchPlan> batch_plans;
+  std::map<uint32_t, cudaGraphExec_t> batch_graphs;
+
+  ~gpumc_engine();
+  int rebuild_batch();
+  int launch_batch_sweep();
+  int run_graph(uint32_t n);
+  void drop_graphs();
+  int alloc_slots(int n, int& first);
+  int alloc_group(int& g);
+};
+
+struct gpumc_sim {
+  gpumc_engine* eng = nullptr;
+  bool private_engine = false;
+  gpumc_spec spec{};
+  std::vector<double> betas;
+  gpumc::Layout lay;
+  int n_rep = 1, n_temps = 1, n_cls = 0;
+  int lat0 = -1, group = -1;
+  uint64_t base_seed = 0;
+  std::vector<void*> bufs;  // 2 per replica
+  uint32_t* d_head = nullptr;
+  unsigned long long* d_tail = nullptr;
+  double* d_betas = nullptr;
+  float* d_betas_f = nullptr;
+  int32_t* d_label = nullptr;
+  int32_t* d_rep_at = nullptr;
+  gpumc::Record* d_records = nullptr;
+  int rec_cap = 0, rec_used = 0;
+  int rec_stride = 1;  // records per sweep
+  unsigned long long* d_msc_counters = nullptr;
+  gpumc::TileItem* d_tiles = nullptr;
+  int n_tiles = 0;
+  int32_t* d_gid = nullptr;
+  gpumc::LaunchCtl* d_ctl = nullptr;
+  std::map<uint32_t, cudaGraphExec_t> graphs;
+  uint64_t sweeps = 0;  // host mirror of the device sweep counter
+  uint64_t target = ~0ull;        // sweep target (serving)
+  bool device_schedule = false;   // phases driven by measure_from / target on the device
+  int phase = GPUMC_PHASE_THERMALIZATION;
+  uint32_t pt_interval = 0;
+  std::vector<gpumc_obs> pending;
+
+  ~gpumc_sim();
+  int launch_one_sweep();
+  int launch_msc_measurement();
+  int run_graph(uint32_t n);
+  int drain_records();
+  int push_phase_flags();
+  int upload_tables();
+  void drop_graphs();
+  int recompute(std::vector<double>& out, bool store);
+  template <class T>
+  int set_lat_field(int r, size_t offset, const T& v) {
+    return cudaMemcpyAsync(reinterpret_cast<char*>(eng->d_lats + lat0 + r) + offset, &v, sizeof(T),
+                           cudaMemcpyHostToDevice, eng->stream) == cudaSuccess
+               ? GPUMC_OK
+               : gpumc::fail(GPUMC_ECUDA, "descriptor update failed");
+  }
+  template <class T>
+  int set_group_field(size_t offset, const T& v) {
+    return cudaMemcpyAsync(reinterpret_cast<char*>(eng->d_groups + group) + offset, &v, sizeof(T),
+                           cudaMemcpyHostToDevice, eng->stream) == cudaSuccess
+               ? GPUMC_OK
+               : gpumc::fail(GPUMC_ECUDA, "descriptor update failed");
+  }
+};

@@ -1,0 +1,661 @@
+// Simulation handles: ClassicalMC-style construction, sweeps, observables,
+// spin I/O and the parallel-tempering contract over the C ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gpumc.h"
+#include "engine.h"
+#include "host_internal.h"
+
+namespace gpumc {
+__global__ void k_init_discrete(int8_t*, int, int, int, int, int, int, uint64_t, int);
+__global__ void k_init_o3(float*, int, int, int, int, uint64_t, int);
+__global__ void k_init_msc(unsigned long long*, int, int, int, int, const uint64_t*, int);
+__global__ void k_energy_int(const void*, int, int, int, int, int, unsigned long long*);
+__global__ void k_energy_o3(const float*, int, int, int, int, double, double*);
+__global__ void k_philox_probe(const uint4*, const uint2*, uint4*, int);
+}  // namespace gpumc
+
+using namespace gpumc;
+
+#define CUDA_TRY(expr)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? GPUMC_ENOMEM : GPUMC_ECUDA,   \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+#define RC_TRY(expr)      \
+  do {                    \
+    int rc_ = (expr);     \
+    if (rc_) return rc_;  \
+  } while (0)
+
+static const int kInitBlocks = 1184;
+
+gpumc_sim::~gpumc_sim() {
+  cudaSetDevice(eng->device);
+  cudaStreamSynchronize(eng->stream);
+  drop_graphs();
+  for (void* b : bufs) cudaFree(b);
+  cudaFree(d_head);
+  cudaFree(d_tail);
+  cudaFree(d_betas);
+  cudaFree(d_betas_f);
+  cudaFree(d_label);
+  cudaFree(d_rep_at);
+  cudaFree(d_records);
+  cudaFree(d_msc_counters);
+  cudaFree(d_tiles);
+  cudaFree(d_gid);
+  cudaFree(d_ctl);
+}
+
+void gpumc_sim::drop_graphs() {
+  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  graphs.clear();
+}
+
+int gpumc_sim::upload_tables() {
+  std::vector<uint32_t> head((size_t)n_temps * n_cls);
+  std::vector<unsigned long long> tail((size_t)n_temps * n_cls);
+  std::vector<float> bf(n_temps);
+  for (int t = 0; t < n_temps; ++t) {
+    build_table(lay.model == MSC ? ISING : lay.model, lay.dims, spec.J, betas[t], &head[(size_t)t * n_cls],
+                &tail[(size_t)t * n_cls]);
+    bf[t] = (float)betas[t];
+  }
+  CUDA_TRY(cudaMemcpyAsync(d_head, head.data(), head.size() * 4, cudaMemcpyHostToDevice, eng->stream));
+  CUDA_TRY(cudaMemcpyAsync(d_tail, tail.data(), tail.size() * 8, cudaMemcpyHostToDevice, eng->stream));
+  CUDA_TRY(cudaMemcpyAsync(d_betas, betas.data(), betas.size() * 8, cudaMemcpyHostToDevice, eng->stream));
+  CUDA_TRY(cudaMemcpyAsync(d_betas_f, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, eng->stream));
+  CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return GPUMC_OK;
+}
+
+int gpumc_sim::push_phase_flags() {
+  const int32_t measure = phase == GPUMC_PHASE_MEASUREMENT ? 1 : 0;
+  RC_TRY(set_group_field(offsetof(GroupDesc, measure), measure));
+  if (lay.model == O3) {
+    const int32_t adapt = phase == GPUMC_PHASE_THERMALIZATION ? 1 : 0;
+    for (int r = 0; r < n_rep; ++r) RC_TRY(set_lat_field(r, offsetof(LatDesc, adapt), adapt));
+  }
+  CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return GPUMC_OK;
+}
+
+int gpumc_sim::launch_msc_measurement() {
+  for (int r = 0; r < n_rep; ++r)
+    RC_TRY(launch_msc_measure(eng->stream, lay, eng->d_lats, lat0 + r, d_msc_counters + (size_t)r * 128));
+  return launch_msc_record(eng->stream, eng->d_lats, eng->d_groups, group, d_msc_counters);
+}
+
+int gpumc_sim::launch_one_sweep() {
+  RC_TRY(launch_sweep_kernel(eng->stream, kernel_kind(lay.model, lay.dims), d_tiles, n_tiles,
+                             eng->d_lats, eng->d_groups, d_ctl, lay.smem));
+  return GPUMC_OK;
+}
+
+int gpumc_sim::run_graph(uint32_t n) {
+  const uint32_t key = n;
+  auto it = graphs.find(key);
+  if (it == graphs.end()) {
+    cudaGraph_t g;
+    CUDA_TRY(cudaStreamBeginCapture(eng->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = GPUMC_OK;
+    for (uint32_t i = 0; i < n && rc == GPUMC_OK; ++i) {
+      rc = launch_one_sweep();
+      if (rc == GPUMC_OK && lay.model == MSC && phase == GPUMC_PHASE_MEASUREMENT)
+        rc = launch_msc_measurement();
+    }
+    cudaError_t e = cudaStreamEndCapture(eng->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    it = graphs.emplace(key, ex).first;
+  }
+  CUDA_TRY(cudaGraphLaunch(it->second, eng->stream));
+  return GPUMC_OK;
+}
+
+int gpumc_sim::drain_records() {
+  CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  GroupDesc g;
+  CUDA_TRY(cudaMemcpy(&g, eng->d_groups + group, sizeof(GroupDesc), cudaMemcpyDeviceToHost));
+  if (g.overflow) return fail(GPUMC_ESTATE, "record buffer overflow (internal scheduling error)");
+  const int cnt = g.rec_count;
+  if (cnt > 0) {
+    std::vector<Record> recs((size_t)cnt * rec_stride);
+    CUDA_TRY(cudaMemcpy(recs.data(), d_records, recs.size() * sizeof(Record), cudaMemcpyDeviceToHost));
+    const double n = (double)lay.n_sites;
+    for (int i = 0; i < cnt; ++i) {
+      for (int r = 0; r < rec_stride; ++r) {
+        const Record& R = recs[(size_t)i * rec_stride + r];
+        gpumc_obs o;
+        o.sweep = R.sweep;
+        o.replica = r;
+        o.temp_index = R.label;
+        o.beta = betas[std::min(std::max(R.label, 0), n_temps - 1)];
+        o.energy = R.energy;
+        if (lay.model == POTTS)
+          o.magnetization = ((double)spec.q * R.m[0] - n) / (n * (double)(spec.q - 1));
+        else if (lay.model == O3)
+          o.magnetization = std::sqrt(R.m[0] * R.m[0] + R.m[1] * R.m[1] + R.m[2] * R.m[2]) / n;
+        else
+          o.magnetization = std::fabs(R.m[0]) / n;
+        o.acceptance = R.accepted / n;
+        pending.push_back(o);
+      }
+    }
+    const int32_t zero = 0;
+    RC_TRY(set_group_field(offsetof(GroupDesc, rec_count), zero));
+    CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  }
+  rec_used = 0;
+  return GPUMC_OK;
+}
+
+int gpumc_sim::recompute(std::vector<double>& out, bool store) {
+  out.assign(n_rep, 0.0);
+  unsigned long long* d_acc = nullptr;
+  CUDA_TRY(cudaMalloc(&d_acc, 8 * (size_t)n_rep));
+  CUDA_TRY(cudaMemsetAsync(d_acc, 0, 8 * (size_t)n_rep, eng->stream));
+  const int blocks = (int)std::min<int64_t>(kInitBlocks, (lay.n_sites + 255) / 256);
+  for (int r = 0; r < n_rep; ++r) {
+    const void* buf = bufs[2 * r + (sweeps & 1)];
+    if (lay.model == O3)
+      k_energy_o3<<<blocks, 256, 0, eng->stream>>>((const float*)buf, lay.lx, lay.ly, lay.lz, lay.pitch,
+                                                    spec.J, (double*)(d_acc + r));
+    else
+      k_energy_int<<<blocks, 256, 0, eng->stream>>>(buf, lay.model, lay.lx, lay.ly, lay.lz, lay.pitch,
+                                                     d_acc + r);
+  }
+  std::vector<unsigned long long> h(n_rep);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_acc, 8 * (size_t)n_rep, cudaMemcpyDeviceToHost, eng->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
+  cudaFree(d_acc);
+  if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("energy recompute: ") + cudaGetErrorString(e));
+  for (int r = 0; r < n_rep; ++r) {
+    if (lay.model == O3) {
+      double v;
+      std::memcpy(&v, &h[r], 8);
+      out[r] = v;
+      if (store) RC_TRY(set_lat_field(r, offsetof(LatDesc, e_f), v));
+    } else {
+      const long long ei = (long long)h[r];
+      out[r] = spec.J * (double)ei;
+      if (store) RC_TRY(set_lat_field(r, offsetof(LatDesc, e_int), ei));
+    }
+  }
+  if (store) CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return GPUMC_OK;
+}
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+int gpumc_validate(const gpumc_spec* spec) { return validate_spec(spec); }
+
+int gpumc_footprint(const gpumc_spec* spec, size_t* bytes) {
+  RC_TRY(validate_spec(spec));
+  if (!bytes) return fail(GPUMC_EINVAL, "bytes: null");
+  *bytes = footprint_bytes(spec);
+  return GPUMC_OK;
+}
+
+int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, gpumc_sim** out) {
+  RC_TRY(validate_spec(spec));
+  if (!out) return fail(GPUMC_EINVAL, "out: null pointer");
+  bool priv = false;
+  if (!eng) {
+    RC_TRY(gpumc_engine_create(0, &eng));
+    priv = true;
+  }
+  CUDA_TRY(cudaSetDevice(eng->device));
+  gpumc_sim* s = new gpumc_sim();
+  s->eng = eng;
+  s->private_engine = priv;
+  s->spec = *spec;
+  s->betas.assign(spec->betas, spec->betas + spec->n_temps);
+  s->spec.betas = nullptr;
+  s->lay = plan_layout(spec);
+  s->n_rep = spec->n_replicas;
+  s->n_temps = spec->n_temps;
+  s->n_cls = n_classes(s->lay.model == MSC ? ISING : s->lay.model, s->lay.dims);
+  s->base_seed = base_seed;
+  s->rec_cap = spec->record_capacity;
+  s->rec_stride = s->lay.model == MSC ? 64 * s->n_rep : s->n_rep;
+  auto cleanup = [&](int rc) {
+    if (s->lat0 >= 0)
+      for (int r = 0; r < s->n_rep; ++r) eng->lat_used[s->lat0 + r] = false;
+    if (s->group >= 0) eng->group_used[s->group] = false;
+    delete s;
+    if (priv) gpumc_engine_destroy(eng);
+    return rc;
+  };
+  int rc = eng->alloc_slots(s->n_rep, s->lat0);
+  if (rc) return cleanup(rc);
+  rc = eng->alloc_group(s->group);
+  if (rc) return cleanup(rc);
+#define CUDA_CLEAN(expr)                                                              \
+  do {                                                                                \
+    cudaError_t e_ = (expr);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return cleanup(fail(e_ == cudaErrorMemoryAllocation ? GPUMC_ENOMEM : GPUMC_ECUDA, \
+                          std::string(#expr) + ": " + cudaGetErrorString(e_)));        \
+  } while (0)
+  // device buffers
+  s->bufs.assign(2 * s->n_rep, nullptr);
+  for (int i = 0; i < 2 * s->n_rep; ++i) {
+    CUDA_CLEAN(cudaMalloc(&s->bufs[i], s->lay.buf_bytes));
+    CUDA_CLEAN(cudaMemsetAsync(s->bufs[i], 0, s->lay.buf_bytes, eng->stream));
+  }
+  CUDA_CLEAN(cudaMalloc(&s->d_head, 4 * (size_t)s->n_temps * s->n_cls));
+  CUDA_CLEAN(cudaMalloc(&s->d_tail, 8 * (size_t)s->n_temps * s->n_cls));
+  CUDA_CLEAN(cudaMalloc(&s->d_betas, 8 * (size_t)s->n_temps));
+  CUDA_CLEAN(cudaMalloc(&s->d_betas_f, 4 * (size_t)s->n_temps));
+  CUDA_CLEAN(cudaMalloc(&s->d_label, 4 * (size_t)s->n_rep));
+  CUDA_CLEAN(cudaMalloc(&s->d_rep_at, 4 * (size_t)s->n_rep));
+  CUDA_CLEAN(cudaMalloc(&s->d_records, sizeof(Record) * (size_t)s->rec_cap * s->rec_stride));
+  if (s->lay.model == MSC) {
+    CUDA_CLEAN(cudaMalloc(&s->d_msc_counters, 8 * 128 * (size_t)s->n_rep));
+    CUDA_CLEAN(cudaMemsetAsync(s->d_msc_counters, 0, 8 * 128 * (size_t)s->n_rep, eng->stream));
+  }
+  rc = s->upload_tables();
+  if (rc) return cleanup(rc);
+  std::vector<int32_t> labels(s->n_rep);
+  for (int r = 0; r < s->n_rep; ++r) labels[r] = s->n_temps == 1 ? 0 : r;
+  CUDA_CLEAN(cudaMemcpy(s->d_label, labels.data(), 4 * (size_t)s->n_rep, cudaMemcpyHostToDevice));
+  // tiles and launch control of the plain path
+  std::vector<TileItem> tiles;
+  for (int r = 0; r < s->n_rep; ++r) enumerate_tiles(s->lay, s->lat0 + r, tiles);
+  s->n_tiles = (int)tiles.size();
+  CUDA_CLEAN(cudaMalloc(&s->d_tiles, sizeof(TileItem) * tiles.size()));
+  CUDA_CLEAN(cudaMemcpy(s->d_tiles, tiles.data(), sizeof(TileItem) * tiles.size(), cudaMemcpyHostToDevice));
+  CUDA_CLEAN(cudaMalloc(&s->d_gid, sizeof(int32_t)));
+  CUDA_CLEAN(cudaMemcpy(s->d_gid, &s->group, sizeof(int32_t), cudaMemcpyHostToDevice));
+  CUDA_CLEAN(cudaMalloc(&s->d_ctl, sizeof(LaunchCtl)));
+  LaunchCtl c;
+  c.done = 0;
+  c.n_groups = 1;
+  c.group_ids = s->d_gid;
+  CUDA_CLEAN(cudaMemcpy(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  // descriptors
+  const float omc = (float)(2.0 * std::sin(0.5 * spec->cone_half_angle) * std::sin(0.5 * spec->cone_half_angle));
+  for (int r = 0; r < s->n_rep; ++r) {
+    LatDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.model = s->lay.model;
+    d.dims = s->lay.dims;
+    d.lx = s->lay.lx;
+    d.ly = s->lay.ly;
+    d.lz = s->lay.lz;
+    d.pitch = s->lay.pitch;
+    d.q = spec->q;
+    d.z = 2 * s->lay.dims;
+    d.tile_cx = s->lay.tile_cx;
+    d.tile_y = s->lay.tile_y;
+    d.tile_z = s->lay.tile_z;
+    d.group = s->group;
+    d.replica = r;
+    d.n_sites = s->lay.n_sites;
+    d.buf[0] = s->bufs[2 * r];
+    d.buf[1] = s->bufs[2 * r + 1];
+    const uint64_t rid = s->lay.model == MSC ? 64ull * r : (uint64_t)r;
+    d.key = stream_key(base_seed, rid, 0, 1);
+    d.sweep = 0;
+    d.target = ~0ull;
+    d.omc = omc;
+    d.adapt = 1;
+    CUDA_CLEAN(cudaMemcpy(eng->d_lats + s->lat0 + r, &d, sizeof(d), cudaMemcpyHostToDevice));
+  }
+  GroupDesc g;
+  std::memset(&g, 0, sizeof(g));
+  g.first_lat = s->lat0;
+  g.n_rep = s->n_rep;
+  g.n_cls = s->n_cls;
+  g.pt_interval = 0;
+  g.measure = 0;
+  g.rec_cap = s->rec_cap;
+  g.label = s->d_label;
+  g.rep_at = s->d_rep_at;
+  g.head = s->d_head;
+  g.tail = s->d_tail;
+  g.betas = s->d_betas;
+  g.betas_f = s->d_betas_f;
+  g.J = spec->J;
+  g.Jf = (float)spec->J;
+  g.measure_from = 0;
+  g.adapt_until = ~0ull;
+  g.pt_key = stream_key(base_seed, 0, 3, 0);
+  g.records = s->d_records;
+  CUDA_CLEAN(cudaMemcpy(eng->d_groups + s->group, &g, sizeof(g), cudaMemcpyHostToDevice));
+  // initial state
+  const int blocks = (int)std::min<int64_t>(kInitBlocks, (s->lay.n_sites + 255) / 256);
+  const int hot = spec->init == GPUMC_INIT_HOT;
+  uint64_t* d_keys = nullptr;
+  if (s->lay.model == MSC) CUDA_CLEAN(cudaMalloc(&d_keys, 8 * 64));
+  for (int r = 0; r < s->n_rep; ++r) {
+    const uint64_t kinit = stream_key(base_seed, (uint64_t)r, 0, 0);
+    if (s->lay.model == ISING || s->lay.model == POTTS) {
+      k_init_discrete<<<blocks, 256, 0, eng->stream>>>((int8_t*)s->bufs[2 * r], s->lay.model, s->lay.lx,
+                                                        s->lay.ly, s->lay.lz, s->lay.pitch, spec->q,
+                                                        kinit, hot);
+    } else if (s->lay.model == O3) {
+      k_init_o3<<<blocks, 256, 0, eng->stream>>>((float*)s->bufs[2 * r], s->lay.lx, s->lay.ly, s->lay.lz,
+                                                  s->lay.pitch, kinit, hot);
+    } else {
+      uint64_t keys[64];
+      for (int b = 0; b < 64; ++b) keys[b] = stream_key(base_seed, 64ull * r + b, 0, 0);
+      CUDA_CLEAN(cudaMemcpy(d_keys, keys, sizeof(keys), cudaMemcpyHostToDevice));
+      k_init_msc<<<blocks, 256, 0, eng->stream>>>((unsigned long long*)s->bufs[2 * r], s->lay.lx,
+                                                   s->lay.ly, s->lay.lz, s->lay.pitch, d_keys, hot);
+      CUDA_CLEAN(cudaStreamSynchronize(eng->stream));
+    }
+  }
+  CUDA_CLEAN(cudaGetLastError());
+  CUDA_CLEAN(cudaStreamSynchronize(eng->stream));
+  if (d_keys) cudaFree(d_keys);
+  std::vector<double> e0;
+  rc = s->recompute(e0, true);
+  if (rc) return cleanup(rc);
+  rc = s->push_phase_flags();
+  if (rc) return cleanup(rc);
+#undef CUDA_CLEAN
+  eng->sims.insert(s);
+  eng->batch_dirty = true;
+  *out = s;
+  return GPUMC_OK;
+}
+
+int gpumc_destroy(gpumc_sim* sim) {
+  if (!sim) return GPUMC_OK;
+  gpumc_engine* eng = sim->eng;
+  const bool priv = sim->private_engine;
+  eng->sims.erase(sim);
+  eng->batch_dirty = true;
+  for (int r = 0; r < sim->n_rep; ++r) eng->lat_used[sim->lat0 + r] = false;
+  eng->group_used[sim->group] = false;
+  delete sim;
+  if (priv) gpumc_engine_destroy(eng);
+  return GPUMC_OK;
+}
+
+int gpumc_set_phase(gpumc_sim* sim, int32_t phase) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (phase != GPUMC_PHASE_THERMALIZATION && phase != GPUMC_PHASE_MEASUREMENT)
+    return fail(GPUMC_EINVAL, "phase: expected THERMALIZATION or MEASUREMENT");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  if (phase == sim->phase) return GPUMC_OK;
+  sim->phase = phase;
+  sim->drop_graphs();
+  sim->eng->drop_graphs();
+  return sim->push_phase_flags();
+}
+
+int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  uint32_t left = n_sweeps;
+  while (left > 0) {
+    uint32_t room = left;
+    if (sim->phase == GPUMC_PHASE_MEASUREMENT) {
+      if (sim->rec_used >= sim->rec_cap) RC_TRY(sim->drain_records());
+      room = std::min<uint32_t>(room, (uint32_t)(sim->rec_cap - sim->rec_used));
+    }
+    const uint32_t chunk = std::min<uint32_t>(room, 64);
+    RC_TRY(sim->run_graph(chunk));
+    sim->sweeps += chunk;
+    if (sim->phase == GPUMC_PHASE_MEASUREMENT) sim->rec_used += (int)chunk;
+    left -= chunk;
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_observables(gpumc_sim* sim, gpumc_obs* out, size_t cap, size_t* n) {
+  if (!sim || !n) return fail(GPUMC_EINVAL, "sim/n: null");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  RC_TRY(sim->drain_records());
+  const size_t k = std::min(cap, sim->pending.size());
+  if (k && !out) return fail(GPUMC_EINVAL, "out: null");
+  std::copy(sim->pending.begin(), sim->pending.begin() + k, out);
+  sim->pending.erase(sim->pending.begin(), sim->pending.begin() + k);
+  *n = k;
+  return GPUMC_OK;
+}
+
+static size_t host_site_bytes(int model) {
+  return model == GPUMC_O3 ? 12 : model == GPUMC_ISING_MSC64 ? 8 : 1;
+}
+
+int gpumc_get_spins(gpumc_sim* sim, int32_t replica, void* host, size_t nbytes) {
+  if (!sim || !host) return fail(GPUMC_EINVAL, "sim/host: null");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  const Layout& L = sim->lay;
+  const size_t need = host_site_bytes(L.model) * (size_t)L.n_sites;
+  if (nbytes < need) return fail(GPUMC_EINVAL, "nbytes: buffer too small");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  const void* buf = sim->bufs[2 * replica + (sim->sweeps & 1)];
+  const size_t rows = (size_t)L.ly * L.lz;
+  if (L.model == ISING || L.model == POTTS) {
+    CUDA_TRY(cudaMemcpy2D(host, L.lx, buf, L.pitch, L.lx, rows, cudaMemcpyDeviceToHost));
+  } else if (L.model == MSC) {
+    CUDA_TRY(cudaMemcpy2D(host, 8 * (size_t)L.lx, buf, 8 * (size_t)L.pitch, 8 * (size_t)L.lx, rows,
+                          cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> comp((size_t)L.n_sites * 3);
+    for (int c = 0; c < 3; ++c)
+      CUDA_TRY(cudaMemcpy2D(comp.data() + (size_t)c * L.n_sites, 4 * (size_t)L.lx,
+                            (const float*)buf + (size_t)c * L.pitch * rows, 4 * (size_t)L.pitch,
+                            4 * (size_t)L.lx, rows, cudaMemcpyDeviceToHost));
+    float* h = (float*)host;
+    for (int64_t i = 0; i < L.n_sites; ++i)
+      for (int c = 0; c < 3; ++c) h[3 * i + c] = comp[(size_t)c * L.n_sites + i];
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_set_spins(gpumc_sim* sim, int32_t replica, const void* host, size_t nbytes) {
+  if (!sim || !host) return fail(GPUMC_EINVAL, "sim/host: null");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  const Layout& L = sim->lay;
+  const size_t need = host_site_bytes(L.model) * (size_t)L.n_sites;
+  if (nbytes != need) return fail(GPUMC_EINVAL, "nbytes: does not match the lattice");
+  // validate_spin of the reference models (CMC.rs/src/lattice/models.rs)
+  if (L.model == ISING) {
+    const int8_t* v = (const int8_t*)host;
+    for (int64_t i = 0; i < L.n_sites; ++i)
+      if (v[i] != 1 && v[i] != -1) return fail(GPUMC_EINVAL, "spins: Ising spin must be exactly -1 or +1");
+  } else if (L.model == POTTS) {
+    const int8_t* v = (const int8_t*)host;
+    for (int64_t i = 0; i < L.n_sites; ++i)
+      if (v[i] < 0 || v[i] >= sim->spec.q) return fail(GPUMC_EINVAL, "spins: Potts spin must be in [0, q)");
+  } else if (L.model == O3) {
+    const float* v = (const float*)host;
+    for (int64_t i = 0; i < L.n_sites; ++i) {
+      const double n2 = (double)v[3 * i] * v[3 * i] + (double)v[3 * i + 1] * v[3 * i + 1] +
+                        (double)v[3 * i + 2] * v[3 * i + 2];
+      if (!std::isfinite(n2) || std::fabs(n2 - 1.0) > 1e-5)
+        return fail(GPUMC_EINVAL, "spins: O(3) spin must have unit norm (|n^2 - 1| <= 1e-5 in float32)");
+    }
+  }
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  void* buf = sim->bufs[2 * replica + (sim->sweeps & 1)];
+  const size_t rows = (size_t)L.ly * L.lz;
+  if (L.model == ISING || L.model == POTTS) {
+    CUDA_TRY(cudaMemcpy2D(buf, L.pitch, host, L.lx, L.lx, rows, cudaMemcpyHostToDevice));
+  } else if (L.model == MSC) {
+    CUDA_TRY(cudaMemcpy2D(buf, 8 * (size_t)L.pitch, host, 8 * (size_t)L.lx, 8 * (size_t)L.lx, rows,
+                          cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> comp((size_t)L.n_sites * 3);
+    const float* h = (const float*)host;
+    for (int64_t i = 0; i < L.n_sites; ++i)
+      for (int c = 0; c < 3; ++c) comp[(size_t)c * L.n_sites + i] = h[3 * i + c];
+    for (int c = 0; c < 3; ++c)
+      CUDA_TRY(cudaMemcpy2D((float*)buf + (size_t)c * L.pitch * rows, 4 * (size_t)L.pitch,
+                            comp.data() + (size_t)c * L.n_sites, 4 * (size_t)L.lx, 4 * (size_t)L.lx, rows,
+                            cudaMemcpyHostToDevice));
+  }
+  std::vector<double> e;
+  return sim->recompute(e, true);
+}
+
+int gpumc_energy(gpumc_sim* sim, double* energies) {
+  if (!sim || !energies) return fail(GPUMC_EINVAL, "sim/energies: null");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  std::vector<LatDesc> d(sim->n_rep);
+  CUDA_TRY(cudaMemcpy(d.data(), sim->eng->d_lats + sim->lat0, sizeof(LatDesc) * sim->n_rep,
+                      cudaMemcpyDeviceToHost));
+  for (int r = 0; r < sim->n_rep; ++r)
+    energies[r] = sim->lay.model == O3 ? d[r].e_f : sim->spec.J * (double)d[r].e_int;
+  return GPUMC_OK;
+}
+
+int gpumc_recompute_energy(gpumc_sim* sim, double* energies) {
+  if (!sim || !energies) return fail(GPUMC_EINVAL, "sim/energies: null");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  std::vector<double> e;
+  RC_TRY(sim->recompute(e, false));
+  std::copy(e.begin(), e.end(), energies);
+  return GPUMC_OK;
+}
+
+int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* energy64,
+                                  double* mag64) {
+  if (!sim || !energy64 || !mag64) return fail(GPUMC_EINVAL, "null argument");
+  if (sim->lay.model != MSC) return fail(GPUMC_EINVAL, "model: not a multi-spin simulation");
+  if (word_lattice < 0 || word_lattice >= sim->n_rep) return fail(GPUMC_EINVAL, "word_lattice: out of range");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  unsigned long long* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, 8 * 128));
+  CUDA_TRY(cudaMemset(d, 0, 8 * 128));
+  int rc = launch_msc_measure(sim->eng->stream, sim->lay, sim->eng->d_lats, sim->lat0 + word_lattice, d);
+  unsigned long long h[128];
+  cudaError_t e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, sim->eng->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sim->eng->stream);
+  cudaFree(d);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(GPUMC_ECUDA, cudaGetErrorString(e));
+  const double n = (double)sim->lay.n_sites;
+  const double bonds = (double)sim->lay.dims * n;
+  for (int r = 0; r < 64; ++r) {
+    energy64[r] = -sim->spec.J * (bonds - 2.0 * (double)h[64 + r]);
+    mag64[r] = std::fabs(2.0 * (double)h[r] - n) / n;
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_sweep_count(gpumc_sim* sim, uint64_t* out) {
+  if (!sim || !out) return fail(GPUMC_EINVAL, "null argument");
+  *out = sim->sweeps;
+  return GPUMC_OK;
+}
+
+int gpumc_acceptance(gpumc_sim* sim, int32_t replica, double* cone_half_angle) {
+  if (!sim || !cone_half_angle) return fail(GPUMC_EINVAL, "null argument");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  LatDesc d;
+  CUDA_TRY(cudaMemcpy(&d, sim->eng->d_lats + sim->lat0 + replica, sizeof(d), cudaMemcpyDeviceToHost));
+  // omc = 1 - cos(alpha) = 2 sin^2(alpha / 2)
+  *cone_half_angle = 2.0 * std::asin(std::sqrt(std::min(1.0, 0.5 * (double)d.omc)));
+  return GPUMC_OK;
+}
+
+int gpumc_log_weight_ratio(gpumc_sim* sim, int32_t replica, double new_beta, double* out) {
+  if (!sim || !out) return fail(GPUMC_EINVAL, "null argument");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  std::vector<double> e(sim->n_rep);
+  RC_TRY(gpumc_energy(sim, e.data()));
+  std::vector<int32_t> lab(sim->n_rep);
+  CUDA_TRY(cudaMemcpy(lab.data(), sim->d_label, 4 * (size_t)sim->n_rep, cudaMemcpyDeviceToHost));
+  // ClassicalMC::log_weight_ratio: (beta - beta') * E (classical_mc.rs:209-214)
+  *out = (sim->betas[lab[replica]] - new_beta) * e[replica];
+  return GPUMC_OK;
+}
+
+int gpumc_change_parameter(gpumc_sim* sim, int32_t replica, double new_beta) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  if (!std::isfinite(new_beta) || new_beta < 0.0)
+    return fail(GPUMC_EINVAL, "beta: must be finite and non-negative");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  std::vector<int32_t> lab(sim->n_rep);
+  CUDA_TRY(cudaMemcpy(lab.data(), sim->d_label, 4 * (size_t)sim->n_rep, cudaMemcpyDeviceToHost));
+  sim->betas[lab[replica]] = new_beta;
+  RC_TRY(sim->upload_tables());
+  // ClassicalMC::change_parameter recomputes the energy exactly (classical_mc.rs:216-228)
+  std::vector<double> e;
+  return sim->recompute(e, true);
+}
+
+int gpumc_pt_configure(gpumc_sim* sim, uint32_t interval) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (interval > 0 && sim->n_temps != sim->n_rep)
+    return fail(GPUMC_EINVAL, "parallel tempering needs one ladder entry per replica (n_temps = n_replicas)");
+  if (interval > 0 && sim->n_rep > 256) return fail(GPUMC_EINVAL, "parallel tempering: at most 256 replicas");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  sim->pt_interval = interval;
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, pt_interval), (int32_t)interval));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  return GPUMC_OK;
+}
+
+int gpumc_pt_labels(gpumc_sim* sim, int32_t* labels) {
+  if (!sim || !labels) return fail(GPUMC_EINVAL, "null argument");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  CUDA_TRY(cudaMemcpy(labels, sim->d_label, 4 * (size_t)sim->n_rep, cudaMemcpyDeviceToHost));
+  return GPUMC_OK;
+}
+
+int gpumc_pt_stats(gpumc_sim* sim, uint64_t* exchange_steps, uint64_t* accepted_swaps) {
+  if (!sim || !exchange_steps || !accepted_swaps) return fail(GPUMC_EINVAL, "null argument");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  GroupDesc g;
+  CUDA_TRY(cudaMemcpy(&g, sim->eng->d_groups + sim->group, sizeof(g), cudaMemcpyDeviceToHost));
+  *exchange_steps = g.pt_step;
+  *accepted_swaps = g.pt_accepted;
+  return GPUMC_OK;
+}
+
+int gpumc_philox_probe(const uint32_t* ctr4, const uint32_t* key2, uint32_t* out4, int32_t n) {
+  if (!ctr4 || !key2 || !out4 || n <= 0) return fail(GPUMC_EINVAL, "null argument");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(GPUMC_ENODEV, "no usable CUDA device");
+  uint4 *dc = nullptr, *dout = nullptr;
+  uint2* dk = nullptr;
+  CUDA_TRY(cudaMalloc(&dc, 16 * (size_t)n));
+  CUDA_TRY(cudaMalloc(&dk, 8 * (size_t)n));
+  CUDA_TRY(cudaMalloc(&dout, 16 * (size_t)n));
+  CUDA_TRY(cudaMemcpy(dc, ctr4, 16 * (size_t)n, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dk, key2, 8 * (size_t)n, cudaMemcpyHostToDevice));
+  k_philox_probe<<<(n + 255) / 256, 256>>>(dc, dk, dout, n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out4, dout, 16 * (size_t)n, cudaMemcpyDeviceToHost);
+  cudaFree(dc);
+  cudaFree(dk);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail(GPUMC_ECUDA, cudaGetErrorString(e));
+  return GPUMC_OK;
+}

@@ -1,0 +1,101 @@
+"""CPU tests of the host side: the C-ABI library loads and exports every entry
+point include/gpumc.h declares, spec validation follows the reference's
+InvalidConfig rules, and the Python mirror parses the reference's parameter
+keys.  No compute call needs a GPU here."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "gpumc.h")).read()
+    return sorted(set(re.findall(r"^int (gpumc_\w+)\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol(gpumc):
+    lib = gpumc._lib.load()
+    names = _declared()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(gpumc._lib.SIGNATURES), "Python bindings out of sync with the header"
+
+
+def _spec(gpumc, **kw):
+    from scamper_b200.mc import spec_from_params
+    p = {"lattice_type": "square", "Lx": 8, "Ly": 8, "beta": 0.4}
+    p.update(kw)
+    return spec_from_params(p, model=kw.pop("model", None) if "model" in kw else None)
+
+
+@pytest.mark.parametrize("bad", [
+    dict(Lx=7), dict(Ly=2), dict(beta=-0.5), dict(beta=float("inf")), dict(J=float("nan")),
+    dict(pbc="false"), dict(model="potts", q=1), dict(model="potts", q=9),
+])
+def test_validate_rejects_invalid_specs(gpumc, bad):
+    from scamper_b200.mc import spec_from_params
+    p = {"lattice_type": "square", "Lx": 8, "Ly": 8, "beta": 0.4}
+    model = bad.pop("model", None)
+    p.update(bad)
+    spec, keep = spec_from_params(p, model=model)
+    rc = gpumc._lib.load().gpumc_validate(ctypes.byref(spec))
+    assert rc == gpumc._lib.EINVAL
+    assert gpumc._lib.last_error()
+
+
+def test_validate_accepts_reference_configs(gpumc):
+    from scamper_b200.mc import spec_from_params
+    for p, model in [
+        ({"L": 64, "beta": 0.4407}, "ising"),
+        ({"lattice_type": "square", "Lx": 8192, "beta": 0.4407}, "ising"),
+        ({"lattice_type": "cubic", "L": 128, "beta": 0.2}, "ising"),
+        ({"lattice_type": "square", "L": 2048, "q": 4, "beta": 1.1}, "potts"),
+        ({"lattice_type": "cubic", "L": 64, "beta": 0.7, "cone_half_angle": 0.9}, "o3"),
+        ({"lattice_type": "hypercubic", "Lx": 34, "Ly": 10, "Lz": 6, "beta": 0.7}, "o3"),
+    ]:
+        spec, keep = spec_from_params(p, model=model)
+        assert gpumc._lib.load().gpumc_validate(ctypes.byref(spec)) == 0, gpumc._lib.last_error()
+        n = ctypes.c_size_t()
+        assert gpumc._lib.load().gpumc_footprint(ctypes.byref(spec), ctypes.byref(n)) == 0
+        assert n.value > 0
+
+
+def test_footprint_counts_both_ping_pong_buffers(gpumc):
+    from scamper_b200.mc import spec_from_params
+    spec, keep = spec_from_params({"lattice_type": "square", "Lx": 8192, "beta": 0.44}, model="ising",
+                                  record_capacity=1)
+    n = ctypes.c_size_t()
+    gpumc._lib.call("gpumc_footprint", ctypes.byref(spec), ctypes.byref(n))
+    assert 2 * 8192 * 8192 <= n.value < 2 * 8192 * 8192 + (1 << 20)
+
+
+def test_unknown_lattice_and_model_raise(gpumc):
+    from scamper_b200.mc import spec_from_params
+    with pytest.raises(gpumc.InvalidConfig):
+        spec_from_params({"lattice_type": "kagome", "Lx": 8}, model="ising")
+    with pytest.raises(gpumc.InvalidConfig):
+        spec_from_params({"Lx": 8}, model="xy")
+    with pytest.raises(gpumc.InvalidConfig):
+        spec_from_params({"Lx": 8, "initial_state": "lukewarm"}, model="ising")
+
+
+def test_no_device_fails_loudly_without_cpu_fallback(gpumc):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    e = ctypes.c_void_p()
+    rc = gpumc._lib.load().gpumc_engine_create(0, ctypes.byref(e))
+    assert rc == gpumc._lib.ENODEV
+    with pytest.raises(gpumc.GpumcError):
+        gpumc.ClassicalMC.from_params({"Lx": 8, "Ly": 8}, 1)
+
+
+def test_geometric_ladder(gpumc):
+    b = gpumc.geometric_ladder_betas(1.5, 3.5, 64)
+    assert len(b) == 64
+    assert 1 / b[0] == pytest.approx(1.5) and 1 / b[-1] == pytest.approx(3.5)
+    assert all(x > y for x, y in zip(b, b[1:]))

@@ -1,0 +1,289 @@
+"""CPU tests of the oracle: pinned against published known-answer vectors
+and against the reference's own tests (known answers, exact enumeration,
+transfer matrices), before it is trusted as the parity checker."""
+import math
+
+import numpy as np
+import pytest
+
+from tests import exact
+
+
+# ---- Philox4x32-10 published known-answer vectors (Random123 KAT) ----------
+KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+@pytest.mark.parametrize("ctr,key,expect", KAT)
+def test_philox_known_answers(oracle, ctr, key, expect):
+    assert tuple(int(x) for x in oracle.philox(ctr, key)) == expect
+
+
+def test_stream_seed_is_deterministic_and_domain_separated(oracle):
+    # Carlo.rs/src/rng_stream.rs:161-194
+    k = oracle.stream_seed(42, 3, 7, 2, 5, 1, 2, 11)
+    assert k == oracle.stream_seed(42, 3, 7, 2, 5, 1, 2, 11)
+    base = dict(base=123)
+    seeds = {
+        oracle.stream_seed(123),
+        oracle.stream_seed(123, task=1),
+        oracle.stream_seed(123, run=1),
+        oracle.stream_seed(123, chain=1),
+        oracle.stream_seed(123, replica=1),
+        oracle.stream_seed(123, thread=1),
+        oracle.stream_seed(123, phase=2),
+        oracle.stream_seed(123, substream=1),
+    }
+    assert len(seeds) == 8, base
+
+
+def test_threshold_encoding(oracle):
+    assert oracle.threshold(1.0) == (65536, 0)
+    assert oracle.threshold(2.5) == (65536, 0)
+    assert oracle.threshold(0.0) == (0, 0)
+    assert oracle.threshold(float("nan")) == (0, 0)
+    assert oracle.threshold(0.5) == (32768, 0)
+    for p in [math.exp(-4.0), math.exp(-8 * 0.4407), 0.123456789, 1e-30]:
+        h, t = oracle.threshold(p)
+        val = (h * 2.0 ** 64 + t) / 2.0 ** 80
+        assert abs(val - p) <= 2.0 ** -79 + p * 1e-15
+
+
+def test_multispin_lut_matches_reference_values(oracle):
+    # CMC.rs/src/multi_spin.rs:433-441: chain (z = 2), beta = 1, J = 1:
+    # log_acceptance[aligned = 2] = -4, [1] = [0] = 0.  Classes here are
+    # anti-aligned counts k = z - aligned.
+    head, tail = oracle.table(oracle.MSC, 1, 1.0, 1.0)
+    assert len(head) == 3
+    assert head[1] == 65536 and head[2] == 65536
+    p = (int(head[0]) * 2.0 ** 64 + int(tail[0])) / 2.0 ** 80
+    assert abs(math.log(p) + 4.0) < 1e-10
+
+
+def test_single_flip_delta_matches_recompute(oracle):
+    # CMC.rs/tests/physics/lattice_exact.rs:23-97 and usage_exact.rs:26-60:
+    # every single-site change equals the difference of full recomputations.
+    rng = np.random.default_rng(3)
+    for dims, shape in [(2, (6, 4)), (3, (4, 4, 6))]:
+        for model, q in [(oracle.ISING, 2), (oracle.POTTS, 3)]:
+            lat = oracle.Lattice(model, shape, q=q, beta=0.3, seed=5)
+            z = 2 * dims
+            for _ in range(10):
+                s = lat.spins.copy()
+                e0 = lat.energy()
+                site = int(rng.integers(lat.n))
+                # neighbours of the site in the fixed order
+                coords = np.unravel_index(site, tuple(reversed(shape)))[::-1]
+                nbs = []
+                for a in range(dims):
+                    for d in (-1, 1):
+                        c = list(coords)
+                        c[a] = (c[a] + d) % shape[a]
+                        nbs.append(int(np.ravel_multi_index(tuple(reversed(c)), tuple(reversed(shape)))))
+                if model == oracle.ISING:
+                    k = sum(s[nb] != s[site] for nb in nbs)
+                    lat.spins[site] = -s[site]
+                    assert lat.energy() - e0 == pytest.approx(2 * (z - 2 * k))
+                else:
+                    t = (int(s[site]) + 1) % q
+                    d = sum(s[nb] == t for nb in nbs) - sum(s[nb] == s[site] for nb in nbs)
+                    lat.spins[site] = t
+                    assert lat.energy() - e0 == pytest.approx(-d)
+                lat.set_state(s)
+
+
+@pytest.mark.parametrize("model", ["ising", "potts"])
+def test_energy_cache_does_not_drift(oracle, model):
+    # CMC.rs/tests/exact/classic_models.rs:279-311 (cached energy vs exact over
+    # long 3D runs)
+    m = oracle.ISING if model == "ising" else oracle.POTTS
+    lat = oracle.Lattice(m, (6, 6, 6), q=3, beta=0.25, seed=11)
+    for _ in range(1500):
+        lat.sweep()
+    assert lat.cached_energy() == lat.energy()
+
+
+def _chain_moments(lat, therm, meas, nbins=25):
+    for _ in range(therm):
+        lat.sweep()
+    es, ms = [], []
+    for _ in range(meas):
+        lat.sweep()
+        es.append(lat.cached_energy())
+        if lat.model == 0:
+            ms.append((lat.spins.astype(np.float64).sum() / lat.n) ** 2)
+    return es, ms
+
+
+def test_checkerboard_replay_samples_exact_ising_4x4(oracle):
+    """The replay of the engine's method samples the Boltzmann distribution:
+    <E>, <m^2> on the 4x4 torus against exact enumeration (2^16 states),
+    multi-seed z-scores as in CMC.rs/tests/physics/zscore_validation.rs."""
+    beta = 0.4
+    ex = exact.ising_enumeration(4, 4, beta)
+    zs_e, zs_m = [], []
+    for seed in range(1, 9):
+        lat = oracle.Lattice(oracle.ISING, (4, 4), beta=beta, seed=seed)
+        es, ms = _chain_moments(lat, 200, 8000)
+        me, se = exact.binned(es)
+        mm, sm = exact.binned(ms)
+        zs_e.append(exact.zscore(me, se, ex["E"]))
+        zs_m.append(exact.zscore(mm, sm, ex["M2"]))
+    for zs in (zs_e, zs_m):
+        assert max(abs(z) for z in zs) < 4.0
+        assert abs(np.mean(zs)) < 2.0
+        assert sum(zs) > -2.0 * math.sqrt(len(zs))
+
+
+def test_checkerboard_replay_samples_exact_potts_q3(oracle):
+    """q = 3 Potts <E> on a 4x4 torus against the row transfer matrix."""
+    beta = exact.math.log(1.0 + math.sqrt(3.0))
+    ex = exact.potts_transfer_matrix(4, 4, 3, beta)
+    zs = []
+    for seed in range(1, 7):
+        lat = oracle.Lattice(oracle.POTTS, (4, 4), q=3, beta=beta, seed=seed)
+        es, _ = _chain_moments(lat, 200, 8000)
+        me, se = exact.binned(es)
+        zs.append(exact.zscore(me, se, ex["E"]))
+    assert max(abs(z) for z in zs) < 4.0
+    assert abs(np.mean(zs)) < 2.0
+
+
+def test_reference_sampler_samples_exact_ising_4x4(oracle):
+    """The restated reference sampler (random-permutation order, log-space
+    acceptance) against exact enumeration: it is the statistical yardstick."""
+    beta = 0.4
+    ex = exact.ising_enumeration(4, 4, beta)
+    zs = []
+    for seed in range(1, 7):
+        r = oracle.RefSampler(oracle.ISING, (4, 4), beta=beta, seed=seed)
+        r.sweep(200)
+        es = []
+        for _ in range(6000):
+            r.sweep()
+            es.append(r.measure()[0])
+        me, se = exact.binned(es)
+        zs.append(exact.zscore(me, se, ex["E"]))
+        assert r.recompute_energy() == pytest.approx(r.measure()[0], abs=1e-9)
+    assert max(abs(z) for z in zs) < 4.0
+    assert abs(np.mean(zs)) < 2.0
+
+
+def test_multispin_replicas_sample_exact_ising_4x4(oracle):
+    """Each of the 64 bit-replicas of the multi-spin replay samples the 4x4
+    Boltzmann distribution (pooled over replicas, cf.
+    CMC.rs/tests/physics/multispin_cross_solver.rs:86-204)."""
+    beta = 0.4
+    ex = exact.ising_enumeration(4, 4, beta)
+    lat = oracle.Lattice(oracle.MSC, (4, 4), beta=beta, seed=9)
+    for _ in range(200):
+        lat.sweep()
+    rows = []
+    for _ in range(1500):
+        lat.sweep()
+        e, m = lat.msc_observables()
+        rows.append(e)
+    rows = np.array(rows)  # sweeps x 64
+    per_rep = rows.mean(axis=0)
+    pooled = per_rep.mean()
+    se = per_rep.std(ddof=1) / math.sqrt(64)
+    assert abs(exact.zscore(pooled, se, ex["E"])) < 4.0
+
+
+def test_o3_engine_math_accuracy(oracle):
+    lib = oracle.lib()
+    for x in np.linspace(-80.0, 0.0, 2001):
+        v = lib.orc_exp_neg(float(x))
+        assert v == pytest.approx(math.exp(float(np.float32(x))), rel=2e-5, abs=1e-37)
+    c = np.zeros(1, dtype=np.float32)
+    s = np.zeros(1, dtype=np.float32)
+    import ctypes
+    for u in np.linspace(0, 2 ** 32 - 1, 5001).astype(np.uint64):
+        lib.orc_sincos_turn(int(u), c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                            s.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        phi = 2.0 * math.pi * (int(u) >> 5 << 5) / 2.0 ** 32
+        assert abs(c[0] - math.cos(phi)) < 2e-6 and abs(s[0] - math.sin(phi)) < 2e-6
+
+
+def test_o3_replay_keeps_unit_norm_and_energy_cache(oracle):
+    lat = oracle.Lattice(oracle.O3, (6, 6, 6), beta=0.7, seed=4, omc=float(np.float32(1.0 - math.cos(1.0))))
+    for i in range(300):
+        lat.sweep(adapt=i < 100)
+    st = lat.state().astype(np.float64)
+    assert np.abs((st ** 2).sum(axis=1) - 1.0).max() < 1e-5
+    assert lat.cached_energy() == pytest.approx(lat.energy(), rel=1e-9, abs=1e-6)
+
+
+# ---- replica exchange: Carlo.rs/tests/unit/pt_exchange_rule.rs -------------
+def test_accept_log_boundaries(oracle):
+    lib = oracle.lib()
+    for u in [0, 1, 2 ** 63, 2 ** 64 - 1, 12345678901234567]:
+        for d in [0.0, -0.0, np.finfo(float).eps, np.finfo(float).tiny, 1.0, float("inf")]:
+            assert lib.orc_accept_log(d, u) == 1
+        assert lib.orc_accept_log(float("-inf"), u) == 0
+        assert lib.orc_accept_log(float("nan"), u) == 0
+
+
+def test_exchange_rate_matches_exp_delta(oracle):
+    # two chains, equal rate e^delta = 0.3: (b0 - b1)(E0 - E1) = ln 0.3
+    betas = np.array([1.0, 2.0])
+    d = math.log(0.3)
+    energies = np.array([0.0, d])  # (1-2)*(0-d) = d
+    key = oracle.exchange_key(2024)
+    acc = 0
+    n = 100000
+    labels = np.array([0, 1], dtype=np.int32)
+    for step in range(1, 2 * n + 1, 2):  # odd steps pair (0,1)
+        lab, k, _ = oracle.pt_exchange(betas, energies, labels, key, step)
+        acc += k
+    emp = acc / n
+    assert abs(emp - 0.3) <= 5 * math.sqrt(0.3 * 0.7 / n)
+
+
+def test_exchange_keeps_labels_a_permutation_and_pairs_by_parity(oracle):
+    n = 9
+    betas = np.linspace(0.2, 1.0, n)
+    rng = np.random.default_rng(1)
+    labels = np.arange(n, dtype=np.int32)
+    key = oracle.exchange_key(7)
+    for step in range(1, 200):
+        e = rng.normal(size=n) * 5
+        lab, k, acc = oracle.pt_exchange(betas, e, labels, key, step)
+        assert sorted(lab.tolist()) == list(range(n))
+        # only ladder pairs (t, t+1) with t % 2 == (step - 1) % 2 may swap
+        moved = np.nonzero(lab != labels)[0]
+        for r in moved:
+            t_old, t_new = labels[r], lab[r]
+            assert abs(int(t_old) - int(t_new)) == 1
+            assert min(t_old, t_new) % 2 == (step - 1) % 2
+        labels = lab
+
+
+# ---- carlo-rs accumulator (Carlo.rs/tests/unit/accumulator.rs) ------------
+def test_accumulator_matches_reference_unit_tests():
+    from scamper_b200.measurements import Accumulator, binder_cumulant, specific_heat
+    a = Accumulator(10)
+    for i in range(1, 11):
+        a.add(i)
+    assert a.finalize().mean == pytest.approx(5.5)
+    a = Accumulator(5)
+    for i in range(1, 16):
+        a.add(i)
+    e = a.finalize()
+    assert e.mean == pytest.approx(8.0) and e.stderr > 0 and e.n_bins == 3
+    a = Accumulator(10)
+    for i in range(1, 16):
+        a.add(i)
+    assert a.finalize().n_bins == 2
+    assert Accumulator(10).finalize().n_bins == 0
+    a = Accumulator(10)
+    a.add(1.0)
+    e = a.finalize()
+    assert e.n_bins == 1 and e.mean == pytest.approx(1.0)
+    assert binder_cumulant(0.0, 0.0) is None
+    assert binder_cumulant(0.5, 0.25) == pytest.approx(1 - 0.25 / 0.75)
+    assert specific_heat(-1.0, 2.0, 0.5, 4) == pytest.approx(0.25 / 4 * 1.0)
