@@ -178,19 +178,21 @@ Layout plan_layout(const gpumc_spec* s) {
     L.pitch = (lx + 15) / 16 * 16;
     L.buf_bytes = (size_t)L.pitch * rows;
     const int ncol = L.pitch / 16;
+    // a pass maps threads to (row, chunk column) with rstep rows per sweep of
+    // the CTA; tile heights are multiples of rstep minus the 2 halo rows
     if (L.dims == 2) {
       L.tile_cx = ncol <= 64 ? ncol : 32;
-      const int ty_max = std::min(1536 / L.tile_cx - 2, 120);
-      const int ty_target = std::max(8, 16384 / (16 * L.tile_cx));
-      L.tile_y = std::max(1, std::min(std::min(ty_target, ty_max), ly));
+      const int rstep = kThreads / L.tile_cx;
+      const int m = std::max(1, (16384 + 16 * L.tile_cx * rstep - 1) / (16 * L.tile_cx * rstep));
+      L.tile_y = std::max(1, std::min(std::min(m * rstep - 2, 124), ly));
       L.tile_z = 1;
-      L.smem = (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
+      L.smem = 2 * (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
     } else {
       L.tile_cx = ncol <= 16 ? ncol : 16;
-      const int ty_max = std::min(1024 / L.tile_cx - 2, 120);
-      L.tile_y = std::max(1, std::min(ty_max, ly));
+      const int rstep = kThreads / L.tile_cx;
+      L.tile_y = std::max(1, std::min(std::min(2 * rstep - 2, 124), ly));
       L.tile_z = std::min(lz, 32);
-      L.smem = 4 * (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
+      L.smem = 6 * (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
     }
   } else if (L.model == O3) {
     L.pitch = (lx + 3) / 4 * 4;

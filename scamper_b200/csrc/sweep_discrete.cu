@@ -3,14 +3,14 @@
 //
 // Method (one kernel launch = one full sweep of every lattice in the launch):
 //   * each CTA owns a tile of one lattice: tile_cx 16-site chunks x tile_y
-//     rows (x tile_z planes in 3D, marched plane by plane through a 4-slot
-//     shared-memory ring);
-//   * it stages the tile plus a 2-site halo from the read buffer into shared
-//     memory, updates colour 0 on the tile and a 1-site halo ring (halo sites
-//     are recomputed redundantly: the counter-based RNG makes them identical to
-//     the owner's result), then colour 1 on the tile, and writes the tile to
-//     the other ping-pong buffer.  HBM traffic is one read and one write of
-//     every byte per sweep.
+//     rows (x tile_z planes in 3D, marched plane by plane through shared-memory
+//     rings);
+//   * the tile plus a 2-site halo is staged from the read buffer into shared
+//     memory with cp.async; colour 0 is updated on the tile and a 1-site halo
+//     ring into a second shared plane (halo sites are recomputed redundantly:
+//     the counter-based RNG makes them identical to the owner's result), then
+//     colour 1 on the tile straight to the other ping-pong buffer in HBM.  HBM
+//     traffic is one read and one write of every byte per sweep.
 //   * spins are handled 16 at a time (one uint4): neighbour counts come from
 //     SWAR byte arithmetic on 32-bit words, one Philox4x32-10 call supplies the
 //     eight 16-bit acceptance draws of a chunk's eight same-colour sites, and a
@@ -30,7 +30,6 @@
 
 namespace gpumc {
 
-constexpr int kMaxItems = 6;  // chunk items per thread in one colour pass
 constexpr uint32_t kM2 = 0x02020202u;
 
 struct SiteTab {
@@ -38,96 +37,169 @@ struct SiteTab {
   unsigned long long tail[kMaxClasses];
 };
 
-// Per-chunk update of the sites of one colour.  `bp` = byte parity of the
-// colour's sites, `owned` = bitmask of bytes owned by this tile (for the
-// energy accounting), `site0` = linear site index of byte 0.
+// Philox4x32-10 with the per-sweep uniform part hoisted: the counter words
+// 1..3 (colour/tag, sweep) are the same for every draw of a pass, so round 1
+// needs one multiply, and the bumped keys are computed once per CTA.
+struct PhiloxCtx {
+  uint32_t a, b, c;  // round-1 terms: hi(M1*c2) ^ k0, lo(M1*c2), c3 ^ k1
+  uint32_t k0[10], k1[10];
+};
+
+__device__ __forceinline__ PhiloxCtx make_philox(uint64_t key, uint64_t sweep) {
+  PhiloxCtx P;
+  const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+  const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
+  P.a = __umulhi(0xCD9E8D57u, c2) ^ k0;
+  P.b = 0xCD9E8D57u * c2;
+  P.c = c3 ^ k1;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    P.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
+    P.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
+  }
+  return P;
+}
+
+// draw(key, index, colour, tag, 0, sweep) for index < 2^32; ctrl = colour |
+// tag << 1 (counter word 1).
+__device__ __forceinline__ uint4 philox_fast(const PhiloxCtx& P, uint32_t index, uint32_t ctrl) {
+  uint4 c = make_uint4(P.a ^ ctrl, P.b, __umulhi(0xD2511F53u, index) ^ P.c, 0xD2511F53u * index);
+#pragma unroll
+  for (int r = 1; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ P.k0[r], lo1, hi0 ^ c.w ^ P.k1[r], lo0);
+  }
+  return c;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Per-word update of the two sites of the pass colour.  Words are pre-shifted
+// right by `bsh` (0 or 8) so the two sites sit in bytes 0 and 2.
+template <int DIM>
+__device__ __forceinline__ uint32_t ising_word(uint32_t o, uint32_t lw, uint32_t rw, uint32_t u,
+                                               uint32_t d, uint32_t a, uint32_t b, int bsh,
+                                               uint32_t rnd, const SiteTab& tab, uint64_t key,
+                                               uint32_t site0, uint32_t colour, uint64_t sweep,
+                                               uint32_t own2, int& nacc, int& ksum) {
+  uint32_t k2 = ((o ^ lw) & kM2) + ((o ^ rw) & kM2) + ((o ^ u) & kM2) + ((o ^ d) & kM2);
+  if (DIM == 3) k2 += ((o ^ a) & kM2) + ((o ^ b) & kM2);
+  k2 >>= bsh;
+  const uint32_t kA = (k2 >> 1) & 7u, kB = (k2 >> 17) & 7u;
+  const uint32_t thA = tab.head[kA], thB = tab.head[kB];
+  const uint32_t uA = rnd & 0xFFFFu, uB = rnd >> 16;
+  bool aA = uA < thA, aB = uB < thB;
+  if (__builtin_expect((uA == thA) | (uB == thB), 0)) {
+    const uint32_t sA = site0 + (uint32_t)(bsh >> 3), sB = sA + 2u;
+    if (uA == thA) aA = refine_accept(key, sA, colour, sweep, tab.tail[kA]);
+    if (uB == thB) aB = refine_accept(key, sB, colour, sweep, tab.tail[kB]);
+  }
+  // own2: bit 0 / bit 1 = site A / B owned by this tile (energy accounting)
+  const int oA = (int)(aA & (own2 & 1u)), oB = (int)(aB & ((own2 >> 1) & 1u));
+  nacc += oA + oB;
+  ksum += oA * (int)kA + oB * (int)kB;
+  const uint32_t fm = (aA ? 0xFEu : 0u) | (aB ? 0xFE0000u : 0u);
+  return fm << bsh;  // XOR mask
+}
+
+// Potts: returns the new word (sites of the pass colour replaced on accept).
+template <int DIM>
+__device__ __forceinline__ uint32_t potts_word(uint32_t o, uint32_t lw, uint32_t rw, uint32_t u,
+                                               uint32_t d, uint32_t a, uint32_t b, int bsh,
+                                               uint32_t rnd, uint32_t rprop, const SiteTab& tab,
+                                               int q, uint64_t key, uint32_t site0,
+                                               uint32_t colour, uint64_t sweep, uint32_t own2,
+                                               int& nacc, int& dsum) {
+  constexpr int zc = 2 * DIM;
+  const uint32_t os = o >> bsh;
+  const uint32_t sA = os & 0xFFu, sB = (os >> 16) & 0xFFu;
+  const uint32_t n = (uint32_t)(q - 1);
+  const uint32_t rej = 65536u % n;
+  const uint32_t pA = rprop & 0xFFFFu, pB = rprop >> 16;
+  const uint32_t mA = pA * n, mB = pB * n;
+  uint32_t rA = mA >> 16, rB = mB >> 16;
+  const uint32_t siteA = site0 + (uint32_t)(bsh >> 3), siteB = siteA + 2u;
+  if (__builtin_expect(((mA & 0xFFFFu) < rej) | ((mB & 0xFFFFu) < rej), 0)) {
+    if ((mA & 0xFFFFu) < rej) rA = potts_refine(key, siteA, colour, sweep, n);
+    if ((mB & 0xFFFFu) < rej) rB = potts_refine(key, siteB, colour, sweep, n);
+  }
+  const uint32_t tA = rA < sA ? rA : rA + 1u, tB = rB < sB ? rB : rB + 1u;
+  // byte-equality counts of the neighbours against s and t at bytes 0 and 2
+  const uint32_t S = sA | (sB << 16), T = tA | (tB << 16);
+  uint32_t cs = 0, ct = 0;
+  const uint32_t nbw[6] = {lw >> bsh, rw >> bsh, u >> bsh, d >> bsh, a >> bsh, b >> bsh};
+#pragma unroll
+  for (int i = 0; i < zc; ++i) {
+    const uint32_t xs = (nbw[i] ^ S) & 0x00FF00FFu;
+    const uint32_t xt = (nbw[i] ^ T) & 0x00FF00FFu;
+    cs += ((xs + 0x00FF00FFu) >> 8) & 0x00010001u;  // 1 where the byte is nonzero
+    ct += ((xt + 0x00FF00FFu) >> 8) & 0x00010001u;
+  }
+  // counts of equal neighbours = zc - nonzero counts
+  const int nsA = zc - (int)(cs & 0xFFu), nsB = zc - (int)(cs >> 16);
+  const int ntA = zc - (int)(ct & 0xFFu), ntB = zc - (int)(ct >> 16);
+  const int dA = ntA - nsA, dB = ntB - nsB;
+  const uint32_t cA = (uint32_t)(dA + zc), cB = (uint32_t)(dB + zc);
+  const uint32_t thA = tab.head[cA], thB = tab.head[cB];
+  const uint32_t uA = rnd & 0xFFFFu, uB = rnd >> 16;
+  bool aA = uA < thA, aB = uB < thB;
+  if (__builtin_expect((uA == thA) | (uB == thB), 0)) {
+    if (uA == thA) aA = refine_accept(key, siteA, colour, sweep, tab.tail[cA]);
+    if (uB == thB) aB = refine_accept(key, siteB, colour, sweep, tab.tail[cB]);
+  }
+  const int oA = (int)(aA & (own2 & 1u)), oB = (int)(aB & ((own2 >> 1) & 1u));
+  nacc += oA + oB;
+  dsum += oA * dA + oB * dB;
+  uint32_t ns = os;
+  if (aA) ns = (ns & ~0xFFu) | tA;
+  if (aB) ns = (ns & ~0xFF0000u) | (tB << 16);
+  // bytes 1 and 3 of the shifted word are the other colour: untouched
+  const uint32_t keep = bsh ? 0x00FF00FFu : 0xFF00FF00u;
+  return (o & keep) | (ns << bsh);
+}
+
 template <int MODEL, int DIM>
 __device__ __forceinline__ uint4 update_chunk(const uint4 own, const uint4 up, const uint4 dn,
                                               const uint4 zm, const uint4 zp, uint32_t wprev,
-                                              uint32_t wnext, int bp, const uint4 rnd,
+                                              uint32_t wnext, int bsh, const uint4 rnd,
                                               const uint4 rprop, const SiteTab& tab, int q,
-                                              uint64_t key, uint64_t site0, uint32_t colour,
-                                              uint64_t sweep, uint32_t owned, int& dE, int& nacc) {
-  constexpr int zc = 2 * DIM;
+                                              uint64_t key, uint32_t site0, uint32_t colour,
+                                              uint64_t sweep, uint32_t owned16, int& nacc,
+                                              int& acc2) {
   const uint32_t o[4] = {own.x, own.y, own.z, own.w};
-  const uint32_t u[4] = {up.x, up.y, up.z, up.w};
-  const uint32_t d[4] = {dn.x, dn.y, dn.z, dn.w};
-  const uint32_t a[4] = {zm.x, zm.y, zm.z, zm.w};
-  const uint32_t b[4] = {zp.x, zp.y, zp.z, zp.w};
+  const uint32_t uu[4] = {up.x, up.y, up.z, up.w};
+  const uint32_t dd[4] = {dn.x, dn.y, dn.z, dn.w};
+  const uint32_t aa[4] = {zm.x, zm.y, zm.z, zm.w};
+  const uint32_t bb[4] = {zp.x, zp.y, zp.z, zp.w};
   const uint32_t rr[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
   const uint32_t rp[4] = {rprop.x, rprop.y, rprop.z, rprop.w};
+  const int bp = bsh >> 3;
   uint32_t res[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const uint32_t lw = __funnelshift_l(i == 0 ? wprev : o[i - 1], o[i], 8);
     const uint32_t rw = __funnelshift_r(o[i], i == 3 ? wnext : o[i + 1], 8);
-    uint32_t out = o[i];
+    const uint32_t own2 = ((owned16 >> (4 * i + bp)) & 1u) | (((owned16 >> (4 * i + bp + 2)) & 1u) << 1);
     if (MODEL == ISING) {
-      uint32_t k2 = ((o[i] ^ lw) & kM2) + ((o[i] ^ rw) & kM2) + ((o[i] ^ u[i]) & kM2) +
-                    ((o[i] ^ d[i]) & kM2);
-      if (DIM == 3) k2 += ((o[i] ^ a[i]) & kM2) + ((o[i] ^ b[i]) & kM2);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int sb = bp + 2 * j;
-        const int sh = 8 * sb;
-        const int k = (k2 >> (sh + 1)) & 7;
-        const uint32_t uu = j ? (rr[i] >> 16) : (rr[i] & 0xFFFFu);
-        const uint32_t th = tab.head[k];
-        bool acc = uu < th;
-        if (uu == th)
-          acc = refine_accept(key, site0 + 4 * i + sb, colour, sweep, tab.tail[k]);
-        if (acc) {
-          out ^= 0xFEu << sh;
-          if ((owned >> (4 * i + sb)) & 1u) {
-            dE += 2 * (zc - 2 * k);
-            ++nacc;
-          }
-        }
-      }
+      res[i] = o[i] ^ ising_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, rr[i], tab, key,
+                                      site0 + 4u * i, colour, sweep, own2, nacc, acc2);
     } else {
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int sb = bp + 2 * j;
-        const int sh = 8 * sb;
-        const uint32_t s = (o[i] >> sh) & 0xFFu;
-        const uint32_t pu = j ? (rp[i] >> 16) : (rp[i] & 0xFFFFu);
-        const uint32_t n = (uint32_t)(q - 1);
-        const uint32_t m = pu * n;
-        uint32_t r = m >> 16;
-        if ((m & 0xFFFFu) < (65536u % n)) r = potts_refine(key, site0 + 4 * i + sb, colour, sweep, n);
-        const uint32_t t = r < s ? r : r + 1;
-        const uint32_t nb0 = (lw >> sh) & 0xFFu, nb1 = (rw >> sh) & 0xFFu;
-        const uint32_t nb2 = (u[i] >> sh) & 0xFFu, nb3 = (d[i] >> sh) & 0xFFu;
-        int nold = (nb0 == s) + (nb1 == s) + (nb2 == s) + (nb3 == s);
-        int nnew = (nb0 == t) + (nb1 == t) + (nb2 == t) + (nb3 == t);
-        if (DIM == 3) {
-          const uint32_t nb4 = (a[i] >> sh) & 0xFFu, nb5 = (b[i] >> sh) & 0xFFu;
-          nold += (nb4 == s) + (nb5 == s);
-          nnew += (nb4 == t) + (nb5 == t);
-        }
-        const int dd = nnew - nold;
-        const int cls = dd + zc;
-        const uint32_t uu = j ? (rr[i] >> 16) : (rr[i] & 0xFFFFu);
-        const uint32_t th = tab.head[cls];
-        bool acc = uu < th;
-        if (uu == th)
-          acc = refine_accept(key, site0 + 4 * i + sb, colour, sweep, tab.tail[cls]);
-        if (acc) {
-          out = (out & ~(0xFFu << sh)) | (t << sh);
-          if ((owned >> (4 * i + sb)) & 1u) {
-            dE -= dd;
-            ++nacc;
-          }
-        }
-      }
+      res[i] = potts_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, rr[i], rp[i], tab, q,
+                               key, site0 + 4u * i, colour, sweep, own2, nacc, acc2);
     }
-    res[i] = out;
   }
   return make_uint4(res[0], res[1], res[2], res[3]);
 }
 
-// Scalar update of one halo site held in shared memory at `p` (row stride S,
-// plane pointers zmp/zpp for 3D).  The site's draws come from its own chunk.
+// Scalar update of one halo site (positions x0-1 and x0+Wv, whose draws come
+// from chunks the vector pass does not cover), reading plane `src`.
 template <int MODEL, int DIM>
 __device__ __forceinline__ int8_t update_site(const int8_t* p, int S, const int8_t* zmp,
                                               const int8_t* zpp, int xr, int y, int z, int ly,
@@ -179,168 +251,198 @@ __device__ __forceinline__ int8_t update_site(const int8_t* p, int S, const int8
 }
 
 __device__ __forceinline__ uint32_t owned_bytes(int remaining) {
-  // bit b set for bytes b < remaining (remaining = valid bytes in this chunk)
   if (remaining >= 16) return 0xFFFFu;
   if (remaining <= 0) return 0u;
   return (1u << remaining) - 1u;
 }
 
-struct PlaneGeom {
-  int x0, W, S, Wv, ncv, R;  // R = rows held per plane = Hv + 4
+// Tile geometry shared by the passes.  Shared planes hold rows y0-2 ..
+// y0+hv+1; logical x maps to byte x - x0 + 16 of a row of S bytes.
+struct TileGeom {
+  int x0, y0, W, S, Wv, ncv, hv, R;
+  int lx, ly, pitch, pc;
+  // thread mapping of the vector passes: fixed chunk column, rows strided
+  int col, row0, rstep;
+  bool active;
 };
 
-// Stage rows y0-2 .. y0+Hv+1 of plane z into a shared-memory plane buffer.
-__device__ __forceinline__ void load_plane(uint8_t* plane, const int8_t* src, int pitch, int lx,
-                                           int ly, int y0, int z, const PlaneGeom& g) {
-  const int tid = threadIdx.x;
-  for (int i = tid; i < g.R * g.ncv; i += kThreads) {
-    const int r = i / g.ncv, c = i - r * g.ncv;
-    const int y = wrapi(y0 - 2 + r, ly);
-    const size_t off = ((size_t)z * ly + y) * (size_t)pitch + g.x0 + 16 * c;
-    *(uint4*)(plane + r * g.S + 16 + 16 * c) = __ldg((const uint4*)(src + off));
+__device__ __forceinline__ int wrap_row(int y, int ly) {
+  return y < 0 ? y + ly : (y >= ly ? y - ly : y);
+}
+
+// Stage rows y0-2 .. y0+hv+1 of plane z (cp.async, 16 B per chunk) and fetch
+// the wrapped halo bytes into registers (written by stage_halo after the wait).
+__device__ __forceinline__ void stage_plane(uint8_t* plane, const int8_t* src, int z,
+                                            const TileGeom& g) {
+  if (!g.active) return;
+  const size_t zoff = (size_t)z * g.ly;
+  const int c = g.col;
+  for (int r = g.row0; r < g.R; r += g.rstep) {
+    const int y = wrap_row(g.y0 - 2 + r, g.ly);
+    cp_async16(plane + r * g.S + 16 + 16 * c, src + (zoff + y) * (size_t)g.pitch + g.x0 + 16 * c);
   }
 }
-// Write the wrapped x-halo bytes (x0-2, x0-1, x0+Wv, x0+Wv+1) of every row.
-__device__ __forceinline__ void load_plane_halo(uint8_t* plane, const int8_t* src, int pitch,
-                                                int lx, int ly, int y0, int z,
-                                                const PlaneGeom& g) {
-  const int tid = threadIdx.x;
-  for (int i = tid; i < g.R * 4; i += kThreads) {
-    const int r = i >> 2, j = i & 3;
-    const int pos = j < 2 ? g.x0 - 2 + j : g.x0 + g.Wv + (j - 2);
-    const int y = wrapi(y0 - 2 + r, ly);
-    const int xr = wrapi(pos, lx);
-    plane[r * g.S + 16 + (pos - g.x0)] = src[((size_t)z * ly + y) * (size_t)pitch + xr];
+struct HaloBytes {
+  int8_t v[2];
+  int off[2];
+};
+__device__ __forceinline__ HaloBytes fetch_halo(const int8_t* src, int z, const TileGeom& g) {
+  // thread t < 2R handles row t>>1, side t&1 (two bytes each)
+  HaloBytes h;
+  h.off[0] = h.off[1] = -1;
+  const int t = threadIdx.x;
+  if (t < 2 * g.R) {
+    const int r = t >> 1, side = t & 1;
+    const int y = wrap_row(g.y0 - 2 + r, g.ly);
+    const size_t row = ((size_t)z * g.ly + y) * (size_t)g.pitch;
+    const int p0 = side ? g.x0 + g.Wv : g.x0 - 2;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      int xr = p0 + j;
+      xr = xr < 0 ? xr + g.lx : (xr >= g.lx ? xr - g.lx : xr);
+      h.v[j] = src[row + xr];
+      h.off[j] = r * g.S + 16 + (p0 + j - g.x0);
+    }
+  }
+  return h;
+}
+__device__ __forceinline__ void store_halo(uint8_t* plane, const HaloBytes& h) {
+  if (h.off[0] >= 0) {
+    plane[h.off[0]] = (uint8_t)h.v[0];
+    plane[h.off[1]] = (uint8_t)h.v[1];
   }
 }
 
-// Colour-0 pass on rows [1, R-1) of `plane` (tile + 1-row halo), results held
-// in registers, then written back after a barrier; halo columns x0-1 and
-// x0+Wv are recomputed with the scalar path.
+// Colour 0 on rows [1, R-1) of plane A, written to plane B (all bytes of the
+// chunk: colour-1 bytes are copied unchanged).
 template <int MODEL, int DIM>
-__device__ __forceinline__ void black_pass(uint8_t* plane, const uint8_t* pzm, const uint8_t* pzp,
-                                           const PlaneGeom& g, int y0, int z, int ly, int lx,
-                                           int pc, int hv, const SiteTab& tab, int q, uint64_t key,
-                                           uint64_t sweep, bool owned_plane, int& dE, int& nacc) {
-  const int tid = threadIdx.x;
-  const int rows = g.R - 2;
-  const int nitems = rows * g.ncv;
-  uint4 res[kMaxItems];
+__device__ __forceinline__ void black_pass(const uint8_t* A, const uint8_t* Azm, const uint8_t* Azp,
+                                           uint8_t* B, const TileGeom& g, int z, int lz_wrapped_z,
+                                           const SiteTab& tab, int q, uint64_t key, uint64_t sweep,
+                                           const PhiloxCtx& P, bool owned_plane, int& nacc,
+                                           int& acc2) {
+  (void)lz_wrapped_z;
   const uint4 zero4 = make_uint4(0, 0, 0, 0);
-#pragma unroll
-  for (int it = 0; it < kMaxItems; ++it) {
-    const int i = tid + it * kThreads;
-    if (i < nitems) {
-      const int r = 1 + i / g.ncv, c = i - (r - 1) * g.ncv;
-      const uint8_t* p = plane + r * g.S + 16 + 16 * c;
-      const int y = wrapi(y0 - 2 + r, ly);
-      const int x = g.x0 + 16 * c;
+  if (g.active) {
+    const int c = g.col;
+    const uint32_t owned_full = owned_bytes(g.Wv - 16 * c);
+    for (int r = 1 + g.row0; r < g.R - 1; r += g.rstep) {
+      const int off = r * g.S + 16 + 16 * c;
+      const uint8_t* p = A + off;
+      const int y = wrap_row(g.y0 - 2 + r, g.ly);
+      const uint32_t rho = (uint32_t)y + (uint32_t)g.ly * (uint32_t)z;
+      const uint32_t chunk = rho * (uint32_t)g.pc + (uint32_t)((g.x0 >> 4) + c);
       const uint4 own = *(const uint4*)p;
       const uint4 up = *(const uint4*)(p - g.S);
       const uint4 dn = *(const uint4*)(p + g.S);
-      uint4 zmv = zero4, zpv = zero4;
-      if (DIM == 3) {
-        zmv = *(const uint4*)(pzm + (p - plane));
-        zpv = *(const uint4*)(pzp + (p - plane));
-      }
+      const uint4 zmv = DIM == 3 ? *(const uint4*)(Azm + off) : zero4;
+      const uint4 zpv = DIM == 3 ? *(const uint4*)(Azp + off) : zero4;
       const uint32_t wprev = *(const uint32_t*)(p - 4);
       const uint32_t wnext = *(const uint32_t*)(p + 16);
-      const int bp = (y + z) & 1;
-      const uint64_t rho = (uint64_t)y + (uint64_t)ly * (uint64_t)z;
-      const uint64_t chunk = rho * (uint64_t)pc + (uint64_t)(x >> 4);
-      const uint4 rnd = draw(key, chunk, 0, TAG_ACC, 0, sweep);
-      const uint4 rpr = MODEL == POTTS ? draw(key, chunk, 0, TAG_PROP, 0, sweep) : zero4;
-      const bool row_owned = owned_plane && r >= 2 && r < 2 + hv;
-      const uint32_t owned = row_owned ? owned_bytes(g.Wv - 16 * c) : 0u;
-      res[it] = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bp, rnd, rpr, tab, q,
-                                         key, rho * (uint64_t)lx + (uint64_t)x, 0u, sweep, owned,
-                                         dE, nacc);
+      const int bsh = ((y + z) & 1) << 3;
+      const uint4 rnd = philox_fast(P, chunk, 0u | (TAG_ACC << 1));
+      const uint4 rpr = MODEL == POTTS ? philox_fast(P, chunk, 0u | (TAG_PROP << 1)) : zero4;
+      const bool row_owned = owned_plane && r >= 2 && r < 2 + g.hv;
+      const uint32_t owned = row_owned ? owned_full : 0u;
+      *(uint4*)(B + off) = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, rnd,
+                                                    rpr, tab, q, key,
+                                                    rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c),
+                                                    0u, sweep, owned, nacc, acc2);
     }
   }
-  // scalar halo sites: two per row
-  int8_t hval = 0;
-  int hoff = -1;
-  if (tid < rows * 2) {
-    const int r = 1 + (tid >> 1);
-    const int pos = (tid & 1) ? g.x0 + g.Wv : g.x0 - 1;
-    const int y = wrapi(y0 - 2 + r, ly);
-    const int xr = wrapi(pos, lx);
-    const int off = r * g.S + 16 + (pos - g.x0);
-    if (((xr + y + z) & 1) == 0) {
-      hoff = off;
-      hval = update_site<MODEL, DIM>((const int8_t*)plane + off, g.S, (const int8_t*)pzm + off,
-                                     (const int8_t*)pzp + off, xr, y, z, ly, lx, pc, tab, q, key,
-                                     0u, sweep);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int it = 0; it < kMaxItems; ++it) {
-    const int i = tid + it * kThreads;
-    if (i < nitems) {
-      const int r = 1 + i / g.ncv, c = i - (r - 1) * g.ncv;
-      *(uint4*)(plane + r * g.S + 16 + 16 * c) = res[it];
-    }
-  }
-  __syncthreads();
-  if (hoff >= 0) plane[hoff] = (uint8_t)hval;
-  __syncthreads();
 }
 
-// Colour-1 pass on the tile rows, writing the finished chunks to HBM and
-// accumulating the magnetisation / Potts histogram of owned sites.
+// Scalar halo sites of colour 0 (x0-1 and x0+Wv on rows [1, R-1)), A -> B.
 template <int MODEL, int DIM>
-__device__ __forceinline__ void white_pass(const uint8_t* plane, const uint8_t* pzm,
-                                           const uint8_t* pzp, const PlaneGeom& g, int y0, int z,
-                                           int ly, int lx, int pc, int pitch, int hv,
-                                           const SiteTab& tab, int q, uint64_t key, uint64_t sweep,
-                                           int8_t* dst, int& dE, int& nacc, int& mag,
-                                           int* cnt) {
-  const int tid = threadIdx.x;
-  const int nitems = hv * g.ncv;
+__device__ __forceinline__ void black_halo(const uint8_t* A, const uint8_t* Azm, const uint8_t* Azp,
+                                           uint8_t* B, const TileGeom& g, int z,
+                                           const SiteTab& tab, int q, uint64_t key,
+                                           uint64_t sweep) {
+  const int t = threadIdx.x;
+  if (t < 2 * (g.R - 2)) {
+    const int r = 1 + (t >> 1);
+    const int pos = (t & 1) ? g.x0 + g.Wv : g.x0 - 1;
+    const int y = wrap_row(g.y0 - 2 + r, g.ly);
+    const int xr = pos < 0 ? pos + g.lx : (pos >= g.lx ? pos - g.lx : pos);
+    const int off = r * g.S + 16 + (pos - g.x0);
+    if (((xr + y + z) & 1) == 0)
+      B[off] = (uint8_t)update_site<MODEL, DIM>((const int8_t*)A + off, g.S, (const int8_t*)Azm + off,
+                                                (const int8_t*)Azp + off, xr, y, z, g.ly, g.lx, g.pc,
+                                                tab, q, key, 0u, sweep);
+    else
+      B[off] = A[off];
+  }
+}
+
+// Colour 1 on the tile rows of plane B, written to HBM; magnetisation or
+// Potts histogram of the owned (finished) sites.
+template <int MODEL, int DIM>
+__device__ __forceinline__ void white_pass(const uint8_t* B, const uint8_t* Bzm, const uint8_t* Bzp,
+                                           const TileGeom& g, int z, const SiteTab& tab, int q,
+                                           uint64_t key, uint64_t sweep, const PhiloxCtx& P,
+                                           int8_t* dst, int& nacc, int& acc2, int& mag, int* cnt) {
   const uint4 zero4 = make_uint4(0, 0, 0, 0);
-  for (int i = tid; i < nitems; i += kThreads) {
-    const int r = 2 + i / g.ncv, c = i - (r - 2) * g.ncv;
-    const uint8_t* p = plane + r * g.S + 16 + 16 * c;
-    const int y = wrapi(y0 - 2 + r, ly);
-    const int x = g.x0 + 16 * c;
+  if (!g.active) return;
+  const int c = g.col;
+  const uint32_t owned = owned_bytes(g.Wv - 16 * c);
+  for (int r = 2 + g.row0; r < 2 + g.hv; r += g.rstep) {
+    const int off = r * g.S + 16 + 16 * c;
+    const uint8_t* p = B + off;
+    const int y = wrap_row(g.y0 - 2 + r, g.ly);
+    const uint32_t rho = (uint32_t)y + (uint32_t)g.ly * (uint32_t)z;
+    const uint32_t chunk = rho * (uint32_t)g.pc + (uint32_t)((g.x0 >> 4) + c);
     const uint4 own = *(const uint4*)p;
     const uint4 up = *(const uint4*)(p - g.S);
     const uint4 dn = *(const uint4*)(p + g.S);
-    uint4 zmv = zero4, zpv = zero4;
-    if (DIM == 3) {
-      zmv = *(const uint4*)(pzm + (p - plane));
-      zpv = *(const uint4*)(pzp + (p - plane));
-    }
+    const uint4 zmv = DIM == 3 ? *(const uint4*)(Bzm + off) : zero4;
+    const uint4 zpv = DIM == 3 ? *(const uint4*)(Bzp + off) : zero4;
     const uint32_t wprev = *(const uint32_t*)(p - 4);
     const uint32_t wnext = *(const uint32_t*)(p + 16);
-    const int bp = (1 + y + z) & 1;
-    const uint64_t rho = (uint64_t)y + (uint64_t)ly * (uint64_t)z;
-    const uint64_t chunk = rho * (uint64_t)pc + (uint64_t)(x >> 4);
-    const uint4 rnd = draw(key, chunk, 1, TAG_ACC, 0, sweep);
-    const uint4 rpr = MODEL == POTTS ? draw(key, chunk, 1, TAG_PROP, 0, sweep) : zero4;
-    const uint32_t owned = owned_bytes(g.Wv - 16 * c);
-    const uint4 res = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bp, rnd, rpr,
-                                               tab, q, key, rho * (uint64_t)lx + (uint64_t)x, 1u,
-                                               sweep, owned, dE, nacc);
-    *(uint4*)(dst + rho * (uint64_t)pitch + x) = res;
+    const int bsh = ((1 + y + z) & 1) << 3;
+    const uint4 rnd = philox_fast(P, chunk, 1u | (TAG_ACC << 1));
+    const uint4 rpr = MODEL == POTTS ? philox_fast(P, chunk, 1u | (TAG_PROP << 1)) : zero4;
+    const uint4 res = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, rnd, rpr,
+                                               tab, q, key,
+                                               rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c), 1u,
+                                               sweep, owned, nacc, acc2);
+    *(uint4*)(dst + (size_t)rho * (size_t)g.pitch + g.x0 + 16 * c) = res;
     const uint32_t w[4] = {res.x, res.y, res.z, res.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint32_t nib = (owned >> (4 * k)) & 0xFu;
-      const uint32_t bm = (nib & 1u ? 0xFFu : 0u) | (nib & 2u ? 0xFF00u : 0u) |
-                          (nib & 4u ? 0xFF0000u : 0u) | (nib & 8u ? 0xFF000000u : 0u);
+    if (owned == 0xFFFFu) {
       if (MODEL == ISING) {
-        mag = __dp4a((int)(w[k] & bm), 0x01010101, mag);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) mag = __dp4a((int)w[k], 0x01010101, mag);
       } else {
 #pragma unroll
         for (int s = 0; s < kMaxPottsCounts; ++s) {
           if (s < q) {
-            const uint32_t x8 = w[k] ^ (0x01010101u * (uint32_t)s);
-            // bytes equal to s -> 0x80 flag
-            const uint32_t t8 = ((x8 & 0x7F7F7F7Fu) + 0x7F7F7F7Fu);
-            const uint32_t z8 = ~(t8 | x8 | 0x7F7F7F7Fu) & bm;
-            cnt[s] += __popc(z8);
+            const uint32_t pat = 0x01010101u * (uint32_t)s;
+            int n0 = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const uint32_t x8 = w[k] ^ pat;
+              const uint32_t t8 = (x8 & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+              n0 += __popc(~(t8 | x8 | 0x7F7F7F7Fu));
+            }
+            cnt[s] += n0;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t nib = (owned >> (4 * k)) & 0xFu;
+        const uint32_t bm = (nib & 1u ? 0xFFu : 0u) | (nib & 2u ? 0xFF00u : 0u) |
+                            (nib & 4u ? 0xFF0000u : 0u) | (nib & 8u ? 0xFF000000u : 0u);
+        if (MODEL == ISING) {
+          mag = __dp4a((int)(w[k] & bm), 0x01010101, mag);
+        } else {
+#pragma unroll
+          for (int s = 0; s < kMaxPottsCounts; ++s) {
+            if (s < q) {
+              const uint32_t x8 = w[k] ^ (0x01010101u * (uint32_t)s);
+              const uint32_t t8 = (x8 & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+              cnt[s] += __popc(~(t8 | x8 | 0x7F7F7F7Fu) & bm);
+            }
           }
         }
       }
@@ -348,10 +450,13 @@ __device__ __forceinline__ void white_pass(const uint8_t* plane, const uint8_t* 
   }
 }
 
-template <int MODEL>
-__device__ __forceinline__ void flush_accumulators(LatDesc* L, int dE, int nacc, int mag,
+template <int MODEL, int DIM>
+__device__ __forceinline__ void flush_accumulators(LatDesc* L, int nacc, int acc2, int mag,
                                                    const int* cnt, int q) {
-  // warp reduction, then one atomic per warp
+  constexpr int zc = 2 * DIM;
+  // Ising: dE = sum over accepted owned flips of 2(z - 2k) = 2 z n - 4 sum k;
+  // Potts: dE = -sum d.
+  long long dE = MODEL == ISING ? 2LL * zc * nacc - 4LL * acc2 : -(long long)acc2;
   const unsigned full = 0xFFFFFFFFu;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -363,8 +468,10 @@ __device__ __forceinline__ void flush_accumulators(LatDesc* L, int dE, int nacc,
 #pragma unroll
   for (int s = 0; s < kMaxPottsCounts; ++s) {
     c[s] = cnt[s];
+    if (MODEL == POTTS) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c[s] += __shfl_xor_sync(full, c[s], o);
+      for (int o = 16; o > 0; o >>= 1) c[s] += __shfl_xor_sync(full, c[s], o);
+    }
   }
   if ((threadIdx.x & 31) == 0) {
     if (dE) atomic_add_i64(&L->acc.dE, dE);
@@ -386,6 +493,27 @@ __device__ __forceinline__ void load_table(SiteTab& tab, const LatDesc* L, const
   }
 }
 
+__device__ __forceinline__ TileGeom make_geom(const TileItem& t, const LatDesc* L) {
+  TileGeom g;
+  g.x0 = t.x0;
+  g.y0 = t.y0;
+  g.lx = L->lx;
+  g.ly = L->ly;
+  g.pitch = L->pitch;
+  g.pc = L->pitch >> 4;
+  g.W = L->tile_cx * 16;
+  g.S = g.W + 32;
+  g.Wv = min(g.W, g.lx - t.x0);
+  g.ncv = (g.Wv + 15) >> 4;
+  g.hv = min(L->tile_y, g.ly - t.y0);
+  g.R = g.hv + 4;
+  g.rstep = kThreads / g.ncv;
+  g.col = threadIdx.x % g.ncv;
+  g.row0 = threadIdx.x / g.ncv;
+  g.active = g.row0 < g.rstep;
+  return g;
+}
+
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads)
     k_sweep_discrete_2d(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
@@ -395,42 +523,42 @@ __global__ void __launch_bounds__(kThreads)
   const TileItem t = tiles[blockIdx.x];
   LatDesc* L = &lats[t.lat];
   const GroupDesc* G = &groups[L->group];
-  const int lx = L->lx, ly = L->ly, pitch = L->pitch, q = L->q;
-  const uint64_t sweep = L->sweep, key = L->key;
+  const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {  // finished lattice: nothing to do this launch
     launch_epilogue(lats, groups, ctl);
     return;
   }
+  const uint64_t key = L->key;
+  const int q = L->q;
   const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
   int8_t* nxt = (int8_t*)L->buf[(sweep & 1) ^ 1];
+  const TileGeom g = make_geom(t, L);
+  uint8_t* A = smem;
+  uint8_t* B = smem + g.R * g.S;
+  stage_plane(A, cur, 0, g);
+  const HaloBytes hb = fetch_halo(cur, 0, g);
   load_table(tab, L, G);
-  PlaneGeom g;
-  g.x0 = t.x0;
-  g.W = L->tile_cx * 16;
-  g.S = g.W + 32;
-  g.Wv = min(g.W, lx - t.x0);
-  g.ncv = (g.Wv + 15) >> 4;
-  const int hv = min(L->tile_y, ly - t.y0);
-  g.R = hv + 4;
-  const int pc = pitch >> 4;
-  load_plane(smem, cur, pitch, lx, ly, t.y0, 0, g);
+  const PhiloxCtx P = make_philox(key, sweep);
+  cp_async_wait_all();
   __syncthreads();
-  load_plane_halo(smem, cur, pitch, lx, ly, t.y0, 0, g);
+  store_halo(A, hb);
   __syncthreads();
-  int dE = 0, nacc = 0, mag = 0;
+  int nacc = 0, acc2 = 0, mag = 0;
   int cnt[kMaxPottsCounts] = {0, 0, 0, 0, 0, 0, 0, 0};
-  black_pass<MODEL, 2>(smem, smem, smem, g, t.y0, 0, ly, lx, pc, hv, tab, q, key, sweep, true, dE,
-                       nacc);
-  white_pass<MODEL, 2>(smem, smem, smem, g, t.y0, 0, ly, lx, pc, pitch, hv, tab, q, key, sweep,
-                       nxt, dE, nacc, mag, cnt);
-  flush_accumulators<MODEL>(L, dE, nacc, mag, cnt, q);
+  black_pass<MODEL, 2>(A, A, A, B, g, 0, 0, tab, q, key, sweep, P, true, nacc, acc2);
+  __syncthreads();
+  black_halo<MODEL, 2>(A, A, A, B, g, 0, tab, q, key, sweep);
+  __syncthreads();
+  white_pass<MODEL, 2>(B, B, B, g, 0, tab, q, key, sweep, P, nxt, nacc, acc2, mag, cnt);
+  flush_accumulators<MODEL, 2>(L, nacc, acc2, mag, cnt, q);
   launch_epilogue(lats, groups, ctl);
 }
 
 // 3D: the tile is tile_cx chunks x tile_y rows in the xy plane, marched over
-// tile_z planes.  Step s loads plane z0-2+s, updates colour 0 on plane
-// z0-3+s (its z neighbours are the still-old colour-1 planes around it) and
-// colour 1 on plane z0-4+s (whose z neighbours have finished colour 0).
+// tile_z planes.  Step s stages plane z0-2+s into the A ring, updates colour 0
+// of plane z0-3+s (its z neighbours are still-old A planes) into the B ring,
+// and colour 1 of plane z0-4+s from the B ring (its z neighbours have
+// finished colour 0) to HBM.
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads)
     k_sweep_discrete_3d(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
@@ -440,55 +568,56 @@ __global__ void __launch_bounds__(kThreads)
   const TileItem t = tiles[blockIdx.x];
   LatDesc* L = &lats[t.lat];
   const GroupDesc* G = &groups[L->group];
-  const int lx = L->lx, ly = L->ly, lz = L->lz, pitch = L->pitch, q = L->q;
-  const uint64_t sweep = L->sweep, key = L->key;
+  const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {
     launch_epilogue(lats, groups, ctl);
     return;
   }
+  const uint64_t key = L->key;
+  const int q = L->q, lz = L->lz;
   const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
   int8_t* nxt = (int8_t*)L->buf[(sweep & 1) ^ 1];
-  load_table(tab, L, G);
-  PlaneGeom g;
-  g.x0 = t.x0;
-  g.W = L->tile_cx * 16;
-  g.S = g.W + 32;
-  g.Wv = min(g.W, lx - t.x0);
-  g.ncv = (g.Wv + 15) >> 4;
-  const int hv = min(L->tile_y, ly - t.y0);
+  const TileGeom g = make_geom(t, L);
   const int dv = min(L->tile_z, lz - t.z0);
-  g.R = hv + 4;
-  const int plane_bytes = g.R * g.S;
-  const int pc = pitch >> 4;
-  int dE = 0, nacc = 0, mag = 0;
+  const int pb = g.R * g.S;  // bytes per plane
+  uint8_t* Aring = smem;          // 3 planes
+  uint8_t* Bring = smem + 3 * pb; // 3 planes
+  load_table(tab, L, G);
+  const PhiloxCtx P = make_philox(key, sweep);
+  int nacc = 0, acc2 = 0, mag = 0;
   int cnt[kMaxPottsCounts] = {0, 0, 0, 0, 0, 0, 0, 0};
+  auto slot = [](int v) { return ((v % 3) + 3) % 3; };
   for (int s = 0; s < dv + 4; ++s) {
     const int zl = t.z0 - 2 + s;
-    uint8_t* pl = smem + (s & 3) * plane_bytes;
-    load_plane(pl, cur, pitch, lx, ly, t.y0, wrapi(zl, lz), g);
+    const int zlw = zl < 0 ? zl + lz : (zl >= lz ? zl - lz : zl);
+    uint8_t* Al = Aring + slot(s) * pb;
+    stage_plane(Al, cur, zlw, g);
+    const HaloBytes hb = fetch_halo(cur, zlw, g);
+    cp_async_wait_all();
     __syncthreads();
-    load_plane_halo(pl, cur, pitch, lx, ly, t.y0, wrapi(zl, lz), g);
+    store_halo(Al, hb);
     __syncthreads();
     if (s >= 2) {
       const int zb = zl - 1;
-      uint8_t* pb = smem + ((s - 1) & 3) * plane_bytes;
-      const uint8_t* pm = smem + ((s - 2) & 3) * plane_bytes;
-      const uint8_t* pp = pl;
+      const int zbw = zb < 0 ? zb + lz : (zb >= lz ? zb - lz : zb);
+      const uint8_t* Ab = Aring + slot(s - 1) * pb;
+      const uint8_t* Am = Aring + slot(s - 2) * pb;
+      uint8_t* Bb = Bring + slot(s - 1) * pb;
       const bool owned_plane = zb >= t.z0 && zb < t.z0 + dv;
-      black_pass<MODEL, 3>(pb, pm, pp, g, t.y0, wrapi(zb, lz), ly, lx, pc, hv, tab, q, key, sweep,
-                           owned_plane, dE, nacc);
+      black_pass<MODEL, 3>(Ab, Am, Al, Bb, g, zbw, 0, tab, q, key, sweep, P, owned_plane, nacc, acc2);
+      __syncthreads();
+      black_halo<MODEL, 3>(Ab, Am, Al, Bb, g, zbw, tab, q, key, sweep);
+      __syncthreads();
     }
     if (s >= 4) {
       const int zw = zl - 2;
-      const uint8_t* pw = smem + ((s - 2) & 3) * plane_bytes;
-      const uint8_t* pm = smem + ((s - 3) & 3) * plane_bytes;
-      const uint8_t* pp = smem + ((s - 1) & 3) * plane_bytes;
-      white_pass<MODEL, 3>(pw, pm, pp, g, t.y0, wrapi(zw, lz), ly, lx, pc, pitch, hv, tab, q, key,
-                           sweep, nxt, dE, nacc, mag, cnt);
+      const int zww = zw < 0 ? zw + lz : (zw >= lz ? zw - lz : zw);
+      white_pass<MODEL, 3>(Bring + slot(s - 2) * pb, Bring + slot(s - 3) * pb, Bring + slot(s - 1) * pb,
+                           g, zww, tab, q, key, sweep, P, nxt, nacc, acc2, mag, cnt);
     }
-    __syncthreads();  // the next load overwrites the slot read by this white pass
+    __syncthreads();  // the next stage overwrites A and B slots read in this step
   }
-  flush_accumulators<MODEL>(L, dE, nacc, mag, cnt, q);
+  flush_accumulators<MODEL, 3>(L, nacc, acc2, mag, cnt, q);
   launch_epilogue(lats, groups, ctl);
 }
 
