@@ -197,6 +197,30 @@ int gpumc_philox_probe(const uint32_t* ctr4, const uint32_t* key2, uint32_t* out
  * records): the admission footprint. */
 int gpumc_footprint(const gpumc_spec* spec, size_t* bytes);
 
+/* ---- allocation-free exact energy ---------------------------------------
+ * No counterpart in the reference: an engine-specific entry point for callers
+ * that must not allocate device memory (their memory belongs to another
+ * allocator under a fixed budget, or they cannot absorb the device-wide
+ * synchronization of cudaFree).  Computes what gpumc_recompute_energy computes
+ * - the exact energy in units of J (physical energy = J * value) of int8 Ising
+ * (+-1) or Potts (0..q-1) lattices on periodic square / cubic lattices - but
+ * allocates nothing: no cudaMalloc, cudaFree or allocating library call.
+ *   spins      device pointer: n_lattices lattices back to back, each in the
+ *              reference's site order (x fastest, no padding)
+ *   energy_out device pointer: n_lattices int64 results
+ *   stream     cudaStream_t to run on (NULL = default stream); the call is
+ *              asynchronous with respect to the host
+ * Limits: 1 <= n_lattices <= 64, at most 4e9 sites per lattice; larger
+ * requests return GPUMC_EINVAL.  Its reduction scratch is one file-scope
+ * device array of 128 KiB (64 lattices x 256 partial sums) that every GPU
+ * which loads the library holds until exit.  The first call on a device looks
+ * up that array's device address; make it before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU (different
+ * streams without ordering between them) race and must not be issued. */
+int gpumc_energy_int8_noalloc(int32_t model, int32_t dims, int64_t lx, int64_t ly, int64_t lz,
+                              const int8_t* spins, int32_t n_lattices, long long* energy_out,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -124,6 +124,8 @@ SIGNATURES = {
     "gpumc_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "gpumc_philox_probe": [_P(ctypes.c_uint32), _P(ctypes.c_uint32), _P(ctypes.c_uint32), ctypes.c_int32],
     "gpumc_footprint": [_P(Spec), _P(ctypes.c_size_t)],
+    "gpumc_energy_int8_noalloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                  ctypes.c_int64, _vp, ctypes.c_int32, _vp, _vp],
 }
 
 
