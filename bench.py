@@ -89,7 +89,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -357,7 +357,8 @@ def bench_serving(gpumc, torch, args):
                 lt = "cubic"
             L = max(4, L + (L & 1))
             T = rng.uniform(0.6, 1.4) * tc[kind]
-            sweeps = int(round(math.exp(rng.uniform(math.log(100), math.log(10000)))))
+            sweeps = int(round(math.exp(rng.uniform(math.log(100), math.log(10000)))) * args.serve_sweep_scale)
+            sweeps = max(1, sweeps)
             model = {"ising2": "ising", "potts2": "potts", "ising3": "ising", "o33": "o3"}[kind]
             p = {"lattice_type": lt, "L": L, "beta": 1.0 / T, "q": 3}
             att = float(L ** (2 if lt == "square" else 3)) * sweeps
@@ -383,7 +384,8 @@ def bench_serving(gpumc, torch, args):
         srv.close()
         lat = np.array([r["finish_s"] - r["submit_s"] for r in done.values()])
         total_att = sum(a for _, a in ids.values())
-        out.append({"lambda_per_s": lam, "jobs": len(jobs), "p50_s": float(np.percentile(lat, 50)),
+        out.append({"lambda_per_s": lam, "jobs": len(jobs), "sweep_scale": args.serve_sweep_scale,
+                    "p50_s": float(np.percentile(lat, 50)),
                     "p99_s": float(np.percentile(lat, 99)), "wall_s": wall,
                     "attempts_per_ns": total_att / (wall * 1e9),
                     "busy_attempts_per_ns": st["attempts"] / (st["busy_s"] * 1e9)})
@@ -454,8 +456,9 @@ def main():
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only-headline", action="store_true")
-    ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 100.0, 1000.0])
-    ap.add_argument("--serve-jobs", type=int, default=200)
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[30.0, 300.0])
+    ap.add_argument("--serve-jobs", type=int, default=16)
+    ap.add_argument("--serve-sweep-scale", type=float, default=0.01)
     ap.add_argument("--serve-chunk", type=int, default=20)
     ap.add_argument("--serve-budget-gb", type=float, default=64.0)
     args = ap.parse_args()
@@ -475,7 +478,7 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     alg_bytes_launch = BYTES_PER_ATTEMPT["int8"] * h["attempts_rank"] / args.steps
     achieved = alg_bytes_launch / (per_launch_ms * 1e6)  # GB/s
-    traffic = profiled_traffic().get("k_sweep_discrete_2d<ISING> L=8192 x3")
+    traffic = profiled_traffic().get("k_sweep_ising_bits<2> 2D Ising L=8192 x3")
     workloads = {}
     if rank == 0 and not args.only_headline:
         for name, fn in [("msc", bench_msc), ("pt", bench_pt), ("mixed", bench_mixed),
@@ -501,7 +504,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes_launch,
-                     "kernel": "k_sweep_discrete_2d<ISING>"},
+                     "kernel": "k_sweep_ising_bits<2>"},
         "clocks": h["clocks"], "gpu_launches": h["launches"], "e2e": h["e2e"],
         "energy_cache_audit": h["audit_ok"], "workloads": workloads,
     }

@@ -187,6 +187,27 @@ static int accept_discrete(uint32_t u16, uint32_t head, uint64_t tail, uint64_t 
     return r < tail;
 }
 
+/* Ising decision on bit planes of the site's 64-site row segment */
+static int accept_bits(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t head,
+                       uint64_t tail, uint32_t colour, const uint32_t key[2], uint64_t sweep) {
+    if (head >= 65536u) return 1;
+    int64_t ps = (g->lx + 63) / 64;
+    uint64_t seg = (uint64_t)((y + g->ly * z) * ps + (x >> 6));
+    int bit = (int)((x & 63) >> 1);
+    uint32_t out[4];
+    for (int j = 0; j < 80; ++j) {
+        if ((j & 3) == 0) {
+            uint32_t ctr[4];
+            make_ctr(ctr, seg, colour, ORC_TAG_BITS, (uint32_t)(j >> 2), sweep);
+            orc_philox4x32_10(ctr, key, out);
+        }
+        int ub = (int)((out[j & 3] >> bit) & 1u);
+        int tb = j < 16 ? (int)((head >> (15 - j)) & 1u) : (int)((tail >> (79 - j)) & 1u);
+        if (ub != tb) return ub < tb;
+    }
+    return 0;
+}
+
 /* uniform r in [0, n) for the Potts proposal, Lemire multiply-shift with
  * exact rejection (16-bit first draw, 32-bit retries from a refine batch) */
 static uint32_t potts_draw(uint32_t u16, uint32_t n, uint64_t site, uint32_t colour,
@@ -248,17 +269,16 @@ int64_t orc_sweep_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t 
                     int64_t nb[6];
                     int nn = neighbours(&g, x, y, z, nb);
                     int8_t s = spins[site];
-                    uint32_t u = chunk_u16(&g, x, y, z, colour, ORC_TAG_ACC, key, sweep);
                     if (model == ORC_ISING) {
                         int k = 0;
                         for (int i = 0; i < nn; ++i) k += spins[nb[i]] != s;
-                        if (accept_discrete(u, head[k], tail[k], (uint64_t)site, colour, key,
-                                            sweep)) {
+                        if (accept_bits(&g, x, y, z, head[k], tail[k], colour, key, sweep)) {
                             spins[site] = (int8_t)-s;
                             dE += 2 * (zc - 2 * k);
                             ++acc;
                         }
                     } else {
+                        uint32_t u = chunk_u16(&g, x, y, z, colour, ORC_TAG_ACC, key, sweep);
                         uint32_t pu = chunk_u16(&g, x, y, z, colour, ORC_TAG_PROP, key, sweep);
                         uint32_t r = potts_draw(pu, (uint32_t)(q - 1), (uint64_t)site, colour, key,
                                                 sweep);

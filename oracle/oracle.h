@@ -38,7 +38,8 @@ enum {
     ORC_TAG_INIT = 4,       /* hot initial state                            */
     ORC_TAG_O3 = 5,         /* O(3): cos-theta, phi, acceptance             */
     ORC_TAG_MSC = 6,        /* multi-spin bit planes (plane pair in bits 8+) */
-    ORC_TAG_PT = 7          /* replica exchange decisions                   */
+    ORC_TAG_PT = 7,         /* replica exchange decisions                   */
+    ORC_TAG_BITS = 8        /* Ising bit planes of a 64-site row segment    */
 };
 
 /* Substream ids used with RngStreamKey::with_substream. */
@@ -65,7 +66,14 @@ void orc_threshold(double p, uint32_t* head, uint64_t* tail);
  * d = n(new) - n(old) in -z..z, dE = -J d.  Returns number of classes. */
 int orc_build_table(int model, int dims, double J, double beta, uint32_t* head, uint64_t* tail);
 
-/* --- checkerboard replay: int8 Ising / Potts ----------------------------- */
+/* --- checkerboard replay: int8 Ising / Potts -----------------------------
+ * Ising decisions use bit planes: a row is cut into 64-site segments
+ * (segment id g = rho * ceil(Lx/64) + x/64, rho = y + Ly*z); the 32 sites of
+ * one colour in a segment are numbered i = (x & 63) >> 1; plane j (0 = most
+ * significant) is word j & 3 of Philox(g, colour | TAG_BITS << 1 |
+ * (j >> 2) << 8, sweep), and its bit i is bit j of site i's uniform u.  A site
+ * flips iff u < T[k] compared most-significant bit first over 80 planes.
+ * Potts decisions use the 16-bit chunk draws (TAG_ACC / TAG_PROP). */
 void orc_init_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
                        uint64_t base_seed, uint64_t replica, int hot, int8_t* spins);
 /* One full sweep (colour 0 then colour 1).  Returns the integer energy change
@@ -121,7 +129,8 @@ void orc_ref_set_beta(orc_ref* r, double beta);
 int64_t orc_ref_n_sites(const orc_ref* r);
 /* Run n chains on up to n_threads threads (one chain per thread, like the
  * reference's Rayon task backend): therm + meas sweeps each, measuring every
- * measured sweep.  Returns wall seconds; attempts written to *attempts. */
+ * measured sweep.  Returns the sweep seconds of the slowest thread (lattice
+ * construction excluded); attempts written to *attempts. */
 double orc_ref_run_parallel(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
                             double J, double beta, uint64_t base_seed, int n_chains, int n_threads,
                             int therm, int meas, double* attempts, double* mean_e, double* mean_m);

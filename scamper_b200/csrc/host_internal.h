@@ -28,6 +28,7 @@ void build_table(int model, int dims, double J, double beta, uint32_t* head,
                  unsigned long long* tail);
 int validate_spec(const gpumc_spec* s);
 Layout plan_layout(const gpumc_spec* s);
+bool layout_ok(const Layout& L);
 void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out);
 int kernel_kind(int model, int dims);
 size_t footprint_bytes(const gpumc_spec* s);

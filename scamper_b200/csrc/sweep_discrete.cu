@@ -1,5 +1,6 @@
-// Fused two-colour checkerboard sweep for int8 Ising and q-state Potts spins
-// on periodic square (2D) and cubic (3D) lattices.
+// Fused two-colour checkerboard sweep for int8 q-state Potts spins on
+// periodic square (2D) and cubic (3D) lattices (int8 Ising runs on the
+// bit-sliced kernel of sweep_ising_bits.cu).
 //
 // Method (one kernel launch = one full sweep of every lattice in the launch):
 //   * each CTA owns a tile of one lattice: tile_cx 16-site chunks x tile_y
@@ -83,32 +84,6 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 // Per-word update of the two sites of the pass colour.  Words are pre-shifted
 // right by `bsh` (0 or 8) so the two sites sit in bytes 0 and 2.
-template <int DIM>
-__device__ __forceinline__ uint32_t ising_word(uint32_t o, uint32_t lw, uint32_t rw, uint32_t u,
-                                               uint32_t d, uint32_t a, uint32_t b, int bsh,
-                                               uint32_t rnd, const SiteTab& tab, uint64_t key,
-                                               uint32_t site0, uint32_t colour, uint64_t sweep,
-                                               uint32_t own2, int& nacc, int& ksum) {
-  uint32_t k2 = ((o ^ lw) & kM2) + ((o ^ rw) & kM2) + ((o ^ u) & kM2) + ((o ^ d) & kM2);
-  if (DIM == 3) k2 += ((o ^ a) & kM2) + ((o ^ b) & kM2);
-  k2 >>= bsh;
-  const uint32_t kA = (k2 >> 1) & 7u, kB = (k2 >> 17) & 7u;
-  const uint32_t thA = tab.head[kA], thB = tab.head[kB];
-  const uint32_t uA = rnd & 0xFFFFu, uB = rnd >> 16;
-  bool aA = uA < thA, aB = uB < thB;
-  if (__builtin_expect((uA == thA) | (uB == thB), 0)) {
-    const uint32_t sA = site0 + (uint32_t)(bsh >> 3), sB = sA + 2u;
-    if (uA == thA) aA = refine_accept(key, sA, colour, sweep, tab.tail[kA]);
-    if (uB == thB) aB = refine_accept(key, sB, colour, sweep, tab.tail[kB]);
-  }
-  // own2: bit 0 / bit 1 = site A / B owned by this tile (energy accounting)
-  const int oA = (int)(aA & (own2 & 1u)), oB = (int)(aB & ((own2 >> 1) & 1u));
-  nacc += oA + oB;
-  ksum += oA * (int)kA + oB * (int)kB;
-  const uint32_t fm = (aA ? 0xFEu : 0u) | (aB ? 0xFE0000u : 0u);
-  return fm << bsh;  // XOR mask
-}
-
 // Potts: returns the new word (sites of the pass colour replaced on accept).
 template <int DIM>
 __device__ __forceinline__ uint32_t potts_word(uint32_t o, uint32_t lw, uint32_t rw, uint32_t u,
@@ -187,13 +162,8 @@ __device__ __forceinline__ uint4 update_chunk(const uint4 own, const uint4 up, c
     const uint32_t lw = __funnelshift_l(i == 0 ? wprev : o[i - 1], o[i], 8);
     const uint32_t rw = __funnelshift_r(o[i], i == 3 ? wnext : o[i + 1], 8);
     const uint32_t own2 = ((owned16 >> (4 * i + bp)) & 1u) | (((owned16 >> (4 * i + bp + 2)) & 1u) << 1);
-    if (MODEL == ISING) {
-      res[i] = o[i] ^ ising_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, rr[i], tab, key,
-                                      site0 + 4u * i, colour, sweep, own2, nacc, acc2);
-    } else {
-      res[i] = potts_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, rr[i], rp[i], tab, q,
-                               key, site0 + 4u * i, colour, sweep, own2, nacc, acc2);
-    }
+    res[i] = potts_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, rr[i], rp[i], tab, q, key,
+                             site0 + 4u * i, colour, sweep, own2, nacc, acc2);
   }
   return make_uint4(res[0], res[1], res[2], res[3]);
 }
@@ -621,9 +591,7 @@ __global__ void __launch_bounds__(kThreads)
   launch_epilogue(lats, groups, ctl);
 }
 
-template __global__ void k_sweep_discrete_2d<ISING>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_discrete_2d<POTTS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_discrete_3d<ISING>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_discrete_3d<POTTS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 
 }  // namespace gpumc

@@ -1,0 +1,408 @@
+// Bit-sliced fused checkerboard sweep for int8 Ising spins on periodic square
+// (2D) and cubic (3D) lattices.
+//
+// The int8 lattice is read and written once per sweep (2 B of HBM traffic per
+// attempt), but the update runs on bits: each 64-site row segment is packed
+// into two 32-bit masks, E (even x) and O (odd x), bit = 1 for spin -1.  In a
+// row the two colours of the checkerboard are exactly the two x parities, so
+// a colour pass updates one 32-bit mask per segment:
+//   * neighbour spins are shifts of the other-parity mask of the same row and
+//     the same-parity masks of the rows above/below (and planes in 3D), so the
+//     anti-aligned count of all 32 sites comes from a bit-sliced adder;
+//   * the 32 Metropolis decisions u_i < T[k_i] (T = 80-bit fixed point of
+//     exp(-beta dE), from the host table) are made together by a bit-serial
+//     comparator over Philox bit planes, most significant plane first; the
+//     warp stops drawing planes once every lane's sites are decided.
+// A colour pass reads only the other colour's masks and writes only its own,
+// so both passes update the shared tile in place without races.
+//
+// Random stream (also restated by the oracle): plane j of segment g = rho *
+// ceil(Lx/64) + x/64 (rho = y + Ly z), colour c, is word j & 3 of
+// Philox4x32-10(key, ctr = (g, c | TAG_BITS << 1 | (j >> 2) << 8, sweep));
+// bit i of a plane belongs to the colour site (x & 63) >> 1 = i.
+//
+// Reference semantics: Ising dE = 2J(z - 2k) (CMC.rs/src/lattice/
+// interaction.rs:73-84), acceptance min(1, exp(-beta dE))
+// (Carlo.rs/src/acceptance.rs:11-22), energy cache += dE
+// (CMC.rs/src/lattice/state.rs:127-136), |M| observable
+// (CMC.rs/src/lattice/models.rs:103-110).
+#include "device_common.cuh"
+#include "epilogue.cuh"
+
+namespace gpumc {
+
+// Acceptance table of the pass in the form the comparator uses.  For Ising
+// the classes with p < 1 are those with dE > 0: at most z/2 of them, so the
+// comparator handles up to three "pending" classes; every other class is
+// accepted outright.
+struct BitsTab {
+  int npend;                  // pending classes (0..3)
+  uint32_t pend_neg[3][3];    // pend_neg[i][b] = ~0 if bit b of class pc[i] is 0
+  uint32_t tsel[80][3];       // tsel[j][i] = ~0 if bit j (MSB first) of T[pc[i]] is 1
+};
+
+struct BitsPhilox {
+  uint32_t a, b, c;
+  uint32_t k0[10], k1[10];
+};
+
+__device__ __forceinline__ BitsPhilox make_bits_philox(uint64_t key, uint64_t sweep) {
+  BitsPhilox P;
+  const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+  const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
+  P.a = __umulhi(0xCD9E8D57u, c2) ^ k0;
+  P.b = 0xCD9E8D57u * c2;
+  P.c = c3 ^ k1;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    P.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
+    P.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
+  }
+  return P;
+}
+
+// Philox4x32-10 of counter (index, ctrl, sweep_lo, sweep_hi) with the
+// sweep-uniform part of round 1 precomputed.
+__device__ __forceinline__ uint4 bits_philox(const BitsPhilox& P, uint32_t index, uint32_t ctrl) {
+  uint4 c = make_uint4(P.a ^ ctrl, P.b, __umulhi(0xD2511F53u, index) ^ P.c, 0xD2511F53u * index);
+#pragma unroll
+  for (int r = 1; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ P.k0[r], lo1, hi0 ^ c.w ^ P.k1[r], lo0);
+  }
+  return c;
+}
+
+// 64 int8 spins (x order) -> parity masks (bit set for spin -1).
+__device__ __forceinline__ uint2 pack_segment(const uint4 v0, const uint4 v1, const uint4 v2,
+                                              const uint4 v3) {
+  const uint32_t w[16] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w,
+                          v2.x, v2.y, v2.z, v2.w, v3.x, v3.y, v3.z, v3.w};
+  uint32_t E = 0, O = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t ev = __byte_perm(w[2 * k], w[2 * k + 1], 0x6420);
+    const uint32_t od = __byte_perm(w[2 * k], w[2 * k + 1], 0x7531);
+    // sign bits of the four bytes gathered into bits 28..31 by one multiply
+    E |= (((ev & 0x80808080u) * 0x00204081u) >> (28 - 4 * k)) & (0xFu << (4 * k));
+    O |= (((od & 0x80808080u) * 0x00204081u) >> (28 - 4 * k)) & (0xFu << (4 * k));
+  }
+  return make_uint2(E, O);
+}
+
+// Parity masks -> 64 int8 spins (+1 = 0x01, -1 = 0xFF).
+__device__ __forceinline__ void unpack_segment(uint32_t E, uint32_t O, uint4& v0, uint4& v1,
+                                               uint4& v2, uint4& v3) {
+  uint32_t w[16];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t e4 = (E >> (4 * k)) & 0xFu, o4 = (O >> (4 * k)) & 0xFu;
+    const uint32_t es = 0x01010101u ^ (((e4 * 0x00204081u) & 0x01010101u) * 0xFEu);
+    const uint32_t os = 0x01010101u ^ (((o4 * 0x00204081u) & 0x01010101u) * 0xFEu);
+    w[2 * k] = __byte_perm(es, os, 0x5140);
+    w[2 * k + 1] = __byte_perm(es, os, 0x7362);
+  }
+  v0 = make_uint4(w[0], w[1], w[2], w[3]);
+  v1 = make_uint4(w[4], w[5], w[6], w[7]);
+  v2 = make_uint4(w[8], w[9], w[10], w[11]);
+  v3 = make_uint4(w[12], w[13], w[14], w[15]);
+}
+
+// Tile geometry: shared plane of R rows x NC columns of uint2 {E, O};
+// column cc holds segment s0 + cc - xh (wrapped).
+struct BitsGeom {
+  int lx, ly, pitch, nseg;      // nseg = segments per row (pitch = 64 nseg)
+  int s0, ns, xh, NC;           // first segment, owned segments, halo columns
+  int y0, hv, R;                // rows y0-2 .. y0+hv+1
+  int hlast;                    // valid site pairs of the last segment of a row
+  int col, row0, rstep, iters_load, iters_black, iters_white;
+};
+
+__device__ __forceinline__ int wrap_i(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+__device__ __forceinline__ BitsGeom make_bits_geom(const TileItem& t, const LatDesc* L) {
+  BitsGeom g;
+  g.lx = L->lx;
+  g.ly = L->ly;
+  g.pitch = L->pitch;
+  g.nseg = L->pitch >> 6;
+  g.s0 = t.x0 >> 6;
+  g.ns = min(L->tile_cx, g.nseg - g.s0);
+  g.xh = g.ns < g.nseg ? 1 : 0;
+  g.NC = g.ns + 2 * g.xh;
+  g.y0 = t.y0;
+  g.hv = min(L->tile_y, g.ly - t.y0);
+  g.R = g.hv + 4;
+  g.hlast = (g.lx - 64 * (g.nseg - 1)) >> 1;
+  g.rstep = kThreads / g.NC;
+  g.col = threadIdx.x % g.NC;
+  g.row0 = threadIdx.x / g.NC;
+  g.iters_load = (g.R + g.rstep - 1) / g.rstep;
+  g.iters_black = (g.R - 2 + g.rstep - 1) / g.rstep;
+  g.iters_white = (g.hv + g.rstep - 1) / g.rstep;
+  return g;
+}
+
+// Stage rows y0-2 .. y0+hv+1 of plane z into a shared mask plane.
+__device__ __forceinline__ void load_bits_plane(uint2* pl, const int8_t* src, int z,
+                                                const BitsGeom& g) {
+  if (g.row0 >= g.rstep) return;
+  const int gs = wrap_i(g.s0 + g.col - g.xh, g.nseg);
+  const size_t zrow = (size_t)z * g.ly;
+  for (int it = 0; it < g.iters_load; it += 2) {
+    const int r0 = g.row0 + it * g.rstep, r1 = r0 + g.rstep;
+    uint4 a[4], b[4];
+    const bool ok0 = r0 < g.R, ok1 = r1 < g.R && it + 1 < g.iters_load;
+    if (ok0) {
+      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - 2 + r0, g.ly)) * g.pitch + 64 * gs);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = __ldg(p + k);
+    }
+    if (ok1) {
+      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - 2 + r1, g.ly)) * g.pitch + 64 * gs);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) b[k] = __ldg(p + k);
+    }
+    if (ok0) pl[r0 * g.NC + g.col] = pack_segment(a[0], a[1], a[2], a[3]);
+    if (ok1) pl[r1 * g.NC + g.col] = pack_segment(b[0], b[1], b[2], b[3]);
+  }
+}
+
+struct PassAcc {
+  int nacc, ksum, down, owned_sites;
+};
+
+// One colour pass over rows [rlo, rlo + nrows) and columns [c_lo, c_hi) of
+// plane `pl` (in place).  For 3D, pm/pp are the neighbouring planes.
+template <int DIM>
+__device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint2* pp,
+                                          const BitsGeom& g, int z, int colour, int rlo,
+                                          int nrows, int iters, bool owned_plane, bool write_out,
+                                          int8_t* dst, const BitsTab& tab, const BitsPhilox& P,
+                                          PassAcc& acc) {
+  constexpr int zc = 2 * DIM;
+  const unsigned full = 0xFFFFFFFFu;
+  const int cc = g.col;
+  // columns this pass covers: colour 0 also updates the halo columns
+  const bool col_ok = g.row0 < g.rstep && (colour == 0 || (cc >= g.xh && cc < g.xh + g.ns));
+  const int gs = wrap_i(g.s0 + cc - g.xh, g.nseg);
+  const bool last_seg = gs == g.nseg - 1;
+  const bool first_seg = gs == 0;
+  const uint32_t valid = (last_seg && g.hlast < 32) ? ((1u << g.hlast) - 1u) : 0xFFFFFFFFu;
+  const bool owned_col = cc >= g.xh && cc < g.xh + g.ns;
+  // neighbour columns inside the plane (full-row tiles wrap around the row)
+  const int cprev = g.xh ? cc - 1 : (cc == 0 ? g.NC - 1 : cc - 1);
+  const int cnext = g.xh ? cc + 1 : (cc == g.NC - 1 ? 0 : cc + 1);
+  const bool has_prev = cprev >= 0, has_next = cnext < g.NC;
+  for (int it = 0; it < iters; ++it) {
+    const int r = rlo + g.row0 + it * g.rstep;
+    const bool active = col_ok && r < rlo + nrows;
+    uint32_t own = 0, pending = 0, always = 0, flip = 0;
+    uint32_t b0 = 0, b1 = 0, b2 = 0, segid = 0;
+    uint32_t m[3] = {0, 0, 0};
+    int P_ = 0;
+    if (active) {
+      const int y = wrap_i(g.y0 - 2 + r, g.ly);
+      P_ = (colour + y + z) & 1;  // x parity of this colour's sites in the row
+      const uint2 me = pl[r * g.NC + cc];
+      const uint2 up = pl[(r - 1) * g.NC + cc];
+      const uint2 dn = pl[(r + 1) * g.NC + cc];
+      own = P_ ? me.y : me.x;
+      const uint32_t other = P_ ? me.x : me.y;
+      uint32_t lft, rgt;
+      if (P_ == 0) {
+        // even x = 2i: left = odd 2i-1 (index i-1), right = odd 2i+1 (index i)
+        uint32_t carry = 0;
+        if (has_prev) {
+          const uint32_t po = pl[r * g.NC + cprev].y;
+          carry = first_seg ? (po >> (g.hlast - 1)) & 1u : po >> 31;
+        }
+        lft = (other << 1) | carry;
+        rgt = other;
+      } else {
+        // odd x = 2i+1: left = even 2i (index i), right = even 2i+2 (index i+1)
+        lft = other;
+        const uint32_t ne = has_next ? pl[r * g.NC + cnext].x & 1u : 0u;
+        const int hb = last_seg ? g.hlast - 1 : 31;
+        rgt = ((other >> 1) & ~(1u << hb)) | (ne << hb);
+      }
+      uint32_t x0 = own ^ lft, x1 = own ^ rgt, x2 = own ^ (P_ ? up.y : up.x), x3 = own ^ (P_ ? dn.y : dn.x);
+      if (DIM == 2) {
+        const uint32_t s0 = x0 ^ x1 ^ x2;
+        const uint32_t c0 = (x0 & x1) | (x2 & (x0 ^ x1));
+        b0 = s0 ^ x3;
+        const uint32_t c1 = s0 & x3;
+        b1 = c0 ^ c1;
+        b2 = c0 & c1;
+      } else {
+        const uint2 zm = pm[r * g.NC + cc], zp = pp[r * g.NC + cc];
+        const uint32_t x4 = own ^ (P_ ? zm.y : zm.x), x5 = own ^ (P_ ? zp.y : zp.x);
+        const uint32_t s0 = x0 ^ x1 ^ x2;
+        const uint32_t c0 = (x0 & x1) | (x2 & (x0 ^ x1));
+        const uint32_t s1 = x3 ^ x4 ^ x5;
+        const uint32_t c1 = (x3 & x4) | (x5 & (x3 ^ x4));
+        b0 = s0 ^ s1;
+        const uint32_t c2 = s0 & s1;
+        b1 = c0 ^ c1 ^ c2;
+        b2 = (c0 & c1) | (c2 & (c0 ^ c1));
+      }
+      // masks of the pending classes (class index k = b2 b1 b0 in bits)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        if (i < tab.npend) {
+          m[i] = (b0 ^ tab.pend_neg[i][0]) & (b1 ^ tab.pend_neg[i][1]) & (b2 ^ tab.pend_neg[i][2]) & valid;
+          pending |= m[i];
+        }
+      }
+      always = valid & ~pending;
+      segid = (uint32_t)(y + g.ly * z) * (uint32_t)g.nseg + (uint32_t)gs;
+    }
+    // bit-serial comparison of the 32 uniforms against their thresholds
+    uint32_t lt = 0, eq = pending;
+    const uint32_t ctrl0 = (uint32_t)colour | (TAG_BITS << 1);
+    for (int q = 0; q < 20; ++q) {
+      if (!__any_sync(full, eq)) break;
+      const uint4 o = bits_philox(P, segid, ctrl0 | ((uint32_t)q << 8));
+      const uint32_t pw[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const uint32_t* ts = tab.tsel[4 * q + h];
+        const uint32_t tj = (m[0] & ts[0]) | (m[1] & ts[1]) | (m[2] & ts[2]);
+        lt |= eq & tj & ~pw[h];
+        eq &= ~(tj ^ pw[h]);
+      }
+    }
+    if (active) {
+      flip = (always | lt) & valid;
+      const uint32_t nw = own ^ flip;
+      uint2& me = pl[r * g.NC + cc];
+      if (P_) me.y = nw;
+      else me.x = nw;
+      const bool owned = owned_plane && owned_col && r >= 2 && r < 2 + g.hv;
+      if (owned) {
+        acc.nacc += __popc(flip);
+        acc.ksum += __popc(flip & b0) + 2 * __popc(flip & b1) + 4 * __popc(flip & b2);
+      }
+      if (write_out) {
+        // both colours of this segment are final now: store the int8 row segment
+        const uint2 fin = P_ ? make_uint2(me.x, nw) : make_uint2(nw, me.y);
+        const int y = wrap_i(g.y0 - 2 + r, g.ly);
+        uint4 v0, v1, v2, v3;
+        unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
+        uint4* out = (uint4*)(dst + ((size_t)z * g.ly + y) * g.pitch + 64 * gs);
+        out[0] = v0;
+        out[1] = v1;
+        out[2] = v2;
+        out[3] = v3;
+        const uint32_t vE = valid, vO = valid;
+        acc.down += __popc(fin.x & vE) + __popc(fin.y & vO);
+        acc.owned_sites += 2 * __popc(valid);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, const GroupDesc* G) {
+  const int label = G->label[L->replica];
+  const int n = min(G->n_cls, 7);
+  const uint32_t* head = G->head + label * G->n_cls;
+  const unsigned long long* tail = G->tail + label * G->n_cls;
+  // pending classes in increasing k (at most three for the Ising table)
+  int pc[3] = {0, 0, 0}, np = 0;
+  for (int k = 0; k < n; ++k)
+    if (head[k] < 65536u && np < 3) pc[np++] = k;
+  if (threadIdx.x == 0) {
+    tab.npend = np;
+    for (int i = 0; i < 3; ++i)
+      for (int b = 0; b < 3; ++b)
+        tab.pend_neg[i][b] = (i < np && ((pc[i] >> b) & 1)) ? 0u : 0xFFFFFFFFu;
+  }
+  for (int e = threadIdx.x; e < 80 * 3; e += kThreads) {
+    const int j = e / 3, i = e - 3 * j;
+    uint32_t v = 0;
+    if (i < np) {
+      const uint32_t h = head[pc[i]];
+      const unsigned long long t = tail[pc[i]];
+      const uint32_t bit = j < 16 ? (h >> (15 - j)) & 1u : (uint32_t)((t >> (79 - j)) & 1ull);
+      v = bit ? 0xFFFFFFFFu : 0u;
+    }
+    tab.tsel[j][i] = v;
+  }
+}
+
+__device__ __forceinline__ void flush_bits(LatDesc* L, const PassAcc& a, int zc) {
+  long long dE = 2LL * zc * a.nacc - 4LL * a.ksum;
+  long long mag = (long long)a.owned_sites - 2LL * a.down;
+  long long nacc = a.nacc;
+  const unsigned full = 0xFFFFFFFFu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dE += __shfl_xor_sync(full, dE, o);
+    mag += __shfl_xor_sync(full, mag, o);
+    nacc += __shfl_xor_sync(full, nacc, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (dE) atomic_add_i64(&L->acc.dE, dE);
+    if (mag) atomic_add_i64(&L->acc.mag, mag);
+    if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+    k_sweep_ising_bits(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
+                       GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
+  extern __shared__ __align__(16) uint2 bsm[];
+  __shared__ BitsTab tab;
+  const TileItem t = tiles[blockIdx.x];
+  LatDesc* L = &lats[t.lat];
+  const GroupDesc* G = &groups[L->group];
+  const uint64_t sweep = L->sweep;
+  if (sweep >= L->target) {
+    launch_epilogue(lats, groups, ctl);
+    return;
+  }
+  const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
+  int8_t* nxt = (int8_t*)L->buf[(sweep & 1) ^ 1];
+  const BitsGeom g = make_bits_geom(t, L);
+  load_bits_table(tab, L, G);
+  const BitsPhilox P = make_bits_philox(L->key, sweep);
+  PassAcc acc = {0, 0, 0, 0};
+  if (DIM == 2) {
+    load_bits_plane(bsm, cur, 0, g);
+    __syncthreads();
+    bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, false, nxt, tab, P, acc);
+    __syncthreads();
+    bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, true, nxt, tab, P, acc);
+  } else {
+    const int lz = L->lz;
+    const int dv = min(L->tile_z, lz - t.z0);
+    const int pw = g.R * g.NC;
+    for (int s = 0; s < dv + 4; ++s) {
+      const int zl = t.z0 - 2 + s;
+      uint2* Pl = bsm + (s & 3) * pw;
+      load_bits_plane(Pl, cur, wrap_i(zl, lz), g);
+      __syncthreads();
+      if (s >= 2) {
+        const int zb = zl - 1;
+        bits_pass<3>(bsm + ((s - 1) & 3) * pw, bsm + ((s - 2) & 3) * pw, Pl, g, wrap_i(zb, lz), 0, 1,
+                     g.R - 2, g.iters_black, zb >= t.z0 && zb < t.z0 + dv, false, nxt, tab, P, acc);
+        __syncthreads();
+      }
+      if (s >= 4) {
+        const int zw = zl - 2;
+        bits_pass<3>(bsm + ((s - 2) & 3) * pw, bsm + ((s - 3) & 3) * pw, bsm + ((s - 1) & 3) * pw, g,
+                     wrap_i(zw, lz), 1, 2, g.hv, g.iters_white, true, true, nxt, tab, P, acc);
+      }
+      __syncthreads();  // the next load overwrites the plane slot read above
+    }
+  }
+  flush_bits(L, acc, 2 * DIM);
+  launch_epilogue(lats, groups, ctl);
+}
+
+template __global__ void k_sweep_ising_bits<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_ising_bits<3>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+
+}  // namespace gpumc

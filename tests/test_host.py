@@ -99,3 +99,19 @@ def test_geometric_ladder(gpumc):
     assert len(b) == 64
     assert 1 / b[0] == pytest.approx(1.5) and 1 / b[-1] == pytest.approx(3.5)
     assert all(x > y for x, y in zip(b, b[1:]))
+
+
+@pytest.mark.parametrize("model", [0, 1, 2, 3])
+def test_every_geometry_has_a_tile_plan(gpumc, model):
+    """Each model and extent in the benchmark and serving ranges gets a tile
+    plan with positive steps and shared memory within the device limit."""
+    from scamper_b200.mc import spec_from_params
+    lib = gpumc._lib.load()
+    for dims in (2, 3):
+        sizes = [4, 6, 10, 16, 30, 34, 62, 64, 66, 126, 128, 130, 190, 192]
+        if dims == 2:
+            sizes += [256, 510, 514, 1024, 2046, 2048, 2050, 4096, 8192]
+        for L in sizes:
+            p = {"lattice_type": "square" if dims == 2 else "cubic", "L": L, "beta": 0.4}
+            spec, keep = spec_from_params(p, model=model)
+            assert lib.gpumc_validate(ctypes.byref(spec)) == 0, (model, dims, L, gpumc._lib.last_error())
