@@ -325,12 +325,25 @@ def bench_mixed(gpumc, torch, args):
     for s in sims:
         s.close()
     eng.close()
+    # per-kind breakdown: the same lattices batched by model kind alone
+    kinds = {}
+    for kind in ("potts", "o3"):
+        e2 = gpumc.Engine()
+        sub = [gpumc.ClassicalMC.from_params(p, 300 + i, model=m, engine=e2, record_capacity=8)
+               for i, (m, p, _) in enumerate(specs) if m == kind]
+        e2.sweep(3)
+        ms_k = time_sweeps(torch, e2, e2.stream_ptr(), steps, e2.sweep)
+        att_k = float(sum(n for m, _, n in specs if m == kind)) * steps
+        kinds[kind] = {"lattices": len(sub), "value": att_k / (ms_k * 1e6), "ms_per_sweep": ms_k / steps}
+        for s in sub:
+            s.close()
+        e2.close()
     v_b = att / (ms_b * 1e6)
     v_p = (att_potts + att_o3) * plain_steps / (dt_plain * 1e9)
     bytes_per_sweep = att_potts * 2.0 + att_o3 * 24.0
     return {"config": "256 2D Potts (q 2..4, L 32..2048 log-uniform) + 32 3D O(3) L=64, one launch "
                       "per model kind per sweep", "value": v_b, "unit": "spin-flip attempts/ns",
-            "plain_value": v_p, "batched_over_plain": v_b / v_p,
+            "plain_value": v_p, "batched_over_plain": v_b / v_p, "by_kind": kinds,
             "hbm_gbs_algorithmic": bytes_per_sweep * steps / (ms_b * 1e6),
             "ms_per_sweep": ms_b / steps}
 
@@ -446,7 +459,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--aux-steps", type=int, default=100)
@@ -456,6 +469,8 @@ def main():
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only-headline", action="store_true")
+    ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving"], default=None,
+                    help="run one extra workload alone (profiling)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[30.0, 300.0])
     ap.add_argument("--serve-jobs", type=int, default=16)
     ap.add_argument("--serve-sweep-scale", type=float, default=0.01)
@@ -472,6 +487,10 @@ def main():
     torch.cuda.set_device(local)
     import scamper_b200 as gpumc
 
+    if args.only:
+        fn = {"msc": bench_msc, "pt": bench_pt, "mixed": bench_mixed, "serving": bench_serving}[args.only]
+        print(json.dumps({"workload": args.only, "result": fn(gpumc, torch, args)}), flush=True)
+        return 0
     h = headline(gpumc, torch, args, dist, rank, world)
     value = h["attempts"] / (h["ms"] * 1e6)
     per_launch_ms = h["ms"] / args.steps

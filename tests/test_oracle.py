@@ -287,3 +287,20 @@ def test_accumulator_matches_reference_unit_tests():
     assert binder_cumulant(0.0, 0.0) is None
     assert binder_cumulant(0.5, 0.25) == pytest.approx(1 - 0.25 / 0.75)
     assert specific_heat(-1.0, 2.0, 0.5, 4) == pytest.approx(0.25 / 4 * 1.0)
+
+
+@pytest.mark.parametrize("L,beta", [(4, 0.3), (4, 0.4407), (6, 0.5), (8, 0.4407), (8, 0.2)])
+def test_kaufman_exact_energy_matches_transfer_matrix(L, beta):
+    """The exact finite-torus energy used for the beta_c check agrees with the
+    row transfer matrix (CMC.rs/tests/physics/zscore_extended.rs:60-135)."""
+    tm = exact.potts_transfer_matrix_ising(L, L, beta)["E"]
+    assert exact.kaufman_energy(L, beta) == pytest.approx(tm, rel=1e-6, abs=1e-6)
+
+
+def test_kaufman_energy_approaches_onsager():
+    b = exact.BETA_C_2D_ISING
+    e64 = exact.kaufman_energy(64, b) / 64 ** 2
+    e512 = exact.kaufman_energy(512, b) / 512 ** 2
+    ons = exact.onsager_energy_per_site(b)
+    assert ons == pytest.approx(-math.sqrt(2.0), abs=1e-9)
+    assert abs(e512 - ons) < abs(e64 - ons) < 0.02
