@@ -31,7 +31,7 @@ template <int MODEL>
 __global__ void k_sweep_discrete_2d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int MODEL>
 __global__ void k_sweep_discrete_3d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template <int DIM>
+template <int DIM, int COLOUR>
 __global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
@@ -174,8 +174,8 @@ int validate_spec(const gpumc_spec* s) {
 
 // Every tile step must be positive and the shared-memory plan must fit.
 bool layout_ok(const Layout& L) {
-  return L.buf_bytes > 0 && L.tile_cx > 0 && L.tile_y > 0 && L.tile_z > 0 && L.smem > 0 &&
-         L.smem <= 200 * 1024;
+  return L.buf_bytes > 0 && L.tile_cx > 0 && L.tile_y > 0 && L.tile_z > 0 &&
+         (L.smem > 0 || L.model == O3) && L.smem <= 200 * 1024;
 }
 
 Layout plan_layout(const gpumc_spec* s) {
@@ -231,22 +231,15 @@ Layout plan_layout(const gpumc_spec* s) {
       L.smem = 6 * (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
     }
   } else if (L.model == O3) {
+    // in place, one thread per site of the colour, tiles of whole rows with
+    // about 2048 sites of each colour
     L.pitch = (lx + 3) / 4 * 4;
     L.buf_bytes = 3 * sizeof(float) * (size_t)L.pitch * rows;
-    const int w = std::min(lx, 64);
-    L.tile_cx = (w + 3) / 4;
-    const int W = std::min(lx, L.tile_cx * 4);
-    if (L.dims == 2) {
-      const int ty_max = 2 * 6 * 256 / (W + 2) - 2;
-      L.tile_y = std::max(1, std::min(std::min(ty_max, 40), ly));
-      L.tile_z = 1;
-      L.smem = 3 * sizeof(float) * (size_t)(L.tile_y + 4) * (W + 4);
-    } else {
-      const int ty_max = 2 * 6 * 256 / (W + 2) - 2;
-      L.tile_y = std::max(1, std::min(std::min(ty_max, 16), ly));
-      L.tile_z = std::min(lz, 16);
-      L.smem = 4 * 3 * sizeof(float) * (size_t)(L.tile_y + 4) * (W + 4);
-    }
+    L.inplace = true;
+    L.tile_cx = (lx + 3) / 4;
+    L.tile_y = std::max(1, std::min(ly, 4096 / lx));
+    L.tile_z = L.dims == 3 ? std::max(1, std::min(lz, 4096 / (lx * L.tile_y))) : 1;
+    L.smem = 0;
   } else {  // MSC
     L.pitch = (lx + 1) / 2 * 2;
     L.buf_bytes = sizeof(unsigned long long) * (size_t)L.pitch * rows;
@@ -286,7 +279,7 @@ int kernel_kind(int model, int dims) { return model * 2 + (dims - 2); }
 
 size_t footprint_bytes(const gpumc_spec* s) {
   const Layout L = plan_layout(s);
-  const size_t per = 2 * L.buf_bytes;
+  const size_t per = (L.inplace ? 1 : 2) * L.buf_bytes;
   const size_t rec_entries = (size_t)s->record_capacity * s->n_replicas * (L.model == MSC ? 64 : 1);
   return per * s->n_replicas + rec_entries * sizeof(Record) +
          (size_t)s->n_temps * kMaxClasses * 12 + 4096;
@@ -302,8 +295,8 @@ static SweepKernel kernel_for(int kind) {
     case 1: return k_sweep_ising_bits<3>;
     case 2: return k_sweep_discrete_2d<POTTS>;
     case 3: return k_sweep_discrete_3d<POTTS>;
-    case 4: return k_sweep_o3<2>;
-    case 5: return k_sweep_o3<3>;
+    case 4: return k_sweep_o3<2, 1>;
+    case 5: return k_sweep_o3<3, 1>;
     case 6: return k_sweep_msc<2>;
     default: return k_sweep_msc<3>;
   }
@@ -329,6 +322,9 @@ static int prepare_kernels() {
 int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
                         LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem) {
   if (n_tiles <= 0) return GPUMC_OK;
+  // O(3) sweeps in place: colour 0, then colour 1 (which runs the epilogue)
+  if (kind == 4) k_sweep_o3<2, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == 5) k_sweep_o3<3, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   kernel_for(kind)<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   CUDA_TRY(cudaGetLastError());
   return GPUMC_OK;
@@ -435,7 +431,8 @@ int gpumc_sim_engine(gpumc_sim* sim, gpumc_engine** eng) {
 
 int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n) {
   if (!sim || !n) return fail(GPUMC_EINVAL, "null argument");
-  *n = 1 + ((sim->lay.model == MSC && sim->phase == GPUMC_PHASE_MEASUREMENT) ? sim->n_rep + 1 : 0);
+  *n = (sim->lay.model == O3 ? 2 : 1) +
+       ((sim->lay.model == MSC && sim->phase == GPUMC_PHASE_MEASUREMENT) ? sim->n_rep + 1 : 0);
   return GPUMC_OK;
 }
 

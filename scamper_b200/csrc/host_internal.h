@@ -18,6 +18,7 @@ struct Layout {
   size_t buf_bytes = 0;  // one ping-pong buffer
   int tile_cx = 0, tile_y = 0, tile_z = 1;
   size_t smem = 0;
+  bool inplace = false;  // one buffer, updated in place (O(3)); else ping-pong
 };
 
 int fail(int code, const std::string& msg);

@@ -44,7 +44,8 @@ gpumc_sim::~gpumc_sim() {
   cudaSetDevice(eng->device);
   cudaStreamSynchronize(eng->stream);
   drop_graphs();
-  for (void* b : bufs) cudaFree(b);
+  for (size_t i = 0; i < bufs.size(); ++i)
+    if (bufs[i] && (i % 2 == 0 || bufs[i] != bufs[i - 1])) cudaFree(bufs[i]);
   cudaFree(d_head);
   cudaFree(d_tail);
   cudaFree(d_betas);
@@ -258,6 +259,10 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   // device buffers
   s->bufs.assign(2 * s->n_rep, nullptr);
   for (int i = 0; i < 2 * s->n_rep; ++i) {
+    if (s->lay.inplace && (i & 1)) {  // in-place models: both slots name one buffer
+      s->bufs[i] = s->bufs[i - 1];
+      continue;
+    }
     CUDA_CLEAN(cudaMalloc(&s->bufs[i], s->lay.buf_bytes));
     CUDA_CLEAN(cudaMemsetAsync(s->bufs[i], 0, s->lay.buf_bytes, eng->stream));
   }

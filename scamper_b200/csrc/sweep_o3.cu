@@ -1,5 +1,13 @@
-// Fused two-colour checkerboard sweep for O(3) Heisenberg spins (float32 unit
-// vectors, three component planes) on periodic square and cubic lattices.
+// Checkerboard sweep for O(3) Heisenberg spins (float32 unit vectors, three
+// component planes) on periodic square and cubic lattices.
+//
+// The O(3) update costs ~200 arithmetic instructions per attempt against 24 B
+// of compulsory traffic, so it is bound by instruction throughput, not HBM.
+// It therefore runs in place as two launches per sweep (colour 0, then colour
+// 1), one thread per site: a colour pass reads only the other colour, whose
+// values stay fixed during the pass, so no tiles, halos or barriers are needed
+// and neighbour reads are served by L1/L2.  The colour-1 launch ends with the
+// sweep epilogue.
 //
 // Proposal: a uniform point on the spherical cap of half-angle alpha around
 // the current spin (w = 1 - cos(alpha) stored per lattice, adapted toward 50 %
@@ -16,16 +24,6 @@
 #include "epilogue.cuh"
 
 namespace gpumc {
-
-constexpr int kO3MaxItems = 6;
-
-struct O3Geom {
-  int x0, Wv, S, R, hv;  // S = row stride (floats), R = rows per plane buffer
-};
-
-struct O3Site {
-  float x, y, z;
-};
 
 __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx, float hy,
                                           float hz, uint4 o, float omc, float mJ, float beta,
@@ -75,119 +73,144 @@ __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx
   return ok;
 }
 
-// Shared-memory plane: three component planes of R rows x S floats; logical
-// position x maps to column x - x0 + 2.
-__device__ __forceinline__ void o3_load_plane(float* pl, int plane_floats, const float* src,
-                                              size_t comp_stride, int pitch, int lx, int ly,
-                                              int y0, int z, const O3Geom& g) {
-  const int cols = g.Wv + 4;
-  for (int i = threadIdx.x; i < g.R * cols; i += kThreads) {
-    const int r = i / cols, c = i - r * cols;
-    const int y = wrapi(y0 - 2 + r, ly);
-    const int x = wrapi(g.x0 - 2 + c, lx);
-    const size_t off = ((size_t)z * ly + y) * (size_t)pitch + x;
-    pl[r * g.S + c] = src[off];
-    pl[plane_floats + r * g.S + c] = src[comp_stride + off];
-    pl[2 * plane_floats + r * g.S + c] = src[2 * comp_stride + off];
+// Philox4x32-10 of counter (site, colour | TAG_O3 << 1, sweep) with the
+// sweep-uniform part of round 1 and the bumped keys precomputed.
+struct O3Philox {
+  uint32_t a, b, c;
+  uint32_t k0[10], k1[10];
+};
+__device__ __forceinline__ O3Philox make_o3_philox(uint64_t key, uint64_t sweep, uint32_t ctrl) {
+  O3Philox P;
+  const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+  const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
+  P.a = __umulhi(0xCD9E8D57u, c2) ^ k0 ^ ctrl;
+  P.b = 0xCD9E8D57u * c2;
+  P.c = c3 ^ k1;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    P.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
+    P.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
   }
+  return P;
+}
+__device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
+  uint4 c = make_uint4(P.a, P.b, __umulhi(0xD2511F53u, index) ^ P.c, 0xD2511F53u * index);
+#pragma unroll
+  for (int r = 1; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ P.k0[r], lo1, hi0 ^ c.w ^ P.k1[r], lo0);
+  }
+  return c;
 }
 
-template <int DIM>
-__device__ __forceinline__ void o3_pass(float* pl, const float* pzm, const float* pzp,
-                                        int plane_floats, const O3Geom& g, int colour, int y0,
-                                        int z, int ly, int lx, int pitch, uint64_t key,
-                                        uint64_t sweep, float omc, float mJ, float beta,
-                                        double Jd, bool owned_plane, float* dst, size_t comp_stride,
-                                        double& dEsum, int& nacc, double& mx, double& my,
-                                        double& mz) {
-  // colour 0 covers rows [1, R-1) and positions [x0-1, x0+Wv]; colour 1 the tile
-  const int rlo = colour == 0 ? 1 : 2;
-  const int nrows = colour == 0 ? g.hv + 2 : g.hv;
-  const int xlo = colour == 0 ? g.x0 - 1 : g.x0;
-  const int half = colour == 0 ? (g.Wv + 2) / 2 : g.Wv / 2;
-  const int nitems = nrows * half;
-  float rx[kO3MaxItems], ry[kO3MaxItems], rz[kO3MaxItems];
-  int roff[kO3MaxItems];
-#pragma unroll
-  for (int it = 0; it < kO3MaxItems; ++it) {
-    roff[it] = -1;
-    const int i = threadIdx.x + it * kThreads;
-    if (i < nitems) {
-      const int r = rlo + i / half;
-      const int k = i - (r - rlo) * half;
-      const int y = wrapi(y0 - 2 + r, ly);
-      const int par = ((xlo + y + z + colour) & 1);
-      const int pos = xlo + 2 * k + par;
-      const int c = pos - g.x0 + 2;
-      const int off = r * g.S + c;
-      const float* P0 = pl;
-      const float* P1 = pl + plane_floats;
-      const float* P2 = pl + 2 * plane_floats;
-      float hx = P0[off - 1], hy = P1[off - 1], hz = P2[off - 1];
-      hx = fadd(hx, P0[off + 1]); hy = fadd(hy, P1[off + 1]); hz = fadd(hz, P2[off + 1]);
-      hx = fadd(hx, P0[off - g.S]); hy = fadd(hy, P1[off - g.S]); hz = fadd(hz, P2[off - g.S]);
-      hx = fadd(hx, P0[off + g.S]); hy = fadd(hy, P1[off + g.S]); hz = fadd(hz, P2[off + g.S]);
+// One colour pass over a tile of full rows (y0 .. y0+hv-1, planes z0 ..
+// z0+dv-1), one thread per site of the colour.
+template <int DIM, int COLOUR>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_sweep_o3(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
+               GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
+  const TileItem t = tiles[blockIdx.x];
+  LatDesc* L = &lats[t.lat];
+  const GroupDesc* G = &groups[L->group];
+  const uint64_t sweep = L->sweep;
+  if (sweep >= L->target) {
+    if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+    return;
+  }
+  const int lx = L->lx, ly = L->ly, lz = DIM == 3 ? L->lz : 1, pitch = L->pitch;
+  const uint32_t cs = (uint32_t)pitch * ly * lz;  // component plane stride (< 2^32 elements)
+  float* S = (float*)L->buf[0];  // in place; component planes S, S1, S2
+  float* S1 = S + (size_t)cs;
+  float* S2 = S + 2 * (size_t)cs;
+  const float* Sr = S;
+  const float* Sr1 = S1;
+  const float* Sr2 = S2;
+  const int label = G->label[L->replica];
+  const float beta = G->betas_f[label];
+  const float mJ = -G->Jf;
+  const double Jd = G->J;
+  const float omc = L->omc;
+  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | (TAG_O3 << 1));
+  const int hv = min(L->tile_y, ly - t.y0);
+  const int dv = DIM == 3 ? min(L->tile_z, lz - t.z0) : 1;
+  const int half = lx >> 1;
+  const int rows = hv * dv;
+  // thread mapping: fixed column (or column stride) per thread, rows strided
+  int col0, cstep, r0, rstep;
+  if (half >= kThreads) {
+    col0 = threadIdx.x;
+    cstep = kThreads;
+    r0 = 0;
+    rstep = 1;
+  } else {
+    col0 = threadIdx.x % half;
+    cstep = half;
+    r0 = threadIdx.x / half;
+    rstep = kThreads / half;
+  }
+  double dE = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  int nacc = 0;
+  if (r0 < rstep) {
+    for (int r = r0; r < rows; r += rstep) {
+      const int y = t.y0 + (DIM == 3 ? r % hv : r);
+      const int z = DIM == 3 ? t.z0 + r / hv : 0;
+      const uint32_t rowoff = ((uint32_t)z * ly + y) * (uint32_t)pitch;
+      const int ym = y ? y - 1 : ly - 1, yp = y + 1 < ly ? y + 1 : 0;
+      const uint32_t rm = ((uint32_t)z * ly + ym) * (uint32_t)pitch;
+      const uint32_t rp = ((uint32_t)z * ly + yp) * (uint32_t)pitch;
+      uint32_t zmo = 0, zpo = 0;
       if (DIM == 3) {
-        hx = fadd(hx, pzm[off]);
-        hy = fadd(hy, pzm[plane_floats + off]);
-        hz = fadd(hz, pzm[2 * plane_floats + off]);
-        hx = fadd(hx, pzp[off]);
-        hy = fadd(hy, pzp[plane_floats + off]);
-        hz = fadd(hz, pzp[2 * plane_floats + off]);
+        const int zm = z ? z - 1 : lz - 1, zp = z + 1 < lz ? z + 1 : 0;
+        zmo = ((uint32_t)zm * ly + y) * (uint32_t)pitch;
+        zpo = ((uint32_t)zp * ly + y) * (uint32_t)pitch;
       }
-      const float ax = P0[off], ay = P1[off], az = P2[off];
-      const int xr = wrapi(pos, lx);
-      const uint64_t site = ((uint64_t)z * ly + y) * (uint64_t)lx + (uint64_t)xr;
-      const uint4 o = draw(key, site, (uint32_t)colour, TAG_O3, 0, sweep);
-      float nx, ny, nz, de;
-      const bool ok = o3_update(ax, ay, az, hx, hy, hz, o, omc, mJ, beta, nx, ny, nz, de);
-      const bool owned = owned_plane && r >= 2 && r < 2 + g.hv && pos >= g.x0 && pos < g.x0 + g.Wv;
-      float fx = ax, fy = ay, fz = az;
-      if (ok) {
-        fx = nx; fy = ny; fz = nz;
-        if (owned) {
-          // energy cache: exact fp64 change of the fp32 configuration (the
-          // decision above used the fp32 dE)
-          double hxd = (double)P0[off - 1] + (double)P0[off + 1] + (double)P0[off - g.S] + (double)P0[off + g.S];
-          double hyd = (double)P1[off - 1] + (double)P1[off + 1] + (double)P1[off - g.S] + (double)P1[off + g.S];
-          double hzd = (double)P2[off - 1] + (double)P2[off + 1] + (double)P2[off - g.S] + (double)P2[off + g.S];
-          if (DIM == 3) {
-            hxd += (double)pzm[off] + (double)pzp[off];
-            hyd += (double)pzm[plane_floats + off] + (double)pzp[plane_floats + off];
-            hzd += (double)pzm[2 * plane_floats + off] + (double)pzp[2 * plane_floats + off];
-          }
-          dEsum += -(double)Jd * (((double)nx - (double)ax) * hxd + ((double)ny - (double)ay) * hyd +
-                                  ((double)nz - (double)az) * hzd);
-          ++nacc;
+      const int par = (y + z + COLOUR) & 1;
+      for (int c = col0; c < half; c += cstep) {
+        const int x = 2 * c + par;
+        const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
+        // neighbour sum in the fixed order x-1, x+1, y-1, y+1, z-1, z+1
+        const uint32_t nb[6] = {rowoff + xm, rowoff + xp, rm + x, rp + x, zmo + x, zpo + x};
+        float hx = __ldg(Sr + nb[0]), hy = __ldg(Sr1 + nb[0]), hz = __ldg(Sr2 + nb[0]);
+#pragma unroll
+        for (int i = 1; i < 2 * DIM; ++i) {
+          hx = fadd(hx, __ldg(Sr + nb[i]));
+          hy = fadd(hy, __ldg(Sr1 + nb[i]));
+          hz = fadd(hz, __ldg(Sr2 + nb[i]));
         }
-      }
-      rx[it] = fx; ry[it] = fy; rz[it] = fz;
-      roff[it] = off;
-      if (owned) {
-        const size_t goff = ((size_t)z * ly + y) * (size_t)pitch + xr;
-        dst[goff] = fx;
-        dst[comp_stride + goff] = fy;
-        dst[2 * comp_stride + goff] = fz;
+        const uint32_t me = rowoff + x;
+        const float ax = S[me], ay = S1[me], az = S2[me];
+        const uint32_t site = (uint32_t)((size_t)(z * ly + y) * lx + x);
+        float nx, ny, nz, de;
+        const bool ok = o3_update(ax, ay, az, hx, hy, hz, o3_philox(P, site), omc, mJ, beta, nx, ny,
+                                  nz, de);
+        float fx = ax, fy = ay, fz = az;
+        if (ok) {
+          // energy cache: exact fp64 change of the fp32 configuration (the
+          // decision used the fp32 dE)
+          double hxd = 0.0, hyd = 0.0, hzd = 0.0;
+#pragma unroll
+          for (int i = 0; i < 2 * DIM; ++i) {
+            hxd += (double)__ldg(Sr + nb[i]);
+            hyd += (double)__ldg(Sr1 + nb[i]);
+            hzd += (double)__ldg(Sr2 + nb[i]);
+          }
+          dE += -Jd * (((double)nx - (double)ax) * hxd + ((double)ny - (double)ay) * hyd +
+                       ((double)nz - (double)az) * hzd);
+          ++nacc;
+          fx = nx;
+          fy = ny;
+          fz = nz;
+          S[me] = fx;
+          S1[me] = fy;
+          S2[me] = fz;
+        }
         mx += (double)fx;
         my += (double)fy;
         mz += (double)fz;
       }
     }
   }
-  __syncthreads();
-#pragma unroll
-  for (int it = 0; it < kO3MaxItems; ++it) {
-    if (roff[it] >= 0) {
-      pl[roff[it]] = rx[it];
-      pl[plane_floats + roff[it]] = ry[it];
-      pl[2 * plane_floats + roff[it]] = rz[it];
-    }
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void o3_flush(LatDesc* L, double dE, int nacc, double mx, double my,
-                                         double mz) {
   const unsigned full = 0xFFFFFFFFu;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -204,75 +227,12 @@ __device__ __forceinline__ void o3_flush(LatDesc* L, double dE, int nacc, double
     atomicAdd(&L->acc.mz, mz);
     if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
   }
+  if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(kThreads)
-    k_sweep_o3(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
-               GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
-  extern __shared__ __align__(16) float fsm[];
-  const TileItem t = tiles[blockIdx.x];
-  LatDesc* L = &lats[t.lat];
-  const GroupDesc* G = &groups[L->group];
-  const uint64_t sweep = L->sweep;
-  if (sweep >= L->target) {
-    launch_epilogue(lats, groups, ctl);
-    return;
-  }
-  const int lx = L->lx, ly = L->ly, lz = DIM == 3 ? L->lz : 1, pitch = L->pitch;
-  const uint64_t key = L->key;
-  const size_t comp_stride = (size_t)pitch * ly * lz;
-  const float* cur = (const float*)L->buf[sweep & 1];
-  float* nxt = (float*)L->buf[(sweep & 1) ^ 1];
-  const int label = G->label[L->replica];
-  const float beta = G->betas_f[label];
-  const float mJ = -G->Jf;
-  const float omc = L->omc;
-  O3Geom g;
-  g.x0 = t.x0;
-  g.Wv = min(L->tile_cx * 4, lx - t.x0);
-  g.hv = min(L->tile_y, ly - t.y0);
-  g.S = g.Wv + 4;
-  g.R = g.hv + 4;
-  const int plane_floats = g.R * g.S;
-  double dE = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-  int nacc = 0;
-  if (DIM == 2) {
-    o3_load_plane(fsm, plane_floats, cur, comp_stride, pitch, lx, ly, t.y0, 0, g);
-    __syncthreads();
-    o3_pass<2>(fsm, fsm, fsm, plane_floats, g, 0, t.y0, 0, ly, lx, pitch, key, sweep, omc, mJ,
-               beta, G->J, true, nxt, comp_stride, dE, nacc, mx, my, mz);
-    o3_pass<2>(fsm, fsm, fsm, plane_floats, g, 1, t.y0, 0, ly, lx, pitch, key, sweep, omc, mJ,
-               beta, G->J, true, nxt, comp_stride, dE, nacc, mx, my, mz);
-  } else {
-    const int dv = min(L->tile_z, lz - t.z0);
-    const int slot_floats = 3 * plane_floats;
-    for (int s = 0; s < dv + 4; ++s) {
-      const int zl = t.z0 - 2 + s;
-      float* pl = fsm + (s & 3) * slot_floats;
-      o3_load_plane(pl, plane_floats, cur, comp_stride, pitch, lx, ly, t.y0, wrapi(zl, lz), g);
-      __syncthreads();
-      if (s >= 2) {
-        const int zb = zl - 1;
-        o3_pass<3>(fsm + ((s - 1) & 3) * slot_floats, fsm + ((s - 2) & 3) * slot_floats, pl,
-                   plane_floats, g, 0, t.y0, wrapi(zb, lz), ly, lx, pitch, key, sweep, omc, mJ,
-                   beta, G->J, zb >= t.z0 && zb < t.z0 + dv, nxt, comp_stride, dE, nacc, mx, my, mz);
-      }
-      if (s >= 4) {
-        const int zw = zl - 2;
-        o3_pass<3>(fsm + ((s - 2) & 3) * slot_floats, fsm + ((s - 3) & 3) * slot_floats,
-                   fsm + ((s - 1) & 3) * slot_floats, plane_floats, g, 1, t.y0, wrapi(zw, lz), ly,
-                   lx, pitch, key, sweep, omc, mJ, beta, G->J, true, nxt, comp_stride, dE, nacc, mx,
-                   my, mz);
-      }
-      __syncthreads();
-    }
-  }
-  o3_flush(L, dE, nacc, mx, my, mz);
-  launch_epilogue(lats, groups, ctl);
-}
-
-template __global__ void k_sweep_o3<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_o3<3>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_o3<2, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_o3<2, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_o3<3, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_o3<3, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 
 }  // namespace gpumc

@@ -100,9 +100,12 @@ def test_batched_engine_matches_plain_path(gpumc):
     eng.sweep(70)
     for p in plain:
         p.sweep(70)
-    for b, p in zip(batched, plain):
+    for (model, _, _), b, p in zip(specs, batched, plain):
         np.testing.assert_array_equal(b.spins(), p.spins())
-        np.testing.assert_array_equal(b.energy(), p.energy())
+        if model == "o3":  # fp64 energy cache summed by atomics in launch order
+            np.testing.assert_allclose(b.energy(), p.energy(), rtol=1e-12)
+        else:
+            np.testing.assert_array_equal(b.energy(), p.energy())
         assert b.sweep_count() == p.sweep_count() == 70
     for m in batched + plain:
         m.close()
