@@ -41,7 +41,6 @@ __global__ void k_msc_record(LatDesc*, GroupDesc*, int, unsigned long long*);
 __global__ void k_init_discrete(int8_t*, int, int, int, int, int, int, uint64_t, int);
 __global__ void k_init_o3(float*, int, int, int, int, uint64_t, int);
 __global__ void k_init_msc(unsigned long long*, int, int, int, int, const uint64_t*, int);
-__global__ void k_energy_int(const void*, int, int, int, int, int, unsigned long long*);
 __global__ void k_energy_o3(const float*, int, int, int, int, double, double*);
 __global__ void k_philox_probe(const uint4*, const uint2*, uint4*, int);
 
@@ -178,7 +177,38 @@ bool layout_ok(const Layout& L) {
          (L.smem > 0 || L.model == O3) && L.smem <= 200 * 1024;
 }
 
-Layout plan_layout(const gpumc_spec* s) {
+// Rows per whole-row Ising tile.  A tile of hv rows costs its CTA
+// ceil((hv+4)/r) + ceil((hv+2)/r) + ceil(hv/r) row steps (load, black pass
+// with its halo rows, white pass; r = rows the CTA covers per step), and the
+// n_rep lattices of ly rows run in ceil(tiles / slots) waves of the device's
+// resident CTA slots.  The height minimising waves x steps is chosen (the
+// taller one on a tie, which does less halo work), among heights that fit
+// the shared-memory budget and are at least 8 rows unless the lattice is
+// smaller.
+int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots) {
+  const int r = std::max(1, kThreads / nseg);
+  int best = std::min(ly, hv_max);
+  double best_t = 1e300;
+  int last_hv = -1;
+  for (int nty = 1; nty <= ly; ++nty) {
+    const int hv = (ly + nty - 1) / nty;
+    if (hv == last_hv) continue;
+    last_hv = hv;
+    if (hv > hv_max) continue;
+    if (hv < 8 && hv < ly) break;
+    const int tiles = ((ly + hv - 1) / hv) * n_rep;
+    const double waves = std::max(1.0, std::ceil((double)tiles / slots));
+    const double steps = std::ceil((hv + 4.0) / r) + std::ceil((hv + 2.0) / r) + std::ceil((double)hv / r);
+    const double t = waves * steps;
+    if (t < best_t - 1e-9) {
+      best_t = t;
+      best = hv;
+    }
+  }
+  return best;
+}
+
+Layout plan_layout(const gpumc_spec* s, int slots) {
   Layout L;
   L.model = s->model;
   L.dims = s->dims;
@@ -189,26 +219,37 @@ Layout plan_layout(const gpumc_spec* s) {
   L.n_sites = (int64_t)lx * ly * lz;
   const size_t rows = (size_t)ly * lz;
   if (L.model == ISING) {
-    // bit-sliced kernel: 64-site row segments; x-split tiles of 32 segments
-    // (plus one halo segment per side) when the row is a whole number of
-    // segments longer than 2048 sites, else whole-row tiles
+    // bit-sliced kernel: 64-site row segments.  2D lattices whose rows are at
+    // most 256 segments use whole-row tiles (no column halo, the threads of a
+    // CTA cover whole rows); the tile height trades the two halo rows of the
+    // black pass against filling the GPU's CTA slots in whole waves.  Longer
+    // rows (and 3D) use x-split tiles of 32 segments plus one halo segment
+    // per side when the row is a whole number of segments.
     L.pitch = (lx + 63) / 64 * 64;
     L.buf_bytes = (size_t)L.pitch * rows;
     const int nseg = L.pitch / 64;
-    const bool xsplit = (lx % 64 == 0) && nseg > 32;
-    L.tile_cx = xsplit ? 32 : nseg;
-    const int nc = L.tile_cx + (xsplit ? 2 : 0);
-    const int items = L.dims == 2 ? 2048 : 1024;
-    const int hv_max = std::max(1, items / nc - 2);
-    const int nty = (ly + hv_max - 1) / hv_max;
-    L.tile_y = (ly + nty - 1) / nty;
-    if (L.dims == 2) {
+    if (L.dims == 2 && nseg <= 256) {
+      L.tile_cx = nseg;
+      const int hv_max = std::max(1, (int)(kIsingTileSmem / (8 * (size_t)nseg)) - 4);
+      L.tile_y = ising_tile_rows(ly, std::max<int>(1, (int)s->n_replicas), nseg, hv_max, slots);
       L.tile_z = 1;
-      L.smem = 8 * (size_t)(L.tile_y + 4) * nc;
+      L.smem = 8 * (size_t)(L.tile_y + 4) * nseg;
     } else {
-      const int ntz = (lz + 15) / 16;
-      L.tile_z = (lz + ntz - 1) / ntz;
-      L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * nc;
+      const bool xsplit = (lx % 64 == 0) && nseg > 32;
+      L.tile_cx = xsplit ? 32 : nseg;
+      const int nc = L.tile_cx + (xsplit ? 2 : 0);
+      const int items = L.dims == 2 ? 2048 : 1024;
+      const int hv_max = std::max(1, items / nc - 2);
+      const int nty = (ly + hv_max - 1) / hv_max;
+      L.tile_y = (ly + nty - 1) / nty;
+      if (L.dims == 2) {
+        L.tile_z = 1;
+        L.smem = 8 * (size_t)(L.tile_y + 4) * nc;
+      } else {
+        const int ntz = (lz + 15) / 16;
+        L.tile_z = (lz + ntz - 1) / ntz;
+        L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * nc;
+      }
     }
   } else if (L.model == POTTS) {
     L.pitch = (lx + 15) / 16 * 16;
@@ -383,6 +424,15 @@ int gpumc_engine_create(int32_t device, gpumc_engine** out) {
     delete e;
     return fail(GPUMC_ECUDA, std::string("engine allocation: ") + cudaGetErrorString(err));
   }
+  int n_sm = 0, per_sm = 0;
+  err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
+  if (err == cudaSuccess)
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_ising_bits<2>, kThreads, kIsingTileSmem);
+  if (err != cudaSuccess) {
+    delete e;
+    return fail(GPUMC_ECUDA, std::string("device query: ") + cudaGetErrorString(err));
+  }
+  e->slots = std::max(1, n_sm * std::max(1, per_sm));
   e->lat_used.assign(e->lat_cap, false);
   e->group_used.assign(e->group_cap, false);
   *out = e;

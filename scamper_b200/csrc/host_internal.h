@@ -28,7 +28,12 @@ int n_classes(int model, int dims);
 void build_table(int model, int dims, double J, double beta, uint32_t* head,
                  unsigned long long* tail);
 int validate_spec(const gpumc_spec* s);
-Layout plan_layout(const gpumc_spec* s);
+// CTA slots of one B200 (148 SMs x 4 resident sweep CTAs); the engine
+// passes its device's own count.
+constexpr int kDefaultSlots = 148 * 4;
+constexpr size_t kIsingTileSmem = 48 * 1024;  // whole-row Ising tile budget
+Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots);
+int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);
 bool layout_ok(const Layout& L);
 void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out);
 int kernel_kind(int model, int dims);
@@ -68,6 +73,7 @@ struct gpumc_engine {
   std::set<gpumc_sim*> sims;
   bool batch_dirty = true;
   bool use_graphs = true;
+  int slots = gpumc::kDefaultSlots;  // resident sweep CTAs of the device (tile planning)
   std::vector<gpumc::BatchPlan> batch_plans;
   std::map<uint32_t, cudaGraphExec_t> batch_graphs;
 
@@ -121,6 +127,7 @@ struct gpumc_sim {
   int upload_tables();
   void drop_graphs();
   int recompute(std::vector<double>& out, bool store);
+  int launch_energy(const void* buf, unsigned long long* d_e, unsigned int* d_bad);
   template <class T>
   int set_lat_field(int r, size_t offset, const T& v) {
     return cudaMemcpyAsync(reinterpret_cast<char*>(eng->d_lats + lat0 + r) + offset, &v, sizeof(T),

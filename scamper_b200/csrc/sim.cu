@@ -17,7 +17,8 @@ namespace gpumc {
 __global__ void k_init_discrete(int8_t*, int, int, int, int, int, int, uint64_t, int);
 __global__ void k_init_o3(float*, int, int, int, int, uint64_t, int);
 __global__ void k_init_msc(unsigned long long*, int, int, int, int, const uint64_t*, int);
-__global__ void k_energy_int(const void*, int, int, int, int, int, unsigned long long*);
+__global__ void k_energy_i8(const int8_t*, int, int, int, int, int, int, unsigned long long*, unsigned int*);
+__global__ void k_energy_msc(const unsigned long long*, int, int, int, int, unsigned long long*);
 __global__ void k_energy_o3(const float*, int, int, int, int, double, double*);
 __global__ void k_philox_probe(const uint4*, const uint2*, uint4*, int);
 }  // namespace gpumc
@@ -166,26 +167,45 @@ int gpumc_sim::drain_records() {
   return GPUMC_OK;
 }
 
+// Launches the exact energy reduction of one buffer into d_e (int64 units of
+// J for the integer models, f64 for O(3)); for int8 models also counts
+// chunks with invalid spin values into d_bad (if given).
+int gpumc_sim::launch_energy(const void* buf, unsigned long long* d_e, unsigned int* d_bad) {
+  const Layout& L = lay;
+  const int rows = L.ly * L.lz;
+  if (L.model == O3) {
+    const int blocks = (int)std::min<int64_t>(kInitBlocks, (L.n_sites + 255) / 256);
+    k_energy_o3<<<blocks, 256, 0, eng->stream>>>((const float*)buf, L.lx, L.ly, L.lz, L.pitch, spec.J,
+                                                  (double*)d_e);
+  } else if (L.model == MSC) {
+    const int blocks = std::min(kInitBlocks, rows);
+    k_energy_msc<<<blocks, 256, 0, eng->stream>>>((const unsigned long long*)buf, L.lx, L.ly, L.lz,
+                                                   L.pitch, d_e);
+  } else {
+    const int nch = (L.lx + 15) / 16;
+    const int rpi = nch <= 256 ? 256 / nch : 1;
+    const int blocks = std::min(kInitBlocks, (rows + rpi - 1) / rpi);
+    k_energy_i8<<<blocks, 256, 0, eng->stream>>>((const int8_t*)buf, L.model, (int)spec.q, L.lx, L.ly,
+                                                  L.lz, L.pitch, d_e, d_bad);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return GPUMC_OK;
+}
+
 int gpumc_sim::recompute(std::vector<double>& out, bool store) {
   out.assign(n_rep, 0.0);
   unsigned long long* d_acc = nullptr;
   CUDA_TRY(cudaMalloc(&d_acc, 8 * (size_t)n_rep));
-  CUDA_TRY(cudaMemsetAsync(d_acc, 0, 8 * (size_t)n_rep, eng->stream));
-  const int blocks = (int)std::min<int64_t>(kInitBlocks, (lay.n_sites + 255) / 256);
-  for (int r = 0; r < n_rep; ++r) {
-    const void* buf = bufs[2 * r + (sweeps & 1)];
-    if (lay.model == O3)
-      k_energy_o3<<<blocks, 256, 0, eng->stream>>>((const float*)buf, lay.lx, lay.ly, lay.lz, lay.pitch,
-                                                    spec.J, (double*)(d_acc + r));
-    else
-      k_energy_int<<<blocks, 256, 0, eng->stream>>>(buf, lay.model, lay.lx, lay.ly, lay.lz, lay.pitch,
-                                                     d_acc + r);
-  }
+  int rc = GPUMC_OK;
+  cudaError_t e = cudaMemsetAsync(d_acc, 0, 8 * (size_t)n_rep, eng->stream);
+  for (int r = 0; r < n_rep && e == cudaSuccess && rc == GPUMC_OK; ++r)
+    rc = launch_energy(bufs[2 * r + (sweeps & 1)], d_acc + r, nullptr);
   std::vector<unsigned long long> h(n_rep);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_acc, 8 * (size_t)n_rep, cudaMemcpyDeviceToHost, eng->stream);
+  if (e == cudaSuccess && rc == GPUMC_OK)
+    e = cudaMemcpyAsync(h.data(), d_acc, 8 * (size_t)n_rep, cudaMemcpyDeviceToHost, eng->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
   cudaFree(d_acc);
+  if (rc != GPUMC_OK) return rc;
   if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("energy recompute: ") + cudaGetErrorString(e));
   for (int r = 0; r < n_rep; ++r) {
     if (lay.model == O3) {
@@ -230,7 +250,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   s->spec = *spec;
   s->betas.assign(spec->betas, spec->betas + spec->n_temps);
   s->spec.betas = nullptr;
-  s->lay = plan_layout(spec);
+  s->lay = plan_layout(spec, eng->slots);
   s->n_rep = spec->n_replicas;
   s->n_temps = spec->n_temps;
   s->n_cls = n_classes(s->lay.model == MSC ? ISING : s->lay.model, s->lay.dims);
@@ -478,16 +498,38 @@ int gpumc_set_spins(gpumc_sim* sim, int32_t replica, const void* host, size_t nb
   const Layout& L = sim->lay;
   const size_t need = host_site_bytes(L.model) * (size_t)L.n_sites;
   if (nbytes != need) return fail(GPUMC_EINVAL, "nbytes: does not match the lattice");
-  // validate_spin of the reference models (CMC.rs/src/lattice/models.rs)
-  if (L.model == ISING) {
-    const int8_t* v = (const int8_t*)host;
-    for (int64_t i = 0; i < L.n_sites; ++i)
-      if (v[i] != 1 && v[i] != -1) return fail(GPUMC_EINVAL, "spins: Ising spin must be exactly -1 or +1");
-  } else if (L.model == POTTS) {
-    const int8_t* v = (const int8_t*)host;
-    for (int64_t i = 0; i < L.n_sites; ++i)
-      if (v[i] < 0 || v[i] >= sim->spec.q) return fail(GPUMC_EINVAL, "spins: Potts spin must be in [0, q)");
-  } else if (L.model == O3) {
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  const size_t rows = (size_t)L.ly * L.lz;
+  void* cur = sim->bufs[2 * replica + (sim->sweeps & 1)];
+  if (L.model == ISING || L.model == POTTS) {
+    // The state lands in the replica's other ping-pong buffer (rewritten by
+    // the next sweep anyway) and is validated on the device together with
+    // the exact energy (validate_spin, CMC.rs/src/lattice/models.rs:62-75,
+    // :238-252); only a valid state replaces the current one.
+    void* stage = sim->bufs[2 * replica + ((sim->sweeps & 1) ^ 1)];
+    unsigned long long* d_acc = nullptr;
+    CUDA_TRY(cudaMalloc(&d_acc, 16));
+    cudaStream_t st = sim->eng->stream;
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaMemcpy2DAsync(stage, L.pitch, host, L.lx, L.lx, rows, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_acc, 0, 16, st);
+    int rc = e == cudaSuccess ? sim->launch_energy(stage, d_acc, (unsigned int*)(d_acc + 1)) : GPUMC_OK;
+    if (e == cudaSuccess && rc == GPUMC_OK) e = cudaMemcpyAsync(h, d_acc, 16, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && rc == GPUMC_OK) e = cudaStreamSynchronize(st);
+    cudaFree(d_acc);
+    if (rc != GPUMC_OK) return rc;
+    if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("set_spins: ") + cudaGetErrorString(e));
+    if ((unsigned int)h[1] != 0)
+      return fail(GPUMC_EINVAL, L.model == ISING ? "spins: Ising spin must be exactly -1 or +1"
+                                                 : "spins: Potts spin must be in [0, q)");
+    CUDA_TRY(cudaMemcpyAsync(cur, stage, L.buf_bytes, cudaMemcpyDeviceToDevice, st));
+    RC_TRY(sim->set_lat_field(replica, offsetof(LatDesc, e_int), (long long)h[0]));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return GPUMC_OK;
+  }
+  if (L.model == O3) {
+    // validate_spin of ONModel (unit norm, CMC.rs/src/lattice/models.rs:454-475)
     const float* v = (const float*)host;
     for (int64_t i = 0; i < L.n_sites; ++i) {
       const double n2 = (double)v[3 * i] * v[3 * i] + (double)v[3 * i + 1] * v[3 * i + 1] +
@@ -495,25 +537,16 @@ int gpumc_set_spins(gpumc_sim* sim, int32_t replica, const void* host, size_t nb
       if (!std::isfinite(n2) || std::fabs(n2 - 1.0) > 1e-5)
         return fail(GPUMC_EINVAL, "spins: O(3) spin must have unit norm (|n^2 - 1| <= 1e-5 in float32)");
     }
-  }
-  CUDA_TRY(cudaSetDevice(sim->eng->device));
-  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
-  void* buf = sim->bufs[2 * replica + (sim->sweeps & 1)];
-  const size_t rows = (size_t)L.ly * L.lz;
-  if (L.model == ISING || L.model == POTTS) {
-    CUDA_TRY(cudaMemcpy2D(buf, L.pitch, host, L.lx, L.lx, rows, cudaMemcpyHostToDevice));
-  } else if (L.model == MSC) {
-    CUDA_TRY(cudaMemcpy2D(buf, 8 * (size_t)L.pitch, host, 8 * (size_t)L.lx, 8 * (size_t)L.lx, rows,
-                          cudaMemcpyHostToDevice));
-  } else {
     std::vector<float> comp((size_t)L.n_sites * 3);
-    const float* h = (const float*)host;
     for (int64_t i = 0; i < L.n_sites; ++i)
-      for (int c = 0; c < 3; ++c) comp[(size_t)c * L.n_sites + i] = h[3 * i + c];
+      for (int c = 0; c < 3; ++c) comp[(size_t)c * L.n_sites + i] = v[3 * i + c];
     for (int c = 0; c < 3; ++c)
-      CUDA_TRY(cudaMemcpy2D((float*)buf + (size_t)c * L.pitch * rows, 4 * (size_t)L.pitch,
+      CUDA_TRY(cudaMemcpy2D((float*)cur + (size_t)c * L.pitch * rows, 4 * (size_t)L.pitch,
                             comp.data() + (size_t)c * L.n_sites, 4 * (size_t)L.lx, 4 * (size_t)L.lx, rows,
                             cudaMemcpyHostToDevice));
+  } else {  // multi-spin: every 64-bit word is a valid state
+    CUDA_TRY(cudaMemcpy2D(cur, 8 * (size_t)L.pitch, host, 8 * (size_t)L.lx, 8 * (size_t)L.lx, rows,
+                          cudaMemcpyHostToDevice));
   }
   std::vector<double> e;
   return sim->recompute(e, true);

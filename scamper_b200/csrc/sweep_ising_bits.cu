@@ -32,13 +32,17 @@
 namespace gpumc {
 
 // Acceptance table of the pass in the form the comparator uses.  For Ising
-// the classes with p < 1 are those with dE > 0: at most z/2 of them, so the
-// comparator handles up to three "pending" classes; every other class is
-// accepted outright.
+// the classes with p < 1 are those with dE > 0: at most z/2 of them (two on
+// the square lattice, three on the cubic), so the comparator handles up to
+// three "pending" classes; every other class is accepted outright.  The
+// 80-bit thresholds are stored as one 0/1 value per (plane, class), grouped
+// four planes to a 16-byte word so that one shared load serves a Philox
+// draw; the comparator selects a plane's threshold bits with integer
+// multiply-adds of the disjoint class masks.
 struct BitsTab {
   int npend;                  // pending classes (0..3)
   uint32_t pend_neg[3][3];    // pend_neg[i][b] = ~0 if bit b of class pc[i] is 0
-  uint32_t tsel[80][3];       // tsel[j][i] = ~0 if bit j (MSB first) of T[pc[i]] is 1
+  uint4 tq[20][3];            // tq[q][i].{x,y,z,w} = bit 4q+{0,1,2,3} (MSB first) of T[pc[i]]
 };
 
 struct BitsPhilox {
@@ -261,18 +265,29 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
     // bit-serial comparison of the 32 uniforms against their thresholds
     uint32_t lt = 0, eq = pending;
     const uint32_t ctrl0 = (uint32_t)colour | (TAG_BITS << 1);
-    for (int q = 0; q < 20; ++q) {
-      if (!__any_sync(full, eq)) break;
+    int q = 0;
+    do {
       const uint4 o = bits_philox(P, segid, ctrl0 | ((uint32_t)q << 8));
-      const uint32_t pw[4] = {o.x, o.y, o.z, o.w};
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const uint32_t* ts = tab.tsel[4 * q + h];
-        const uint32_t tj = (m[0] & ts[0]) | (m[1] & ts[1]) | (m[2] & ts[2]);
-        lt |= eq & tj & ~pw[h];
-        eq &= ~(tj ^ pw[h]);
+      const uint4 t0 = tab.tq[q][0], t1 = tab.tq[q][1];
+      uint4 tj = make_uint4(m[0] * t0.x + m[1] * t1.x, m[0] * t0.y + m[1] * t1.y,
+                            m[0] * t0.z + m[1] * t1.z, m[0] * t0.w + m[1] * t1.w);
+      if (DIM == 3) {  // a third pending class exists only for z = 6
+        const uint4 t2 = tab.tq[q][2];
+        tj.x += m[2] * t2.x;
+        tj.y += m[2] * t2.y;
+        tj.z += m[2] * t2.z;
+        tj.w += m[2] * t2.w;
       }
-    }
+      lt |= eq & tj.x & ~o.x;
+      eq &= ~(tj.x ^ o.x);
+      lt |= eq & tj.y & ~o.y;
+      eq &= ~(tj.y ^ o.y);
+      lt |= eq & tj.z & ~o.z;
+      eq &= ~(tj.z ^ o.z);
+      lt |= eq & tj.w & ~o.w;
+      eq &= ~(tj.w ^ o.w);
+      ++q;
+    } while (q < 20 && __any_sync(full, eq));
     if (active) {
       flip = (always | lt) & valid;
       const uint32_t nw = own ^ flip;
@@ -324,10 +339,9 @@ __device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, 
     if (i < np) {
       const uint32_t h = head[pc[i]];
       const unsigned long long t = tail[pc[i]];
-      const uint32_t bit = j < 16 ? (h >> (15 - j)) & 1u : (uint32_t)((t >> (79 - j)) & 1ull);
-      v = bit ? 0xFFFFFFFFu : 0u;
+      v = j < 16 ? (h >> (15 - j)) & 1u : (uint32_t)((t >> (79 - j)) & 1ull);
     }
-    tab.tsel[j][i] = v;
+    reinterpret_cast<uint32_t*>(&tab.tq[j >> 2][i])[j & 3] = v;
   }
 }
 

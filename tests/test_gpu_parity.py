@@ -148,6 +148,43 @@ def test_cold_start_and_set_spins_roundtrip(gpumc, oracle):
     mc.close()
 
 
+@pytest.mark.parametrize("model,shape,q", [("ising", (200, 34), 2), ("ising", (6, 10, 12), 2),
+                                           ("potts", (130, 18), 3), ("potts", (34, 6, 8), 4),
+                                           ("ising", (1024, 8), 2)])
+def test_set_spins_validates_on_device_and_keeps_state(gpumc, oracle, model, shape, q):
+    """set_spins stages the state on the device, checks every value
+    (validate_spin) and computes the exact energy in one pass; an invalid
+    value anywhere rejects the whole state and keeps the old one."""
+    kw = dict(beta=0.3) if model == "ising" else dict(beta=0.9, q=q)
+    mc = gpumc.ClassicalMC.from_params(_params(shape, **kw), 3, model=model)
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(11)
+    vals = np.array([-1, 1], dtype=np.int8) if model == "ising" else np.arange(q, dtype=np.int8)
+    s = rng.choice(vals, size=n)
+    mc.set_spins(0, s)
+    np.testing.assert_array_equal(mc.spins().ravel(), s)
+    mid = oracle.ISING if model == "ising" else oracle.POTTS
+    orc = oracle.Lattice(mid, shape, q=q, beta=kw["beta"], seed=3)
+    orc.set_state(s)
+    assert mc.energy()[0] == orc.energy()
+    np.testing.assert_array_equal(mc.recompute_energy(), mc.energy())
+    bad_values = [0, 2, -2] if model == "ising" else [-1, q, 100]
+    for pos in [0, n // 2 + 1, n - 1]:
+        for v in bad_values:
+            t = rng.choice(vals, size=n)
+            t[pos] = v
+            with pytest.raises(gpumc.InvalidConfig):
+                mc.set_spins(0, t)
+    np.testing.assert_array_equal(mc.spins().ravel(), s)
+    assert mc.energy()[0] == orc.energy()
+    mc.sweep(3)  # the sweeps continue from the accepted state
+    for _ in range(3):
+        orc.sweep()
+    np.testing.assert_array_equal(mc.spins().ravel(), orc.state())
+    assert mc.energy()[0] == orc.cached_energy()
+    mc.close()
+
+
 def test_philox_device_matches_known_answers_and_oracle(gpumc, oracle):
     import ctypes
     from scamper_b200 import _lib
