@@ -316,7 +316,7 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
       for (int x0 = 0; x0 < L.lx; x0 += tw) out.push_back(TileItem{lat, x0, y0, z0});
 }
 
-int kernel_kind(int model, int dims) { return model * 2 + (dims - 2); }
+int kernel_kind(const Layout& L) { return L.model * 2 + (L.dims - 2); }
 
 size_t footprint_bytes(const gpumc_spec* s) {
   const Layout L = plan_layout(s);
@@ -504,7 +504,7 @@ int gpumc_engine::rebuild_batch() {
   std::map<int, std::vector<TileItem>> tiles;
   std::map<int, std::vector<int32_t>> gids;
   for (gpumc_sim* s : sims) {
-    const int kind = kernel_kind(s->lay.model, s->lay.dims);
+    const int kind = kernel_kind(s->lay);
     BatchPlan& p = plans[kind];
     p.kind = kind;
     p.smem = std::max(p.smem, s->lay.smem);

@@ -36,7 +36,7 @@ Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots);
 int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);
 bool layout_ok(const Layout& L);
 void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out);
-int kernel_kind(int model, int dims);
+int kernel_kind(const Layout& L);
 size_t footprint_bytes(const gpumc_spec* s);
 int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
                         LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem);

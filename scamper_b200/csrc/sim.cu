@@ -100,7 +100,7 @@ int gpumc_sim::launch_msc_measurement() {
 }
 
 int gpumc_sim::launch_one_sweep() {
-  RC_TRY(launch_sweep_kernel(eng->stream, kernel_kind(lay.model, lay.dims), d_tiles, n_tiles,
+  RC_TRY(launch_sweep_kernel(eng->stream, kernel_kind(lay), d_tiles, n_tiles,
                              eng->d_lats, eng->d_groups, d_ctl, lay.smem));
   return GPUMC_OK;
 }

@@ -185,7 +185,6 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
                                           int nrows, int iters, bool owned_plane, bool write_out,
                                           int8_t* dst, const BitsTab& tab, const BitsPhilox& P,
                                           PassAcc& acc) {
-  constexpr int zc = 2 * DIM;
   const unsigned full = 0xFFFFFFFFu;
   const int cc = g.col;
   // columns this pass covers: colour 0 also updates the halo columns
