@@ -1,0 +1,68 @@
+"""Writes tests/golden/replay_fingerprints.json: SHA-256 fingerprints of the
+oracle's checkerboard replay for fixed (model, shape, beta, seed, sweeps)
+cases, with the final cached energy.  The oracle is pinned to the reference's
+own known answers and exact results by tests/test_oracle.py; these fixtures
+freeze its output so that (a) a change of the oracle shows up on the CPU and
+(b) the device is checked against committed values without running the
+oracle.  Run from the repository root:  python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import math
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+CASES = [
+    # model, shape, beta, seed, sweeps, extra
+    ("ising", [64, 64], 0.4407, 101, 6, {}),
+    ("ising", [130, 302], 0.5, 102, 3, {}),
+    ("ising", [34, 6], 0.35, 103, 8, {"J": -1.0}),
+    ("ising", [6, 8, 10], 0.2216, 104, 5, {}),
+    ("ising", [288, 6, 4], 0.3, 105, 3, {}),
+    ("potts", [130, 20], 1.0051, 106, 5, {"q": 3}),
+    ("potts", [34, 6, 36], 0.6, 107, 4, {"q": 4}),
+    ("potts", [1040, 8], 0.8814, 108, 3, {"q": 2}),
+    ("o3", [66, 10], 0.7, 109, 4, {"alpha": 1.0}),
+    ("o3", [8, 6, 20], 0.69, 110, 3, {"alpha": 0.8}),
+    ("msc", [66, 10], 0.4407, 111, 3, {}),
+    ("msc", [34, 6, 20], 0.2216, 112, 2, {}),
+]
+
+
+def omc(alpha):
+    return float(np.float32(2.0 * math.sin(0.5 * alpha) * math.sin(0.5 * alpha)))
+
+
+def fingerprint(state):
+    return hashlib.sha256(np.ascontiguousarray(state).tobytes()).hexdigest()
+
+
+def run_case(oracle, model, shape, beta, seed, sweeps, extra):
+    mid = {"ising": oracle.ISING, "potts": oracle.POTTS, "o3": oracle.O3, "msc": oracle.MSC}[model]
+    lat = oracle.Lattice(mid, tuple(shape), q=extra.get("q", 3), J=extra.get("J", 1.0), beta=beta,
+                         seed=seed, omc=omc(extra.get("alpha", 1.0)))
+    for _ in range(sweeps):
+        lat.sweep(adapt=False)
+    st = lat.state()
+    energy = float(lat.energy())
+    return {"model": model, "shape": shape, "beta": beta, "seed": seed, "sweeps": sweeps,
+            "extra": extra, "sha256": fingerprint(st), "energy": energy}
+
+
+def main():
+    import oracle
+    oracle.build()
+    out = [run_case(oracle, *c) for c in CASES]
+    path = os.path.join(ROOT, "tests", "golden", "replay_fingerprints.json")
+    with open(path, "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": out}, f, indent=1)
+    print(f"wrote {len(out)} cases to {path}")
+
+
+if __name__ == "__main__":
+    main()

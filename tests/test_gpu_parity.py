@@ -186,6 +186,41 @@ def test_set_spins_validates_on_device_and_keeps_state(gpumc, oracle, model, sha
     mc.close()
 
 
+def _golden_cases():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "replay_fingerprints.json")
+    with open(path) as f:
+        return json.load(f)["cases"]
+
+
+@pytest.mark.parametrize("case", _golden_cases(),
+                         ids=[f"{c['model']}-{'x'.join(map(str, c['shape']))}" for c in _golden_cases()])
+def test_device_matches_committed_golden_fingerprints(gpumc, case):
+    """The device against the committed fixtures, without the oracle."""
+    import hashlib
+    from scamper_b200 import _lib
+    shape, extra = tuple(case["shape"]), case["extra"]
+    params = _params(shape, beta=case["beta"], q=extra.get("q", 3), J=extra.get("J", 1.0),
+                     cone_half_angle=extra.get("alpha", 1.0))
+    if case["model"] == "msc":
+        mc = gpumc.MultiSpinIsing.from_params(params, case["seed"])
+    else:
+        mc = gpumc.ClassicalMC.from_params(params, case["seed"], model=case["model"])
+    mc.on_phase_start(_lib.PHASE_MEASUREMENT)  # no cone adaptation (O(3))
+    mc.sweep(case["sweeps"])
+    st = np.ascontiguousarray(_gpu_state(mc))
+    assert hashlib.sha256(st.tobytes()).hexdigest() == case["sha256"]
+    if case["model"] == "o3":
+        assert mc.energy()[0] == pytest.approx(case["energy"], rel=1e-9, abs=1e-9)
+    elif case["model"] == "msc":
+        e64, _ = mc.replica_observables(0)
+        assert float(e64.sum()) == case["energy"]
+    else:
+        assert mc.energy()[0] == case["energy"]
+    mc.close()
+
+
 def test_philox_device_matches_known_answers_and_oracle(gpumc, oracle):
     import ctypes
     from scamper_b200 import _lib
