@@ -35,6 +35,8 @@ template <int DIM, int COLOUR>
 __global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+__global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
+                                       uint2*, int, int);
 template <int DIM>
 __global__ void k_msc_measure(const LatDesc*, int, unsigned long long*);
 __global__ void k_msc_record(LatDesc*, GroupDesc*, int, unsigned long long*);
@@ -354,6 +356,9 @@ static int prepare_kernels() {
                                            (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
     }
+    cudaError_t e = cudaFuncSetAttribute(k_sweep_ising_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kIsingTileSmem);
+    if (e != cudaSuccess) status = e;
   });
   if (status != cudaSuccess)
     return fail(GPUMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(status));
@@ -493,7 +498,74 @@ void BatchPlan::release() {
   d_tiles = nullptr;
   d_gids = nullptr;
   d_ctl = nullptr;
+  res.release();
 }
+
+void ResidentPlan::release() {
+  if (d_nbr) cudaFree(d_nbr);
+  if (d_xchg) cudaFree(d_xchg);
+  d_nbr = nullptr;
+  d_xchg = nullptr;
+  on = false;
+}
+
+int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
+                          const std::map<int, const Layout*>& layout_of_lat, size_t smem, ResidentPlan& rp) {
+  rp.release();
+  if (tiles.empty() || smem > kIsingTileSmem) return GPUMC_OK;
+  // every tile a whole-row 2D Ising tile of >= 2 rows; a lattice's tiles are
+  // consecutive in y order (enumerate_tiles), so its neighbours are the
+  // previous and next tile of its run, cyclically
+  int wmax = 0;
+  std::vector<int2> nbr(tiles.size());
+  for (size_t i = 0; i < tiles.size();) {
+    auto it = layout_of_lat.find(tiles[i].lat);
+    if (it == layout_of_lat.end()) return GPUMC_OK;
+    const Layout& L = *it->second;
+    if (L.model != ISING || L.dims != 2 || L.tile_cx != L.pitch / 64) return GPUMC_OK;
+    size_t j = i;
+    while (j < tiles.size() && tiles[j].lat == tiles[i].lat) ++j;
+    const int n = (int)(j - i);
+    for (int k = 0; k < n; ++k) {
+      const TileItem& t = tiles[i + k];
+      if (t.x0 != 0 || t.y0 != k * L.tile_y || std::min(L.tile_y, L.ly - t.y0) < 2) return GPUMC_OK;
+      nbr[i + k] = make_int2((int)i + (k + n - 1) % n, (int)i + (k + 1) % n);
+    }
+    wmax = std::max(wmax, L.pitch / 64);
+    i = j;
+  }
+  int coop = 0, n_sm = 0, per_sm = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_ising_resident, kThreads, smem));
+  if (!coop || (int64_t)per_sm * n_sm < (int64_t)tiles.size()) return GPUMC_OK;
+  rp.xstride = 2 * 4 * wmax;
+  CUDA_TRY(cudaMalloc(&rp.d_nbr, sizeof(int2) * nbr.size()));
+  CUDA_TRY(cudaMemcpy(rp.d_nbr, nbr.data(), sizeof(int2) * nbr.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&rp.d_xchg, sizeof(uint2) * (size_t)rp.xstride * tiles.size()));
+  rp.on = true;
+  return GPUMC_OK;
+}
+
+int gpumc::launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
+                           GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
+                           int n_sweeps) {
+  // bar and err are adjacent: one memset clears both
+  CUDA_TRY(cudaMemsetAsync(&ctl->bar, 0, sizeof(unsigned int) + sizeof(int32_t), st));
+  const int2* nbr = rp.d_nbr;
+  uint2* xchg = rp.d_xchg;
+  int xstride = rp.xstride;
+  void* args[] = {(void*)&tiles, (void*)&lats, (void*)&groups, (void*)&ctl,
+                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps};
+  CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_sweep_ising_resident, dim3(n_tiles), dim3(kThreads),
+                                       args, smem, st));
+  int32_t err = 0;
+  CUDA_TRY(cudaMemcpyAsync(&err, &ctl->err, sizeof(err), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (err) return fail(GPUMC_ECUDA, "resident sweep: a grid-barrier wait timed out");
+  return GPUMC_OK;
+}
+
 
 int gpumc_engine::rebuild_batch() {
   if (!batch_dirty) return GPUMC_OK;
@@ -503,12 +575,16 @@ int gpumc_engine::rebuild_batch() {
   std::map<int, BatchPlan> plans;
   std::map<int, std::vector<TileItem>> tiles;
   std::map<int, std::vector<int32_t>> gids;
+  std::map<int, const Layout*> layout_of_lat;
   for (gpumc_sim* s : sims) {
     const int kind = kernel_kind(s->lay);
     BatchPlan& p = plans[kind];
     p.kind = kind;
     p.smem = std::max(p.smem, s->lay.smem);
-    for (int r = 0; r < s->n_rep; ++r) enumerate_tiles(s->lay, s->lat0 + r, tiles[kind]);
+    for (int r = 0; r < s->n_rep; ++r) {
+      enumerate_tiles(s->lay, s->lat0 + r, tiles[kind]);
+      layout_of_lat[s->lat0 + r] = &s->lay;
+    }
     gids[kind].push_back(s->group);
   }
   for (auto& kv : plans) {
@@ -527,14 +603,30 @@ int gpumc_engine::rebuild_batch() {
     c.n_groups = p.n_groups;
     c.group_ids = p.d_gids;
     CUDA_TRY(cudaMemcpy(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+    if (p.kind == 0) {
+      int rc = build_resident(device, tv, layout_of_lat, p.smem, p.res);
+      if (rc) {
+        p.release();
+        return rc;
+      }
+    }
     batch_plans.push_back(p);
   }
   batch_dirty = false;
   return GPUMC_OK;
 }
 
+bool gpumc_engine::has_per_sweep_work() const {
+  for (const auto& p : batch_plans)
+    if (!p.res.on) return true;
+  for (gpumc_sim* s : sims)
+    if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) return true;
+  return false;
+}
+
 int gpumc_engine::launch_batch_sweep() {
   for (auto& p : batch_plans) {
+    if (p.res.on) continue;  // resident plans run whole chunks in one launch
     int rc = launch_sweep_kernel(stream, p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
     if (rc) return rc;
   }
@@ -566,11 +658,17 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
       room = std::min<uint32_t>(room, (uint32_t)(s->rec_cap - s->rec_used));
     }
     const uint32_t chunk = std::min<uint32_t>(room, 64);
-    if (eng->use_graphs) {
-      rc = eng->run_graph(chunk);
-    } else {
-      for (uint32_t i = 0; i < chunk && rc == GPUMC_OK; ++i) rc = eng->launch_batch_sweep();
+    if (eng->has_per_sweep_work()) {
+      if (eng->use_graphs) {
+        rc = eng->run_graph(chunk);
+      } else {
+        for (uint32_t i = 0; i < chunk && rc == GPUMC_OK; ++i) rc = eng->launch_batch_sweep();
+      }
     }
+    for (auto& p : eng->batch_plans)
+      if (rc == GPUMC_OK && p.res.on)
+        rc = launch_resident(eng->stream, p.d_tiles, p.n_tiles, eng->d_lats, eng->d_groups, p.d_ctl, p.res,
+                             p.smem, (int)chunk);
     if (rc) return rc;
     for (gpumc_sim* s : eng->sims) {
       s->sweeps = std::min<uint64_t>(s->sweeps + chunk, s->target);

@@ -100,11 +100,14 @@ struct TileItem {
   int32_t lat, x0, y0, z0;
 };
 
-// Device-side bookkeeping of one launch (last-CTA epilogue).
+// Device-side bookkeeping of one launch (last-CTA epilogue; grid barrier of
+// the resident Ising kernel).
 struct LaunchCtl {
   unsigned int done;
   int32_t n_groups;
   const int32_t* group_ids;  // [n_groups] indices into the group pool
+  unsigned int bar = 0;      // resident kernel: grid-barrier arrivals of this launch
+  int32_t err = 0;           // resident kernel: 1 = a barrier wait gave up
 };
 
 }  // namespace gpumc

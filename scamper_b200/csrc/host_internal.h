@@ -47,6 +47,17 @@ size_t g_last_error_size();
 int launch_msc_record(cudaStream_t st, LatDesc* lats, GroupDesc* groups, int group,
                       unsigned long long* counters);
 
+// Resident (temporally blocked) launch of whole-row 2D Ising tiles: the
+// neighbour table (tile above / below of each tile) and the edge-row
+// exchange buffer of a tile list that qualifies (see build_resident).
+struct ResidentPlan {
+  bool on = false;
+  int2* d_nbr = nullptr;
+  uint2* d_xchg = nullptr;
+  int xstride = 0;  // uint2 words of exchange space per tile
+  void release();
+};
+
 struct BatchPlan {
   int kind = 0;
   size_t smem = 0;
@@ -55,8 +66,21 @@ struct BatchPlan {
   int32_t* d_gids = nullptr;
   int n_groups = 0;
   LaunchCtl* d_ctl = nullptr;
+  ResidentPlan res;
   void release();
 };
+
+// Qualifies a tile list for the resident Ising kernel (every tile a
+// whole-row 2D Ising tile of at least two rows, all tiles co-resident on the
+// device) and allocates its neighbour table and exchange buffer; leaves
+// rp.on false when the list does not qualify.
+int build_resident(int device, const std::vector<TileItem>& tiles,
+                   const std::map<int, const Layout*>& layout_of_lat, size_t smem, ResidentPlan& rp);
+// n_sweeps sweeps of every tile in one cooperative launch; waits for it and
+// reports a barrier timeout as an error.
+int launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
+                    GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
+                    int n_sweeps);
 
 }  // namespace gpumc
 
@@ -80,6 +104,7 @@ struct gpumc_engine {
   ~gpumc_engine();
   int rebuild_batch();
   int launch_batch_sweep();
+  bool has_per_sweep_work() const;
   int run_graph(uint32_t n);
   void drop_graphs();
   int alloc_slots(int n, int& first);
@@ -110,6 +135,7 @@ struct gpumc_sim {
   int n_tiles = 0;
   int32_t* d_gid = nullptr;
   gpumc::LaunchCtl* d_ctl = nullptr;
+  gpumc::ResidentPlan res;  // plain path: resident Ising launch, when it qualifies
   std::map<uint32_t, cudaGraphExec_t> graphs;
   uint64_t sweeps = 0;  // host mirror of the device sweep counter
   uint64_t target = ~0ull;        // sweep target (serving)

@@ -58,6 +58,7 @@ gpumc_sim::~gpumc_sim() {
   cudaFree(d_tiles);
   cudaFree(d_gid);
   cudaFree(d_ctl);
+  res.release();
 }
 
 void gpumc_sim::drop_graphs() {
@@ -316,6 +317,12 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   c.n_groups = 1;
   c.group_ids = s->d_gid;
   CUDA_CLEAN(cudaMemcpy(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  if (kernel_kind(s->lay) == 0) {
+    std::map<int, const Layout*> lay_of;
+    for (int r = 0; r < s->n_rep; ++r) lay_of[s->lat0 + r] = &s->lay;
+    rc = build_resident(eng->device, tiles, lay_of, s->lay.smem, s->res);
+    if (rc) return cleanup(rc);
+  }
   // descriptors
   const float omc = (float)(2.0 * std::sin(0.5 * spec->cone_half_angle) * std::sin(0.5 * spec->cone_half_angle));
   for (int r = 0; r < s->n_rep; ++r) {
@@ -440,7 +447,11 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
       room = std::min<uint32_t>(room, (uint32_t)(sim->rec_cap - sim->rec_used));
     }
     const uint32_t chunk = std::min<uint32_t>(room, 64);
-    RC_TRY(sim->run_graph(chunk));
+    if (sim->res.on)
+      RC_TRY(launch_resident(sim->eng->stream, sim->d_tiles, sim->n_tiles, sim->eng->d_lats, sim->eng->d_groups,
+                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk));
+    else
+      RC_TRY(sim->run_graph(chunk));
     sim->sweeps += chunk;
     if (sim->phase == GPUMC_PHASE_MEASUREMENT) sim->rec_used += (int)chunk;
     left -= chunk;

@@ -182,7 +182,7 @@ struct PassAcc {
 template <int DIM>
 __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint2* pp,
                                           const BitsGeom& g, int z, int colour, int rlo,
-                                          int nrows, int iters, bool owned_plane, bool write_out,
+                                          int nrows, int iters, bool owned_plane, int out_mode,
                                           int8_t* dst, const BitsTab& tab, const BitsPhilox& P,
                                           PassAcc& acc) {
   const unsigned full = 0xFFFFFFFFu;
@@ -298,19 +298,21 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
         acc.nacc += __popc(flip);
         acc.ksum += __popc(flip & b0) + 2 * __popc(flip & b1) + 4 * __popc(flip & b2);
       }
-      if (write_out) {
-        // both colours of this segment are final now: store the int8 row segment
+      if (out_mode != 0) {
+        // both colours of this segment are final now: count its down spins
+        // and (mode 1) store the int8 row segment
         const uint2 fin = P_ ? make_uint2(me.x, nw) : make_uint2(nw, me.y);
-        const int y = wrap_i(g.y0 - 2 + r, g.ly);
-        uint4 v0, v1, v2, v3;
-        unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
-        uint4* out = (uint4*)(dst + ((size_t)z * g.ly + y) * g.pitch + 64 * gs);
-        out[0] = v0;
-        out[1] = v1;
-        out[2] = v2;
-        out[3] = v3;
-        const uint32_t vE = valid, vO = valid;
-        acc.down += __popc(fin.x & vE) + __popc(fin.y & vO);
+        if (out_mode == 1) {
+          const int y = wrap_i(g.y0 - 2 + r, g.ly);
+          uint4 v0, v1, v2, v3;
+          unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
+          uint4* out = (uint4*)(dst + ((size_t)z * g.ly + y) * g.pitch + 64 * gs);
+          out[0] = v0;
+          out[1] = v1;
+          out[2] = v2;
+          out[3] = v3;
+        }
+        acc.down += __popc(fin.x & valid) + __popc(fin.y & valid);
         acc.owned_sites += 2 * __popc(valid);
       }
     }
@@ -318,7 +320,9 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
 }
 
 __device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, const GroupDesc* G) {
-  const int label = G->label[L->replica];
+  // the label can change between the sweeps of a resident launch: read it
+  // from L2, not from a possibly stale L1 line
+  const int label = __ldcg(&G->label[L->replica]);
   const int n = min(G->n_cls, 7);
   const uint32_t* head = G->head + label * G->n_cls;
   const unsigned long long* tail = G->tail + label * G->n_cls;
@@ -385,9 +389,9 @@ __global__ void __launch_bounds__(kThreads)
   if (DIM == 2) {
     load_bits_plane(bsm, cur, 0, g);
     __syncthreads();
-    bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, false, nxt, tab, P, acc);
+    bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nxt, tab, P, acc);
     __syncthreads();
-    bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, true, nxt, tab, P, acc);
+    bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
   } else {
     const int lz = L->lz;
     const int dv = min(L->tile_z, lz - t.z0);
@@ -400,19 +404,155 @@ __global__ void __launch_bounds__(kThreads)
       if (s >= 2) {
         const int zb = zl - 1;
         bits_pass<3>(bsm + ((s - 1) & 3) * pw, bsm + ((s - 2) & 3) * pw, Pl, g, wrap_i(zb, lz), 0, 1,
-                     g.R - 2, g.iters_black, zb >= t.z0 && zb < t.z0 + dv, false, nxt, tab, P, acc);
+                     g.R - 2, g.iters_black, zb >= t.z0 && zb < t.z0 + dv, 0, nxt, tab, P, acc);
         __syncthreads();
       }
       if (s >= 4) {
         const int zw = zl - 2;
         bits_pass<3>(bsm + ((s - 2) & 3) * pw, bsm + ((s - 3) & 3) * pw, bsm + ((s - 1) & 3) * pw, g,
-                     wrap_i(zw, lz), 1, 2, g.hv, g.iters_white, true, true, nxt, tab, P, acc);
+                     wrap_i(zw, lz), 1, 2, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
       }
       __syncthreads();  // the next load overwrites the plane slot read above
     }
   }
   flush_bits(L, acc, 2 * DIM);
   launch_epilogue(lats, groups, ctl);
+}
+
+// ---------------------------------------------------------------------------
+// Resident whole-row 2D tiles: temporal blocking across the sweeps of a launch.
+//
+// The packed parity masks of a tile (1 bit per site, 1/8 of the int8 rows)
+// stay in shared memory for all the sweeps of one cooperative launch; with
+// whole-row tiles sized to the device's CTA slots, every tile of the three
+// headline lattices (3 x 8 MiB of bits) is resident at once.  A sweep is the
+// same black and white pass as k_sweep_ising_bits, on the same random
+// stream, so the trajectory is bit-identical to the per-sweep kernel.  The
+// int8 buffer is read once at the start of the launch and the owned rows are
+// written once at the end (to the buffer of the final sweep count), so HBM
+// traffic per sweep is only the edge rows exchanged between tiles:
+//   * after its white pass a tile publishes its first two and last two owned
+//     rows (packed) to its exchange slot for that sweep's parity;
+//   * a grid barrier ends the sweep; block 0 then runs the sweep epilogue of
+//     every group (records, energy caches, sweep counters, PT exchange), and a
+//     second grid barrier publishes it;
+//   * the next sweep refreshes the tile's four halo rows from the two
+//     neighbours' slots (tile above: its last two rows; tile below: its first
+//     two) and recomputes the black halo rows as usual.
+// Every barrier wait is bounded: a CTA that waits too long (or sees another
+// CTA's error) sets ctl->err and returns, every other CTA then leaves at its
+// next barrier, and the host reports the error.  The cooperative launch
+// guarantees that all CTAs are co-resident.
+// ---------------------------------------------------------------------------
+constexpr long long kGridSpinLimit = 1ll << 22;  // polls (128 ns sleeps) per barrier wait
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t* p) {
+  return *(const volatile uint64_t*)p;
+}
+
+__device__ bool resident_grid_sync(LaunchCtl* ctl, unsigned int target) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(&ctl->bar, 1u);
+    int good = 1;
+    long long it = 0;
+    while (ld_acquire_u32(&ctl->bar) < target) {
+      if (*(volatile int32_t*)&ctl->err != 0 || ++it > kGridSpinLimit) {
+        atomicExch(&ctl->err, 1);
+        good = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+    if (good && *(volatile int32_t*)&ctl->err != 0) good = 0;
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Owned rows (local rows 2 .. hv+1) of a whole-row tile to int8 spins.
+__device__ __forceinline__ void store_owned_rows(const uint2* pl, const BitsGeom& g, int8_t* dst) {
+  if (g.row0 >= g.rstep) return;
+  const int gs = wrap_i(g.s0 + g.col - g.xh, g.nseg);
+  for (int it = 0; it < g.iters_white; ++it) {
+    const int r = 2 + g.row0 + it * g.rstep;
+    if (r >= 2 + g.hv) break;
+    const uint2 fin = pl[r * g.NC + g.col];
+    const int y = wrap_i(g.y0 - 2 + r, g.ly);
+    uint4 v0, v1, v2, v3;
+    unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
+    uint4* out = (uint4*)(dst + (size_t)y * g.pitch + 64 * gs);
+    out[0] = v0;
+    out[1] = v1;
+    out[2] = v2;
+    out[3] = v3;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 4)
+    k_sweep_ising_resident(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
+                           GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl,
+                           const int2* __restrict__ nbr, uint2* __restrict__ xchg, int xstride,
+                           int n_sweeps) {
+  extern __shared__ __align__(16) uint2 bsm[];
+  __shared__ BitsTab tab;
+  const TileItem t = tiles[blockIdx.x];
+  LatDesc* L = &lats[t.lat];
+  const GroupDesc* G = &groups[L->group];
+  const BitsGeom g = make_bits_geom(t, L);
+  const int W = g.NC;  // whole rows: one column per segment, no column halo
+  const size_t slot = (size_t)4 * W;
+  uint2* mine = xchg + (size_t)blockIdx.x * xstride;  // [parity][4 rows][W]
+  const int2 nb = nbr[blockIdx.x];
+  load_bits_plane(bsm, (const int8_t*)L->buf[ld_volatile_u64(&L->sweep) & 1], 0, g);
+  unsigned int phase = 0;
+  for (int k = 0; k < n_sweeps; ++k) {
+    const uint64_t sweep = ld_volatile_u64(&L->sweep);
+    if (sweep < L->target) {
+      if (k > 0) {
+        const uint2* up = xchg + (size_t)nb.x * xstride + ((k - 1) & 1) * slot;
+        const uint2* dn = xchg + (size_t)nb.y * xstride + ((k - 1) & 1) * slot;
+        for (int i = threadIdx.x; i < 4 * W; i += kThreads) {
+          const int sl = i / W, c = i - sl * W;
+          const int row = sl < 2 ? sl : g.hv + sl;  // local rows 0, 1, hv+2, hv+3
+          bsm[(size_t)row * W + c] = sl < 2 ? __ldcg(up + (size_t)(2 + sl) * W + c)
+                                            : __ldcg(dn + (size_t)(sl - 2) * W + c);
+        }
+      }
+      load_bits_table(tab, L, G);
+      __syncthreads();
+      const BitsPhilox P = make_bits_philox(L->key, sweep);
+      PassAcc acc = {0, 0, 0, 0};
+      bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nullptr, tab, P, acc);
+      __syncthreads();
+      bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 2, nullptr, tab, P, acc);
+      flush_bits(L, acc, 4);
+      __syncthreads();
+      uint2* out = mine + (size_t)(k & 1) * slot;
+      for (int i = threadIdx.x; i < 4 * W; i += kThreads) {
+        const int sl = i / W, c = i - sl * W;
+        const int row = sl < 2 ? 2 + sl : g.hv + sl - 2;  // local rows 2, 3, hv, hv+1
+        __stcg(out + (size_t)sl * W + c, bsm[(size_t)row * W + c]);
+      }
+    }
+    if (!resident_grid_sync(ctl, ++phase * gridDim.x)) return;
+    if (blockIdx.x == 0) {
+      const int ng = ctl->n_groups;
+      for (int gi = threadIdx.x; gi < ng; gi += blockDim.x) finish_group(lats, &groups[ctl->group_ids[gi]]);
+      __threadfence();
+    }
+    if (!resident_grid_sync(ctl, ++phase * gridDim.x)) return;
+  }
+  store_owned_rows(bsm, g, (int8_t*)L->buf[ld_volatile_u64(&L->sweep) & 1]);
 }
 
 template __global__ void k_sweep_ising_bits<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);

@@ -73,6 +73,29 @@ def test_ising_2d_bit_exact(gpumc, oracle, shape, beta):
     _run_parity(gpumc, oracle, "ising", shape, beta, seed=17, sweeps=4)[0].close()
 
 
+@pytest.mark.parametrize("shape,beta,sweeps", [((256, 300), 0.4407, 7), ((130, 302), 0.5, 5),
+                                              ((2054, 4), 0.35, 3), ((64, 64), 0.3, 70)])
+def test_ising_multi_sweep_call_matches_oracle(gpumc, oracle, shape, beta, sweeps):
+    """Many sweeps in one call (one resident launch for whole-row 2D tiles:
+    the packed tiles stay on chip and exchange edge rows between sweeps)
+    against the oracle, with every sweep's record."""
+    from scamper_b200 import _lib
+    mc = gpumc.ClassicalMC.from_params(_params(shape, beta=beta), 41, record_capacity=128)
+    mc.on_phase_start(_lib.PHASE_MEASUREMENT)
+    orc = oracle.Lattice(oracle.ISING, shape, beta=beta, seed=41)
+    mc.sweep(sweeps)
+    energies = []
+    for _ in range(sweeps):
+        orc.sweep()
+        energies.append(orc.cached_energy())
+    np.testing.assert_array_equal(mc.spins().ravel(), orc.state())
+    recs = mc.observables()
+    assert [r["energy"] for r in recs] == energies
+    assert recs[-1]["magnetization"] == pytest.approx(abs(int(orc.state().astype(np.int64).sum())) / orc.n)
+    assert mc.energy()[0] == orc.energy()
+    mc.close()
+
+
 @pytest.mark.parametrize("shape", ISING_3D)
 def test_ising_3d_bit_exact(gpumc, oracle, shape):
     _run_parity(gpumc, oracle, "ising", shape, 0.2216, seed=5, sweeps=4)[0].close()
