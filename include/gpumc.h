@@ -110,6 +110,20 @@ int gpumc_sim_engine(gpumc_sim* sim, gpumc_engine** eng);
 /* Kernel launches one sweep of this handle issues (sweep kernel plus, for a
  * measuring multi-spin handle, its measurement kernels). */
 int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n);
+/* Temporal blocking of 2D Ising sweeps (default on): when every tile of the
+ * handle's lattices fits on the device at once, a run of up to 64 sweeps is
+ * one persistent launch that keeps the packed lattice in shared memory and
+ * touches HBM only at its ends; off = one streaming launch per sweep.  Both
+ * give identical spins, energies and records.  The _engine_ form applies to
+ * gpumc_engine_sweep, the other to gpumc_sweep of one handle.  (The
+ * reference has no counterpart: its sweep is one CPU loop per chain.) */
+int gpumc_set_temporal_blocking(gpumc_sim* sim, int32_t enable);
+int gpumc_engine_set_temporal_blocking(gpumc_engine* eng, int32_t enable);
+/* Kernel launches issued so far by gpumc_sweep of this handle / by
+ * gpumc_engine_sweep of this engine (sweep, measurement and resident
+ * launches; host copies excluded). */
+int gpumc_launch_count(gpumc_sim* sim, uint64_t* n);
+int gpumc_engine_launch_count(gpumc_engine* eng, uint64_t* n);
 
 /* ---- simulation handle: ClassicalMC<H, MetropolisCore, _> ------------- */
 /* FromParams::from_params (Carlo.rs/src/monte_carlo.rs:80-88;

@@ -95,6 +95,10 @@ SIGNATURES = {
     "gpumc_engine_stream": [_vp, _P(_vp)],
     "gpumc_sim_engine": [_vp, _P(_vp)],
     "gpumc_launches_per_sweep": [_vp, _P(ctypes.c_int32)],
+    "gpumc_set_temporal_blocking": [_vp, ctypes.c_int32],
+    "gpumc_engine_set_temporal_blocking": [_vp, ctypes.c_int32],
+    "gpumc_launch_count": [_vp, _P(ctypes.c_uint64)],
+    "gpumc_engine_launch_count": [_vp, _P(ctypes.c_uint64)],
     "gpumc_create": [_vp, _P(Spec), ctypes.c_uint64, _P(_vp)],
     "gpumc_validate": [_P(Spec)],
     "gpumc_destroy": [_vp],

@@ -36,7 +36,7 @@ __global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
-                                       uint2*, int, int);
+                                       uint2*, int, int, int);
 template <int DIM>
 __global__ void k_msc_measure(const LatDesc*, int, unsigned long long*);
 __global__ void k_msc_record(LatDesc*, GroupDesc*, int, unsigned long long*);
@@ -484,6 +484,21 @@ int gpumc_sim_engine(gpumc_sim* sim, gpumc_engine** eng) {
   return GPUMC_OK;
 }
 
+int gpumc_engine_set_temporal_blocking(gpumc_engine* eng, int32_t enable) {
+  if (!eng) return fail(GPUMC_EINVAL, "engine: null");
+  if (eng->blocking != (enable != 0)) {
+    eng->blocking = enable != 0;
+    eng->drop_graphs();  // captured sweeps depend on which plans run resident
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_engine_launch_count(gpumc_engine* eng, uint64_t* n) {
+  if (!eng || !n) return fail(GPUMC_EINVAL, "null argument");
+  *n = eng->launches;
+  return GPUMC_OK;
+}
+
 int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n) {
   if (!sim || !n) return fail(GPUMC_EINVAL, "null argument");
   *n = (sim->lay.model == O3 ? 2 : 1) +
@@ -549,14 +564,15 @@ int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
 
 int gpumc::launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
                            GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
-                           int n_sweeps) {
+                           int n_sweeps, bool pt_any) {
   // bar and err are adjacent: one memset clears both
   CUDA_TRY(cudaMemsetAsync(&ctl->bar, 0, sizeof(unsigned int) + sizeof(int32_t), st));
   const int2* nbr = rp.d_nbr;
   uint2* xchg = rp.d_xchg;
   int xstride = rp.xstride;
+  int pt = pt_any ? 1 : 0;
   void* args[] = {(void*)&tiles, (void*)&lats, (void*)&groups, (void*)&ctl,
-                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps};
+                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps, (void*)&pt};
   CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_sweep_ising_resident, dim3(n_tiles), dim3(kThreads),
                                        args, smem, st));
   int32_t err = 0;
@@ -616,17 +632,21 @@ int gpumc_engine::rebuild_batch() {
   return GPUMC_OK;
 }
 
-bool gpumc_engine::has_per_sweep_work() const {
+bool gpumc_engine::has_per_sweep_work() const { return launches_per_batch_sweep() > 0; }
+
+// Kernel launches of one launch_batch_sweep (resident plans excluded).
+uint64_t gpumc_engine::launches_per_batch_sweep() const {
+  uint64_t n = 0;
   for (const auto& p : batch_plans)
-    if (!p.res.on) return true;
+    if (!(p.res.on && blocking)) n += (p.kind == 4 || p.kind == 5) ? 2 : 1;
   for (gpumc_sim* s : sims)
-    if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) return true;
-  return false;
+    if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) n += (uint64_t)s->n_rep + 1;
+  return n;
 }
 
 int gpumc_engine::launch_batch_sweep() {
   for (auto& p : batch_plans) {
-    if (p.res.on) continue;  // resident plans run whole chunks in one launch
+    if (p.res.on && blocking) continue;  // resident plans run whole chunks in one launch
     int rc = launch_sweep_kernel(stream, p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
     if (rc) return rc;
   }
@@ -664,11 +684,17 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
       } else {
         for (uint32_t i = 0; i < chunk && rc == GPUMC_OK; ++i) rc = eng->launch_batch_sweep();
       }
+      eng->launches += (uint64_t)chunk * eng->launches_per_batch_sweep();
     }
+    bool pt_any = false;  // exchanges happen inside a resident launch
+    for (gpumc_sim* s : eng->sims)
+      if (kernel_kind(s->lay) == 0 && s->pt_interval > 0) pt_any = true;
     for (auto& p : eng->batch_plans)
-      if (rc == GPUMC_OK && p.res.on)
+      if (rc == GPUMC_OK && p.res.on && eng->blocking) {
         rc = launch_resident(eng->stream, p.d_tiles, p.n_tiles, eng->d_lats, eng->d_groups, p.d_ctl, p.res,
-                             p.smem, (int)chunk);
+                             p.smem, (int)chunk, pt_any);
+        eng->launches += 1;
+      }
     if (rc) return rc;
     for (gpumc_sim* s : eng->sims) {
       s->sweeps = std::min<uint64_t>(s->sweeps + chunk, s->target);

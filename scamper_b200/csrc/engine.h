@@ -69,6 +69,7 @@ struct LatDesc {
   float omc;                        // O(3): 1 - cos(cone half-angle)
   int32_t adapt;                    // O(3): adapt omc during this sweep
   Accum acc;
+  Accum acc2;                       // resident kernel: accumulators of odd launch-local sweeps
 };
 
 // A group is a set of lattices that share a temperature ladder and a record

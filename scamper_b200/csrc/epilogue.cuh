@@ -64,7 +64,8 @@ static __device__ void pt_exchange(LatDesc* lats, GroupDesc* G) {
   G->pt_accepted += accepted;
 }
 
-static __device__ void finish_group(LatDesc* lats, GroupDesc* G) {
+// slot 1 drains the second accumulator set (odd sweeps of a resident launch).
+static __device__ void finish_group(LatDesc* lats, GroupDesc* G, int slot = 0) {
   if (lats[G->first_lat].sweep >= lats[G->first_lat].target) return;  // finished job
   // multi-spin records (64 per word lattice) are written by k_msc_record
   const bool msc = lats[G->first_lat].model == MSC;
@@ -73,18 +74,19 @@ static __device__ void finish_group(LatDesc* lats, GroupDesc* G) {
   uint64_t sweep_after = 0;
   for (int r = 0; r < G->n_rep; ++r) {
     LatDesc* L = &lats[G->first_lat + r];
-    const long long dE = take_i64(&L->acc.dE);
-    const long long nacc = take_i64(&L->acc.accepted);
-    const long long mag = take_i64(&L->acc.mag);
+    Accum* A = slot ? &L->acc2 : &L->acc;
+    const long long dE = take_i64(&A->dE);
+    const long long nacc = take_i64(&A->accepted);
+    const long long mag = take_i64(&A->mag);
     Record R;
     R.m[0] = R.m[1] = R.m[2] = 0.0;
     if (L->model == O3) {
-      const double dEf = take_f64(&L->acc.dEf);
+      const double dEf = take_f64(&A->dEf);
       L->e_f += dEf;
       R.energy = L->e_f;
-      R.m[0] = take_f64(&L->acc.mx);
-      R.m[1] = take_f64(&L->acc.my);
-      R.m[2] = take_f64(&L->acc.mz);
+      R.m[0] = take_f64(&A->mx);
+      R.m[1] = take_f64(&A->my);
+      R.m[2] = take_f64(&A->mz);
       if (L->adapt && L->sweep < G->adapt_until) L->omc = o3_adapt(L->omc, nacc, L->n_sites);
     } else {
       L->e_int += dE;
@@ -92,7 +94,7 @@ static __device__ void finish_group(LatDesc* lats, GroupDesc* G) {
       if (L->model == POTTS) {
         long long best = 0;
         for (int s = 0; s < kMaxPottsCounts; ++s) {
-          const long long c = take_i64(&L->acc.counts[s]);
+          const long long c = take_i64(&A->counts[s]);
           best = c > best ? c : best;
         }
         R.m[0] = (double)best;

@@ -80,7 +80,7 @@ int build_resident(int device, const std::vector<TileItem>& tiles,
 // reports a barrier timeout as an error.
 int launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
                     GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
-                    int n_sweeps);
+                    int n_sweeps, bool pt_any);
 
 }  // namespace gpumc
 
@@ -97,6 +97,8 @@ struct gpumc_engine {
   std::set<gpumc_sim*> sims;
   bool batch_dirty = true;
   bool use_graphs = true;
+  bool blocking = true;       // temporal blocking of qualifying Ising plans
+  uint64_t launches = 0;      // kernel launches issued by gpumc_engine_sweep
   int slots = gpumc::kDefaultSlots;  // resident sweep CTAs of the device (tile planning)
   std::vector<gpumc::BatchPlan> batch_plans;
   std::map<uint32_t, cudaGraphExec_t> batch_graphs;
@@ -105,6 +107,7 @@ struct gpumc_engine {
   int rebuild_batch();
   int launch_batch_sweep();
   bool has_per_sweep_work() const;
+  uint64_t launches_per_batch_sweep() const;
   int run_graph(uint32_t n);
   void drop_graphs();
   int alloc_slots(int n, int& first);
@@ -136,6 +139,8 @@ struct gpumc_sim {
   int32_t* d_gid = nullptr;
   gpumc::LaunchCtl* d_ctl = nullptr;
   gpumc::ResidentPlan res;  // plain path: resident Ising launch, when it qualifies
+  bool blocking = true;      // plain path: use `res` when it is on
+  uint64_t launches = 0;     // kernel launches issued by gpumc_sweep
   std::map<uint32_t, cudaGraphExec_t> graphs;
   uint64_t sweeps = 0;  // host mirror of the device sweep counter
   uint64_t target = ~0ull;        // sweep target (serving)

@@ -447,11 +447,16 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
       room = std::min<uint32_t>(room, (uint32_t)(sim->rec_cap - sim->rec_used));
     }
     const uint32_t chunk = std::min<uint32_t>(room, 64);
-    if (sim->res.on)
+    if (sim->res.on && sim->blocking) {
       RC_TRY(launch_resident(sim->eng->stream, sim->d_tiles, sim->n_tiles, sim->eng->d_lats, sim->eng->d_groups,
-                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk));
-    else
+                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk, sim->pt_interval > 0));
+      sim->launches += 1;
+    } else {
       RC_TRY(sim->run_graph(chunk));
+      int32_t lps = 0;
+      gpumc_launches_per_sweep(sim, &lps);
+      sim->launches += (uint64_t)chunk * (uint64_t)lps;
+    }
     sim->sweeps += chunk;
     if (sim->phase == GPUMC_PHASE_MEASUREMENT) sim->rec_used += (int)chunk;
     left -= chunk;
@@ -608,6 +613,18 @@ int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* 
     energy64[r] = -sim->spec.J * (bonds - 2.0 * (double)h[64 + r]);
     mag64[r] = std::fabs(2.0 * (double)h[r] - n) / n;
   }
+  return GPUMC_OK;
+}
+
+int gpumc_set_temporal_blocking(gpumc_sim* sim, int32_t enable) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  sim->blocking = enable != 0;
+  return GPUMC_OK;
+}
+
+int gpumc_launch_count(gpumc_sim* sim, uint64_t* n) {
+  if (!sim || !n) return fail(GPUMC_EINVAL, "null argument");
+  *n = sim->launches;
   return GPUMC_OK;
 }
 

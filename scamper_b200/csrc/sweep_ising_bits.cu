@@ -348,7 +348,7 @@ __device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, 
   }
 }
 
-__device__ __forceinline__ void flush_bits(LatDesc* L, const PassAcc& a, int zc) {
+__device__ __forceinline__ void flush_bits(Accum* A, const PassAcc& a, int zc) {
   long long dE = 2LL * zc * a.nacc - 4LL * a.ksum;
   long long mag = (long long)a.owned_sites - 2LL * a.down;
   long long nacc = a.nacc;
@@ -360,9 +360,9 @@ __device__ __forceinline__ void flush_bits(LatDesc* L, const PassAcc& a, int zc)
     nacc += __shfl_xor_sync(full, nacc, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    if (dE) atomic_add_i64(&L->acc.dE, dE);
-    if (mag) atomic_add_i64(&L->acc.mag, mag);
-    if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
+    if (dE) atomic_add_i64(&A->dE, dE);
+    if (mag) atomic_add_i64(&A->mag, mag);
+    if (nacc) atomic_add_i64(&A->accepted, nacc);
   }
 }
 
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(kThreads)
       __syncthreads();  // the next load overwrites the plane slot read above
     }
   }
-  flush_bits(L, acc, 2 * DIM);
+  flush_bits(&L->acc, acc, 2 * DIM);
   launch_epilogue(lats, groups, ctl);
 }
 
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_ising_resident(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                            GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl,
                            const int2* __restrict__ nbr, uint2* __restrict__ xchg, int xstride,
-                           int n_sweeps) {
+                           int n_sweeps, int pt_any) {
   extern __shared__ __align__(16) uint2 bsm[];
   __shared__ BitsTab tab;
   const TileItem t = tiles[blockIdx.x];
@@ -513,11 +513,15 @@ __global__ void __launch_bounds__(kThreads, 4)
   const size_t slot = (size_t)4 * W;
   uint2* mine = xchg + (size_t)blockIdx.x * xstride;  // [parity][4 rows][W]
   const int2 nb = nbr[blockIdx.x];
-  load_bits_plane(bsm, (const int8_t*)L->buf[ld_volatile_u64(&L->sweep) & 1], 0, g);
+  // sweep index of launch-local iteration k: s0 + k (the epilogue advances
+  // L->sweep the same way, stopping at the target)
+  const uint64_t s0 = ld_volatile_u64(&L->sweep);
+  const uint64_t target = L->target;
+  load_bits_plane(bsm, (const int8_t*)L->buf[s0 & 1], 0, g);
   unsigned int phase = 0;
   for (int k = 0; k < n_sweeps; ++k) {
-    const uint64_t sweep = ld_volatile_u64(&L->sweep);
-    if (sweep < L->target) {
+    const uint64_t sweep = s0 + (uint64_t)k;
+    if (sweep < target) {
       if (k > 0) {
         const uint2* up = xchg + (size_t)nb.x * xstride + ((k - 1) & 1) * slot;
         const uint2* dn = xchg + (size_t)nb.y * xstride + ((k - 1) & 1) * slot;
@@ -535,7 +539,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nullptr, tab, P, acc);
       __syncthreads();
       bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 2, nullptr, tab, P, acc);
-      flush_bits(L, acc, 4);
+      flush_bits((k & 1) ? &L->acc2 : &L->acc, acc, 4);
       __syncthreads();
       uint2* out = mine + (size_t)(k & 1) * slot;
       for (int i = threadIdx.x; i < 4 * W; i += kThreads) {
@@ -546,13 +550,19 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
     if (!resident_grid_sync(ctl, ++phase * gridDim.x)) return;
     if (blockIdx.x == 0) {
+      // the epilogue of sweep k drains accumulator slot k & 1, which no CTA
+      // touches again before the next barrier (its next use is sweep k + 2)
       const int ng = ctl->n_groups;
-      for (int gi = threadIdx.x; gi < ng; gi += blockDim.x) finish_group(lats, &groups[ctl->group_ids[gi]]);
+      for (int gi = threadIdx.x; gi < ng; gi += blockDim.x)
+        finish_group(lats, &groups[ctl->group_ids[gi]], k & 1);
       __threadfence();
     }
-    if (!resident_grid_sync(ctl, ++phase * gridDim.x)) return;
+    // a PT exchange changes labels (acceptance tables) for the next sweep:
+    // then every CTA waits for the epilogue
+    if (pt_any && !resident_grid_sync(ctl, ++phase * gridDim.x)) return;
   }
-  store_owned_rows(bsm, g, (int8_t*)L->buf[ld_volatile_u64(&L->sweep) & 1]);
+  const uint64_t s_end = s0 + (uint64_t)n_sweeps < target ? s0 + (uint64_t)n_sweeps : (s0 > target ? s0 : target);
+  store_owned_rows(bsm, g, (int8_t*)L->buf[s_end & 1]);
 }
 
 template __global__ void k_sweep_ising_bits<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);

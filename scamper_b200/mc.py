@@ -134,6 +134,14 @@ class Engine:
         _lib.call("gpumc_engine_stream", self.h, ctypes.byref(v))
         return v.value
 
+    def set_temporal_blocking(self, enable):
+        _lib.call("gpumc_engine_set_temporal_blocking", self.h, 1 if enable else 0)
+
+    def launch_count(self):
+        v = ctypes.c_uint64()
+        _lib.call("gpumc_engine_launch_count", self.h, ctypes.byref(v))
+        return v.value
+
     def close(self):
         if self.h:
             _lib.call("gpumc_engine_destroy", self.h)
@@ -264,6 +272,17 @@ class ClassicalMC:
     def launches_per_sweep(self):
         v = ctypes.c_int32()
         _lib.call("gpumc_launches_per_sweep", self.h, ctypes.byref(v))
+        return v.value
+
+    def set_temporal_blocking(self, enable):
+        """Run qualifying 2D Ising sweeps as resident multi-sweep launches
+        (default) or as one streaming launch per sweep; results identical."""
+        _lib.call("gpumc_set_temporal_blocking", self.h, 1 if enable else 0)
+
+    def launch_count(self):
+        """Kernel launches issued so far by this handle's sweeps."""
+        v = ctypes.c_uint64()
+        _lib.call("gpumc_launch_count", self.h, ctypes.byref(v))
         return v.value
 
     def sweep_count(self):

@@ -112,6 +112,49 @@ def test_batched_engine_matches_plain_path(gpumc):
     eng.close()
 
 
+@pytest.mark.parametrize("shape,n_rep,interval", [((256, 300), 3, 0), ((8, 6), 8, 3), ((1024, 64), 2, 0)])
+def test_temporal_blocking_matches_streaming_kernel(gpumc, shape, n_rep, interval):
+    """Resident multi-sweep launches (temporal blocking) and one streaming
+    launch per sweep give the same spins, energies, records and PT labels,
+    on the plain path and in a batched engine."""
+    from scamper_b200 import _lib
+    betas = gpumc.geometric_ladder_betas(1.5, 3.5, n_rep)
+    runs = []
+    for blocking in (True, False):
+        mc = gpumc.ClassicalMC.from_params(_params(shape), 77, model="ising", n_replicas=n_rep,
+                                           betas=betas, record_capacity=256)
+        mc.set_temporal_blocking(blocking)
+        mc.on_phase_start(_lib.PHASE_MEASUREMENT)
+        if interval:
+            mc.pt_configure(interval)
+        n0 = mc.launch_count()
+        mc.sweep(150)
+        launches = mc.launch_count() - n0
+        recs = mc.observables()
+        runs.append((np.stack([mc.spins(r) for r in range(n_rep)]), mc.energy(),
+                     [(r["sweep"], r["replica"], r["energy"], r["magnetization"], r["temp_index"]) for r in recs],
+                     mc.pt_labels(), launches))
+        mc.close()
+    (s1, e1, r1, l1, n1), (s2, e2, r2, l2, n2) = runs
+    np.testing.assert_array_equal(s1, s2)
+    np.testing.assert_array_equal(e1, e2)
+    assert r1 == r2 and len(r1) == 150 * n_rep
+    np.testing.assert_array_equal(l1, l2)
+    assert n2 == 150 and n1 == 3  # 150 streaming launches vs 3 resident chunks of <= 64 sweeps
+    eng_runs = []
+    for blocking in (True, False):
+        eng = gpumc.Engine()
+        eng.set_temporal_blocking(blocking)
+        mc = gpumc.ClassicalMC.from_params(_params(shape), 78, model="ising", n_replicas=n_rep, betas=betas,
+                                           engine=eng)
+        eng.sweep(70)
+        eng_runs.append((np.stack([mc.spins(r) for r in range(n_rep)]), mc.energy()))
+        mc.close()
+        eng.close()
+    np.testing.assert_array_equal(eng_runs[0][0], eng_runs[1][0])
+    np.testing.assert_array_equal(eng_runs[0][1], eng_runs[1][1])
+
+
 def test_server_results_identical_alone_and_in_mix(gpumc):
     """Continuous batching: jobs admitted while others run give the same
     spins as the same job run alone through the plain path."""
