@@ -36,7 +36,7 @@ __global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
-                                       uint2*, int, int, int);
+                                       uint2*, int, int);
 template <int DIM>
 __global__ void k_msc_measure(const LatDesc*, int, unsigned long long*);
 __global__ void k_msc_record(LatDesc*, GroupDesc*, int, unsigned long long*);
@@ -210,7 +210,7 @@ int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots) {
   return best;
 }
 
-Layout plan_layout(const gpumc_spec* s, int slots) {
+Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
   Layout L;
   L.model = s->model;
   L.dims = s->dims;
@@ -236,6 +236,28 @@ Layout plan_layout(const gpumc_spec* s, int slots) {
       L.tile_y = ising_tile_rows(ly, std::max<int>(1, (int)s->n_replicas), nseg, hv_max, slots);
       L.tile_z = 1;
       L.smem = 8 * (size_t)(L.tile_y + 4) * nseg;
+    } else if (L.dims == 3 && nseg <= 256 && (size_t)ly * nseg * 8 * 4 <= kIsingTileSmem) {
+      // whole-plane 3D tiles: four packed planes in the ring, rows wrap
+      // inside the tile (no y halo); the z extent per tile minimises
+      // (CTA waves) x (planes loaded + black-updated + white-updated)
+      L.tile_cx = nseg;
+      L.tile_y = ly;
+      const int n_rep = std::max<int>(1, (int)s->n_replicas);
+      int best = std::min(lz, 16);
+      double best_t = 1e300;
+      for (int ntz = 1; ntz <= lz; ++ntz) {
+        const int dv = (lz + ntz - 1) / ntz;
+        if (dv < 4 && dv < lz) break;
+        const int tiles = ((lz + dv - 1) / dv) * n_rep;
+        const double waves = std::max(1.0, std::ceil((double)tiles / slots3));
+        const double t = waves * (3.0 * dv + 6.0);
+        if (t < best_t - 1e-9) {
+          best_t = t;
+          best = dv;
+        }
+      }
+      L.tile_z = best;
+      L.smem = 4 * 8 * (size_t)ly * nseg;
     } else {
       const bool xsplit = (lx % 64 == 0) && nseg > 32;
       L.tile_cx = xsplit ? 32 : nseg;
@@ -438,6 +460,13 @@ int gpumc_engine_create(int32_t device, gpumc_engine** out) {
     return fail(GPUMC_ECUDA, std::string("device query: ") + cudaGetErrorString(err));
   }
   e->slots = std::max(1, n_sm * std::max(1, per_sm));
+  int per_sm3 = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_sweep_ising_bits<3>, kThreads, 16 * 1024);
+  if (err != cudaSuccess) {
+    delete e;
+    return fail(GPUMC_ECUDA, std::string("device query: ") + cudaGetErrorString(err));
+  }
+  e->slots3 = std::max(1, n_sm * std::max(1, per_sm3));
   e->lat_used.assign(e->lat_cap, false);
   e->group_used.assign(e->group_cap, false);
   *out = e;
@@ -564,15 +593,14 @@ int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
 
 int gpumc::launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
                            GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
-                           int n_sweeps, bool pt_any) {
-  // bar and err are adjacent: one memset clears both
-  CUDA_TRY(cudaMemsetAsync(&ctl->bar, 0, sizeof(unsigned int) + sizeof(int32_t), st));
+                           int n_sweeps) {
+  // bar, err and epi are adjacent: one memset clears them
+  CUDA_TRY(cudaMemsetAsync(&ctl->bar, 0, 2 * sizeof(unsigned int) + sizeof(int32_t), st));
   const int2* nbr = rp.d_nbr;
   uint2* xchg = rp.d_xchg;
   int xstride = rp.xstride;
-  int pt = pt_any ? 1 : 0;
   void* args[] = {(void*)&tiles, (void*)&lats, (void*)&groups, (void*)&ctl,
-                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps, (void*)&pt};
+                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps};
   CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_sweep_ising_resident, dim3(n_tiles), dim3(kThreads),
                                        args, smem, st));
   int32_t err = 0;
@@ -686,13 +714,10 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
       }
       eng->launches += (uint64_t)chunk * eng->launches_per_batch_sweep();
     }
-    bool pt_any = false;  // exchanges happen inside a resident launch
-    for (gpumc_sim* s : eng->sims)
-      if (kernel_kind(s->lay) == 0 && s->pt_interval > 0) pt_any = true;
     for (auto& p : eng->batch_plans)
       if (rc == GPUMC_OK && p.res.on && eng->blocking) {
         rc = launch_resident(eng->stream, p.d_tiles, p.n_tiles, eng->d_lats, eng->d_groups, p.d_ctl, p.res,
-                             p.smem, (int)chunk, pt_any);
+                             p.smem, (int)chunk);
         eng->launches += 1;
       }
     if (rc) return rc;

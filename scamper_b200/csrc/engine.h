@@ -109,6 +109,7 @@ struct LaunchCtl {
   const int32_t* group_ids;  // [n_groups] indices into the group pool
   unsigned int bar = 0;      // resident kernel: grid-barrier arrivals of this launch
   int32_t err = 0;           // resident kernel: 1 = a barrier wait gave up
+  unsigned int epi = 0;      // resident kernel: launch-local sweeps whose epilogue is done
 };
 
 }  // namespace gpumc

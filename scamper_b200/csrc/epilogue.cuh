@@ -35,87 +35,169 @@ __device__ __forceinline__ float o3_adapt(float omc, long long accepted, long lo
   return w;
 }
 
-static __device__ void pt_exchange(LatDesc* lats, GroupDesc* G) {
-  const int n = G->n_rep;
-  if (n < 2 || n > kMaxPtReplicas) return;
-  const uint64_t step = ++G->pt_step;
-  int32_t* at = G->rep_at;
-  for (int r = 0; r < n; ++r) at[G->label[r]] = r;
-  const int offset = (int)((step - 1) & 1u);
-  unsigned long long accepted = 0;
-  for (int t = offset; t + 1 < n; t += 2) {
-    const int a = at[t], b = at[t + 1];
-    const LatDesc* La = &lats[G->first_lat + a];
-    const LatDesc* Lb = &lats[G->first_lat + b];
-    const double ea = La->model == O3 ? La->e_f : G->J * (double)La->e_int;
-    const double eb = Lb->model == O3 ? Lb->e_f : G->J * (double)Lb->e_int;
-    const double wa = (G->betas[t] - G->betas[t + 1]) * ea;
-    const double wb = (G->betas[t + 1] - G->betas[t]) * eb;
-    const uint4 o = draw(G->pt_key, (uint64_t)t, 0u, TAG_PT, 0u, step);
-    const unsigned long long u = (unsigned long long)o.x | ((unsigned long long)o.y << 32);
-    if (accept_log(wa + wb, u)) {
-      G->label[a] = t + 1;
-      G->label[b] = t;
-      at[t] = b;
-      at[t + 1] = a;
-      ++accepted;
+// Epilogue flags of a group for the sweep being finished (GroupDesc::epi).
+constexpr int32_t kEpiFinished = 1, kEpiMeasuring = 2, kEpiRecord = 4, kEpiMsc = 8, kEpiExchange = 16;
+
+// Per-replica part of the sweep epilogue: drain the accumulators of slot
+// `slot`, update the cached energy, write the record, advance the sweep.
+static __device__ void finish_replica(LatDesc* lats, GroupDesc* G, int r, int32_t flags, int slot) {
+  LatDesc* L = &lats[G->first_lat + r];
+  Accum* A = slot ? &L->acc2 : &L->acc;
+  const long long dE = take_i64(&A->dE);
+  const long long nacc = take_i64(&A->accepted);
+  const long long mag = take_i64(&A->mag);
+  Record R;
+  R.m[0] = R.m[1] = R.m[2] = 0.0;
+  if (L->model == O3) {
+    const double dEf = take_f64(&A->dEf);
+    L->e_f += dEf;
+    R.energy = L->e_f;
+    R.m[0] = take_f64(&A->mx);
+    R.m[1] = take_f64(&A->my);
+    R.m[2] = take_f64(&A->mz);
+    if (L->adapt && L->sweep < G->adapt_until) L->omc = o3_adapt(L->omc, nacc, L->n_sites);
+  } else {
+    L->e_int += dE;
+    R.energy = G->J * (double)L->e_int;
+    if (L->model == POTTS) {
+      long long best = 0;
+      for (int s = 0; s < kMaxPottsCounts; ++s) {
+        const long long c = take_i64(&A->counts[s]);
+        best = c > best ? c : best;
+      }
+      R.m[0] = (double)best;
+    } else {
+      R.m[0] = (double)mag;
     }
   }
-  G->pt_accepted += accepted;
+  R.accepted = (double)nacc;
+  R.label = G->label[r];
+  R.pad = 0;
+  R.sweep = L->sweep;
+  if (flags & kEpiRecord) G->records[(size_t)G->rec_count * G->n_rep + r] = R;
+  L->sweep += 1;
 }
 
-// slot 1 drains the second accumulator set (odd sweeps of a resident launch).
-static __device__ void finish_group(LatDesc* lats, GroupDesc* G, int slot = 0) {
-  if (lats[G->first_lat].sweep >= lats[G->first_lat].target) return;  // finished job
-  // multi-spin records (64 per word lattice) are written by k_msc_record
-  const bool msc = lats[G->first_lat].model == MSC;
-  const bool measuring = G->measure && lats[G->first_lat].sweep >= G->measure_from;
-  const bool rec = !msc && measuring && G->rec_count < G->rec_cap;
-  uint64_t sweep_after = 0;
-  for (int r = 0; r < G->n_rep; ++r) {
-    LatDesc* L = &lats[G->first_lat + r];
-    Accum* A = slot ? &L->acc2 : &L->acc;
-    const long long dE = take_i64(&A->dE);
-    const long long nacc = take_i64(&A->accepted);
-    const long long mag = take_i64(&A->mag);
-    Record R;
-    R.m[0] = R.m[1] = R.m[2] = 0.0;
-    if (L->model == O3) {
-      const double dEf = take_f64(&A->dEf);
-      L->e_f += dEf;
-      R.energy = L->e_f;
-      R.m[0] = take_f64(&A->mx);
-      R.m[1] = take_f64(&A->my);
-      R.m[2] = take_f64(&A->mz);
-      if (L->adapt && L->sweep < G->adapt_until) L->omc = o3_adapt(L->omc, nacc, L->n_sites);
-    } else {
-      L->e_int += dE;
-      R.energy = G->J * (double)L->e_int;
-      if (L->model == POTTS) {
-        long long best = 0;
-        for (int s = 0; s < kMaxPottsCounts; ++s) {
-          const long long c = take_i64(&A->counts[s]);
-          best = c > best ? c : best;
-        }
-        R.m[0] = (double)best;
+// Sweep epilogue of the groups ids[0..ng), run by one whole CTA of kThreads
+// threads (every thread must call it).  Groups are taken kThreads at a time;
+// per batch, phases separated by block barriers:
+//   0. one thread per group decides (from the state before the sweep
+//      counter moves) whether the group is finished, measuring, recording,
+//      and the batch's replica counts are prefix-summed in shared memory;
+//   1. one thread per (group, replica) runs finish_replica (the group of a
+//      flattened replica index is found by binary search over the offsets);
+//   2. one thread per group counts the record and decides whether a PT
+//      exchange is due (sweep count a multiple of the interval);
+//   3. for each group with an exchange due, one thread per neighbour pair:
+//      the pairs of one exchange step are disjoint and their decisions
+//      independent, so they run in parallel with the same outcome as a
+//      sequential loop over t = offset, offset + 2, ...
+// Multi-spin records (64 per word lattice) are written by k_msc_record.
+static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int32_t* ids, int ng,
+                                     int slot) {
+  __shared__ int s_off[kThreads + 1];
+  __shared__ int32_t s_f[kThreads];
+  __shared__ int s_due[kThreads];
+  __shared__ int s_ndue;
+  __shared__ unsigned long long s_acc;
+  const int t = threadIdx.x;
+  for (int base = 0; base < ng; base += kThreads) {
+    const int nb = min(kThreads, ng - base);
+    GroupDesc* G = t < nb ? &groups[ids[base + t]] : nullptr;
+    int n = 0;
+    if (G) {
+      const LatDesc* L0 = &lats[G->first_lat];
+      int32_t f = 0;
+      if (L0->sweep >= L0->target) {
+        f = kEpiFinished;
       } else {
-        R.m[0] = (double)mag;
+        const bool msc = L0->model == MSC;
+        const bool measuring = G->measure && L0->sweep >= G->measure_from;
+        f = (msc ? kEpiMsc : 0) | (measuring ? kEpiMeasuring : 0) |
+            ((!msc && measuring && G->rec_count < G->rec_cap) ? kEpiRecord : 0);
+        n = G->n_rep;
+      }
+      s_f[t] = f;
+    }
+    // inclusive scan of n over the batch: warp scans, then warp totals
+    int v = n;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+      if ((t & 31) >= o) v += u;
+    }
+    __shared__ int s_warp[kThreads / 32];
+    if ((t & 31) == 31) s_warp[t >> 5] = v;
+    if (t == 0) {
+      s_ndue = 0;
+      s_off[0] = 0;
+    }
+    __syncthreads();
+    int add = 0;
+    for (int w = 0; w < (t >> 5); ++w) add += s_warp[w];
+    s_off[t + 1] = v + add;  // s_off[i] = replicas of groups base .. base + i - 1
+    __syncthreads();
+    const int total = s_off[nb];
+    for (int fi = t; fi < total; fi += kThreads) {
+      int lo = 0, hi = nb - 1;  // last group index with s_off[g] <= fi
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_off[mid] <= fi) lo = mid;
+        else hi = mid - 1;
+      }
+      finish_replica(lats, &groups[ids[base + lo]], fi - s_off[lo], s_f[lo], slot);
+    }
+    __syncthreads();
+    if (G) {
+      const int32_t f = s_f[t];
+      if (!(f & kEpiFinished)) {
+        if ((f & kEpiMeasuring) && !(f & kEpiMsc)) {
+          if (f & kEpiRecord) G->rec_count += 1;
+          else G->overflow = 1;
+        }
+        const uint64_t sweep_after = lats[G->first_lat].sweep;
+        if (G->pt_interval > 0 && sweep_after > 0 && (sweep_after % (uint64_t)G->pt_interval) == 0 &&
+            G->n_rep >= 2 && G->n_rep <= kMaxPtReplicas) {
+          G->pt_step += 1;
+          s_due[atomicAdd(&s_ndue, 1)] = base + t;
+        }
       }
     }
-    R.accepted = (double)nacc;
-    R.label = G->label[r];
-    R.pad = 0;
-    R.sweep = L->sweep;
-    if (rec) G->records[(size_t)G->rec_count * G->n_rep + r] = R;
-    L->sweep += 1;
-    sweep_after = L->sweep;
+    __syncthreads();
+    const int ndue = s_ndue;
+    for (int i = 0; i < ndue; ++i) {
+      GroupDesc* H = &groups[ids[s_due[i]]];
+      const int m = H->n_rep;
+      const uint64_t step = H->pt_step;
+      int32_t* at = H->rep_at;
+      if (t == 0) s_acc = 0;
+      for (int r = t; r < m; r += kThreads) at[H->label[r]] = r;
+      __syncthreads();
+      const int offset = (int)((step - 1) & 1u);
+      for (int p = t; offset + 2 * p + 1 < m; p += kThreads) {
+        const int tt = offset + 2 * p;
+        const int a = at[tt], b = at[tt + 1];
+        const LatDesc* La = &lats[H->first_lat + a];
+        const LatDesc* Lb = &lats[H->first_lat + b];
+        const double ea = La->model == O3 ? La->e_f : H->J * (double)La->e_int;
+        const double eb = Lb->model == O3 ? Lb->e_f : H->J * (double)Lb->e_int;
+        const double wa = (H->betas[tt] - H->betas[tt + 1]) * ea;
+        const double wb = (H->betas[tt + 1] - H->betas[tt]) * eb;
+        const uint4 o = draw(H->pt_key, (uint64_t)tt, 0u, TAG_PT, 0u, step);
+        const unsigned long long u = (unsigned long long)o.x | ((unsigned long long)o.y << 32);
+        if (accept_log(wa + wb, u)) {
+          H->label[a] = tt + 1;
+          H->label[b] = tt;
+          at[tt] = b;
+          at[tt + 1] = a;
+          atomicAdd(&s_acc, 1ull);
+        }
+      }
+      __syncthreads();
+      if (t == 0) H->pt_accepted += s_acc;
+      __syncthreads();
+    }
+    __syncthreads();  // the next batch rewrites the shared arrays read above
   }
-  if (measuring && !msc) {
-    if (rec) G->rec_count += 1;
-    else G->overflow = 1;
-  }
-  if (G->pt_interval > 0 && sweep_after > 0 && (sweep_after % (uint64_t)G->pt_interval) == 0)
-    pt_exchange(lats, G);
 }
 
 __device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl) {
@@ -129,8 +211,7 @@ __device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  const int ng = ctl->n_groups;
-  for (int gi = threadIdx.x; gi < ng; gi += blockDim.x) finish_group(lats, &groups[ctl->group_ids[gi]]);
+  finish_groups(lats, groups, ctl->group_ids, ctl->n_groups, 0);
   __syncthreads();
   if (threadIdx.x == 0) ctl->done = 0;
 }

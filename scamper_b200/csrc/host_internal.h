@@ -32,7 +32,8 @@ int validate_spec(const gpumc_spec* s);
 // passes its device's own count.
 constexpr int kDefaultSlots = 148 * 4;
 constexpr size_t kIsingTileSmem = 48 * 1024;  // whole-row Ising tile budget
-Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots);
+constexpr int kDefaultSlots3 = 148 * 2;  // resident 3D Ising sweep CTAs of one B200
+Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots, int slots3 = kDefaultSlots3);
 int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);
 bool layout_ok(const Layout& L);
 void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out);
@@ -80,7 +81,7 @@ int build_resident(int device, const std::vector<TileItem>& tiles,
 // reports a barrier timeout as an error.
 int launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
                     GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
-                    int n_sweeps, bool pt_any);
+                    int n_sweeps);
 
 }  // namespace gpumc
 
@@ -100,6 +101,7 @@ struct gpumc_engine {
   bool blocking = true;       // temporal blocking of qualifying Ising plans
   uint64_t launches = 0;      // kernel launches issued by gpumc_engine_sweep
   int slots = gpumc::kDefaultSlots;  // resident sweep CTAs of the device (tile planning)
+  int slots3 = gpumc::kDefaultSlots3;  // the same for the 3D Ising kernel
   std::vector<gpumc::BatchPlan> batch_plans;
   std::map<uint32_t, cudaGraphExec_t> batch_graphs;
 

@@ -251,7 +251,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   s->spec = *spec;
   s->betas.assign(spec->betas, spec->betas + spec->n_temps);
   s->spec.betas = nullptr;
-  s->lay = plan_layout(spec, eng->slots);
+  s->lay = plan_layout(spec, eng->slots, eng->slots3);
   s->n_rep = spec->n_replicas;
   s->n_temps = spec->n_temps;
   s->n_cls = n_classes(s->lay.model == MSC ? ISING : s->lay.model, s->lay.dims);
@@ -449,7 +449,7 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
     const uint32_t chunk = std::min<uint32_t>(room, 64);
     if (sim->res.on && sim->blocking) {
       RC_TRY(launch_resident(sim->eng->stream, sim->d_tiles, sim->n_tiles, sim->eng->d_lats, sim->eng->d_groups,
-                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk, sim->pt_interval > 0));
+                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk));
       sim->launches += 1;
     } else {
       RC_TRY(sim->run_graph(chunk));

@@ -118,7 +118,9 @@ __device__ __forceinline__ void unpack_segment(uint32_t E, uint32_t O, uint4& v0
 struct BitsGeom {
   int lx, ly, pitch, nseg;      // nseg = segments per row (pitch = 64 nseg)
   int s0, ns, xh, NC;           // first segment, owned segments, halo columns
-  int y0, hv, R;                // rows y0-2 .. y0+hv+1
+  int y0, hv, R;                // rows y0-yo .. y0+hv+yo-1
+  int yo;                       // halo rows above the tile (2), or 0 for a
+  bool yw;                      // whole-plane 3D tile: rows wrap inside the tile
   int hlast;                    // valid site pairs of the last segment of a row
   int col, row0, rstep, iters_load, iters_black, iters_white;
 };
@@ -137,13 +139,16 @@ __device__ __forceinline__ BitsGeom make_bits_geom(const TileItem& t, const LatD
   g.NC = g.ns + 2 * g.xh;
   g.y0 = t.y0;
   g.hv = min(L->tile_y, g.ly - t.y0);
-  g.R = g.hv + 4;
+  // a 3D tile that spans whole planes needs no y halo: its rows wrap
+  g.yw = L->dims == 3 && t.y0 == 0 && L->tile_y >= g.ly && g.xh == 0;
+  g.yo = g.yw ? 0 : 2;
+  g.R = g.yw ? g.hv : g.hv + 4;
   g.hlast = (g.lx - 64 * (g.nseg - 1)) >> 1;
   g.rstep = kThreads / g.NC;
   g.col = threadIdx.x % g.NC;
   g.row0 = threadIdx.x / g.NC;
   g.iters_load = (g.R + g.rstep - 1) / g.rstep;
-  g.iters_black = (g.R - 2 + g.rstep - 1) / g.rstep;
+  g.iters_black = (g.R - 2 + 2 * (g.yo == 0) + g.rstep - 1) / g.rstep;
   g.iters_white = (g.hv + g.rstep - 1) / g.rstep;
   return g;
 }
@@ -159,12 +164,12 @@ __device__ __forceinline__ void load_bits_plane(uint2* pl, const int8_t* src, in
     uint4 a[4], b[4];
     const bool ok0 = r0 < g.R, ok1 = r1 < g.R && it + 1 < g.iters_load;
     if (ok0) {
-      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - 2 + r0, g.ly)) * g.pitch + 64 * gs);
+      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - g.yo + r0, g.ly)) * g.pitch + 64 * gs);
 #pragma unroll
       for (int k = 0; k < 4; ++k) a[k] = __ldg(p + k);
     }
     if (ok1) {
-      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - 2 + r1, g.ly)) * g.pitch + 64 * gs);
+      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - g.yo + r1, g.ly)) * g.pitch + 64 * gs);
 #pragma unroll
       for (int k = 0; k < 4; ++k) b[k] = __ldg(p + k);
     }
@@ -206,11 +211,13 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
     uint32_t m[3] = {0, 0, 0};
     int P_ = 0;
     if (active) {
-      const int y = wrap_i(g.y0 - 2 + r, g.ly);
+      const int y = wrap_i(g.y0 - g.yo + r, g.ly);
       P_ = (colour + y + z) & 1;  // x parity of this colour's sites in the row
       const uint2 me = pl[r * g.NC + cc];
-      const uint2 up = pl[(r - 1) * g.NC + cc];
-      const uint2 dn = pl[(r + 1) * g.NC + cc];
+      const int ru = g.yw && r == 0 ? g.R - 1 : r - 1;
+      const int rd = g.yw && r == g.R - 1 ? 0 : r + 1;
+      const uint2 up = pl[ru * g.NC + cc];
+      const uint2 dn = pl[rd * g.NC + cc];
       own = P_ ? me.y : me.x;
       const uint32_t other = P_ ? me.x : me.y;
       uint32_t lft, rgt;
@@ -293,7 +300,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       uint2& me = pl[r * g.NC + cc];
       if (P_) me.y = nw;
       else me.x = nw;
-      const bool owned = owned_plane && owned_col && r >= 2 && r < 2 + g.hv;
+      const bool owned = owned_plane && owned_col && r >= g.yo && r < g.yo + g.hv;
       if (owned) {
         acc.nacc += __popc(flip);
         acc.ksum += __popc(flip & b0) + 2 * __popc(flip & b1) + 4 * __popc(flip & b2);
@@ -303,7 +310,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
         // and (mode 1) store the int8 row segment
         const uint2 fin = P_ ? make_uint2(me.x, nw) : make_uint2(nw, me.y);
         if (out_mode == 1) {
-          const int y = wrap_i(g.y0 - 2 + r, g.ly);
+          const int y = wrap_i(g.y0 - g.yo + r, g.ly);
           uint4 v0, v1, v2, v3;
           unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
           uint4* out = (uint4*)(dst + ((size_t)z * g.ly + y) * g.pitch + 64 * gs);
@@ -367,7 +374,7 @@ __device__ __forceinline__ void flush_bits(Accum* A, const PassAcc& a, int zc) {
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
     k_sweep_ising_bits(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                        GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
   extern __shared__ __align__(16) uint2 bsm[];
@@ -403,14 +410,15 @@ __global__ void __launch_bounds__(kThreads)
       __syncthreads();
       if (s >= 2) {
         const int zb = zl - 1;
-        bits_pass<3>(bsm + ((s - 1) & 3) * pw, bsm + ((s - 2) & 3) * pw, Pl, g, wrap_i(zb, lz), 0, 1,
-                     g.R - 2, g.iters_black, zb >= t.z0 && zb < t.z0 + dv, 0, nxt, tab, P, acc);
+        bits_pass<3>(bsm + ((s - 1) & 3) * pw, bsm + ((s - 2) & 3) * pw, Pl, g, wrap_i(zb, lz), 0,
+                     g.yo / 2, g.yw ? g.R : g.R - 2, g.iters_black, zb >= t.z0 && zb < t.z0 + dv, 0, nxt,
+                     tab, P, acc);
         __syncthreads();
       }
       if (s >= 4) {
         const int zw = zl - 2;
         bits_pass<3>(bsm + ((s - 2) & 3) * pw, bsm + ((s - 3) & 3) * pw, bsm + ((s - 1) & 3) * pw, g,
-                     wrap_i(zw, lz), 1, 2, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
+                     wrap_i(zw, lz), 1, g.yo, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
       }
       __syncthreads();  // the next load overwrites the plane slot read above
     }
@@ -479,6 +487,27 @@ __device__ bool resident_grid_sync(LaunchCtl* ctl, unsigned int target) {
   return ok != 0;
 }
 
+// Bounded wait until block 0 has finished the epilogue of launch-local sweep
+// `k1 - 1` (ctl->epi >= k1); on giving up, flags the error like a barrier.
+__device__ bool resident_wait_epilogue(LaunchCtl* ctl, unsigned int k1) {
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    int good = 1;
+    long long it = 0;
+    while (ld_acquire_u32(&ctl->epi) < k1) {
+      if (*(volatile int32_t*)&ctl->err != 0 || ++it > kGridSpinLimit) {
+        atomicExch(&ctl->err, 1);
+        good = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
 // Owned rows (local rows 2 .. hv+1) of a whole-row tile to int8 spins.
 __device__ __forceinline__ void store_owned_rows(const uint2* pl, const BitsGeom& g, int8_t* dst) {
   if (g.row0 >= g.rstep) return;
@@ -502,7 +531,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_ising_resident(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                            GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl,
                            const int2* __restrict__ nbr, uint2* __restrict__ xchg, int xstride,
-                           int n_sweeps, int pt_any) {
+                           int n_sweeps) {
   extern __shared__ __align__(16) uint2 bsm[];
   __shared__ BitsTab tab;
   const TileItem t = tiles[blockIdx.x];
@@ -552,14 +581,17 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (blockIdx.x == 0) {
       // the epilogue of sweep k drains accumulator slot k & 1, which no CTA
       // touches again before the next barrier (its next use is sweep k + 2)
-      const int ng = ctl->n_groups;
-      for (int gi = threadIdx.x; gi < ng; gi += blockDim.x)
-        finish_group(lats, &groups[ctl->group_ids[gi]], k & 1);
-      __threadfence();
+      finish_groups(lats, groups, ctl->group_ids, ctl->n_groups, k & 1);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicExch(&ctl->epi, (unsigned int)(k + 1));
+      }
+    } else if (G->pt_interval > 0 && sweep < target && ((sweep + 1) % (uint64_t)G->pt_interval) == 0) {
+      // a PT exchange after this sweep changes this group's labels (its
+      // acceptance tables for the next sweep): wait for the epilogue
+      if (!resident_wait_epilogue(ctl, (unsigned int)(k + 1))) return;
     }
-    // a PT exchange changes labels (acceptance tables) for the next sweep:
-    // then every CTA waits for the epilogue
-    if (pt_any && !resident_grid_sync(ctl, ++phase * gridDim.x)) return;
   }
   const uint64_t s_end = s0 + (uint64_t)n_sweeps < target ? s0 + (uint64_t)n_sweeps : (s0 > target ? s0 : target);
   store_owned_rows(bsm, g, (int8_t*)L->buf[s_end & 1]);

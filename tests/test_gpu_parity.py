@@ -64,7 +64,7 @@ def _run_parity(gpumc, oracle, model_name, shape, beta, seed, sweeps, q=3, J=1.0
 
 ISING_2D = [(4, 4), (8, 8), (34, 6), (64, 64), (130, 20), (16, 130), (1040, 8), (2054, 4), (256, 300),
             (130, 302)]
-ISING_3D = [(4, 4, 4), (6, 8, 10), (34, 6, 4), (16, 16, 36), (288, 6, 4)]
+ISING_3D = [(4, 4, 4), (6, 8, 10), (34, 6, 4), (16, 16, 36), (288, 6, 4), (128, 800, 4), (128, 64, 40)]
 
 
 @pytest.mark.parametrize("shape", ISING_2D)
