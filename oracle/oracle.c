@@ -432,22 +432,23 @@ double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float
                     float st = sqrtf(w * (2.0f - w));
                     float cp, sp;
                     orc_sincos_turn(o[1], &cp, &sp);
-                    float e1x, e1y, e1z;
-                    if (fabsf(az) < 0.9f) {
-                        float a = sqrtf(ax * ax + ay * ay);
-                        e1x = ay / a; e1y = -ax / a; e1z = 0.0f;
-                    } else {
-                        float a = sqrtf(ay * ay + az * az);
-                        e1x = 0.0f; e1y = az / a; e1z = -ay / a;
-                    }
-                    float e2x = ay * e1z - az * e1y;
-                    float e2y = az * e1x - ax * e1z;
-                    float e2z = ax * e1y - ay * e1x;
-                    float nx = ct * ax + st * (cp * e1x + sp * e2x);
-                    float ny = ct * ay + st * (cp * e1y + sp * e2y);
-                    float nz = ct * az + st * (cp * e1z + sp * e2z);
-                    float r = sqrtf((nx * nx + ny * ny) + nz * nz);
-                    nx = nx / r; ny = ny / r; nz = nz / r;
+                    /* cap sample through the Duff et al. (2017) orthonormal basis */
+                    float vx = st * cp, vy = st * sp;
+                    float sg = az >= 0.0f ? 1.0f : -1.0f;
+                    float k = -1.0f / (sg + az);
+                    float b = (ax * ay) * k;
+                    float e1x = 1.0f + (sg * (ax * ax)) * k;
+                    float e1y = sg * b;
+                    float e1z = -(sg * ax);
+                    float e2x = b;
+                    float e2y = sg + (ay * ay) * k;
+                    float e2z = -ay;
+                    float nx = (vx * e1x + vy * e2x) + ct * ax;
+                    float ny = (vx * e1y + vy * e2y) + ct * ay;
+                    float nz = (vx * e1z + vy * e2z) + ct * az;
+                    float n2 = (nx * nx + ny * ny) + nz * nz;
+                    float f = 1.5f - 0.5f * n2;      /* one Newton step of 1/sqrt(n2) from 1 */
+                    nx = nx * f; ny = ny * f; nz = nz * f;
                     float dot = ((nx - ax) * hx + (ny - ay) * hy) + (nz - az) * hz;
                     float dE = mJ * dot;
                     int ok;

@@ -25,6 +25,15 @@
 
 namespace gpumc {
 
+// Cap proposal around a = (ax, ay, az): local sample v = (st cos phi,
+// st sin phi, ct) mapped through the orthonormal basis {e1, e2, a} of Duff,
+// Burgess, Christensen, Hery, Kensler, Liani, Villemin, "Building an
+// Orthonormal Basis, Revisited" (JCGT 6(1), 2017): with s = sign(az),
+// k = -1 / (s + az), b = ax ay k,
+//   e1 = (1 + s ax^2 k, s b, -s ax),  e2 = (b, s + ay^2 k, -ay),
+// one division and no square root, never singular since |s + az| >= 1.  The
+// result is renormalised by one Newton step of 1/sqrt(n2) from 1
+// (f = 1.5 - 0.5 n2; n2 is within a few ulp of 1, so f is exact to fp32).
 __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx, float hy,
                                           float hz, uint4 o, float omc, float mJ, float beta,
                                           float& nx, float& ny, float& nz, float& dE) {
@@ -33,28 +42,24 @@ __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx
   const float st = fsqrt(fmul(w, fsub(2.0f, w)));
   float cp, sp;
   sincos_turn(o.y, cp, sp);
-  float e1x, e1y, e1z;
-  if (fabsf(az) < 0.9f) {
-    const float a = fsqrt(fadd(fmul(ax, ax), fmul(ay, ay)));
-    e1x = fdiv(ay, a);
-    e1y = fdiv(-ax, a);
-    e1z = 0.0f;
-  } else {
-    const float a = fsqrt(fadd(fmul(ay, ay), fmul(az, az)));
-    e1x = 0.0f;
-    e1y = fdiv(az, a);
-    e1z = fdiv(-ay, a);
-  }
-  const float e2x = fsub(fmul(ay, e1z), fmul(az, e1y));
-  const float e2y = fsub(fmul(az, e1x), fmul(ax, e1z));
-  const float e2z = fsub(fmul(ax, e1y), fmul(ay, e1x));
-  float px = fadd(fmul(ct, ax), fmul(st, fadd(fmul(cp, e1x), fmul(sp, e2x))));
-  float py = fadd(fmul(ct, ay), fmul(st, fadd(fmul(cp, e1y), fmul(sp, e2y))));
-  float pz = fadd(fmul(ct, az), fmul(st, fadd(fmul(cp, e1z), fmul(sp, e2z))));
-  const float r = fsqrt(fadd(fadd(fmul(px, px), fmul(py, py)), fmul(pz, pz)));
-  px = fdiv(px, r);
-  py = fdiv(py, r);
-  pz = fdiv(pz, r);
+  const float vx = fmul(st, cp), vy = fmul(st, sp);
+  const float sg = az >= 0.0f ? 1.0f : -1.0f;
+  const float k = fdiv(-1.0f, fadd(sg, az));
+  const float b = fmul(fmul(ax, ay), k);
+  const float e1x = fadd(1.0f, fmul(fmul(sg, fmul(ax, ax)), k));
+  const float e1y = fmul(sg, b);
+  const float e1z = -fmul(sg, ax);
+  const float e2x = b;
+  const float e2y = fadd(sg, fmul(fmul(ay, ay), k));
+  const float e2z = -ay;
+  float px = fadd(fadd(fmul(vx, e1x), fmul(vy, e2x)), fmul(ct, ax));
+  float py = fadd(fadd(fmul(vx, e1y), fmul(vy, e2y)), fmul(ct, ay));
+  float pz = fadd(fadd(fmul(vx, e1z), fmul(vy, e2z)), fmul(ct, az));
+  const float n2 = fadd(fadd(fmul(px, px), fmul(py, py)), fmul(pz, pz));
+  const float f = fsub(1.5f, fmul(0.5f, n2));
+  px = fmul(px, f);
+  py = fmul(py, f);
+  pz = fmul(pz, f);
   const float dot =
       fadd(fadd(fmul(fsub(px, ax), hx), fmul(fsub(py, ay), hy)), fmul(fsub(pz, az), hz));
   const float de = fmul(mJ, dot);
@@ -74,40 +79,89 @@ __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx
 }
 
 // Philox4x32-10 of counter (site, colour | TAG_O3 << 1, sweep) with the
-// sweep-uniform part of round 1 and the bumped keys precomputed.
+// sweep-uniform part of round 1 precomputed; the round keys are bumped on the
+// fly (two adds per round instead of twenty live registers: this kernel is
+// bound by load latency, so registers, i.e. resident warps, matter more).
 struct O3Philox {
-  uint32_t a, b, c;
-  uint32_t k0[10], k1[10];
+  uint32_t a, b, c, k0, k1;
 };
 __device__ __forceinline__ O3Philox make_o3_philox(uint64_t key, uint64_t sweep, uint32_t ctrl) {
   O3Philox P;
-  const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+  P.k0 = (uint32_t)key;
+  P.k1 = (uint32_t)(key >> 32);
   const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
-  P.a = __umulhi(0xCD9E8D57u, c2) ^ k0 ^ ctrl;
+  P.a = __umulhi(0xCD9E8D57u, c2) ^ P.k0 ^ ctrl;
   P.b = 0xCD9E8D57u * c2;
-  P.c = c3 ^ k1;
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    P.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
-    P.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
-  }
+  P.c = c3 ^ P.k1;
   return P;
 }
 __device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
   uint4 c = make_uint4(P.a, P.b, __umulhi(0xD2511F53u, index) ^ P.c, 0xD2511F53u * index);
+  uint32_t k0 = P.k0, k1 = P.k1;
 #pragma unroll
   for (int r = 1; r < 10; ++r) {
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
     const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
     const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-    c = make_uint4(hi1 ^ c.y ^ P.k0[r], lo1, hi0 ^ c.w ^ P.k1[r], lo0);
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
   }
   return c;
+}
+
+// One site of a colour pass: its own spin and the fp32 (decision) and exact
+// fp64 (energy cache) sums of its neighbours, loaded before any update of
+// the thread's sites so that the loads of two sites overlap.
+struct O3Site {
+  uint32_t me, site;
+  float ax, ay, az, hx, hy, hz;
+  double hxd, hyd, hzd;
+};
+
+template <int DIM>
+__device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const float* S1, const float* S2,
+                                             int x, int y, int z, int lx, int ly, int lz, int pitch) {
+  const uint32_t rowoff = ((uint32_t)z * ly + y) * (uint32_t)pitch;
+  const int ym = y ? y - 1 : ly - 1, yp = y + 1 < ly ? y + 1 : 0;
+  const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
+  uint32_t zmo = 0, zpo = 0;
+  if (DIM == 3) {
+    const int zm = z ? z - 1 : lz - 1, zp = z + 1 < lz ? z + 1 : 0;
+    zmo = ((uint32_t)zm * ly + y) * (uint32_t)pitch + x;
+    zpo = ((uint32_t)zp * ly + y) * (uint32_t)pitch + x;
+  }
+  // neighbour sum in the fixed order x-1, x+1, y-1, y+1, z-1, z+1
+  const uint32_t nb[6] = {rowoff + xm, rowoff + xp, ((uint32_t)z * ly + ym) * (uint32_t)pitch + x,
+                          ((uint32_t)z * ly + yp) * (uint32_t)pitch + x, zmo, zpo};
+  float hx = __ldg(S + nb[0]), hy = __ldg(S1 + nb[0]), hz = __ldg(S2 + nb[0]);
+  double hxd = (double)hx, hyd = (double)hy, hzd = (double)hz;
+#pragma unroll
+  for (int i = 1; i < 2 * DIM; ++i) {
+    const float vx = __ldg(S + nb[i]), vy = __ldg(S1 + nb[i]), vz = __ldg(S2 + nb[i]);
+    hx = fadd(hx, vx);
+    hy = fadd(hy, vy);
+    hz = fadd(hz, vz);
+    hxd += (double)vx;
+    hyd += (double)vy;
+    hzd += (double)vz;
+  }
+  q.me = rowoff + x;
+  q.ax = S[q.me];
+  q.ay = S1[q.me];
+  q.az = S2[q.me];
+  q.hx = hx;
+  q.hy = hy;
+  q.hz = hz;
+  q.hxd = hxd;
+  q.hyd = hyd;
+  q.hzd = hzd;
+  q.site = (uint32_t)((size_t)(z * ly + y) * lx + x);
 }
 
 // One colour pass over a tile of full rows (y0 .. y0+hv-1, planes z0 ..
 // z0+dv-1), one thread per site of the colour.
 template <int DIM, int COLOUR>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 4)
     k_sweep_o3(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
   const TileItem t = tiles[blockIdx.x];
@@ -151,65 +205,62 @@ __global__ void __launch_bounds__(kThreads, 3)
   }
   double dE = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
   int nacc = 0;
-  if (r0 < rstep) {
-    for (int r = r0; r < rows; r += rstep) {
-      const int y = t.y0 + (DIM == 3 ? r % hv : r);
-      const int z = DIM == 3 ? t.z0 + r / hv : 0;
-      const uint32_t rowoff = ((uint32_t)z * ly + y) * (uint32_t)pitch;
-      const int ym = y ? y - 1 : ly - 1, yp = y + 1 < ly ? y + 1 : 0;
-      const uint32_t rm = ((uint32_t)z * ly + ym) * (uint32_t)pitch;
-      const uint32_t rp = ((uint32_t)z * ly + yp) * (uint32_t)pitch;
-      uint32_t zmo = 0, zpo = 0;
-      if (DIM == 3) {
-        const int zm = z ? z - 1 : lz - 1, zp = z + 1 < lz ? z + 1 : 0;
-        zmo = ((uint32_t)zm * ly + y) * (uint32_t)pitch;
-        zpo = ((uint32_t)zp * ly + y) * (uint32_t)pitch;
-      }
-      const int par = (y + z + COLOUR) & 1;
-      for (int c = col0; c < half; c += cstep) {
-        const int x = 2 * c + par;
-        const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
-        // neighbour sum in the fixed order x-1, x+1, y-1, y+1, z-1, z+1
-        const uint32_t nb[6] = {rowoff + xm, rowoff + xp, rm + x, rp + x, zmo + x, zpo + x};
-        float hx = __ldg(Sr + nb[0]), hy = __ldg(Sr1 + nb[0]), hz = __ldg(Sr2 + nb[0]);
-#pragma unroll
-        for (int i = 1; i < 2 * DIM; ++i) {
-          hx = fadd(hx, __ldg(Sr + nb[i]));
-          hy = fadd(hy, __ldg(Sr1 + nb[i]));
-          hz = fadd(hz, __ldg(Sr2 + nb[i]));
-        }
-        const uint32_t me = rowoff + x;
-        const float ax = S[me], ay = S1[me], az = S2[me];
-        const uint32_t site = (uint32_t)((size_t)(z * ly + y) * lx + x);
-        float nx, ny, nz, de;
-        const bool ok = o3_update(ax, ay, az, hx, hy, hz, o3_philox(P, site), omc, mJ, beta, nx, ny,
-                                  nz, de);
-        float fx = ax, fy = ay, fz = az;
-        if (ok) {
-          // energy cache: exact fp64 change of the fp32 configuration (the
-          // decision used the fp32 dE)
-          double hxd = 0.0, hyd = 0.0, hzd = 0.0;
-#pragma unroll
-          for (int i = 0; i < 2 * DIM; ++i) {
-            hxd += (double)__ldg(Sr + nb[i]);
-            hyd += (double)__ldg(Sr1 + nb[i]);
-            hzd += (double)__ldg(Sr2 + nb[i]);
-          }
-          dE += -Jd * (((double)nx - (double)ax) * hxd + ((double)ny - (double)ay) * hyd +
-                       ((double)nz - (double)az) * hzd);
-          ++nacc;
-          fx = nx;
-          fy = ny;
-          fz = nz;
-          S[me] = fx;
-          S1[me] = fy;
-          S2[me] = fz;
-        }
-        mx += (double)fx;
-        my += (double)fy;
-        mz += (double)fz;
+  // this thread's sites, row-major: rows r0, r0 + rstep, ... of the tile's
+  // rows (y fastest, then z), columns col0, col0 + cstep, ...; taken two at a
+  // time, with the (row, column) cursor advanced without divisions
+  const int nc = (r0 < rstep && col0 < half) ? (half - col0 + cstep - 1) / cstep : 0;
+  const int nr = r0 < rstep ? (rows - r0 + rstep - 1) / rstep : 0;
+  const int n_items = nc * nr;
+  int cy = t.y0 + (DIM == 3 ? r0 % hv : r0), cz = DIM == 3 ? t.z0 + r0 / hv : 0, cc = 0;
+  const int ry = DIM == 3 ? rstep % hv : rstep, rz = DIM == 3 ? rstep / hv : 0;
+  auto next_site = [&](int& x, int& y, int& z) {
+    y = cy;
+    z = cz;
+    x = 2 * (col0 + cc * cstep) + ((y + z + COLOUR) & 1);
+    if (++cc == nc) {
+      cc = 0;
+      cy += ry;
+      cz += rz;
+      if (cy >= t.y0 + hv) {
+        cy -= hv;
+        cz += 1;
       }
     }
+  };
+  auto update = [&](const O3Site& q) {
+    float nx, ny, nz, de;
+    const bool ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx,
+                              ny, nz, de);
+    float fx = q.ax, fy = q.ay, fz = q.az;
+    if (ok) {
+      // energy cache: exact fp64 change of the fp32 configuration (the
+      // decision used the fp32 dE)
+      dE += -Jd * (((double)nx - (double)q.ax) * q.hxd + ((double)ny - (double)q.ay) * q.hyd +
+                   ((double)nz - (double)q.az) * q.hzd);
+      ++nacc;
+      fx = nx;
+      fy = ny;
+      fz = nz;
+      S[q.me] = fx;
+      S1[q.me] = fy;
+      S2[q.me] = fz;
+    }
+    mx += (double)fx;
+    my += (double)fy;
+    mz += (double)fz;
+  };
+  for (int k = 0; k < n_items; k += 2) {
+    int x, y, z;
+    O3Site qa, qb;
+    next_site(x, y, z);
+    o3_load_site<DIM>(qa, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
+    const bool two = k + 1 < n_items;
+    if (two) {
+      next_site(x, y, z);
+      o3_load_site<DIM>(qb, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
+    }
+    update(qa);
+    if (two) update(qb);
   }
   const unsigned full = 0xFFFFFFFFu;
 #pragma unroll
