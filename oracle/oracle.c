@@ -208,6 +208,57 @@ static int accept_bits(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t 
     return 0;
 }
 
+/* Potts (q <= 4) on bit planes of the site's 64-site row segment: the
+ * proposal v in [0, q-1) (q = 2: 0; q = 3: one bit; q = 4: two bits, v = 3
+ * redrawn from the next pair of planes, at most 32 rounds, then 0) and the
+ * bit-serial acceptance against the 80-bit threshold of the class. */
+static uint64_t potts_segment(const geom* g, int64_t x, int64_t y, int64_t z) {
+    int64_t ps = (g->lx + 63) / 64;
+    return (uint64_t)((y + g->ly * z) * ps + (x >> 6));
+}
+
+static uint32_t potts_bits_proposal(const geom* g, int64_t x, int64_t y, int64_t z, int q,
+                                    uint32_t colour, const uint32_t key[2], uint64_t sweep) {
+    if (q == 2) return 0;
+    uint64_t seg = potts_segment(g, x, y, z);
+    int bit = (int)((x & 63) >> 1);
+    uint32_t ctr[4], out[4];
+    if (q == 3) {
+        make_ctr(ctr, seg, colour, ORC_TAG_PBITS, 0, sweep);
+        orc_philox4x32_10(ctr, key, out);
+        return (out[0] >> bit) & 1u;
+    }
+    for (int r = 0; r < 32; ++r) {
+        if ((r & 1) == 0) {
+            make_ctr(ctr, seg, colour, ORC_TAG_PBITS, (uint32_t)(r >> 1), sweep);
+            orc_philox4x32_10(ctr, key, out);
+        }
+        uint32_t b0 = (out[2 * (r & 1)] >> bit) & 1u, b1 = (out[2 * (r & 1) + 1] >> bit) & 1u;
+        uint32_t v = 2 * b1 + b0;
+        if (v < 3) return v;
+    }
+    return 0;
+}
+
+static int potts_bits_accept(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t head,
+                             uint64_t tail, uint32_t colour, const uint32_t key[2], uint64_t sweep) {
+    if (head >= 65536u) return 1;
+    uint64_t seg = potts_segment(g, x, y, z);
+    int bit = (int)((x & 63) >> 1);
+    uint32_t out[4];
+    for (int j = 0; j < 80; ++j) {
+        if ((j & 3) == 0) {
+            uint32_t ctr[4];
+            make_ctr(ctr, seg, colour, ORC_TAG_PACC, (uint32_t)(j >> 2), sweep);
+            orc_philox4x32_10(ctr, key, out);
+        }
+        int ub = (int)((out[j & 3] >> bit) & 1u);
+        int tb = j < 16 ? (int)((head >> (15 - j)) & 1u) : (int)((tail >> (79 - j)) & 1u);
+        if (ub != tb) return ub < tb;
+    }
+    return 0;
+}
+
 /* uniform r in [0, n) for the Potts proposal, Lemire multiply-shift with
  * exact rejection (16-bit first draw, 32-bit retries from a refine batch) */
 static uint32_t potts_draw(uint32_t u16, uint32_t n, uint64_t site, uint32_t colour,
@@ -260,6 +311,9 @@ int64_t orc_sweep_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t 
     uint32_t key[2];
     key_of(key64, key);
     int64_t dE = 0, acc = 0;
+    /* Potts on bit planes when q <= 4 and rows are at most 128 segments of 64
+     * sites or a whole number of segments; else the 16-bit chunk method */
+    int potts_bits = q <= 4 && ((lx + 63) / 64 <= 128 || lx % 64 == 0);
     for (uint32_t colour = 0; colour < 2; ++colour) {
         for (int64_t z = 0; z < g.lz; ++z)
             for (int64_t y = 0; y < g.ly; ++y)
@@ -275,6 +329,21 @@ int64_t orc_sweep_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t 
                         if (accept_bits(&g, x, y, z, head[k], tail[k], colour, key, sweep)) {
                             spins[site] = (int8_t)-s;
                             dE += 2 * (zc - 2 * k);
+                            ++acc;
+                        }
+                    } else if (potts_bits) {
+                        uint32_t v = potts_bits_proposal(&g, x, y, z, q, colour, key, sweep);
+                        int8_t t = (int8_t)((int)v < s ? (int)v : (int)v + 1);
+                        int nold = 0, nnew = 0;
+                        for (int i = 0; i < nn; ++i) {
+                            nold += spins[nb[i]] == s;
+                            nnew += spins[nb[i]] == t;
+                        }
+                        int d = nnew - nold;
+                        if (potts_bits_accept(&g, x, y, z, head[d + zc], tail[d + zc], colour, key,
+                                              sweep)) {
+                            spins[site] = t;
+                            dE += -d;
                             ++acc;
                         }
                     } else {

@@ -39,7 +39,9 @@ enum {
     ORC_TAG_O3 = 5,         /* O(3): cos-theta, phi, acceptance             */
     ORC_TAG_MSC = 6,        /* multi-spin bit planes (plane pair in bits 8+) */
     ORC_TAG_PT = 7,         /* replica exchange decisions                   */
-    ORC_TAG_BITS = 8        /* Ising bit planes of a 64-site row segment    */
+    ORC_TAG_BITS = 8,       /* Ising bit planes of a 64-site row segment    */
+    ORC_TAG_PBITS = 9,      /* Potts (q <= 4) proposal bit planes           */
+    ORC_TAG_PACC = 10       /* Potts (q <= 4) acceptance bit planes         */
 };
 
 /* Substream ids used with RngStreamKey::with_substream. */

@@ -35,6 +35,8 @@ template <int DIM, int COLOUR>
 __global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM>
+__global__ void k_sweep_potts_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
                                        uint2*, int, int);
 template <int DIM>
@@ -173,10 +175,37 @@ int validate_spec(const gpumc_spec* s) {
   return GPUMC_OK;
 }
 
-// Every tile step must be positive and the shared-memory plan must fit.
+// Shared memory a bit-sliced tile needs, with the geometry the kernels derive
+// from it (make_bits_geom): packed segments of 8 B (Ising) or 16 B (Potts
+// q <= 4), NC columns (owned + halo), R rows (two halo rows each side unless
+// a 3D tile spans whole planes), four planes in 3D.
+static size_t bits_tile_smem(const Layout& L, const TileItem& t) {
+  const int nseg = L.pitch / 64;
+  const int s0 = t.x0 >> 6;
+  const int ns = std::min(L.tile_cx, nseg - s0);
+  const int xh = ns < nseg ? 1 : 0;
+  const int nc = ns + 2 * xh;
+  const int hv = std::min(L.tile_y, L.ly - t.y0);
+  const bool yw = L.dims == 3 && t.y0 == 0 && L.tile_y >= L.ly && xh == 0;
+  const int r = yw ? hv : hv + 4;
+  if (nc > kThreads) return ~(size_t)0;  // a CTA covers at least one whole tile row
+  const size_t elem = L.model == ISING ? 8 : 16;
+  return elem * (size_t)r * nc * (L.dims == 3 ? 4 : 1);
+}
+
+// Every tile step must be positive and the shared-memory plan must fit, for
+// every tile the plan enumerates.
 bool layout_ok(const Layout& L) {
-  return L.buf_bytes > 0 && L.tile_cx > 0 && L.tile_y > 0 && L.tile_z > 0 &&
-         (L.smem > 0 || L.model == O3) && L.smem <= 200 * 1024;
+  if (!(L.buf_bytes > 0 && L.tile_cx > 0 && L.tile_y > 0 && L.tile_z > 0 &&
+        (L.smem > 0 || L.model == O3) && L.smem <= 200 * 1024))
+    return false;
+  if (L.model == ISING || (L.model == POTTS && L.bits)) {
+    std::vector<TileItem> tiles;
+    enumerate_tiles(L, 0, tiles);
+    for (const TileItem& t : tiles)
+      if (t.x0 % 64 != 0 || bits_tile_smem(L, t) > L.smem) return false;
+  }
+  return true;
 }
 
 // Rows per whole-row Ising tile.  A tile of hv rows costs its CTA
@@ -213,6 +242,7 @@ int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots) {
 Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
   Layout L;
   L.model = s->model;
+  L.q = (int)s->q;
   L.dims = s->dims;
   L.lx = (int)s->lx;
   L.ly = (int)s->ly;
@@ -275,6 +305,39 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
         L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * nc;
       }
     }
+  } else if (L.model == POTTS && s->q <= 4 && ((lx + 63) / 64 <= 128 || lx % 64 == 0)) {
+    // bit-sliced kernel (two bit planes per parity, 16 B per packed 64-site
+    // segment): whole-row tiles up to 128 segments per row, else x-split
+    // tiles of 32 segments plus one halo segment per side; about 1536
+    // packed segments per tile (2D) or per plane (3D), y halo of two rows
+    // unless a 3D tile spans whole planes
+    L.bits = true;
+    L.pitch = (lx + 63) / 64 * 64;
+    L.buf_bytes = (size_t)L.pitch * rows;
+    const int nseg = L.pitch / 64;
+    if (L.dims == 3 && nseg <= 128 && (size_t)ly * nseg * 16 * 4 <= kIsingTileSmem) {
+      L.tile_cx = nseg;
+      L.tile_y = ly;
+      const int ntz = (lz + 15) / 16;
+      L.tile_z = (lz + ntz - 1) / ntz;
+      L.smem = 4 * 16 * (size_t)ly * nseg;
+    } else {
+      const bool xsplit = (lx % 64 == 0) && nseg > 128;
+      L.tile_cx = xsplit ? 32 : nseg;
+      const int nc = L.tile_cx + (xsplit ? 2 : 0);
+      const int items = L.dims == 2 ? 1536 : 768;
+      const int hv_max = std::max(1, items / nc - 4);
+      const int nty = (ly + hv_max - 1) / hv_max;
+      L.tile_y = (ly + nty - 1) / nty;
+      if (L.dims == 2) {
+        L.tile_z = 1;
+        L.smem = 16 * (size_t)(L.tile_y + 4) * nc;
+      } else {
+        const int ntz = (lz + 15) / 16;
+        L.tile_z = (lz + ntz - 1) / ntz;
+        L.smem = 4 * 16 * (size_t)(L.tile_y + 4) * nc;
+      }
+    }
   } else if (L.model == POTTS) {
     L.pitch = (lx + 15) / 16 * 16;
     L.buf_bytes = (size_t)L.pitch * rows;
@@ -327,7 +390,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
 
 int tile_width_sites(const Layout& L) {
   if (L.model == ISING) return 64 * L.tile_cx;
-  if (L.model == POTTS) return 16 * L.tile_cx;
+  if (L.model == POTTS) return (L.bits ? 64 : 16) * L.tile_cx;
   if (L.model == O3) return 4 * L.tile_cx;
   return 2 * L.tile_cx;
 }
@@ -340,7 +403,12 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
       for (int x0 = 0; x0 < L.lx; x0 += tw) out.push_back(TileItem{lat, x0, y0, z0});
 }
 
-int kernel_kind(const Layout& L) { return L.model * 2 + (L.dims - 2); }
+// Kernel of a layout: model x dims; Potts planned on bit planes (q <= 4)
+// runs the bit-sliced kernel (kinds 8 / 9).
+int kernel_kind(const Layout& L) {
+  if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
+  return L.model * 2 + (L.dims - 2);
+}
 
 size_t footprint_bytes(const gpumc_spec* s) {
   const Layout L = plan_layout(s);
@@ -363,7 +431,9 @@ static SweepKernel kernel_for(int kind) {
     case 4: return k_sweep_o3<2, 1>;
     case 5: return k_sweep_o3<3, 1>;
     case 6: return k_sweep_msc<2>;
-    default: return k_sweep_msc<3>;
+    case 7: return k_sweep_msc<3>;
+    case 8: return k_sweep_potts_bits<2>;
+    default: return k_sweep_potts_bits<3>;
   }
 }
 
@@ -373,7 +443,7 @@ static int prepare_kernels() {
   static std::once_flag once;
   static cudaError_t status = cudaSuccess;
   std::call_once(once, [] {
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < 10; ++k) {
       cudaError_t e = cudaFuncSetAttribute(kernel_for(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;

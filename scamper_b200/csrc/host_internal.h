@@ -14,6 +14,8 @@ namespace gpumc {
 
 struct Layout {
   int model = 0, dims = 2, lx = 0, ly = 0, lz = 1, pitch = 0;
+  int q = 2;             // Potts states
+  bool bits = false;     // Potts on the bit-sliced kernel (q <= 4)
   int64_t n_sites = 0;
   size_t buf_bytes = 0;  // one ping-pong buffer
   int tile_cx = 0, tile_y = 0, tile_z = 1;

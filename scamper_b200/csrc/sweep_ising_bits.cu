@@ -26,7 +26,7 @@
 // (Carlo.rs/src/acceptance.rs:11-22), energy cache += dE
 // (CMC.rs/src/lattice/state.rs:127-136), |M| observable
 // (CMC.rs/src/lattice/models.rs:103-110).
-#include "device_common.cuh"
+#include "bits_common.cuh"
 #include "epilogue.cuh"
 
 namespace gpumc {
@@ -44,39 +44,6 @@ struct BitsTab {
   uint32_t pend_neg[3][3];    // pend_neg[i][b] = ~0 if bit b of class pc[i] is 0
   uint4 tq[20][3];            // tq[q][i].{x,y,z,w} = bit 4q+{0,1,2,3} (MSB first) of T[pc[i]]
 };
-
-struct BitsPhilox {
-  uint32_t a, b, c;
-  uint32_t k0[10], k1[10];
-};
-
-__device__ __forceinline__ BitsPhilox make_bits_philox(uint64_t key, uint64_t sweep) {
-  BitsPhilox P;
-  const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
-  const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
-  P.a = __umulhi(0xCD9E8D57u, c2) ^ k0;
-  P.b = 0xCD9E8D57u * c2;
-  P.c = c3 ^ k1;
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    P.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
-    P.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
-  }
-  return P;
-}
-
-// Philox4x32-10 of counter (index, ctrl, sweep_lo, sweep_hi) with the
-// sweep-uniform part of round 1 precomputed.
-__device__ __forceinline__ uint4 bits_philox(const BitsPhilox& P, uint32_t index, uint32_t ctrl) {
-  uint4 c = make_uint4(P.a ^ ctrl, P.b, __umulhi(0xD2511F53u, index) ^ P.c, 0xD2511F53u * index);
-#pragma unroll
-  for (int r = 1; r < 10; ++r) {
-    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-    c = make_uint4(hi1 ^ c.y ^ P.k0[r], lo1, hi0 ^ c.w ^ P.k1[r], lo0);
-  }
-  return c;
-}
 
 // 64 int8 spins (x order) -> parity masks (bit set for spin -1).
 __device__ __forceinline__ uint2 pack_segment(const uint4 v0, const uint4 v1, const uint4 v2,
@@ -111,46 +78,6 @@ __device__ __forceinline__ void unpack_segment(uint32_t E, uint32_t O, uint4& v0
   v1 = make_uint4(w[4], w[5], w[6], w[7]);
   v2 = make_uint4(w[8], w[9], w[10], w[11]);
   v3 = make_uint4(w[12], w[13], w[14], w[15]);
-}
-
-// Tile geometry: shared plane of R rows x NC columns of uint2 {E, O};
-// column cc holds segment s0 + cc - xh (wrapped).
-struct BitsGeom {
-  int lx, ly, pitch, nseg;      // nseg = segments per row (pitch = 64 nseg)
-  int s0, ns, xh, NC;           // first segment, owned segments, halo columns
-  int y0, hv, R;                // rows y0-yo .. y0+hv+yo-1
-  int yo;                       // halo rows above the tile (2), or 0 for a
-  bool yw;                      // whole-plane 3D tile: rows wrap inside the tile
-  int hlast;                    // valid site pairs of the last segment of a row
-  int col, row0, rstep, iters_load, iters_black, iters_white;
-};
-
-__device__ __forceinline__ int wrap_i(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
-
-__device__ __forceinline__ BitsGeom make_bits_geom(const TileItem& t, const LatDesc* L) {
-  BitsGeom g;
-  g.lx = L->lx;
-  g.ly = L->ly;
-  g.pitch = L->pitch;
-  g.nseg = L->pitch >> 6;
-  g.s0 = t.x0 >> 6;
-  g.ns = min(L->tile_cx, g.nseg - g.s0);
-  g.xh = g.ns < g.nseg ? 1 : 0;
-  g.NC = g.ns + 2 * g.xh;
-  g.y0 = t.y0;
-  g.hv = min(L->tile_y, g.ly - t.y0);
-  // a 3D tile that spans whole planes needs no y halo: its rows wrap
-  g.yw = L->dims == 3 && t.y0 == 0 && L->tile_y >= g.ly && g.xh == 0;
-  g.yo = g.yw ? 0 : 2;
-  g.R = g.yw ? g.hv : g.hv + 4;
-  g.hlast = (g.lx - 64 * (g.nseg - 1)) >> 1;
-  g.rstep = kThreads / g.NC;
-  g.col = threadIdx.x % g.NC;
-  g.row0 = threadIdx.x / g.NC;
-  g.iters_load = (g.R + g.rstep - 1) / g.rstep;
-  g.iters_black = (g.R - 2 + 2 * (g.yo == 0) + g.rstep - 1) / g.rstep;
-  g.iters_white = (g.hv + g.rstep - 1) / g.rstep;
-  return g;
 }
 
 // Stage rows y0-2 .. y0+hv+1 of plane z into a shared mask plane.

@@ -27,6 +27,8 @@ CASES = [
     ("potts", [130, 20], 1.0051, 106, 5, {"q": 3}),
     ("potts", [34, 6, 36], 0.6, 107, 4, {"q": 4}),
     ("potts", [1040, 8], 0.8814, 108, 3, {"q": 2}),
+    ("potts", [200, 130], 1.2, 113, 3, {"q": 4}),
+    ("potts", [66, 10], 1.0, 114, 4, {"q": 5}),
     ("o3", [66, 10], 0.7, 109, 4, {"alpha": 1.0}),
     ("o3", [8, 6, 20], 0.69, 110, 3, {"alpha": 0.8}),
     ("msc", [66, 10], 0.4407, 111, 3, {}),

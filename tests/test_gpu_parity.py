@@ -101,8 +101,9 @@ def test_ising_3d_bit_exact(gpumc, oracle, shape):
     _run_parity(gpumc, oracle, "ising", shape, 0.2216, seed=5, sweeps=4)[0].close()
 
 
-@pytest.mark.parametrize("shape", [(4, 4), (34, 6), (130, 20), (1040, 8), (4, 4, 4), (6, 8, 10), (34, 6, 36)])
-@pytest.mark.parametrize("q", [2, 3, 4])
+@pytest.mark.parametrize("shape", [(4, 4), (34, 6), (130, 20), (1040, 8), (2048, 64), (8256, 6), (4, 4, 4),
+                                   (6, 8, 10), (34, 6, 36), (128, 400, 4)])
+@pytest.mark.parametrize("q", [2, 3, 4, 5])
 def test_potts_bit_exact(gpumc, oracle, shape, q):
     beta = math.log(1.0 + math.sqrt(q)) * (1.0 if len(shape) == 2 else 0.6)
     _run_parity(gpumc, oracle, "potts", shape, beta, seed=3 + q, sweeps=4, q=q)[0].close()

@@ -104,14 +104,21 @@ def test_geometric_ladder(gpumc):
 @pytest.mark.parametrize("model", [0, 1, 2, 3])
 def test_every_geometry_has_a_tile_plan(gpumc, model):
     """Each model and extent in the benchmark and serving ranges gets a tile
-    plan with positive steps and shared memory within the device limit."""
+    plan with positive steps, and every tile it enumerates fits its shared
+    memory plan (validation re-derives each bit-sliced tile's geometry)."""
     from scamper_b200.mc import spec_from_params
     lib = gpumc._lib.load()
-    for dims in (2, 3):
-        sizes = [4, 6, 10, 16, 30, 34, 62, 64, 66, 126, 128, 130, 190, 192]
-        if dims == 2:
-            sizes += [256, 510, 514, 1024, 2046, 2048, 2050, 4096, 8192]
-        for L in sizes:
-            p = {"lattice_type": "square" if dims == 2 else "cubic", "L": L, "beta": 0.4}
-            spec, keep = spec_from_params(p, model=model)
-            assert lib.gpumc_validate(ctypes.byref(spec)) == 0, (model, dims, L, gpumc._lib.last_error())
+    for q in ([2, 3, 4, 5, 8] if model == 1 else [3]):
+        for dims in (2, 3):
+            sizes = [4, 6, 10, 16, 30, 34, 62, 64, 66, 126, 128, 130, 190, 192]
+            if dims == 2:
+                sizes += [256, 510, 514, 1024, 2046, 2048, 2050, 4096, 8192, 8256, 16384, 20032]
+            for L in sizes:
+                p = {"lattice_type": "square" if dims == 2 else "cubic", "L": L, "beta": 0.4, "q": q}
+                spec, keep = spec_from_params(p, model=model)
+                assert lib.gpumc_validate(ctypes.byref(spec)) == 0, (model, q, dims, L, gpumc._lib.last_error())
+            if dims == 2:
+                for shape in [(130, 66), (8256, 6), (20032, 10), (34, 34)]:
+                    p = {"lattice_type": "square", "Lx": shape[0], "Ly": shape[1], "beta": 0.4, "q": q}
+                    spec, keep = spec_from_params(p, model=model)
+                    assert lib.gpumc_validate(ctypes.byref(spec)) == 0, (model, q, shape, gpumc._lib.last_error())

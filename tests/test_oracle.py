@@ -139,13 +139,16 @@ def test_checkerboard_replay_samples_exact_ising_4x4(oracle):
         assert sum(zs) > -2.0 * math.sqrt(len(zs))
 
 
-def test_checkerboard_replay_samples_exact_potts_q3(oracle):
-    """q = 3 Potts <E> on a 4x4 torus against the row transfer matrix."""
-    beta = exact.math.log(1.0 + math.sqrt(3.0))
-    ex = exact.potts_transfer_matrix(4, 4, 3, beta)
+@pytest.mark.parametrize("q", [2, 3, 4, 5])
+def test_checkerboard_replay_samples_exact_potts(oracle, q):
+    """q-state Potts <E> on a 4x4 torus at beta_c(q) against the row transfer
+    matrix: q <= 4 runs the bit-plane method (q = 4 with its rejection-drawn
+    proposals), q = 5 the 16-bit chunk method."""
+    beta = exact.math.log(1.0 + math.sqrt(q))
+    ex = exact.potts_transfer_matrix(4, 4, q, beta)
     zs = []
     for seed in range(1, 7):
-        lat = oracle.Lattice(oracle.POTTS, (4, 4), q=3, beta=beta, seed=seed)
+        lat = oracle.Lattice(oracle.POTTS, (4, 4), q=q, beta=beta, seed=seed)
         es, _ = _chain_moments(lat, 200, 8000)
         me, se = exact.binned(es)
         zs.append(exact.zscore(me, se, ex["E"]))
