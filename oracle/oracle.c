@@ -400,14 +400,14 @@ float orc_exp_neg(float x) {
     float n = floorf(y + 0.5f);
     float f = y - n;
     float t = f * 0x1.62e430p-1f;           /* ln 2 */
-    float p = 0x1.a01a02p-13f;              /* 1/7! */
-    p = p * t + 0x1.6c16c2p-10f;            /* 1/6! */
-    p = p * t + 0x1.111112p-7f;             /* 1/5! */
-    p = p * t + 0x1.555556p-5f;             /* 1/4! */
-    p = p * t + 0x1.555556p-3f;             /* 1/3! */
-    p = p * t + 0.5f;
-    p = p * t + 1.0f;
-    p = p * t + 1.0f;
+    float p = 0x1.a01a02p-13f;              /* 1/7! ; Horner steps fused (fmaf) */
+    p = fmaf(p, t, 0x1.6c16c2p-10f);        /* 1/6! */
+    p = fmaf(p, t, 0x1.111112p-7f);         /* 1/5! */
+    p = fmaf(p, t, 0x1.555556p-5f);         /* 1/4! */
+    p = fmaf(p, t, 0x1.555556p-3f);         /* 1/3! */
+    p = fmaf(p, t, 0.5f);
+    p = fmaf(p, t, 1.0f);
+    p = fmaf(p, t, 1.0f);
     int ni = (int)n;                        /* -126 <= ni <= 0 */
     uint32_t bits = (uint32_t)(ni + 127) << 23;
     float scale;
@@ -421,18 +421,18 @@ void orc_sincos_turn(uint32_t u, float* c, float* s) {
     if (octant & 1u) t = 1.0f - t;
     float th = t * 0x1.921fb6p-1f;          /* pi / 4 */
     float t2 = th * th;
-    float sp = 0x1.71de3ap-19f;             /* 1/9! */
-    sp = sp * t2 - 0x1.a01a02p-13f;         /* 1/7! */
-    sp = sp * t2 + 0x1.111112p-7f;          /* 1/5! */
-    sp = sp * t2 - 0x1.555556p-3f;          /* 1/3! */
-    sp = sp * t2 + 1.0f;
+    float sp = 0x1.71de3ap-19f;             /* 1/9! ; Horner steps fused (fmaf) */
+    sp = fmaf(sp, t2, -0x1.a01a02p-13f);    /* 1/7! */
+    sp = fmaf(sp, t2, 0x1.111112p-7f);      /* 1/5! */
+    sp = fmaf(sp, t2, -0x1.555556p-3f);     /* 1/3! */
+    sp = fmaf(sp, t2, 1.0f);
     float sn = th * sp;
     float cp = -0x1.27e4fcp-22f;            /* -1/10! */
-    cp = cp * t2 + 0x1.a01a02p-16f;         /* 1/8! */
-    cp = cp * t2 - 0x1.6c16c2p-10f;         /* 1/6! */
-    cp = cp * t2 + 0x1.555556p-5f;          /* 1/4! */
-    cp = cp * t2 - 0.5f;
-    float cs = cp * t2 + 1.0f;
+    cp = fmaf(cp, t2, 0x1.a01a02p-16f);     /* 1/8! */
+    cp = fmaf(cp, t2, -0x1.6c16c2p-10f);    /* 1/6! */
+    cp = fmaf(cp, t2, 0x1.555556p-5f);      /* 1/4! */
+    cp = fmaf(cp, t2, -0.5f);
+    float cs = fmaf(cp, t2, 1.0f);
     float rc, rs;
     switch (octant) {
         case 0: rc = cs;  rs = sn;  break;

@@ -37,6 +37,8 @@ template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_potts_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int COLOUR>
+__global__ void k_sweep_o3_march(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
                                        uint2*, int, int);
 template <int DIM>
@@ -365,9 +367,23 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     L.buf_bytes = 3 * sizeof(float) * (size_t)L.pitch * rows;
     L.inplace = true;
     L.tile_cx = (lx + 3) / 4;
-    L.tile_y = std::max(1, std::min(ly, 4096 / lx));
-    L.tile_z = L.dims == 3 ? std::max(1, std::min(lz, 4096 / (lx * L.tile_y))) : 1;
-    L.smem = 0;
+    // 3D: tiles of whole rows marched along z through a ring of four shared
+    // planes (3 components x (rows + 2 halo rows) x pitch floats each) of at
+    // most 56 KB (three CTAs per SM), up to 16 rows x 22 planes per tile (for
+    // 32 lattices of 64^3: 384 tiles, one wave of 148 x 3 CTAs)
+    const int ty_max = (int)(kO3MarchSmem / (48 * (size_t)L.pitch)) - 2;
+    if (L.dims == 3 && ty_max >= 1) {
+      L.march = true;
+      const int nty = (ly + std::min(16, ty_max) - 1) / std::min(16, ty_max);
+      L.tile_y = (ly + nty - 1) / nty;
+      const int ntz = (lz + 21) / 22;
+      L.tile_z = (lz + ntz - 1) / ntz;
+      L.smem = 48 * (size_t)(L.tile_y + 2) * L.pitch;
+    } else {
+      L.tile_y = std::max(1, std::min(ly, 4096 / lx));
+      L.tile_z = L.dims == 3 ? std::max(1, std::min(lz, 4096 / (lx * L.tile_y))) : 1;
+      L.smem = 0;
+    }
   } else {  // MSC
     L.pitch = (lx + 1) / 2 * 2;
     L.buf_bytes = sizeof(unsigned long long) * (size_t)L.pitch * rows;
@@ -407,6 +423,7 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
 // runs the bit-sliced kernel (kinds 8 / 9).
 int kernel_kind(const Layout& L) {
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
+  if (L.model == O3 && L.march) return 10;
   return L.model * 2 + (L.dims - 2);
 }
 
@@ -433,7 +450,8 @@ static SweepKernel kernel_for(int kind) {
     case 6: return k_sweep_msc<2>;
     case 7: return k_sweep_msc<3>;
     case 8: return k_sweep_potts_bits<2>;
-    default: return k_sweep_potts_bits<3>;
+    case 9: return k_sweep_potts_bits<3>;
+    default: return k_sweep_o3_march<1>;
   }
 }
 
@@ -443,13 +461,15 @@ static int prepare_kernels() {
   static std::once_flag once;
   static cudaError_t status = cudaSuccess;
   std::call_once(once, [] {
-    for (int k = 0; k < 10; ++k) {
+    for (int k = 0; k < 11; ++k) {
       cudaError_t e = cudaFuncSetAttribute(kernel_for(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
     }
     cudaError_t e = cudaFuncSetAttribute(k_sweep_ising_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kIsingTileSmem);
+    if (e != cudaSuccess) status = e;
+    e = cudaFuncSetAttribute(k_sweep_o3_march<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
     if (e != cudaSuccess) status = e;
   });
   if (status != cudaSuccess)
@@ -463,6 +483,7 @@ int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_
   // O(3) sweeps in place: colour 0, then colour 1 (which runs the epilogue)
   if (kind == 4) k_sweep_o3<2, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == 5) k_sweep_o3<3, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == 10) k_sweep_o3_march<0><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   kernel_for(kind)<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   CUDA_TRY(cudaGetLastError());
   return GPUMC_OK;
@@ -736,7 +757,7 @@ bool gpumc_engine::has_per_sweep_work() const { return launches_per_batch_sweep(
 uint64_t gpumc_engine::launches_per_batch_sweep() const {
   uint64_t n = 0;
   for (const auto& p : batch_plans)
-    if (!(p.res.on && blocking)) n += (p.kind == 4 || p.kind == 5) ? 2 : 1;
+    if (!(p.res.on && blocking)) n += (p.kind == 4 || p.kind == 5 || p.kind == 10) ? 2 : 1;
   for (gpumc_sim* s : sims)
     if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) n += (uint64_t)s->n_rep + 1;
   return n;

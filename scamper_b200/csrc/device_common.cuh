@@ -80,21 +80,23 @@ __device__ __forceinline__ float exp_neg(float x) {
   const float n = floorf(fadd(y, 0.5f));
   const float f = fsub(y, n);
   const float t = fmul(f, 0x1.62e430p-1f);
+  // Horner steps as fused multiply-adds (one rounding each)
   float p = 0x1.a01a02p-13f;
-  p = fadd(fmul(p, t), 0x1.6c16c2p-10f);
-  p = fadd(fmul(p, t), 0x1.111112p-7f);
-  p = fadd(fmul(p, t), 0x1.555556p-5f);
-  p = fadd(fmul(p, t), 0x1.555556p-3f);
-  p = fadd(fmul(p, t), 0.5f);
-  p = fadd(fmul(p, t), 1.0f);
-  p = fadd(fmul(p, t), 1.0f);
+  p = __fmaf_rn(p, t, 0x1.6c16c2p-10f);
+  p = __fmaf_rn(p, t, 0x1.111112p-7f);
+  p = __fmaf_rn(p, t, 0x1.555556p-5f);
+  p = __fmaf_rn(p, t, 0x1.555556p-3f);
+  p = __fmaf_rn(p, t, 0.5f);
+  p = __fmaf_rn(p, t, 1.0f);
+  p = __fmaf_rn(p, t, 1.0f);
   const int ni = (int)n;
   const float scale = __int_as_float((ni + 127) << 23);
   return fmul(p, scale);
 }
 
 // (cos, sin) of 2*pi*u/2^32: octant from the top 3 bits, the angle inside the
-// octant from the next 24 bits, Taylor polynomials on [0, pi/4].
+// octant from the next 24 bits, Taylor polynomials on [0, pi/4] evaluated
+// with fused multiply-adds; the octant swaps and negates the pair.
 __device__ __forceinline__ void sincos_turn(uint32_t u, float& c, float& s) {
   const uint32_t octant = u >> 29;
   float t = fmul((float)((u >> 5) & 0xFFFFFFu), 0x1p-24f);
@@ -102,27 +104,22 @@ __device__ __forceinline__ void sincos_turn(uint32_t u, float& c, float& s) {
   const float th = fmul(t, 0x1.921fb6p-1f);
   const float t2 = fmul(th, th);
   float sp = 0x1.71de3ap-19f;
-  sp = fsub(fmul(sp, t2), 0x1.a01a02p-13f);
-  sp = fadd(fmul(sp, t2), 0x1.111112p-7f);
-  sp = fsub(fmul(sp, t2), 0x1.555556p-3f);
-  sp = fadd(fmul(sp, t2), 1.0f);
+  sp = __fmaf_rn(sp, t2, -0x1.a01a02p-13f);
+  sp = __fmaf_rn(sp, t2, 0x1.111112p-7f);
+  sp = __fmaf_rn(sp, t2, -0x1.555556p-3f);
+  sp = __fmaf_rn(sp, t2, 1.0f);
   const float sn = fmul(th, sp);
   float cp = -0x1.27e4fcp-22f;
-  cp = fadd(fmul(cp, t2), 0x1.a01a02p-16f);
-  cp = fsub(fmul(cp, t2), 0x1.6c16c2p-10f);
-  cp = fadd(fmul(cp, t2), 0x1.555556p-5f);
-  cp = fsub(fmul(cp, t2), 0.5f);
-  const float cs = fadd(fmul(cp, t2), 1.0f);
-  switch (octant) {
-    case 0: c = cs; s = sn; break;
-    case 1: c = sn; s = cs; break;
-    case 2: c = -sn; s = cs; break;
-    case 3: c = -cs; s = sn; break;
-    case 4: c = -cs; s = -sn; break;
-    case 5: c = -sn; s = -cs; break;
-    case 6: c = sn; s = -cs; break;
-    default: c = cs; s = -sn; break;
-  }
+  cp = __fmaf_rn(cp, t2, 0x1.a01a02p-16f);
+  cp = __fmaf_rn(cp, t2, -0x1.6c16c2p-10f);
+  cp = __fmaf_rn(cp, t2, 0x1.555556p-5f);
+  cp = __fmaf_rn(cp, t2, -0.5f);
+  const float cs = __fmaf_rn(cp, t2, 1.0f);
+  // octants 1, 2, 5, 6 swap; cos < 0 in octants 2..5, sin < 0 in 4..7
+  const bool sw = ((octant + 1u) & 2u) != 0u;
+  const float a = sw ? sn : cs, b = sw ? cs : sn;
+  c = ((octant + 2u) & 4u) ? -a : a;
+  s = (octant & 4u) ? -b : b;
 }
 
 // log-space Metropolis decision of Carlo.rs/src/acceptance.rs:11-22 with u

@@ -16,6 +16,7 @@ struct Layout {
   int model = 0, dims = 2, lx = 0, ly = 0, lz = 1, pitch = 0;
   int q = 2;             // Potts states
   bool bits = false;     // Potts on the bit-sliced kernel (q <= 4)
+  bool march = false;    // 3D O(3) on the shared-memory z-march kernel
   int64_t n_sites = 0;
   size_t buf_bytes = 0;  // one ping-pong buffer
   int tile_cx = 0, tile_y = 0, tile_z = 1;
@@ -34,6 +35,7 @@ int validate_spec(const gpumc_spec* s);
 // passes its device's own count.
 constexpr int kDefaultSlots = 148 * 4;
 constexpr size_t kIsingTileSmem = 48 * 1024;  // whole-row Ising tile budget
+constexpr size_t kO3MarchSmem = 56 * 1024;   // ring of four O(3) planes per tile
 constexpr int kDefaultSlots3 = 148 * 2;  // resident 3D Ising sweep CTAs of one B200
 Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots, int slots3 = kDefaultSlots3);
 int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);

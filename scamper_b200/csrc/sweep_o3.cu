@@ -281,6 +281,183 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
 
+// ---------------------------------------------------------------------------
+// 3D colour pass marched along z through a ring of four shared-memory planes.
+//
+// A tile is whole rows y0 .. y0+hv-1 of planes z0 .. z0+dv-1.  Each plane the
+// tile touches (z0-1 .. z0+dv) is copied once, rows y0-1 .. y0+hv with all
+// three components, by 16-byte cp.async into a ring slot, and serves as the
+// z-1, z and z+1 plane of three consecutive steps; the copy of plane z+2 is in
+// flight while plane z is computed.  Every neighbour read is then a
+// shared-memory read.  The pass reads only the other colour's values (and its
+// own sites' old values, which only this tile writes), so copying planes that
+// other tiles update in place is race-free.  The site arithmetic and its
+// operation order are those of k_sweep_o3.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void o3_cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <int COLOUR>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
+                     GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
+  extern __shared__ __align__(16) float osm[];
+  const TileItem t = tiles[blockIdx.x];
+  LatDesc* L = &lats[t.lat];
+  const GroupDesc* G = &groups[L->group];
+  const uint64_t sweep = L->sweep;
+  if (sweep >= L->target) {
+    if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+    return;
+  }
+  const int lx = L->lx, ly = L->ly, lz = L->lz, pitch = L->pitch;
+  const size_t cs = (size_t)pitch * ly * lz;  // component plane stride
+  float* S = (float*)L->buf[0];
+  const int label = G->label[L->replica];
+  const float beta = G->betas_f[label];
+  const float mJ = -G->Jf;
+  const double Jd = G->J;
+  const float omc = L->omc;
+  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | (TAG_O3 << 1));
+  const int hv = min(L->tile_y, ly - t.y0);
+  const int dv = min(L->tile_z, lz - t.z0);
+  const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
+  const size_t slot = (size_t)3 * RW * pitch;  // floats per ring slot
+  const int nvec = pitch >> 2;              // 16-byte chunks per row
+  auto copy_plane = [&](int sl, int z) {
+    const int zz = z < 0 ? z + lz : (z >= lz ? z - lz : z);
+    float* dst = osm + sl * slot;
+    for (int i = threadIdx.x; i < 3 * RW * nvec; i += kThreads) {
+      const int cr = i / nvec, v = i - cr * nvec;
+      const int c = cr / RW, r = cr - c * RW;
+      int y = t.y0 - 1 + r;
+      y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
+      o3_cp_async16(dst + (size_t)cr * pitch + 4 * v, S + c * cs + ((size_t)zz * ly + y) * pitch + 4 * v);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  double dE = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  int nacc = 0;
+  const int half = lx >> 1;
+  const int n_items = hv * half;  // colour sites of the tile's rows in one plane
+  const int dr = kThreads / half, dj = kThreads - dr * half;  // cursor step of kThreads items
+  auto update = [&](const O3Site& q) {
+    float nx, ny, nz, de;
+    const bool ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx,
+                              ny, nz, de);
+    float fx = q.ax, fy = q.ay, fz = q.az;
+    if (ok) {
+      // energy cache: exact fp64 change of the fp32 configuration
+      dE += -Jd * (((double)nx - (double)q.ax) * q.hxd + ((double)ny - (double)q.ay) * q.hyd +
+                   ((double)nz - (double)q.az) * q.hzd);
+      ++nacc;
+      fx = nx;
+      fy = ny;
+      fz = nz;
+      S[q.me] = fx;
+      S[cs + q.me] = fy;
+      S[2 * cs + q.me] = fz;
+    }
+    mx += (double)fx;
+    my += (double)fy;
+    mz += (double)fz;
+  };
+  copy_plane(0, t.z0 - 1);
+  copy_plane(1, t.z0);
+  copy_plane(2, t.z0 + 1);
+  for (int k = 0; k < dv; ++k) {
+    const int z = t.z0 + k;
+    // plane z+2 (needed as z+1 of the next step) into the slot freed by the
+    // previous step; an empty group keeps the count when it is not needed
+    if (k + 1 < dv) {
+      copy_plane((k + 3) & 3, z + 2);
+    } else {
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // planes z-1, z, z+1 landed
+    __syncthreads();
+    const float* pm = osm + (k & 3) * slot;
+    const float* pc = osm + ((k + 1) & 3) * slot;
+    const float* pp = osm + ((k + 2) & 3) * slot;
+    auto load_site = [&](O3Site& q, int rl, int j) {  // local owned row, colour column
+      const int y = t.y0 + rl;
+      const int x = 2 * j + ((y + z + COLOUR) & 1);
+      const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
+      const int r = rl + 1;  // slot row of y
+      // neighbour order x-1, x+1, y-1, y+1, z-1, z+1 (as k_sweep_o3)
+      float h[3];
+      double hd[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float* row = pc + (size_t)(c * RW + r) * pitch;
+        const float v0 = row[xm], v1 = row[xp];
+        const float v2 = pc[(size_t)(c * RW + r - 1) * pitch + x];
+        const float v3 = pc[(size_t)(c * RW + r + 1) * pitch + x];
+        const float v4 = pm[(size_t)(c * RW + r) * pitch + x];
+        const float v5 = pp[(size_t)(c * RW + r) * pitch + x];
+        h[c] = fadd(fadd(fadd(fadd(fadd(v0, v1), v2), v3), v4), v5);
+        hd[c] = (((((double)v0 + (double)v1) + (double)v2) + (double)v3) + (double)v4) + (double)v5;
+      }
+      q.ax = pc[(size_t)(0 * RW + r) * pitch + x];
+      q.ay = pc[(size_t)(1 * RW + r) * pitch + x];
+      q.az = pc[(size_t)(2 * RW + r) * pitch + x];
+      q.hx = h[0];
+      q.hy = h[1];
+      q.hz = h[2];
+      q.hxd = hd[0];
+      q.hyd = hd[1];
+      q.hzd = hd[2];
+      q.me = (uint32_t)(((size_t)z * ly + y) * pitch + x);
+      q.site = (uint32_t)((size_t)(z * ly + y) * lx + x);
+    };
+    // items i = threadIdx.x, + kThreads, ... as (row, column) cursors
+    int ra = threadIdx.x / half, ja = threadIdx.x - ra * half;
+    for (int i = threadIdx.x; i < n_items; i += 2 * kThreads) {
+      O3Site qa, qb;
+      load_site(qa, ra, ja);
+      int rb = ra + dr, jb = ja + dj;
+      if (jb >= half) {
+        jb -= half;
+        rb += 1;
+      }
+      const bool two = i + kThreads < n_items;
+      if (two) load_site(qb, rb, jb);
+      update(qa);
+      if (two) update(qb);
+      ra = rb + dr;
+      ja = jb + dj;
+      if (ja >= half) {
+        ja -= half;
+        ra += 1;
+      }
+    }
+    __syncthreads();  // the next copy overwrites the z-1 slot read above
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  const unsigned full = 0xFFFFFFFFu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dE += __shfl_xor_sync(full, dE, o);
+    nacc += __shfl_xor_sync(full, nacc, o);
+    mx += __shfl_xor_sync(full, mx, o);
+    my += __shfl_xor_sync(full, my, o);
+    mz += __shfl_xor_sync(full, mz, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&L->acc.dEf, dE);
+    atomicAdd(&L->acc.mx, mx);
+    atomicAdd(&L->acc.my, my);
+    atomicAdd(&L->acc.mz, mz);
+    if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
+  }
+  if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+}
+
+template __global__ void k_sweep_o3_march<0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_o3_march<1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+
 template __global__ void k_sweep_o3<2, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_o3<2, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_o3<3, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
