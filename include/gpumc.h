@@ -157,6 +157,16 @@ int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* 
                                   double* mag64);
 int gpumc_sweep_count(gpumc_sim* sim, uint64_t* out);
 int gpumc_acceptance(gpumc_sim* sim, int32_t replica, double* cone_half_angle);
+/* Resume support for state snapshots (the cmc-rs-snapshot-v2 format of
+ * ClassicalMC::save_snapshot / load_snapshot, CMC.rs/src/classical_mc.rs:
+ * 63-165, carries spins and beta; these carry the rest of this engine's
+ * state).  The sweep counter of every replica (the position of the
+ * counter-based random stream: resuming at the same count continues the same
+ * trajectory), and one replica's O(3) cone parameter 1 - cos(alpha) as the
+ * exact float the device holds. */
+int gpumc_set_sweep_count(gpumc_sim* sim, uint64_t sweeps);
+int gpumc_get_cone_omc(gpumc_sim* sim, int32_t replica, float* omc);
+int gpumc_set_cone_omc(gpumc_sim* sim, int32_t replica, float omc);
 
 /* ---- ParallelTemperingCompatible (Carlo.rs/src/parallel_tempering.rs:71-84;
  * CMC.rs/src/classical_mc.rs:203-229) ------------------------------------ */

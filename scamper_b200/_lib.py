@@ -96,6 +96,9 @@ SIGNATURES = {
     "gpumc_sim_engine": [_vp, _P(_vp)],
     "gpumc_launches_per_sweep": [_vp, _P(ctypes.c_int32)],
     "gpumc_set_temporal_blocking": [_vp, ctypes.c_int32],
+    "gpumc_set_sweep_count": [_vp, ctypes.c_uint64],
+    "gpumc_get_cone_omc": [_vp, ctypes.c_int32, _P(ctypes.c_float)],
+    "gpumc_set_cone_omc": [_vp, ctypes.c_int32, ctypes.c_float],
     "gpumc_engine_set_temporal_blocking": [_vp, ctypes.c_int32],
     "gpumc_launch_count": [_vp, _P(ctypes.c_uint64)],
     "gpumc_engine_launch_count": [_vp, _P(ctypes.c_uint64)],

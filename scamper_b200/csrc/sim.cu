@@ -646,6 +646,48 @@ int gpumc_acceptance(gpumc_sim* sim, int32_t replica, double* cone_half_angle) {
   return GPUMC_OK;
 }
 
+int gpumc_set_sweep_count(gpumc_sim* sim, uint64_t sweeps) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  std::vector<LatDesc> d(sim->n_rep);
+  CUDA_TRY(cudaMemcpy(d.data(), sim->eng->d_lats + sim->lat0, sizeof(LatDesc) * sim->n_rep,
+                      cudaMemcpyDeviceToHost));
+  for (int r = 0; r < sim->n_rep; ++r) {
+    if (sweeps > d[r].target) return fail(GPUMC_EINVAL, "sweeps: beyond the handle's target");
+    // the current state lives in buf[sweep & 1]: keep it current across the change
+    if (((d[r].sweep ^ sweeps) & 1) && !sim->lay.inplace) {
+      void* from = sim->bufs[2 * r + (d[r].sweep & 1)];
+      void* to = sim->bufs[2 * r + (sweeps & 1)];
+      CUDA_TRY(cudaMemcpy(to, from, sim->lay.buf_bytes, cudaMemcpyDeviceToDevice));
+    }
+    RC_TRY(sim->set_lat_field(r, offsetof(LatDesc, sweep), sweeps));
+  }
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  sim->sweeps = sweeps;
+  return GPUMC_OK;
+}
+
+int gpumc_get_cone_omc(gpumc_sim* sim, int32_t replica, float* omc) {
+  if (!sim || !omc) return fail(GPUMC_EINVAL, "null argument");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  CUDA_TRY(cudaMemcpy(omc, (char*)(sim->eng->d_lats + sim->lat0 + replica) + offsetof(LatDesc, omc),
+                      sizeof(float), cudaMemcpyDeviceToHost));
+  return GPUMC_OK;
+}
+
+int gpumc_set_cone_omc(gpumc_sim* sim, int32_t replica, float omc) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  if (!(omc > 0.0f && omc <= 2.0f)) return fail(GPUMC_EINVAL, "omc: must be in (0, 2]");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  RC_TRY(sim->set_lat_field(replica, offsetof(LatDesc, omc), omc));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  return GPUMC_OK;
+}
+
 int gpumc_log_weight_ratio(gpumc_sim* sim, int32_t replica, double new_beta, double* out) {
   if (!sim || !out) return fail(GPUMC_EINVAL, "null argument");
   if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");

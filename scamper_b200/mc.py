@@ -290,6 +290,30 @@ class ClassicalMC:
         _lib.call("gpumc_sweep_count", self.h, ctypes.byref(v))
         return v.value
 
+    def set_sweep_count(self, sweeps):
+        """Moves every replica's sweep counter (the random-stream position)."""
+        _lib.call("gpumc_set_sweep_count", self.h, int(sweeps))
+
+    def cone_omc(self, replica=0):
+        """O(3) cone parameter 1 - cos(alpha) as the device's float."""
+        v = ctypes.c_float()
+        _lib.call("gpumc_get_cone_omc", self.h, replica, ctypes.byref(v))
+        return v.value
+
+    def set_cone_omc(self, replica, omc):
+        _lib.call("gpumc_set_cone_omc", self.h, replica, ctypes.c_float(omc))
+
+    # -- snapshots (ClassicalMC::save_snapshot / load_snapshot) ---------------
+    def save_snapshot(self, replica=0, renormalize=False):
+        """cmc-rs-snapshot-v2 state of one replica (JSON-ready dict)."""
+        from . import snapshot
+        return snapshot.save_snapshot(self, replica, renormalize=renormalize)
+
+    def load_snapshot(self, snap, replica=0):
+        """Restores one replica; raises CheckpointCorrupted on any mismatch."""
+        from . import snapshot
+        snapshot.load_snapshot(self, snap, replica)
+
     def cone_half_angle(self, replica=0):
         v = ctypes.c_double()
         _lib.call("gpumc_acceptance", self.h, replica, ctypes.byref(v))
