@@ -427,7 +427,15 @@ def cpu_baseline(args, threads=None):
     r = oracle.ref_run_parallel(oracle.ISING, (L, L), HEADLINE_BETAS[1], 1, len(HEADLINE_BETAS),
                                 cores, 0, args.cpu_sweeps)
     v = r["attempts"] / (r["seconds"] * 1e9)
-    return {"value": v, "unit": "spin-flip attempts/ns", "cores": min(cores, len(HEADLINE_BETAS)),
+    n_chains = len(HEADLINE_BETAS)
+    cpu_model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            cpu_model = next((ln.split(":", 1)[1].strip() for ln in f if ln.startswith("model name")), "")
+    except OSError:
+        pass
+    return {"value": v, "unit": "spin-flip attempts/ns", "cores": min(cores, n_chains),
+            "single_core_value": v / min(cores, n_chains), "nproc": os.cpu_count(), "cpu_model": cpu_model,
             "kind": "port",
             "sample": f"{len(HEADLINE_BETAS)} chains (one per beta) of 2D Ising L={L}, "
                       f"{args.cpu_sweeps} sweep(s) each, restated cmc-rs MetropolisCore "
@@ -482,9 +490,9 @@ def main():
     ap.add_argument("--only-headline", action="store_true")
     ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving"], default=None,
                     help="run one extra workload alone (profiling)")
-    ap.add_argument("--serve-rates", type=float, nargs="*", default=[30.0, 300.0])
-    ap.add_argument("--serve-jobs", type=int, default=16)
-    ap.add_argument("--serve-sweep-scale", type=float, default=0.01)
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 100.0, 1000.0])
+    ap.add_argument("--serve-jobs", type=int, default=64)
+    ap.add_argument("--serve-sweep-scale", type=float, default=0.1)
     ap.add_argument("--serve-chunk", type=int, default=20)
     ap.add_argument("--serve-budget-gb", type=float, default=64.0)
     args = ap.parse_args()
