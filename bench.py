@@ -291,6 +291,43 @@ def bench_pt(gpumc, torch, args):
             "pt_accepted_swaps": [acc1, acc2]}
 
 
+def bench_heat_bath(gpumc, torch, args):
+    """Heat-bath sweeps (HeatBathCore / ContinuousHeatBathCore): 2D Ising
+    L=8192 x 3 replicas (the headline lattices, resident launches), 2D Potts
+    q=3 L=2048 x 4 at beta_c, 3D O(3) L=64 x 8 at beta=0.7."""
+    from scamper_b200 import _lib
+    cases = [
+        ("ising", {"lattice_type": "square", "L": HEADLINE_L}, 3, HEADLINE_BETAS, BYTES_PER_ATTEMPT["int8"]),
+        ("potts", {"lattice_type": "square", "L": 2048, "q": 3}, 4, [gpumc.potts_beta_c(3)],
+         BYTES_PER_ATTEMPT["int8"]),
+        ("o3", {"lattice_type": "cubic", "L": 64}, 8, [0.7], BYTES_PER_ATTEMPT["o3"]),
+    ]
+    out = {}
+    for model, params, n_rep, betas, bpa in cases:
+        mc = gpumc.ClassicalMC.from_params(params, 31, model=model, n_replicas=n_rep, betas=betas,
+                                           algorithm="heat_bath", record_capacity=64)
+        mc.on_phase_start(_lib.PHASE_MEASUREMENT)
+        mc.sweep(3)
+        mc.observables()
+        steps = args.aux_steps
+        n0 = mc.launch_count()
+        ms = 0.0
+        done = 0
+        while done < steps:  # drain the record buffer between chunks (untimed)
+            k = min(50, steps - done)
+            ms += time_sweeps(torch, mc, mc.stream_ptr(), k, mc.sweep)
+            mc.observables()
+            done += k
+        launches = mc.launch_count() - n0
+        att = float(mc.n_sites) * n_rep * steps
+        v = att / (ms * 1e6)
+        out[model] = {"config": f"{'2D' if mc.dims == 2 else '3D'} {model} L={params['L']} x {n_rep}",
+                      "value": v, "unit": "spin-flip attempts/ns", "ms_per_sweep": ms / steps,
+                      "hbm_gbs_algorithmic": v * bpa, "launches": launches}
+        mc.close()
+    return out
+
+
 def mixed_specs(seed=2024, n_potts=256, n_o3=32):
     """Uneven mix: 256 Potts lattices (q ~ U{2,3,4}, L log-uniform in
     [32, 2048] rounded to even, beta ~ U[0.8, 1.2] beta_c(q)) and 32 3D O(3)
@@ -488,7 +525,7 @@ def main():
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only-headline", action="store_true")
-    ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving"], default=None,
+    ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving", "heat_bath"], default=None,
                     help="run one extra workload alone (profiling)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 100.0, 1000.0])
     ap.add_argument("--serve-jobs", type=int, default=64)
@@ -507,7 +544,8 @@ def main():
     import scamper_b200 as gpumc
 
     if args.only:
-        fn = {"msc": bench_msc, "pt": bench_pt, "mixed": bench_mixed, "serving": bench_serving}[args.only]
+        fn = {"msc": bench_msc, "pt": bench_pt, "mixed": bench_mixed, "serving": bench_serving,
+              "heat_bath": bench_heat_bath}[args.only]
         print(json.dumps({"workload": args.only, "result": fn(gpumc, torch, args)}), flush=True)
         return 0
     h = headline(gpumc, torch, args, dist, rank, world)
@@ -529,7 +567,7 @@ def main():
     workloads = {}
     if rank == 0 and not args.only_headline:
         for name, fn in [("msc", bench_msc), ("pt", bench_pt), ("mixed", bench_mixed),
-                         ("serving", bench_serving)]:
+                         ("heat_bath", bench_heat_bath), ("serving", bench_serving)]:
             try:
                 workloads[name] = fn(gpumc, torch, args)
             except Exception as exc:  # report, never hide

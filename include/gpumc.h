@@ -45,6 +45,14 @@ extern "C" {
 #define GPUMC_O3 2
 #define GPUMC_ISING_MSC64 3
 
+/* sweep algorithms: MetropolisCore (CMC.rs/src/algorithms/metropolis.rs) and
+ * the heat bath, HeatBathCore (Ising, Potts) / ContinuousHeatBathCore (O(3))
+ * (CMC.rs/src/algorithms/heat_bath.rs:12-134), the algorithm type parameter
+ * of ClassicalMC<H, A> (CMC.rs/src/classical_mc.rs:21-31).  The multi-spin
+ * model has Metropolis only. */
+#define GPUMC_METROPOLIS 0
+#define GPUMC_HEAT_BATH 1
+
 #define GPUMC_INIT_HOT 0  /* "hot" / "random" initial_state */
 #define GPUMC_INIT_COLD 1 /* "cold" / "ordered" */
 
@@ -75,6 +83,7 @@ typedef struct {
   int32_t init;             /* GPUMC_INIT_HOT / GPUMC_INIT_COLD                */
   double cone_half_angle;   /* O(3): initial cap half-angle (radians), (0, pi] */
   int32_t record_capacity;  /* measured sweeps buffered on the device (>= 1)   */
+  int32_t algorithm;        /* GPUMC_METROPOLIS / GPUMC_HEAT_BATH              */
 } gpumc_spec;
 
 /* One measured sweep of one replica (Context::measure of Energy, E2,

@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 ISING, POTTS, O3, MSC = 0, 1, 2, 3
+METROPOLIS, HEAT_BATH = 0, 1
 TAG_ACC, TAG_PROP, TAG_ACC_REFINE, TAG_PROP_REFINE, TAG_INIT, TAG_O3, TAG_MSC, TAG_PT = range(8)
 SUB_INIT, SUB_SWEEP = 0, 1
 
@@ -48,6 +49,13 @@ def lib():
             "orc_exchange_key": (_u64, [_u64]),
             "orc_threshold": (None, [ctypes.c_double, _u32p, _u64p]),
             "orc_build_table": (_int, [_int, _int, ctypes.c_double, ctypes.c_double, _u32p, _u64p]),
+            "orc_build_table_hb": (_int, [_int, _int, ctypes.c_double, ctypes.c_double, _u32p, _u64p]),
+            "orc_sweep_discrete_hb": (_i64, [_int, _int, _i64, _i64, _i64, _int, ctypes.c_double, _u32p,
+                                             _u64p, _u64, _u64, _i8p, _i64p]),
+            "orc_sweep_o3_hb": (ctypes.c_double, [_int, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float,
+                                                  _u64, _u64, _f32p, _f32p, _f32p, _i64p]),
+            "orc_one_minus_exp_neg": (ctypes.c_float, [ctypes.c_float]),
+            "orc_log_one_minus": (ctypes.c_float, [ctypes.c_float]),
             "orc_init_discrete": (None, [_int, _int, _i64, _i64, _i64, _int, _u64, _u64, _int, _i8p]),
             "orc_sweep_discrete": (_i64, [_int, _int, _i64, _i64, _i64, _int, _u32p, _u64p, _u64, _u64,
                                           _i8p, _i64p]),
@@ -118,10 +126,11 @@ def threshold(p):
     return h.value, t.value
 
 
-def table(model, dims, J, beta):
+def table(model, dims, J, beta, algorithm=METROPOLIS):
     head = np.zeros(13, dtype=np.uint32)
     tail = np.zeros(13, dtype=np.uint64)
-    n = lib().orc_build_table(model, dims, J, beta, _p(head, _u32p), _p(tail, _u64p))
+    fn = lib().orc_build_table_hb if algorithm == HEAT_BATH else lib().orc_build_table
+    n = fn(model, dims, J, beta, _p(head, _u32p), _p(tail, _u64p))
     return head[:n].copy(), tail[:n].copy()
 
 
@@ -129,8 +138,9 @@ class Lattice:
     """Oracle replica of one lattice under the engine's checkerboard method."""
 
     def __init__(self, model, shape, q=3, J=1.0, beta=0.44, seed=1, replica=0, hot=True,
-                 omc=None):
+                 omc=None, algorithm=METROPOLIS):
         self.model = model
+        self.algorithm = algorithm
         self.dims = len(shape)
         self.lx, self.ly = shape[0], shape[1]
         self.lz = shape[2] if self.dims == 3 else 1
@@ -170,12 +180,22 @@ class Lattice:
         self.beta = beta
         if self.model != O3:
             tm = ISING if self.model == MSC else self.model
-            self.head, self.tail = table(tm, self.dims, self.J, beta)
+            self.head, self.tail = table(tm, self.dims, self.J, beta, self.algorithm)
 
     def sweep(self, adapt=False):
         L = lib()
         acc = ctypes.c_int64()
-        if self.model in (ISING, POTTS):
+        if self.model in (ISING, POTTS) and self.algorithm == HEAT_BATH:
+            d = L.orc_sweep_discrete_hb(self.model, self.dims, self.lx, self.ly, self.lz, self.q, self.J,
+                                        _p(self.head, _u32p), _p(self.tail, _u64p), self.key,
+                                        self.sweeps, _p(self.spins, _i8p), ctypes.byref(acc))
+            self.e_int += d
+        elif self.model == O3 and self.algorithm == HEAT_BATH:
+            d = L.orc_sweep_o3_hb(self.dims, self.lx, self.ly, self.lz, np.float32(self.J),
+                                  np.float32(self.beta), self.key, self.sweeps, _p(self.sx, _f32p),
+                                  _p(self.sy, _f32p), _p(self.sz, _f32p), ctypes.byref(acc))
+            self.e += d
+        elif self.model in (ISING, POTTS):
             d = L.orc_sweep_discrete(self.model, self.dims, self.lx, self.ly, self.lz, self.q,
                                      _p(self.head, _u32p), _p(self.tail, _u64p), self.key,
                                      self.sweeps, _p(self.spins, _i8p), ctypes.byref(acc))

@@ -130,6 +130,25 @@ int orc_build_table(int model, int dims, double J, double beta, uint32_t* head, 
     return 2 * z + 1;
 }
 
+/* Heat-bath tables: the host side of the engine's heat-bath kernels. */
+int orc_build_table_hb(int model, int dims, double J, double beta, uint32_t* head, uint64_t* tail) {
+    int z = 2 * dims;
+    int n = model == ORC_POTTS ? 2 * z + 1 : z + 1;
+    for (int c = 0; c < n; ++c) { head[c] = 0; tail[c] = 0; }
+    if (model == ORC_POTTS) {
+        for (int d = 0; d <= z; ++d)
+            tail[d] = (uint64_t)ldexp(exp(-(beta * fabs(J)) * (double)d), 60);
+        return n;
+    }
+    for (int k = 0; k <= z; ++k) {
+        double ax = fabs(2.0 * beta * J * (double)(z - 2 * k));
+        double p = 1.0 / (1.0 + exp(-ax));
+        if (p >= 1.0) p = 1.0 - 0x1p-53;
+        orc_threshold(p, &head[k], &tail[k]);
+    }
+    return n;
+}
+
 /* ------------------------------------------------------------------------ */
 /* geometry helpers                                                          */
 /* ------------------------------------------------------------------------ */
@@ -206,6 +225,40 @@ static int accept_bits(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t 
         if (ub != tb) return ub < tb;
     }
     return 0;
+}
+
+/* Heat-bath Ising decision on the bit planes (tag HBITS) of the site's
+ * segment: u < T, with u's bits complemented when `flip` (the negative-field
+ * member of a class pair compares ~u). */
+static int hb_bits_below(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t head,
+                         uint64_t tail, int flip, uint32_t colour, const uint32_t key[2],
+                         uint64_t sweep) {
+    int64_t ps = (g->lx + 63) / 64;
+    uint64_t seg = (uint64_t)((y + g->ly * z) * ps + (x >> 6));
+    int bit = (int)((x & 63) >> 1);
+    uint32_t out[4];
+    for (int j = 0; j < 80; ++j) {
+        if ((j & 3) == 0) {
+            uint32_t ctr[4];
+            make_ctr(ctr, seg, colour, ORC_TAG_HBITS, (uint32_t)(j >> 2), sweep);
+            orc_philox4x32_10(ctr, key, out);
+        }
+        int ub = (int)((out[j & 3] >> bit) & 1u) ^ (flip ? 1 : 0);
+        int tb = j < 16 ? (int)((head >> (15 - j)) & 1u) : (int)((tail >> (79 - j)) & 1u);
+        if (ub != tb) return ub < tb;
+    }
+    return 0;
+}
+
+/* first bit of the site's heat-bath uniform (plane 0) */
+static int hb_bits_first(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t colour,
+                         const uint32_t key[2], uint64_t sweep) {
+    int64_t ps = (g->lx + 63) / 64;
+    uint64_t seg = (uint64_t)((y + g->ly * z) * ps + (x >> 6));
+    uint32_t ctr[4], out[4];
+    make_ctr(ctr, seg, colour, ORC_TAG_HBITS, 0, sweep);
+    orc_philox4x32_10(ctr, key, out);
+    return (int)((out[0] >> ((x & 63) >> 1)) & 1u);
 }
 
 /* Potts (q <= 4) on bit planes of the site's 64-site row segment: the
@@ -368,6 +421,88 @@ int64_t orc_sweep_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t 
                 }
     }
     if (accepted) *accepted = acc;
+    return dE;
+}
+
+int64_t orc_sweep_discrete_hb(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
+                              double J, const uint32_t* head, const uint64_t* tail, uint64_t key64,
+                              uint64_t sweep, int8_t* spins, int64_t* changed) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    int zc = 2 * dims;
+    uint32_t key[2];
+    key_of(key64, key);
+    int64_t dE = 0, nch = 0;
+    int64_t pc = (lx + 15) / 16;
+    for (uint32_t colour = 0; colour < 2; ++colour) {
+        for (int64_t z = 0; z < g.lz; ++z)
+            for (int64_t y = 0; y < g.ly; ++y)
+                for (int64_t x = 0; x < g.lx; ++x) {
+                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
+                    int64_t site = site_of(&g, x, y, z);
+                    int64_t nb[6];
+                    int nn = neighbours(&g, x, y, z, nb);
+                    int8_t s = spins[site];
+                    if (model == ORC_ISING) {
+                        /* k = down neighbours; field h = z - 2k; class pair
+                         * {k, z-k} shares T[k] = p(|x|); the member with
+                         * negative field compares ~u, zero field is u < 1/2 */
+                        int k = 0;
+                        for (int i = 0; i < nn; ++i) k += spins[nb[i]] == -1;
+                        int up;
+                        if (2 * k == zc) {
+                            up = hb_bits_first(&g, x, y, z, colour, key, sweep) == 0;
+                        } else {
+                            int neg = J >= 0.0 ? 2 * k > zc : 2 * k < zc;
+                            int lt = hb_bits_below(&g, x, y, z, head[k], tail[k], neg, colour, key,
+                                                   sweep);
+                            up = neg ? !lt : lt;
+                        }
+                        int8_t t = up ? 1 : -1;
+                        if (t != s) {
+                            spins[site] = t;
+                            dE += 2 * (int64_t)s * (zc - 2 * k);
+                            ++nch;
+                        }
+                    } else {
+                        /* state weights exp(beta J n_t) relative to the site's
+                         * favoured count, as 64-bit integers; x = u * total
+                         * / 2^64; first state whose cumulative weight
+                         * exceeds x */
+                        int n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                        for (int i = 0; i < nn; ++i)
+                            if (spins[nb[i]] >= 0 && spins[nb[i]] < q) ++n[spins[nb[i]]];
+                        int nmax = 0, nmin = 64;
+                        for (int t = 0; t < q; ++t) {
+                            if (n[t] > nmax) nmax = n[t];
+                            if (n[t] < nmin) nmin = n[t];
+                        }
+                        uint64_t w[8], tot = 0;
+                        for (int t = 0; t < q; ++t) {
+                            w[t] = tail[J < 0.0 ? n[t] - nmin : nmax - n[t]];
+                            tot += w[t];
+                        }
+                        uint64_t chunk = (uint64_t)((y + g.ly * z) * pc + (x >> 4));
+                        int slot = (int)((x & 15) >> 1);
+                        uint32_t ctr[4], out[4];
+                        make_ctr(ctr, chunk, colour, ORC_TAG_HB, (uint32_t)(slot >> 1), sweep);
+                        orc_philox4x32_10(ctr, key, out);
+                        uint64_t u = (slot & 1) ? ((uint64_t)out[2] | ((uint64_t)out[3] << 32))
+                                                : ((uint64_t)out[0] | ((uint64_t)out[1] << 32));
+                        uint64_t r = (uint64_t)(((unsigned __int128)u * tot) >> 64);
+                        int t = q - 1;
+                        for (int c = 0; c < q; ++c) {
+                            if (r < w[c]) { t = c; break; }
+                            r -= w[c];
+                        }
+                        if (t != s) {
+                            spins[site] = (int8_t)t;
+                            dE += -(int64_t)(n[t] - n[s]);
+                            ++nch;
+                        }
+                    }
+                }
+    }
+    if (changed) *changed = nch;
     return dE;
 }
 
@@ -545,6 +680,139 @@ double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float
                 }
     }
     if (accepted) *accepted = acc;
+    return dEsum;
+}
+
+/* 1 - exp(-x), x >= 0: Taylor series x (1 - x/2 + ... + x^8/9!) below 1/2
+ * (Horner steps fused), else 1 - exp_neg(-x). */
+float orc_one_minus_exp_neg(float x) {
+    if (x < 0.5f) {
+        float p = 0x1.71de3ap-19f;              /* 1/9! */
+        p = fmaf(p, x, -0x1.a01a02p-16f);       /* -1/8! */
+        p = fmaf(p, x, 0x1.a01a02p-13f);        /* 1/7! */
+        p = fmaf(p, x, -0x1.6c16c2p-10f);       /* -1/6! */
+        p = fmaf(p, x, 0x1.111112p-7f);         /* 1/5! */
+        p = fmaf(p, x, -0x1.555556p-5f);        /* -1/4! */
+        p = fmaf(p, x, 0x1.555556p-3f);         /* 1/3! */
+        p = fmaf(p, x, -0.5f);
+        p = fmaf(p, x, 1.0f);
+        return x * p;
+    }
+    return 1.0f - orc_exp_neg(-x);
+}
+
+/* 2 atanh(s), |s| <= 0.1716: 2 s (1 + s^2/3 + ... + s^10/11) */
+static float two_atanh_small(float s) {
+    float s2 = s * s;
+    float q = 0x1.745d18p-4f;                   /* 1/11 */
+    q = fmaf(q, s2, 0x1.c71c72p-4f);            /* 1/9 */
+    q = fmaf(q, s2, 0x1.24924ap-3f);            /* 1/7 */
+    q = fmaf(q, s2, 0x1.99999ap-3f);            /* 1/5 */
+    q = fmaf(q, s2, 0x1.555556p-2f);            /* 1/3 */
+    q = fmaf(q, s2, 1.0f);
+    return (2.0f * s) * q;
+}
+
+/* ln(1 - y), 0 <= y < 1: from y directly below 1/4, else from z = 1 - y =
+ * m 2^e, m in [sqrt(1/2), sqrt(2)]: e ln 2 + 2 atanh((m - 1) / (m + 1)) */
+float orc_log_one_minus(float y) {
+    if (y < 0.25f) return two_atanh_small(-y / (2.0f - y));
+    float z = 1.0f - y;
+    uint32_t bits;
+    memcpy(&bits, &z, 4);
+    int e = (int)(bits >> 23) - 127;
+    uint32_t mb = (bits & 0x7FFFFFu) | 0x3F800000u;
+    float m;
+    memcpy(&m, &mb, 4);
+    if (m > 0x1.6a09e6p+0f) {                   /* sqrt(2) */
+        m = m * 0.5f;
+        e += 1;
+    }
+    float sm = (m - 1.0f) / (m + 1.0f);
+    return (float)e * 0x1.62e430p-1f + two_atanh_small(sm);
+}
+
+double orc_sweep_o3_hb(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
+                       uint64_t key64, uint64_t sweep, float* sx, float* sy, float* sz,
+                       int64_t* changed) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    uint32_t key[2];
+    key_of(key64, key);
+    double dEsum = 0.0;
+    int64_t nch = 0;
+    for (uint32_t colour = 0; colour < 2; ++colour) {
+        for (int64_t z = 0; z < g.lz; ++z)
+            for (int64_t y = 0; y < g.ly; ++y)
+                for (int64_t x = 0; x < g.lx; ++x) {
+                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
+                    int64_t site = site_of(&g, x, y, z);
+                    int64_t nb[6];
+                    int nn = neighbours(&g, x, y, z, nb);
+                    float hx = sx[nb[0]], hy = sy[nb[0]], hz = sz[nb[0]];
+                    for (int i = 1; i < nn; ++i) {
+                        hx = hx + sx[nb[i]];
+                        hy = hy + sy[nb[i]];
+                        hz = hz + sz[nb[i]];
+                    }
+                    uint32_t ctr[4], o[4];
+                    make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_O3HB, 0, sweep);
+                    orc_philox4x32_10(ctr, key, o);
+                    /* w = 1 - cos(theta) by the inverse CDF of exp(kappa cos) */
+                    float fx = J * hx, fy = J * hy, fz = J * hz;
+                    float nrm = sqrtf((fx * fx + fy * fy) + fz * fz);
+                    float kap = beta * nrm;
+                    float v = (float)(o[0] >> 8) * 0x1p-24f;
+                    float w, ax = 0.0f, ay = 0.0f, az = 1.0f;
+                    if (!(kap >= 0x1p-20f)) {
+                        w = 2.0f * v;                    /* uniform on the sphere */
+                    } else {
+                        float yv = v * orc_one_minus_exp_neg(2.0f * kap);
+                        w = -orc_log_one_minus(yv) / kap;
+                        if (w > 2.0f) w = 2.0f;
+                        ax = fx / nrm;
+                        ay = fy / nrm;
+                        az = fz / nrm;
+                    }
+                    float ct = 1.0f - w;
+                    float st = sqrtf(w * (2.0f - w));
+                    float cp, sp;
+                    orc_sincos_turn(o[1], &cp, &sp);
+                    /* placed around the field direction with the Duff et al.
+                     * (2017) basis and one Newton renormalisation, as the
+                     * cap proposal */
+                    float vx = st * cp, vy = st * sp;
+                    float sg = az >= 0.0f ? 1.0f : -1.0f;
+                    float k = -1.0f / (sg + az);
+                    float b = (ax * ay) * k;
+                    float e1x = 1.0f + (sg * (ax * ax)) * k;
+                    float e1y = sg * b;
+                    float e1z = -(sg * ax);
+                    float e2x = b;
+                    float e2y = sg + (ay * ay) * k;
+                    float e2z = -ay;
+                    float nx = (vx * e1x + vy * e2x) + ct * ax;
+                    float ny = (vx * e1y + vy * e2y) + ct * ay;
+                    float nz = (vx * e1z + vy * e2z) + ct * az;
+                    float n2 = (nx * nx + ny * ny) + nz * nz;
+                    float f = 1.5f - 0.5f * n2;
+                    nx = nx * f; ny = ny * f; nz = nz * f;
+                    float ox = sx[site], oy = sy[site], oz = sz[site];
+                    if (nx != ox || ny != oy || nz != oz) {
+                        double hxd = 0.0, hyd = 0.0, hzd = 0.0;
+                        for (int i = 0; i < nn; ++i) {
+                            hxd += (double)sx[nb[i]];
+                            hyd += (double)sy[nb[i]];
+                            hzd += (double)sz[nb[i]];
+                        }
+                        dEsum += -(double)J * (((double)nx - (double)ox) * hxd +
+                                               ((double)ny - (double)oy) * hyd +
+                                               ((double)nz - (double)oz) * hzd);
+                        sx[site] = nx; sy[site] = ny; sz[site] = nz;
+                        ++nch;
+                    }
+                }
+    }
+    if (changed) *changed = nch;
     return dEsum;
 }
 

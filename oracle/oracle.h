@@ -41,7 +41,10 @@ enum {
     ORC_TAG_PT = 7,         /* replica exchange decisions                   */
     ORC_TAG_BITS = 8,       /* Ising bit planes of a 64-site row segment    */
     ORC_TAG_PBITS = 9,      /* Potts (q <= 4) proposal bit planes           */
-    ORC_TAG_PACC = 10       /* Potts (q <= 4) acceptance bit planes         */
+    ORC_TAG_PACC = 10,      /* Potts (q <= 4) acceptance bit planes         */
+    ORC_TAG_HBITS = 11,     /* heat bath: Ising bit planes                  */
+    ORC_TAG_HB = 12,        /* heat bath: 64-bit uniforms of int8 Potts sites */
+    ORC_TAG_O3HB = 13       /* heat bath: O(3) (cos theta, phi) draws       */
 };
 
 /* Substream ids used with RngStreamKey::with_substream. */
@@ -67,6 +70,12 @@ void orc_threshold(double p, uint32_t* head, uint64_t* tail);
  * anti-aligned neighbours k in 0..z, dE = 2J(z-2k).  Potts: class = d + z,
  * d = n(new) - n(old) in -z..z, dE = -J d.  Returns number of classes. */
 int orc_build_table(int model, int dims, double J, double beta, uint32_t* head, uint64_t* tail);
+/* Heat-bath tables (HeatBathable for IsingModel / PottsModel, CMC.rs/src/
+ * lattice/models.rs:158-186, :340-380).  Ising: T[k] = p(|x_k|) as 80-bit
+ * thresholds, k = down neighbours, x_k = 2 beta J (z - 2k), p(x) = 1 / (1 +
+ * exp(-x)) clamped to 1 - 2^-53.  Potts: tail[d] = floor(2^60 exp(-beta |J|
+ * d)), d = 0..z, head = 0.  Returns the entry count. */
+int orc_build_table_hb(int model, int dims, double J, double beta, uint32_t* head, uint64_t* tail);
 
 /* --- checkerboard replay: int8 Ising / Potts -----------------------------
  * Ising decisions use bit planes: a row is cut into 64-site segments
@@ -90,6 +99,21 @@ void orc_init_o3(int dims, int64_t lx, int64_t ly, int64_t lz, uint64_t base_see
                  uint64_t replica, int hot, float* sx, float* sy, float* sz);
 /* omc = 1 - cos(alpha) of the cone; beta and J as float.  Returns the
  * accumulated energy change (sum of fp32 dE in double). */
+/* One heat-bath sweep (HeatBathCore, CMC.rs/src/algorithms/heat_bath.rs:41-66)
+ * of an int8 Ising or Potts lattice in the engine's checkerboard order and
+ * random streams; returns dE in units of J, *changed = sites whose spin
+ * changed. */
+int64_t orc_sweep_discrete_hb(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
+                              double J, const uint32_t* head, const uint64_t* tail, uint64_t key64,
+                              uint64_t sweep, int8_t* spins, int64_t* changed);
+/* One O(3) heat-bath sweep (ContinuousHeatBathCore, heat_bath.rs:75-134, with
+ * the Langevin inverse CDF of models.rs:617-663) with the engine's fp32
+ * arithmetic; returns the exact fp64 dE. */
+double orc_sweep_o3_hb(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
+                       uint64_t key64, uint64_t sweep, float* sx, float* sy, float* sz,
+                       int64_t* changed);
+float orc_one_minus_exp_neg(float x);
+float orc_log_one_minus(float y);
 double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
                     float omc, uint64_t key64, uint64_t sweep, float* sx, float* sy,
                     float* sz, int64_t* accepted);

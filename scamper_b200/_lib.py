@@ -26,6 +26,8 @@ ISING_MSC64 = 3
 INIT_HOT = 0
 INIT_COLD = 1
 
+METROPOLIS = 0
+HEAT_BATH = 1
 PHASE_THERMALIZATION = 1
 PHASE_MEASUREMENT = 2
 
@@ -46,6 +48,7 @@ class Spec(ctypes.Structure):
         ("init", ctypes.c_int32),
         ("cone_half_angle", ctypes.c_double),
         ("record_capacity", ctypes.c_int32),
+        ("algorithm", ctypes.c_int32),
     ]
 
 

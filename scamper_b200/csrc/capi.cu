@@ -25,20 +25,21 @@
 
 namespace gpumc {
 
-template <int DIM>
+template <int DIM, int ALG>
 __global__ void k_sweep_ising_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template <int MODEL>
+template <int MODEL, int ALG>
 __global__ void k_sweep_discrete_2d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template <int MODEL>
+template <int MODEL, int ALG>
 __global__ void k_sweep_discrete_3d(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template <int DIM, int COLOUR>
+template <int DIM, int COLOUR, int ALG>
 __global__ void k_sweep_o3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_potts_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template <int COLOUR>
+template <int COLOUR, int ALG>
 __global__ void k_sweep_o3_march(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int ALG>
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
                                        uint2*, int, int);
 template <int DIM>
@@ -117,14 +118,43 @@ void threshold80(double p, uint32_t& head, unsigned long long& tail) {
 // Class tables.  Ising / multi-spin: class k = anti-aligned neighbours,
 // dE = 2J(z - 2k) (multi_spin.rs:84-91 indexes by aligned count z - k).
 // Potts: class d + z with d = n(new) - n(old), dE = -J d.
+//
+// Heat bath.  Ising: class k = down neighbours, T[k] = p(|x|) with
+// x = 2 beta J (z - 2k) and p(x) = 1 / (1 + exp(-x)) (IsingModel::
+// heat_bath_sample_site, CMC.rs/src/lattice/models.rs:158-186), clamped below
+// 1 so that every class stays a comparison.  Potts: the weight exp(beta J n)
+// of a state held by n neighbours (PottsModel::heat_bath_sample_site,
+// models.rs:340-380) relative to the site's largest one, as a 64-bit integer:
+// tail[d] = W[d] = floor(2^60 exp(-beta |J| d)), d = 0..z the distance of
+// the state's count from the site's most favoured count (n_max - n for
+// J >= 0, n - n_min for J < 0).  The favoured state weighs exactly 2^60, so
+// a site's total weight is in [2^60, 2^63) for q <= 8.
 int n_classes(int model, int dims) {
   const int z = 2 * dims;
   return (model == POTTS) ? 2 * z + 1 : z + 1;
 }
 void build_table(int model, int dims, double J, double beta, uint32_t* head,
-                 unsigned long long* tail) {
+                 unsigned long long* tail, int alg) {
   const int z = 2 * dims;
   const int n = n_classes(model, dims);
+  if (alg == HEAT_BATH) {
+    for (int c = 0; c < n; ++c) {
+      head[c] = 0;
+      tail[c] = 0;
+    }
+    if (model == POTTS) {
+      for (int d = 0; d <= z; ++d)
+        tail[d] = (unsigned long long)std::ldexp(std::exp(-(beta * std::fabs(J)) * (double)d), 60);
+    } else {
+      for (int k = 0; k <= z; ++k) {
+        const double ax = std::fabs(2.0 * beta * J * (double)(z - 2 * k));
+        double p = 1.0 / (1.0 + std::exp(-ax));
+        if (p >= 1.0) p = 1.0 - 0x1p-53;
+        threshold80(p, head[k], tail[k]);
+      }
+    }
+    return;
+  }
   for (int c = 0; c < n; ++c) {
     const double dE = (model == POTTS) ? -J * (double)(c - z) : 2.0 * J * (double)(z - 2 * c);
     const double logA = -beta * dE;
@@ -172,6 +202,10 @@ int validate_spec(const gpumc_spec* s) {
   if (s->model == GPUMC_O3 && !(s->cone_half_angle > 0.0 && s->cone_half_angle <= M_PI))
     return fail(GPUMC_EINVAL, "cone_half_angle: must be in (0, pi]");
   if (s->record_capacity < 1) return fail(GPUMC_EINVAL, "record_capacity: must be >= 1");
+  if (s->algorithm != GPUMC_METROPOLIS && s->algorithm != GPUMC_HEAT_BATH)
+    return fail(GPUMC_EINVAL, "algorithm: expected metropolis or heat_bath");
+  if (s->algorithm == GPUMC_HEAT_BATH && s->model == GPUMC_ISING_MSC64)
+    return fail(GPUMC_EINVAL, "algorithm: the multi-spin model has Metropolis sweeps only");
   if (!layout_ok(plan_layout(s)))
     return fail(GPUMC_EINVAL, "lattice: no tile plan fits this geometry (row too long for shared memory)");
   return GPUMC_OK;
@@ -244,6 +278,7 @@ int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots) {
 Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
   Layout L;
   L.model = s->model;
+  L.alg = s->algorithm == GPUMC_HEAT_BATH ? HEAT_BATH : METROPOLIS;
   L.q = (int)s->q;
   L.dims = s->dims;
   L.lx = (int)s->lx;
@@ -307,7 +342,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
         L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * nc;
       }
     }
-  } else if (L.model == POTTS && s->q <= 4 && ((lx + 63) / 64 <= 128 || lx % 64 == 0)) {
+  } else if (L.model == POTTS && L.alg == METROPOLIS && s->q <= 4 && ((lx + 63) / 64 <= 128 || lx % 64 == 0)) {
     // bit-sliced kernel (two bit planes per parity, 16 B per packed 64-site
     // segment): whole-row tiles up to 128 segments per row, else x-split
     // tiles of 32 segments plus one halo segment per side; about 1536
@@ -420,11 +455,13 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
 }
 
 // Kernel of a layout: model x dims; Potts planned on bit planes (q <= 4)
-// runs the bit-sliced kernel (kinds 8 / 9).
+// runs the bit-sliced kernel (kinds 8 / 9); heat-bath layouts add
+// kKindHeatBath to the kind of the same model and geometry.
 int kernel_kind(const Layout& L) {
+  const int hb = L.alg == HEAT_BATH ? kKindHeatBath : 0;
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
-  if (L.model == O3 && L.march) return 10;
-  return L.model * 2 + (L.dims - 2);
+  if (L.model == O3 && L.march) return 10 + hb;
+  return L.model * 2 + (L.dims - 2) + hb;
 }
 
 size_t footprint_bytes(const gpumc_spec* s) {
@@ -441,17 +478,25 @@ size_t footprint_bytes(const gpumc_spec* s) {
 typedef void (*SweepKernel)(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 static SweepKernel kernel_for(int kind) {
   switch (kind) {
-    case 0: return k_sweep_ising_bits<2>;
-    case 1: return k_sweep_ising_bits<3>;
-    case 2: return k_sweep_discrete_2d<POTTS>;
-    case 3: return k_sweep_discrete_3d<POTTS>;
-    case 4: return k_sweep_o3<2, 1>;
-    case 5: return k_sweep_o3<3, 1>;
+    case 0: return k_sweep_ising_bits<2, 0>;
+    case 1: return k_sweep_ising_bits<3, 0>;
+    case 2: return k_sweep_discrete_2d<POTTS, 0>;
+    case 3: return k_sweep_discrete_3d<POTTS, 0>;
+    case 4: return k_sweep_o3<2, 1, 0>;
+    case 5: return k_sweep_o3<3, 1, 0>;
     case 6: return k_sweep_msc<2>;
     case 7: return k_sweep_msc<3>;
     case 8: return k_sweep_potts_bits<2>;
     case 9: return k_sweep_potts_bits<3>;
-    default: return k_sweep_o3_march<1>;
+    case 10: return k_sweep_o3_march<1, 0>;
+    case kKindHeatBath + 0: return k_sweep_ising_bits<2, 1>;
+    case kKindHeatBath + 1: return k_sweep_ising_bits<3, 1>;
+    case kKindHeatBath + 2: return k_sweep_discrete_2d<POTTS, 1>;
+    case kKindHeatBath + 3: return k_sweep_discrete_3d<POTTS, 1>;
+    case kKindHeatBath + 4: return k_sweep_o3<2, 1, 1>;
+    case kKindHeatBath + 5: return k_sweep_o3<3, 1, 1>;
+    case kKindHeatBath + 10: return k_sweep_o3_march<1, 1>;
+    default: return nullptr;
   }
 }
 
@@ -461,16 +506,22 @@ static int prepare_kernels() {
   static std::once_flag once;
   static cudaError_t status = cudaSuccess;
   std::call_once(once, [] {
-    for (int k = 0; k < 11; ++k) {
+    for (int k = 0; k < 2 * kKindHeatBath; ++k) {
+      if (!kernel_for(k)) continue;
       cudaError_t e = cudaFuncSetAttribute(kernel_for(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
     }
-    cudaError_t e = cudaFuncSetAttribute(k_sweep_ising_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kIsingTileSmem);
-    if (e != cudaSuccess) status = e;
-    e = cudaFuncSetAttribute(k_sweep_o3_march<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
-    if (e != cudaSuccess) status = e;
+    const void* extra[] = {(const void*)k_sweep_ising_resident<0>, (const void*)k_sweep_ising_resident<1>};
+    for (const void* f : extra) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kIsingTileSmem);
+      if (e != cudaSuccess) status = e;
+    }
+    const void* colour0[] = {(const void*)k_sweep_o3_march<0, 0>, (const void*)k_sweep_o3_march<0, 1>};
+    for (const void* f : colour0) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
+      if (e != cudaSuccess) status = e;
+    }
   });
   if (status != cudaSuccess)
     return fail(GPUMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(status));
@@ -480,11 +531,17 @@ static int prepare_kernels() {
 int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
                         LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem) {
   if (n_tiles <= 0) return GPUMC_OK;
+  const SweepKernel k = kernel_for(kind);
+  if (!k) return fail(GPUMC_EINVAL, "internal: no sweep kernel for this layout");
   // O(3) sweeps in place: colour 0, then colour 1 (which runs the epilogue)
-  if (kind == 4) k_sweep_o3<2, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
-  if (kind == 5) k_sweep_o3<3, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
-  if (kind == 10) k_sweep_o3_march<0><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
-  kernel_for(kind)<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  if (kind == 4) k_sweep_o3<2, 0, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == 5) k_sweep_o3<3, 0, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == 10) k_sweep_o3_march<0, 0><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindHeatBath + 4) k_sweep_o3<2, 0, 1><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindHeatBath + 5) k_sweep_o3<3, 0, 1><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindHeatBath + 10)
+    k_sweep_o3_march<0, 1><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  k<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   CUDA_TRY(cudaGetLastError());
   return GPUMC_OK;
 }
@@ -545,14 +602,14 @@ int gpumc_engine_create(int32_t device, gpumc_engine** out) {
   int n_sm = 0, per_sm = 0;
   err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
   if (err == cudaSuccess)
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_ising_bits<2>, kThreads, kIsingTileSmem);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_ising_bits<2, 0>, kThreads, kIsingTileSmem);
   if (err != cudaSuccess) {
     delete e;
     return fail(GPUMC_ECUDA, std::string("device query: ") + cudaGetErrorString(err));
   }
   e->slots = std::max(1, n_sm * std::max(1, per_sm));
   int per_sm3 = 0;
-  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_sweep_ising_bits<3>, kThreads, 16 * 1024);
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_sweep_ising_bits<3, 0>, kThreads, 16 * 1024);
   if (err != cudaSuccess) {
     delete e;
     return fail(GPUMC_ECUDA, std::string("device query: ") + cudaGetErrorString(err));
@@ -658,6 +715,8 @@ int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
     if (it == layout_of_lat.end()) return GPUMC_OK;
     const Layout& L = *it->second;
     if (L.model != ISING || L.dims != 2 || L.tile_cx != L.pitch / 64) return GPUMC_OK;
+    if (i == 0) rp.alg = L.alg;
+    if (L.alg != rp.alg) return GPUMC_OK;
     size_t j = i;
     while (j < tiles.size() && tiles[j].lat == tiles[i].lat) ++j;
     const int n = (int)(j - i);
@@ -672,7 +731,8 @@ int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
   int coop = 0, n_sm = 0, per_sm = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
   CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_ising_resident, kThreads, smem));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, rp.alg == HEAT_BATH ? k_sweep_ising_resident<1> : k_sweep_ising_resident<0>, kThreads, smem));
   if (!coop || (int64_t)per_sm * n_sm < (int64_t)tiles.size()) return GPUMC_OK;
   rp.xstride = 2 * 4 * wmax;
   CUDA_TRY(cudaMalloc(&rp.d_nbr, sizeof(int2) * nbr.size()));
@@ -692,7 +752,9 @@ int gpumc::launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, 
   int xstride = rp.xstride;
   void* args[] = {(void*)&tiles, (void*)&lats, (void*)&groups, (void*)&ctl,
                   (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps};
-  CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_sweep_ising_resident, dim3(n_tiles), dim3(kThreads),
+  const void* kern = rp.alg == HEAT_BATH ? (const void*)k_sweep_ising_resident<1>
+                                          : (const void*)k_sweep_ising_resident<0>;
+  CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(n_tiles), dim3(kThreads),
                                        args, smem, st));
   int32_t err = 0;
   CUDA_TRY(cudaMemcpyAsync(&err, &ctl->err, sizeof(err), cudaMemcpyDeviceToHost, st));
@@ -738,7 +800,7 @@ int gpumc_engine::rebuild_batch() {
     c.n_groups = p.n_groups;
     c.group_ids = p.d_gids;
     CUDA_TRY(cudaMemcpy(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
-    if (p.kind == 0) {
+    if (p.kind % kKindHeatBath == 0) {  // 2D Ising, either algorithm
       int rc = build_resident(device, tv, layout_of_lat, p.smem, p.res);
       if (rc) {
         p.release();
@@ -757,7 +819,10 @@ bool gpumc_engine::has_per_sweep_work() const { return launches_per_batch_sweep(
 uint64_t gpumc_engine::launches_per_batch_sweep() const {
   uint64_t n = 0;
   for (const auto& p : batch_plans)
-    if (!(p.res.on && blocking)) n += (p.kind == 4 || p.kind == 5 || p.kind == 10) ? 2 : 1;
+    if (!(p.res.on && blocking)) {
+      const int base = p.kind % kKindHeatBath;  // O(3) sweeps are two colour launches
+      n += (base == 4 || base == 5 || base == 10) ? 2 : 1;
+    }
   for (gpumc_sim* s : sims)
     if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) n += (uint64_t)s->n_rep + 1;
   return n;

@@ -122,6 +122,56 @@ __device__ __forceinline__ void sincos_turn(uint32_t u, float& c, float& s) {
   s = (octant & 4u) ? -b : b;
 }
 
+// 1 - exp(-x) for x >= 0: the Taylor series x (1 - x/2 + x^2/6 - ... +
+// x^8/9!) in Horner form with fused multiply-adds below x = 1/2 (truncation
+// < 1e-9 relative), else 1 - exp_neg(-x) (no cancellation there).
+__device__ __forceinline__ float one_minus_exp_neg(float x) {
+  if (x < 0.5f) {
+    float p = 0x1.71de3ap-19f;
+    p = __fmaf_rn(p, x, -0x1.a01a02p-16f);
+    p = __fmaf_rn(p, x, 0x1.a01a02p-13f);
+    p = __fmaf_rn(p, x, -0x1.6c16c2p-10f);
+    p = __fmaf_rn(p, x, 0x1.111112p-7f);
+    p = __fmaf_rn(p, x, -0x1.555556p-5f);
+    p = __fmaf_rn(p, x, 0x1.555556p-3f);
+    p = __fmaf_rn(p, x, -0.5f);
+    p = __fmaf_rn(p, x, 1.0f);
+    return fmul(x, p);
+  }
+  return fsub(1.0f, exp_neg(-x));
+}
+
+// 2 atanh(s) = ln((1 + s) / (1 - s)) for |s| <= 0.1716: 2 s (1 + s^2/3 + ... +
+// s^10/11), Horner in s^2 with fused multiply-adds (truncation < 1e-10).
+__device__ __forceinline__ float two_atanh_small(float s) {
+  const float s2 = fmul(s, s);
+  float q = 0x1.745d18p-4f;
+  q = __fmaf_rn(q, s2, 0x1.c71c72p-4f);
+  q = __fmaf_rn(q, s2, 0x1.24924ap-3f);
+  q = __fmaf_rn(q, s2, 0x1.99999ap-3f);
+  q = __fmaf_rn(q, s2, 0x1.555556p-2f);
+  q = __fmaf_rn(q, s2, 1.0f);
+  return fmul(fmul(2.0f, s), q);
+}
+
+// ln(1 - y) for 0 <= y < 1 - 2^-25.  Below y = 1/4 from y directly
+// (s = -y / (2 - y), no rounding of 1 - y); above, from z = 1 - y (exact for
+// y >= 1/2) split as m 2^e with m in [sqrt(1/2), sqrt(2)]:
+// ln z = e ln 2 + 2 atanh((m - 1) / (m + 1)).
+__device__ __forceinline__ float log_one_minus(float y) {
+  if (y < 0.25f) return two_atanh_small(fdiv(-y, fsub(2.0f, y)));
+  const float z = fsub(1.0f, y);
+  const int bits = __float_as_int(z);
+  int e = (bits >> 23) - 127;
+  float m = __int_as_float((bits & 0x7FFFFF) | 0x3F800000);
+  if (m > 0x1.6a09e6p+0f) {
+    m = fmul(m, 0.5f);
+    e += 1;
+  }
+  const float sm = fdiv(fsub(m, 1.0f), fadd(m, 1.0f));
+  return fadd(fmul((float)e, 0x1.62e430p-1f), two_atanh_small(sm));
+}
+
 // log-space Metropolis decision of Carlo.rs/src/acceptance.rs:11-22 with u
 // built from the top 53 bits of a 64-bit draw.
 __device__ __forceinline__ bool accept_log(double logA, unsigned long long u64) {

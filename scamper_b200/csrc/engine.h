@@ -23,8 +23,13 @@ enum Model : int32_t { ISING = 0, POTTS = 1, O3 = 2, MSC = 3 };
 // Stream tags (counter word 1, bits 1..7; bit 0 holds the colour).
 enum Tag : uint32_t {
   TAG_ACC = 0, TAG_PROP = 1, TAG_ACC_REFINE = 2, TAG_PROP_REFINE = 3,
-  TAG_INIT = 4, TAG_O3 = 5, TAG_MSC = 6, TAG_PT = 7, TAG_BITS = 8, TAG_PBITS = 9, TAG_PACC = 10
+  TAG_INIT = 4, TAG_O3 = 5, TAG_MSC = 6, TAG_PT = 7, TAG_BITS = 8, TAG_PBITS = 9, TAG_PACC = 10,
+  TAG_HBITS = 11,  // heat bath: Ising bit planes
+  TAG_HB = 12,     // heat bath: 64-bit uniforms of int8 Potts sites
+  TAG_O3HB = 13    // heat bath: O(3) (cos theta, phi) draws
 };
+
+enum Algorithm : int32_t { METROPOLIS = 0, HEAT_BATH = 1 };
 
 constexpr int kMaxClasses = 13;    // 2z+1 for z = 6 (Potts on the cubic lattice)
 constexpr int kMaxPottsCounts = 8; // fused order-parameter histogram (q <= 8)

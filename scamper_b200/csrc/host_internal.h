@@ -15,7 +15,8 @@ namespace gpumc {
 struct Layout {
   int model = 0, dims = 2, lx = 0, ly = 0, lz = 1, pitch = 0;
   int q = 2;             // Potts states
-  bool bits = false;     // Potts on the bit-sliced kernel (q <= 4)
+  int alg = METROPOLIS;  // sweep algorithm (METROPOLIS / HEAT_BATH)
+  bool bits = false;     // Potts on the bit-sliced kernel (q <= 4, Metropolis)
   bool march = false;    // 3D O(3) on the shared-memory z-march kernel
   int64_t n_sites = 0;
   size_t buf_bytes = 0;  // one ping-pong buffer
@@ -29,7 +30,10 @@ uint64_t stream_key(uint64_t base, uint64_t replica, uint64_t phase, uint64_t su
 void threshold80(double p, uint32_t& head, unsigned long long& tail);
 int n_classes(int model, int dims);
 void build_table(int model, int dims, double J, double beta, uint32_t* head,
-                 unsigned long long* tail);
+                 unsigned long long* tail, int alg);
+// kernel kinds of heat-bath layouts: the Metropolis kind of the same model and
+// geometry plus this offset
+constexpr int kKindHeatBath = 16;
 int validate_spec(const gpumc_spec* s);
 // CTA slots of one B200 (148 SMs x 4 resident sweep CTAs); the engine
 // passes its device's own count.
@@ -57,6 +61,7 @@ int launch_msc_record(cudaStream_t st, LatDesc* lats, GroupDesc* groups, int gro
 // exchange buffer of a tile list that qualifies (see build_resident).
 struct ResidentPlan {
   bool on = false;
+  int alg = METROPOLIS;  // kernel variant (all tiles of a plan share it)
   int2* d_nbr = nullptr;
   uint2* d_xchg = nullptr;
   int xstride = 0;  // uint2 words of exchange space per tile

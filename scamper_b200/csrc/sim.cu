@@ -72,7 +72,7 @@ int gpumc_sim::upload_tables() {
   std::vector<float> bf(n_temps);
   for (int t = 0; t < n_temps; ++t) {
     build_table(lay.model == MSC ? ISING : lay.model, lay.dims, spec.J, betas[t], &head[(size_t)t * n_cls],
-                &tail[(size_t)t * n_cls]);
+                &tail[(size_t)t * n_cls], lay.alg);
     bf[t] = (float)betas[t];
   }
   CUDA_TRY(cudaMemcpyAsync(d_head, head.data(), head.size() * 4, cudaMemcpyHostToDevice, eng->stream));
@@ -87,7 +87,8 @@ int gpumc_sim::push_phase_flags() {
   const int32_t measure = phase == GPUMC_PHASE_MEASUREMENT ? 1 : 0;
   RC_TRY(set_group_field(offsetof(GroupDesc, measure), measure));
   if (lay.model == O3) {
-    const int32_t adapt = phase == GPUMC_PHASE_THERMALIZATION ? 1 : 0;
+    // the cone adapts during thermalization; the heat bath has no cone
+    const int32_t adapt = phase == GPUMC_PHASE_THERMALIZATION && lay.alg == METROPOLIS ? 1 : 0;
     for (int r = 0; r < n_rep; ++r) RC_TRY(set_lat_field(r, offsetof(LatDesc, adapt), adapt));
   }
   CUDA_TRY(cudaStreamSynchronize(eng->stream));
@@ -317,7 +318,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   c.n_groups = 1;
   c.group_ids = s->d_gid;
   CUDA_CLEAN(cudaMemcpy(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
-  if (kernel_kind(s->lay) == 0) {
+  if (kernel_kind(s->lay) % kKindHeatBath == 0) {  // 2D Ising, either algorithm
     std::map<int, const Layout*> lay_of;
     for (int r = 0; r < s->n_rep; ++r) lay_of[s->lat0 + r] = &s->lay;
     rc = build_resident(eng->device, tiles, lay_of, s->lay.smem, s->res);
@@ -349,7 +350,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
     d.sweep = 0;
     d.target = ~0ull;
     d.omc = omc;
-    d.adapt = 1;
+    d.adapt = s->lay.alg == METROPOLIS ? 1 : 0;
     CUDA_CLEAN(cudaMemcpy(eng->d_lats + s->lat0 + r, &d, sizeof(d), cudaMemcpyHostToDevice));
   }
   GroupDesc g;

@@ -26,6 +26,20 @@
 // (CMC.rs/src/observables/*.rs).  The visit order is the checkerboard, not the
 // reference's random permutation (CMC.rs/src/core/visit.rs:50-56); both
 // sample the same Boltzmann distribution.
+//
+// Heat bath (ALG = 1; HeatBathCore, CMC.rs/src/algorithms/heat_bath.rs:41-66,
+// with PottsModel::heat_bath_sample_site, CMC.rs/src/lattice/models.rs:
+// 340-380): the new state of a site is drawn from all q states with weights
+// exp(beta J n_s), n_s = neighbours in state s.  As in the reference the
+// weights are taken relative to the site's largest one, here as 64-bit
+// integers W[d] = floor(2^60 exp(-beta |J| d)) from the host table (d = the
+// state's count distance from the site's most favoured count), so the draw is
+// exact integer arithmetic: x = floor(u * total / 2^64) for a 64-bit uniform
+// u, then the first state whose cumulative weight exceeds x in state order.
+// Word w (0..3) of a 16-site chunk draws one Philox block, counter (chunk,
+// colour | TAG_HB << 1 | w << 8, sweep): words 0-1 are the uniform of its
+// first pass-colour site, words 2-3 of its second.  "Accepted" counts the
+// sites whose state changed.
 #include "device_common.cuh"
 #include "epilogue.cuh"
 
@@ -35,8 +49,87 @@ constexpr uint32_t kM2 = 0x02020202u;
 
 struct SiteTab {
   uint32_t head[kMaxClasses];
-  unsigned long long tail[kMaxClasses];
+  unsigned long long tail[kMaxClasses];  // heat bath: the weights W[d]
+  int32_t jneg;                          // heat bath: J < 0 (favoured = fewest neighbours)
 };
+
+// Heat-bath draw of one Potts site from its neighbour counts n[0..q-1], old
+// state s and 64-bit uniform u; returns the new state t and sets dn = n[t] -
+// n[s] (dE = -J dn).  Exact integer arithmetic (restated by the oracle).
+__device__ __forceinline__ uint32_t potts_hb_pick(const int (&n)[kMaxPottsCounts], int q, uint32_t s,
+                                                  unsigned long long u, const SiteTab& tab, int& dn) {
+  int nmax = 0, nmin = 64;
+#pragma unroll
+  for (int k = 0; k < kMaxPottsCounts; ++k)
+    if (k < q) {
+      nmax = max(nmax, n[k]);
+      nmin = min(nmin, n[k]);
+    }
+  unsigned long long tot = 0;
+#pragma unroll
+  for (int k = 0; k < kMaxPottsCounts; ++k)
+    if (k < q) tot += tab.tail[tab.jneg ? n[k] - nmin : nmax - n[k]];
+  unsigned long long x = __umul64hi(u, tot);
+  uint32_t t = (uint32_t)(q - 1);
+  int nt = 0, ns = 0;
+  bool found = false;
+#pragma unroll
+  for (int k = 0; k < kMaxPottsCounts; ++k)
+    if (k < q) {
+      const unsigned long long w = tab.tail[tab.jneg ? n[k] - nmin : nmax - n[k]];
+      if (!found) {
+        if (x < w) {
+          t = (uint32_t)k;
+          nt = n[k];
+          found = true;
+        } else {
+          x -= w;
+        }
+      }
+      if ((uint32_t)k == s) ns = n[k];
+      if (!found && k == q - 1) nt = n[k];  // unreachable: x < total
+    }
+  dn = nt - ns;
+  return t;
+}
+
+// Heat bath of the two pass-colour sites of one word (bytes 0 and 2 after the
+// pre-shift), from one Philox block r.
+template <int DIM>
+__device__ __forceinline__ uint32_t potts_hb_word(uint32_t o, uint32_t lw, uint32_t rw, uint32_t u,
+                                                  uint32_t d, uint32_t a, uint32_t b, int bsh,
+                                                  const uint4 r, const SiteTab& tab, int q,
+                                                  uint32_t own2, int& nacc, int& dsum) {
+  constexpr int zc = 2 * DIM;
+  const uint32_t os = o >> bsh;
+  const uint32_t sA = os & 0xFFu, sB = (os >> 16) & 0xFFu;
+  const uint32_t nbw[6] = {lw >> bsh, rw >> bsh, u >> bsh, d >> bsh, a >> bsh, b >> bsh};
+  int nA[kMaxPottsCounts], nB[kMaxPottsCounts];
+#pragma unroll
+  for (int k = 0; k < kMaxPottsCounts; ++k) {
+    nA[k] = nB[k] = 0;
+    if (k < q) {
+      const uint32_t pat = (uint32_t)k * 0x00010001u;
+      uint32_t c = 0;  // bytes 0 and 2: neighbours NOT in state k
+#pragma unroll
+      for (int i = 0; i < zc; ++i) {
+        const uint32_t x = (nbw[i] ^ pat) & 0x00FF00FFu;
+        c += ((x + 0x00FF00FFu) >> 8) & 0x00010001u;
+      }
+      nA[k] = zc - (int)(c & 0xFFu);
+      nB[k] = zc - (int)(c >> 16);
+    }
+  }
+  int dA, dB;
+  const uint32_t tA = potts_hb_pick(nA, q, sA, (unsigned long long)r.x | ((unsigned long long)r.y << 32), tab, dA);
+  const uint32_t tB = potts_hb_pick(nB, q, sB, (unsigned long long)r.z | ((unsigned long long)r.w << 32), tab, dB);
+  const int oA = (int)((tA != sA) & (own2 & 1u)), oB = (int)((tB != sB) & ((own2 >> 1) & 1u));
+  nacc += oA + oB;
+  dsum += oA * dA + oB * dB;
+  const uint32_t ns = (os & ~0x00FF00FFu) | tA | (tB << 16);
+  const uint32_t keep = bsh ? 0x00FF00FFu : 0xFF00FF00u;
+  return (o & keep) | (ns << bsh);
+}
 
 // Philox4x32-10 with the per-sweep uniform part hoisted: the counter words
 // 1..3 (colour/tag, sweep) are the same for every draw of a pass, so round 1
@@ -168,9 +261,33 @@ __device__ __forceinline__ uint4 update_chunk(const uint4 own, const uint4 up, c
   return make_uint4(res[0], res[1], res[2], res[3]);
 }
 
+template <int DIM>
+__device__ __forceinline__ uint4 update_chunk_hb(const uint4 own, const uint4 up, const uint4 dn,
+                                                 const uint4 zm, const uint4 zp, uint32_t wprev,
+                                                 uint32_t wnext, int bsh, const PhiloxCtx& P,
+                                                 uint32_t chunk, uint32_t colour, const SiteTab& tab,
+                                                 int q, uint32_t owned16, int& nacc, int& acc2) {
+  const uint32_t o[4] = {own.x, own.y, own.z, own.w};
+  const uint32_t uu[4] = {up.x, up.y, up.z, up.w};
+  const uint32_t dd[4] = {dn.x, dn.y, dn.z, dn.w};
+  const uint32_t aa[4] = {zm.x, zm.y, zm.z, zm.w};
+  const uint32_t bb[4] = {zp.x, zp.y, zp.z, zp.w};
+  const int bp = bsh >> 3;
+  uint32_t res[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t lw = __funnelshift_l(i == 0 ? wprev : o[i - 1], o[i], 8);
+    const uint32_t rw = __funnelshift_r(o[i], i == 3 ? wnext : o[i + 1], 8);
+    const uint32_t own2 = ((owned16 >> (4 * i + bp)) & 1u) | (((owned16 >> (4 * i + bp + 2)) & 1u) << 1);
+    const uint4 r = philox_fast(P, chunk, colour | (TAG_HB << 1) | ((uint32_t)i << 8));
+    res[i] = potts_hb_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, r, tab, q, own2, nacc, acc2);
+  }
+  return make_uint4(res[0], res[1], res[2], res[3]);
+}
+
 // Scalar update of one halo site (positions x0-1 and x0+Wv, whose draws come
 // from chunks the vector pass does not cover), reading plane `src`.
-template <int MODEL, int DIM>
+template <int MODEL, int DIM, int ALG>
 __device__ __forceinline__ int8_t update_site(const int8_t* p, int S, const int8_t* zmp,
                                               const int8_t* zpp, int xr, int y, int z, int ly,
                                               int lx, int pc, const SiteTab& tab, int q,
@@ -186,6 +303,20 @@ __device__ __forceinline__ int8_t update_site(const int8_t* p, int S, const int8
   const uint64_t chunk = rho * (uint64_t)pc + (uint64_t)(xr >> 4);
   const uint64_t site = rho * (uint64_t)lx + (uint64_t)xr;
   const int slot = (xr & 15) >> 1;
+  if (ALG) {
+    int n[kMaxPottsCounts];
+#pragma unroll
+    for (int k = 0; k < kMaxPottsCounts; ++k) {
+      n[k] = 0;
+#pragma unroll
+      for (int i = 0; i < zc; ++i) n[k] += (k < q && nb[i] == k) ? 1 : 0;
+    }
+    const uint4 hv = draw(key, chunk, colour, TAG_HB, (uint32_t)(slot >> 1), sweep);
+    const unsigned long long u = (slot & 1) ? ((unsigned long long)hv.z | ((unsigned long long)hv.w << 32))
+                                            : ((unsigned long long)hv.x | ((unsigned long long)hv.y << 32));
+    int dn;
+    return (int8_t)potts_hb_pick(n, q, (uint32_t)s, u, tab, dn);
+  }
   const uint4 rv = draw(key, chunk, colour, TAG_ACC, 0, sweep);
   const uint32_t w = (slot >> 1) == 0 ? rv.x : (slot >> 1) == 1 ? rv.y : (slot >> 1) == 2 ? rv.z : rv.w;
   const uint32_t uu = (slot & 1) ? (w >> 16) : (w & 0xFFFFu);
@@ -285,7 +416,7 @@ __device__ __forceinline__ void store_halo(uint8_t* plane, const HaloBytes& h) {
 
 // Colour 0 on rows [1, R-1) of plane A, written to plane B (all bytes of the
 // chunk: colour-1 bytes are copied unchanged).
-template <int MODEL, int DIM>
+template <int MODEL, int DIM, int ALG>
 __device__ __forceinline__ void black_pass(const uint8_t* A, const uint8_t* Azm, const uint8_t* Azp,
                                            uint8_t* B, const TileGeom& g, int z, int lz_wrapped_z,
                                            const SiteTab& tab, int q, uint64_t key, uint64_t sweep,
@@ -310,20 +441,25 @@ __device__ __forceinline__ void black_pass(const uint8_t* A, const uint8_t* Azm,
       const uint32_t wprev = *(const uint32_t*)(p - 4);
       const uint32_t wnext = *(const uint32_t*)(p + 16);
       const int bsh = ((y + z) & 1) << 3;
-      const uint4 rnd = philox_fast(P, chunk, 0u | (TAG_ACC << 1));
-      const uint4 rpr = MODEL == POTTS ? philox_fast(P, chunk, 0u | (TAG_PROP << 1)) : zero4;
       const bool row_owned = owned_plane && r >= 2 && r < 2 + g.hv;
       const uint32_t owned = row_owned ? owned_full : 0u;
-      *(uint4*)(B + off) = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, rnd,
-                                                    rpr, tab, q, key,
-                                                    rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c),
-                                                    0u, sweep, owned, nacc, acc2);
+      if (ALG) {
+        *(uint4*)(B + off) = update_chunk_hb<DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, P, chunk, 0u,
+                                                  tab, q, owned, nacc, acc2);
+      } else {
+        const uint4 rnd = philox_fast(P, chunk, 0u | (TAG_ACC << 1));
+        const uint4 rpr = MODEL == POTTS ? philox_fast(P, chunk, 0u | (TAG_PROP << 1)) : zero4;
+        *(uint4*)(B + off) = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, rnd,
+                                                      rpr, tab, q, key,
+                                                      rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c),
+                                                      0u, sweep, owned, nacc, acc2);
+      }
     }
   }
 }
 
 // Scalar halo sites of colour 0 (x0-1 and x0+Wv on rows [1, R-1)), A -> B.
-template <int MODEL, int DIM>
+template <int MODEL, int DIM, int ALG>
 __device__ __forceinline__ void black_halo(const uint8_t* A, const uint8_t* Azm, const uint8_t* Azp,
                                            uint8_t* B, const TileGeom& g, int z,
                                            const SiteTab& tab, int q, uint64_t key,
@@ -336,7 +472,7 @@ __device__ __forceinline__ void black_halo(const uint8_t* A, const uint8_t* Azm,
     const int xr = pos < 0 ? pos + g.lx : (pos >= g.lx ? pos - g.lx : pos);
     const int off = r * g.S + 16 + (pos - g.x0);
     if (((xr + y + z) & 1) == 0)
-      B[off] = (uint8_t)update_site<MODEL, DIM>((const int8_t*)A + off, g.S, (const int8_t*)Azm + off,
+      B[off] = (uint8_t)update_site<MODEL, DIM, ALG>((const int8_t*)A + off, g.S, (const int8_t*)Azm + off,
                                                 (const int8_t*)Azp + off, xr, y, z, g.ly, g.lx, g.pc,
                                                 tab, q, key, 0u, sweep);
     else
@@ -346,7 +482,7 @@ __device__ __forceinline__ void black_halo(const uint8_t* A, const uint8_t* Azm,
 
 // Colour 1 on the tile rows of plane B, written to HBM; magnetisation or
 // Potts histogram of the owned (finished) sites.
-template <int MODEL, int DIM>
+template <int MODEL, int DIM, int ALG>
 __device__ __forceinline__ void white_pass(const uint8_t* B, const uint8_t* Bzm, const uint8_t* Bzp,
                                            const TileGeom& g, int z, const SiteTab& tab, int q,
                                            uint64_t key, uint64_t sweep, const PhiloxCtx& P,
@@ -369,12 +505,17 @@ __device__ __forceinline__ void white_pass(const uint8_t* B, const uint8_t* Bzm,
     const uint32_t wprev = *(const uint32_t*)(p - 4);
     const uint32_t wnext = *(const uint32_t*)(p + 16);
     const int bsh = ((1 + y + z) & 1) << 3;
-    const uint4 rnd = philox_fast(P, chunk, 1u | (TAG_ACC << 1));
-    const uint4 rpr = MODEL == POTTS ? philox_fast(P, chunk, 1u | (TAG_PROP << 1)) : zero4;
-    const uint4 res = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, rnd, rpr,
-                                               tab, q, key,
-                                               rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c), 1u,
-                                               sweep, owned, nacc, acc2);
+    uint4 res;
+    if (ALG) {
+      res = update_chunk_hb<DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, P, chunk, 1u, tab, q, owned,
+                                 nacc, acc2);
+    } else {
+      const uint4 rnd = philox_fast(P, chunk, 1u | (TAG_ACC << 1));
+      const uint4 rpr = MODEL == POTTS ? philox_fast(P, chunk, 1u | (TAG_PROP << 1)) : zero4;
+      res = update_chunk<MODEL, DIM>(own, up, dn, zmv, zpv, wprev, wnext, bsh, rnd, rpr, tab, q, key,
+                                     rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c), 1u, sweep, owned,
+                                     nacc, acc2);
+    }
     *(uint4*)(dst + (size_t)rho * (size_t)g.pitch + g.x0 + 16 * c) = res;
     const uint32_t w[4] = {res.x, res.y, res.z, res.w};
     if (owned == 0xFFFFu) {
@@ -461,6 +602,7 @@ __device__ __forceinline__ void load_table(SiteTab& tab, const LatDesc* L, const
     tab.head[i] = G->head[label * G->n_cls + i];
     tab.tail[i] = G->tail[label * G->n_cls + i];
   }
+  if (threadIdx.x == 0) tab.jneg = G->J < 0.0 ? 1 : 0;
 }
 
 __device__ __forceinline__ TileGeom make_geom(const TileItem& t, const LatDesc* L) {
@@ -484,7 +626,7 @@ __device__ __forceinline__ TileGeom make_geom(const TileItem& t, const LatDesc* 
   return g;
 }
 
-template <int MODEL>
+template <int MODEL, int ALG>
 __global__ void __launch_bounds__(kThreads)
     k_sweep_discrete_2d(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                         GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
@@ -515,11 +657,11 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   int nacc = 0, acc2 = 0, mag = 0;
   int cnt[kMaxPottsCounts] = {0, 0, 0, 0, 0, 0, 0, 0};
-  black_pass<MODEL, 2>(A, A, A, B, g, 0, 0, tab, q, key, sweep, P, true, nacc, acc2);
+  black_pass<MODEL, 2, ALG>(A, A, A, B, g, 0, 0, tab, q, key, sweep, P, true, nacc, acc2);
   __syncthreads();
-  black_halo<MODEL, 2>(A, A, A, B, g, 0, tab, q, key, sweep);
+  black_halo<MODEL, 2, ALG>(A, A, A, B, g, 0, tab, q, key, sweep);
   __syncthreads();
-  white_pass<MODEL, 2>(B, B, B, g, 0, tab, q, key, sweep, P, nxt, nacc, acc2, mag, cnt);
+  white_pass<MODEL, 2, ALG>(B, B, B, g, 0, tab, q, key, sweep, P, nxt, nacc, acc2, mag, cnt);
   flush_accumulators<MODEL, 2>(L, nacc, acc2, mag, cnt, q);
   launch_epilogue(lats, groups, ctl);
 }
@@ -529,7 +671,7 @@ __global__ void __launch_bounds__(kThreads)
 // of plane z0-3+s (its z neighbours are still-old A planes) into the B ring,
 // and colour 1 of plane z0-4+s from the B ring (its z neighbours have
 // finished colour 0) to HBM.
-template <int MODEL>
+template <int MODEL, int ALG>
 __global__ void __launch_bounds__(kThreads)
     k_sweep_discrete_3d(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                         GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
@@ -574,15 +716,15 @@ __global__ void __launch_bounds__(kThreads)
       const uint8_t* Am = Aring + slot(s - 2) * pb;
       uint8_t* Bb = Bring + slot(s - 1) * pb;
       const bool owned_plane = zb >= t.z0 && zb < t.z0 + dv;
-      black_pass<MODEL, 3>(Ab, Am, Al, Bb, g, zbw, 0, tab, q, key, sweep, P, owned_plane, nacc, acc2);
+      black_pass<MODEL, 3, ALG>(Ab, Am, Al, Bb, g, zbw, 0, tab, q, key, sweep, P, owned_plane, nacc, acc2);
       __syncthreads();
-      black_halo<MODEL, 3>(Ab, Am, Al, Bb, g, zbw, tab, q, key, sweep);
+      black_halo<MODEL, 3, ALG>(Ab, Am, Al, Bb, g, zbw, tab, q, key, sweep);
       __syncthreads();
     }
     if (s >= 4) {
       const int zw = zl - 2;
       const int zww = zw < 0 ? zw + lz : (zw >= lz ? zw - lz : zw);
-      white_pass<MODEL, 3>(Bring + slot(s - 2) * pb, Bring + slot(s - 3) * pb, Bring + slot(s - 1) * pb,
+      white_pass<MODEL, 3, ALG>(Bring + slot(s - 2) * pb, Bring + slot(s - 3) * pb, Bring + slot(s - 1) * pb,
                            g, zww, tab, q, key, sweep, P, nxt, nacc, acc2, mag, cnt);
     }
     __syncthreads();  // the next stage overwrites A and B slots read in this step
@@ -591,7 +733,9 @@ __global__ void __launch_bounds__(kThreads)
   launch_epilogue(lats, groups, ctl);
 }
 
-template __global__ void k_sweep_discrete_2d<POTTS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_discrete_3d<POTTS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_discrete_2d<POTTS, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_discrete_3d<POTTS, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_discrete_2d<POTTS, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_discrete_3d<POTTS, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 
 }  // namespace gpumc

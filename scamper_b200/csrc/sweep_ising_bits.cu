@@ -26,6 +26,19 @@
 // (Carlo.rs/src/acceptance.rs:11-22), energy cache += dE
 // (CMC.rs/src/lattice/state.rs:127-136), |M| observable
 // (CMC.rs/src/lattice/models.rs:103-110).
+//
+// Heat bath (ALG = 1; HeatBathCore, CMC.rs/src/algorithms/heat_bath.rs:41-66,
+// with IsingModel::heat_bath_sample_site, CMC.rs/src/lattice/models.rs:158-186):
+// the new spin is +1 with probability p(x) = 1 / (1 + exp(-x)), x = 2 beta J h,
+// h = sum of the neighbour spins = z - 2k with k the number of DOWN neighbours
+// (the adder counts neighbour bits, not anti-aligned ones).  The host table
+// holds T[k] = p(|x_k|) as 80-bit fixed point; classes k and z - k have the
+// same |x| and share one comparator slot.  For the member whose field is
+// positive the site goes up iff u < T; for the negative one it goes down iff
+// ~u < T (the complemented uniform, same distribution), so one threshold and
+// one bit-serial comparison serve both.  The zero-field class k = z/2 goes up
+// iff the first bit of u is 0 (u < 1/2).  The planes come from tag
+// TAG_HBITS.  "Accepted" counts the sites whose spin changed.
 #include "bits_common.cuh"
 #include "epilogue.cuh"
 
@@ -41,7 +54,10 @@ namespace gpumc {
 // multiply-adds of the disjoint class masks.
 struct BitsTab {
   int npend;                  // pending classes (0..3)
-  uint32_t pend_neg[3][3];    // pend_neg[i][b] = ~0 if bit b of class pc[i] is 0
+  uint32_t pend_neg[3][3];    // pend_neg[i][b] = ~0 if bit b of class pc[i] is 0 (heat
+                              // bath: of the positive-field member of pair i)
+  uint32_t pair_neg[3][3];    // heat bath: the same for the negative-field member
+  uint32_t half_neg[3];       // heat bath: the same for the zero-field class z/2
   uint4 tq[20][3];            // tq[q][i].{x,y,z,w} = bit 4q+{0,1,2,3} (MSB first) of T[pc[i]]
 };
 
@@ -111,7 +127,7 @@ struct PassAcc {
 
 // One colour pass over rows [rlo, rlo + nrows) and columns [c_lo, c_hi) of
 // plane `pl` (in place).  For 3D, pm/pp are the neighbouring planes.
-template <int DIM>
+template <int DIM, int ALG>
 __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint2* pp,
                                           const BitsGeom& g, int z, int colour, int rlo,
                                           int nrows, int iters, bool owned_plane, int out_mode,
@@ -136,6 +152,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
     uint32_t own = 0, pending = 0, always = 0, flip = 0;
     uint32_t b0 = 0, b1 = 0, b2 = 0, segid = 0;
     uint32_t m[3] = {0, 0, 0};
+    uint32_t negm = 0, half = 0;  // heat bath: negative-field and zero-field lanes
     int P_ = 0;
     if (active) {
       const int y = wrap_i(g.y0 - g.yo + r, g.ly);
@@ -164,7 +181,9 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
         const int hb = last_seg ? g.hlast - 1 : 31;
         rgt = ((other >> 1) & ~(1u << hb)) | (ne << hb);
       }
-      uint32_t x0 = own ^ lft, x1 = own ^ rgt, x2 = own ^ (P_ ? up.y : up.x), x3 = own ^ (P_ ? dn.y : dn.x);
+      // Metropolis counts anti-aligned neighbours, the heat bath down ones
+      const uint32_t ox = ALG ? 0u : own;
+      uint32_t x0 = ox ^ lft, x1 = ox ^ rgt, x2 = ox ^ (P_ ? up.y : up.x), x3 = ox ^ (P_ ? dn.y : dn.x);
       if (DIM == 2) {
         const uint32_t s0 = x0 ^ x1 ^ x2;
         const uint32_t c0 = (x0 & x1) | (x2 & (x0 ^ x1));
@@ -174,7 +193,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
         b2 = c0 & c1;
       } else {
         const uint2 zm = pm[r * g.NC + cc], zp = pp[r * g.NC + cc];
-        const uint32_t x4 = own ^ (P_ ? zm.y : zm.x), x5 = own ^ (P_ ? zp.y : zp.x);
+        const uint32_t x4 = ox ^ (P_ ? zm.y : zm.x), x5 = ox ^ (P_ ? zp.y : zp.x);
         const uint32_t s0 = x0 ^ x1 ^ x2;
         const uint32_t c0 = (x0 & x1) | (x2 & (x0 ^ x1));
         const uint32_t s1 = x3 ^ x4 ^ x5;
@@ -189,18 +208,32 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       for (int i = 0; i < 3; ++i) {
         if (i < tab.npend) {
           m[i] = (b0 ^ tab.pend_neg[i][0]) & (b1 ^ tab.pend_neg[i][1]) & (b2 ^ tab.pend_neg[i][2]) & valid;
+          if (ALG) {
+            const uint32_t mn =
+                (b0 ^ tab.pair_neg[i][0]) & (b1 ^ tab.pair_neg[i][1]) & (b2 ^ tab.pair_neg[i][2]) & valid;
+            m[i] |= mn;
+            negm |= mn;
+          }
           pending |= m[i];
         }
       }
+      if (ALG) half = (b0 ^ tab.half_neg[0]) & (b1 ^ tab.half_neg[1]) & (b2 ^ tab.half_neg[2]) & valid;
       always = valid & ~pending;
       segid = (uint32_t)(y + g.ly * z) * (uint32_t)g.nseg + (uint32_t)gs;
     }
     // bit-serial comparison of the 32 uniforms against their thresholds
     uint32_t lt = 0, eq = pending;
-    const uint32_t ctrl0 = (uint32_t)colour | (TAG_BITS << 1);
+    const uint32_t ctrl0 = (uint32_t)colour | ((ALG ? TAG_HBITS : TAG_BITS) << 1);
     int q = 0;
     do {
-      const uint4 o = bits_philox(P, segid, ctrl0 | ((uint32_t)q << 8));
+      uint4 o = bits_philox(P, segid, ctrl0 | ((uint32_t)q << 8));
+      if (ALG) {
+        if (q == 0) lt = half & ~o.x;  // zero field: up iff u < 1/2
+        o.x ^= negm;                   // negative field: compare ~u
+        o.y ^= negm;
+        o.z ^= negm;
+        o.w ^= negm;
+      }
       const uint4 t0 = tab.tq[q][0], t1 = tab.tq[q][1];
       uint4 tj = make_uint4(m[0] * t0.x + m[1] * t1.x, m[0] * t0.y + m[1] * t1.y,
                             m[0] * t0.z + m[1] * t1.z, m[0] * t0.w + m[1] * t1.w);
@@ -222,7 +255,8 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       ++q;
     } while (q < 20 && __any_sync(full, eq));
     if (active) {
-      flip = (always | lt) & valid;
+      // heat bath: the new spin is down iff (lt == neg), i.e. ~(lt ^ neg)
+      flip = ALG ? (own ^ ~(lt ^ negm)) & valid : (always | lt) & valid;
       const uint32_t nw = own ^ flip;
       uint2& me = pl[r * g.NC + cc];
       if (P_) me.y = nw;
@@ -230,7 +264,14 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       const bool owned = owned_plane && owned_col && r >= g.yo && r < g.yo + g.hv;
       if (owned) {
         acc.nacc += __popc(flip);
-        acc.ksum += __popc(flip & b0) + 2 * __popc(flip & b1) + 4 * __popc(flip & b2);
+        if (ALG) {
+          // anti-aligned neighbours of a flipped site: k if it was up, z - k if down
+          const uint32_t fu = flip & ~own, fd = flip & own;
+          acc.ksum += __popc(fu & b0) + 2 * __popc(fu & b1) + 4 * __popc(fu & b2) - __popc(fd & b0) -
+                      2 * __popc(fd & b1) - 4 * __popc(fd & b2) + 2 * DIM * __popc(fd);
+        } else {
+          acc.ksum += __popc(flip & b0) + 2 * __popc(flip & b1) + 4 * __popc(flip & b2);
+        }
       }
       if (out_mode != 0) {
         // both colours of this segment are final now: count its down spins
@@ -253,6 +294,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
   }
 }
 
+template <int ALG>
 __device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, const GroupDesc* G) {
   // the label can change between the sweeps of a resident launch: read it
   // from L2, not from a possibly stale L1 line
@@ -260,22 +302,38 @@ __device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, 
   const int n = min(G->n_cls, 7);
   const uint32_t* head = G->head + label * G->n_cls;
   const unsigned long long* tail = G->tail + label * G->n_cls;
-  // pending classes in increasing k (at most three for the Ising table)
-  int pc[3] = {0, 0, 0}, np = 0;
-  for (int k = 0; k < n; ++k)
-    if (head[k] < 65536u && np < 3) pc[np++] = k;
+  // Metropolis: pending classes in increasing k (at most three for the
+  // Ising table).  Heat bath: pair i = classes {i, z - i} (i < z/2) with the
+  // threshold T[i]; its positive-field member is i for J >= 0, else z - i.
+  int pc[3] = {0, 0, 0}, pn[3] = {0, 0, 0}, np = 0;
+  const int zc = n - 1;
+  if (ALG) {
+    const bool jpos = G->J >= 0.0;
+    for (int i = 0; i < zc / 2 && i < 3; ++i) {
+      pc[i] = jpos ? i : zc - i;
+      pn[i] = jpos ? zc - i : i;
+      ++np;
+    }
+  } else {
+    for (int k = 0; k < n; ++k)
+      if (head[k] < 65536u && np < 3) pc[np++] = k;
+  }
   if (threadIdx.x == 0) {
     tab.npend = np;
     for (int i = 0; i < 3; ++i)
-      for (int b = 0; b < 3; ++b)
+      for (int b = 0; b < 3; ++b) {
         tab.pend_neg[i][b] = (i < np && ((pc[i] >> b) & 1)) ? 0u : 0xFFFFFFFFu;
+        tab.pair_neg[i][b] = (i < np && ((pn[i] >> b) & 1)) ? 0u : 0xFFFFFFFFu;
+      }
+    for (int b = 0; b < 3; ++b) tab.half_neg[b] = (((zc / 2) >> b) & 1) ? 0u : 0xFFFFFFFFu;
   }
   for (int e = threadIdx.x; e < 80 * 3; e += kThreads) {
     const int j = e / 3, i = e - 3 * j;
     uint32_t v = 0;
     if (i < np) {
-      const uint32_t h = head[pc[i]];
-      const unsigned long long t = tail[pc[i]];
+      const int k = ALG ? i : pc[i];
+      const uint32_t h = head[k];
+      const unsigned long long t = tail[k];
       v = j < 16 ? (h >> (15 - j)) & 1u : (uint32_t)((t >> (79 - j)) & 1ull);
     }
     reinterpret_cast<uint32_t*>(&tab.tq[j >> 2][i])[j & 3] = v;
@@ -300,7 +358,7 @@ __device__ __forceinline__ void flush_bits(Accum* A, const PassAcc& a, int zc) {
   }
 }
 
-template <int DIM>
+template <int DIM, int ALG>
 __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
     k_sweep_ising_bits(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                        GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
@@ -317,15 +375,15 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
   const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
   int8_t* nxt = (int8_t*)L->buf[(sweep & 1) ^ 1];
   const BitsGeom g = make_bits_geom(t, L);
-  load_bits_table(tab, L, G);
+  load_bits_table<ALG>(tab, L, G);
   const BitsPhilox P = make_bits_philox(L->key, sweep);
   PassAcc acc = {0, 0, 0, 0};
   if (DIM == 2) {
     load_bits_plane(bsm, cur, 0, g);
     __syncthreads();
-    bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nxt, tab, P, acc);
+    bits_pass<2, ALG>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nxt, tab, P, acc);
     __syncthreads();
-    bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
+    bits_pass<2, ALG>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
   } else {
     const int lz = L->lz;
     const int dv = min(L->tile_z, lz - t.z0);
@@ -337,14 +395,14 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
       __syncthreads();
       if (s >= 2) {
         const int zb = zl - 1;
-        bits_pass<3>(bsm + ((s - 1) & 3) * pw, bsm + ((s - 2) & 3) * pw, Pl, g, wrap_i(zb, lz), 0,
+        bits_pass<3, ALG>(bsm + ((s - 1) & 3) * pw, bsm + ((s - 2) & 3) * pw, Pl, g, wrap_i(zb, lz), 0,
                      g.yo / 2, g.yw ? g.R : g.R - 2, g.iters_black, zb >= t.z0 && zb < t.z0 + dv, 0, nxt,
                      tab, P, acc);
         __syncthreads();
       }
       if (s >= 4) {
         const int zw = zl - 2;
-        bits_pass<3>(bsm + ((s - 2) & 3) * pw, bsm + ((s - 3) & 3) * pw, bsm + ((s - 1) & 3) * pw, g,
+        bits_pass<3, ALG>(bsm + ((s - 2) & 3) * pw, bsm + ((s - 3) & 3) * pw, bsm + ((s - 1) & 3) * pw, g,
                      wrap_i(zw, lz), 1, g.yo, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
       }
       __syncthreads();  // the next load overwrites the plane slot read above
@@ -454,6 +512,7 @@ __device__ __forceinline__ void store_owned_rows(const uint2* pl, const BitsGeom
   }
 }
 
+template <int ALG>
 __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_ising_resident(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                            GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl,
@@ -488,13 +547,13 @@ __global__ void __launch_bounds__(kThreads, 4)
                                             : __ldcg(dn + (size_t)(sl - 2) * W + c);
         }
       }
-      load_bits_table(tab, L, G);
+      load_bits_table<ALG>(tab, L, G);
       __syncthreads();
       const BitsPhilox P = make_bits_philox(L->key, sweep);
       PassAcc acc = {0, 0, 0, 0};
-      bits_pass<2>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nullptr, tab, P, acc);
+      bits_pass<2, ALG>(bsm, bsm, bsm, g, 0, 0, 1, g.R - 2, g.iters_black, true, 0, nullptr, tab, P, acc);
       __syncthreads();
-      bits_pass<2>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 2, nullptr, tab, P, acc);
+      bits_pass<2, ALG>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 2, nullptr, tab, P, acc);
       flush_bits((k & 1) ? &L->acc2 : &L->acc, acc, 4);
       __syncthreads();
       uint2* out = mine + (size_t)(k & 1) * slot;
@@ -524,7 +583,13 @@ __global__ void __launch_bounds__(kThreads, 4)
   store_owned_rows(bsm, g, (int8_t*)L->buf[s_end & 1]);
 }
 
-template __global__ void k_sweep_ising_bits<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_ising_bits<3>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_ising_bits<2, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_ising_bits<3, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_ising_bits<2, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_ising_bits<3, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template __global__ void k_sweep_ising_resident<0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*,
+                                                   const int2*, uint2*, int, int);
+template __global__ void k_sweep_ising_resident<1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*,
+                                                   const int2*, uint2*, int, int);
 
 }  // namespace gpumc

@@ -17,9 +17,20 @@
 // dE = -J (s' - s) . h, h the sum of the neighbour spins
 // (ONModel::bond_energy, CMC.rs/src/lattice/models.rs:440-452).
 //
-// Every fp32 operation is an explicitly rounded intrinsic and exp / sin / cos
-// are the engine's own polynomials, so a CPU replay in the same operation
-// order reproduces the device trajectory bit for bit.
+// Heat bath (ALG = 1; ContinuousHeatBathCore, CMC.rs/src/algorithms/
+// heat_bath.rs:75-134, with ContinuousHeatBathable for ONModel<3>,
+// CMC.rs/src/lattice/models.rs:617-663): the new spin is drawn from
+// p(s) ~ exp(beta f . s), f = J h the local field, by inverting the CDF of
+// w = 1 - cos(theta) around f: w = -ln(1 - v (1 - exp(-2 kappa))) / kappa,
+// kappa = beta |f|, v uniform in [0, 1), phi uniform; below kappa = 2^-20 the
+// draw is uniform on the sphere (w = 2v), as the reference's kappa < 1e-12
+// branch.  The sample is placed with the same basis and renormalisation as
+// the cap proposal.  Draws come from tag TAG_O3HB (word 0: v, word 1: phi);
+// there is no cone to adapt, and "accepted" counts the sites that changed.
+//
+// Every fp32 operation is an explicitly rounded intrinsic and exp / log /
+// sin / cos are the engine's own polynomials, so a CPU replay in the same
+// operation order reproduces the device trajectory bit for bit.
 #include "device_common.cuh"
 #include "epilogue.cuh"
 
@@ -34,14 +45,8 @@ namespace gpumc {
 // one division and no square root, never singular since |s + az| >= 1.  The
 // result is renormalised by one Newton step of 1/sqrt(n2) from 1
 // (f = 1.5 - 0.5 n2; n2 is within a few ulp of 1, so f is exact to fp32).
-__device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx, float hy,
-                                          float hz, uint4 o, float omc, float mJ, float beta,
-                                          float& nx, float& ny, float& nz, float& dE) {
-  const float w = fmul(fmul((float)(o.x >> 8), 0x1p-24f), omc);
-  const float ct = fsub(1.0f, w);
-  const float st = fsqrt(fmul(w, fsub(2.0f, w)));
-  float cp, sp;
-  sincos_turn(o.y, cp, sp);
+__device__ __forceinline__ void o3_place(float ax, float ay, float az, float ct, float st, float cp,
+                                         float sp, float& px, float& py, float& pz) {
   const float vx = fmul(st, cp), vy = fmul(st, sp);
   const float sg = az >= 0.0f ? 1.0f : -1.0f;
   const float k = fdiv(-1.0f, fadd(sg, az));
@@ -52,14 +57,28 @@ __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx
   const float e2x = b;
   const float e2y = fadd(sg, fmul(fmul(ay, ay), k));
   const float e2z = -ay;
-  float px = fadd(fadd(fmul(vx, e1x), fmul(vy, e2x)), fmul(ct, ax));
-  float py = fadd(fadd(fmul(vx, e1y), fmul(vy, e2y)), fmul(ct, ay));
-  float pz = fadd(fadd(fmul(vx, e1z), fmul(vy, e2z)), fmul(ct, az));
+  px = fadd(fadd(fmul(vx, e1x), fmul(vy, e2x)), fmul(ct, ax));
+  py = fadd(fadd(fmul(vx, e1y), fmul(vy, e2y)), fmul(ct, ay));
+  pz = fadd(fadd(fmul(vx, e1z), fmul(vy, e2z)), fmul(ct, az));
   const float n2 = fadd(fadd(fmul(px, px), fmul(py, py)), fmul(pz, pz));
   const float f = fsub(1.5f, fmul(0.5f, n2));
   px = fmul(px, f);
   py = fmul(py, f);
   pz = fmul(pz, f);
+}
+
+// Metropolis step with the cap proposal: returns the decision and the
+// proposed spin and its fp32 dE.
+__device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx, float hy,
+                                          float hz, uint4 o, float omc, float mJ, float beta,
+                                          float& nx, float& ny, float& nz, float& dE) {
+  const float w = fmul(fmul((float)(o.x >> 8), 0x1p-24f), omc);
+  const float ct = fsub(1.0f, w);
+  const float st = fsqrt(fmul(w, fsub(2.0f, w)));
+  float cp, sp;
+  sincos_turn(o.y, cp, sp);
+  float px, py, pz;
+  o3_place(ax, ay, az, ct, st, cp, sp, px, py, pz);
   const float dot =
       fadd(fadd(fmul(fsub(px, ax), hx), fmul(fsub(py, ay), hy)), fmul(fsub(pz, az), hz));
   const float de = fmul(mJ, dot);
@@ -76,6 +95,31 @@ __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx
   nz = pz;
   dE = de;
   return ok;
+}
+
+// Heat-bath draw of a site with neighbour sum h (fp32) under coupling Jf.
+__device__ __forceinline__ void o3_heat_bath(float hx, float hy, float hz, uint4 o, float Jf, float beta,
+                                             float& nx, float& ny, float& nz) {
+  const float fx = fmul(Jf, hx), fy = fmul(Jf, hy), fz = fmul(Jf, hz);
+  const float nrm = fsqrt(fadd(fadd(fmul(fx, fx), fmul(fy, fy)), fmul(fz, fz)));
+  const float kap = fmul(beta, nrm);
+  const float v = fmul((float)(o.x >> 8), 0x1p-24f);
+  float w, ax = 0.0f, ay = 0.0f, az = 1.0f;
+  if (!(kap >= 0x1p-20f)) {
+    w = fmul(2.0f, v);
+  } else {
+    const float y = fmul(v, one_minus_exp_neg(fmul(2.0f, kap)));
+    w = fdiv(-log_one_minus(y), kap);
+    if (w > 2.0f) w = 2.0f;
+    ax = fdiv(fx, nrm);
+    ay = fdiv(fy, nrm);
+    az = fdiv(fz, nrm);
+  }
+  const float ct = fsub(1.0f, w);
+  const float st = fsqrt(fmul(w, fsub(2.0f, w)));
+  float cp, sp;
+  sincos_turn(o.y, cp, sp);
+  o3_place(ax, ay, az, ct, st, cp, sp, nx, ny, nz);
 }
 
 // Philox4x32-10 of counter (site, colour | TAG_O3 << 1, sweep) with the
@@ -160,7 +204,7 @@ __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const fl
 
 // One colour pass over a tile of full rows (y0 .. y0+hv-1, planes z0 ..
 // z0+dv-1), one thread per site of the colour.
-template <int DIM, int COLOUR>
+template <int DIM, int COLOUR, int ALG>
 __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_o3(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
@@ -185,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   const float mJ = -G->Jf;
   const double Jd = G->J;
   const float omc = L->omc;
-  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | (TAG_O3 << 1));
+  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(L->tile_y, ly - t.y0);
   const int dv = DIM == 3 ? min(L->tile_z, lz - t.z0) : 1;
   const int half = lx >> 1;
@@ -229,8 +273,13 @@ __global__ void __launch_bounds__(kThreads, 4)
   };
   auto update = [&](const O3Site& q) {
     float nx, ny, nz, de;
-    const bool ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx,
-                              ny, nz, de);
+    bool ok;
+    if (ALG) {
+      o3_heat_bath(q.hx, q.hy, q.hz, o3_philox(P, q.site), -mJ, beta, nx, ny, nz);
+      ok = (nx != q.ax) | (ny != q.ay) | (nz != q.az);
+    } else {
+      ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx, ny, nz, de);
+    }
     float fx = q.ax, fy = q.ay, fz = q.az;
     if (ok) {
       // energy cache: exact fp64 change of the fp32 configuration (the
@@ -299,7 +348,7 @@ __device__ __forceinline__ void o3_cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
-template <int COLOUR>
+template <int COLOUR, int ALG>
 __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                      GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
@@ -320,7 +369,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   const float mJ = -G->Jf;
   const double Jd = G->J;
   const float omc = L->omc;
-  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | (TAG_O3 << 1));
+  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(L->tile_y, ly - t.y0);
   const int dv = min(L->tile_z, lz - t.z0);
   const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
@@ -345,8 +394,13 @@ __global__ void __launch_bounds__(kThreads, 4)
   const int dr = kThreads / half, dj = kThreads - dr * half;  // cursor step of kThreads items
   auto update = [&](const O3Site& q) {
     float nx, ny, nz, de;
-    const bool ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx,
-                              ny, nz, de);
+    bool ok;
+    if (ALG) {
+      o3_heat_bath(q.hx, q.hy, q.hz, o3_philox(P, q.site), -mJ, beta, nx, ny, nz);
+      ok = (nx != q.ax) | (ny != q.ay) | (nz != q.az);
+    } else {
+      ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx, ny, nz, de);
+    }
     float fx = q.ax, fy = q.ay, fz = q.az;
     if (ok) {
       // energy cache: exact fp64 change of the fp32 configuration
@@ -455,12 +509,14 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
 
-template __global__ void k_sweep_o3_march<0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_o3_march<1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-
-template __global__ void k_sweep_o3<2, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_o3<2, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_o3<3, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template __global__ void k_sweep_o3<3, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+#define O3_INSTANTIATE(ALG)                                                                          \
+  template __global__ void k_sweep_o3_march<0, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \
+  template __global__ void k_sweep_o3_march<1, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \
+  template __global__ void k_sweep_o3<2, 0, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);    \
+  template __global__ void k_sweep_o3<2, 1, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);    \
+  template __global__ void k_sweep_o3<3, 0, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);    \
+  template __global__ void k_sweep_o3<3, 1, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+O3_INSTANTIATE(0)
+O3_INSTANTIATE(1)
 
 }  // namespace gpumc

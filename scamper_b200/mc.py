@@ -50,6 +50,24 @@ class Params(dict):
 
 
 MODELS = {"ising": _lib.ISING, "potts": _lib.POTTS, "heisenberg": _lib.O3, "o3": _lib.O3}
+# the algorithm type parameter of ClassicalMC<H, A> (CMC.rs/src/classical_mc.rs:21-31):
+# MetropolisCore, or HeatBathCore / ContinuousHeatBathCore
+# (CMC.rs/src/algorithms/heat_bath.rs:12-134)
+ALGORITHMS = {"metropolis": _lib.METROPOLIS, "metropolis-hastings": _lib.METROPOLIS,
+              "heat_bath": _lib.HEAT_BATH, "heatbath": _lib.HEAT_BATH,
+              "continuous_heat_bath": _lib.HEAT_BATH}
+
+
+def algorithm_id(algorithm):
+    if algorithm is None:
+        return _lib.METROPOLIS
+    if isinstance(algorithm, int):
+        return algorithm
+    a = str(algorithm).lower()
+    if a not in ALGORITHMS:
+        raise InvalidConfig(_lib.EINVAL, f"algorithm: unknown algorithm `{algorithm}` "
+                                         "(expected metropolis or heat_bath)")
+    return ALGORITHMS[a]
 
 
 def _positive(params, key, default):
@@ -85,7 +103,7 @@ def lattice_from_params(params):
                         "engine (square, cubic, hypercubic)")
 
 
-def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capacity=1024):
+def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capacity=1024, algorithm=None):
     params = params if isinstance(params, Params) else Params(params)
     mname = model if model is not None else str(params.get("model", "ising")).lower()
     if isinstance(mname, int):
@@ -111,7 +129,7 @@ def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capaci
                      q=params.get_as("q", int, 3), J=params.get_as("J", float, 1.0),
                      n_replicas=n_replicas, n_temps=len(betas), betas=arr, init=init_id,
                      cone_half_angle=params.get_as("cone_half_angle", float, 1.0),
-                     record_capacity=record_capacity)
+                     record_capacity=record_capacity, algorithm=algorithm_id(algorithm))
     return spec, arr
 
 
@@ -167,23 +185,30 @@ class ClassicalMC:
         self.n_sites = int(np.prod(self.shape))
         self.n_replicas = spec.n_replicas
         self.betas = [spec.betas[i] for i in range(spec.n_temps)]
+        self.algorithm = spec.algorithm
         self.phase = _lib.PHASE_THERMALIZATION
 
     # -- FromParams -----------------------------------------------------------
     @staticmethod
-    def validate_params(params, model=None):
-        spec, _keep = spec_from_params(params, model=model)
+    def validate_params(params, model=None, algorithm=None):
+        spec, _keep = spec_from_params(params, model=model, algorithm=algorithm)
         _lib.call("gpumc_validate", ctypes.byref(spec))
 
     @classmethod
     def from_params(cls, params, seed, model=None, n_replicas=1, betas=None, engine=None,
-                    record_capacity=1024):
+                    record_capacity=1024, algorithm=None):
+        """`algorithm`: "metropolis" (MetropolisCore, the default) or
+        "heat_bath" (HeatBathCore for Ising / Potts, ContinuousHeatBathCore
+        for O(3))."""
         spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas,
-                                      record_capacity=record_capacity)
+                                      record_capacity=record_capacity, algorithm=algorithm)
         return cls(spec, seed, engine=engine, _keep=keep)
 
     # -- MonteCarlo -----------------------------------------------------------
     def name(self):
+        """Algorithm::name (CMC.rs/src/algorithms/heat_bath.rs:69-71, :131-133)."""
+        if self.algorithm == _lib.HEAT_BATH:
+            return "ContinuousHeatBath" if self.model == _lib.O3 else "HeatBath"
         return self.NAME
 
     def on_phase_start(self, phase):
@@ -433,8 +458,10 @@ class Server:
                   ctypes.byref(self.h))
         self._keep = {}
 
-    def submit(self, params, seed, n_sweeps, n_therm=0, model=None, n_replicas=1, betas=None):
-        spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas)
+    def submit(self, params, seed, n_sweeps, n_therm=0, model=None, n_replicas=1, betas=None,
+               algorithm=None):
+        spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas,
+                                      algorithm=algorithm)
         job = _lib.Job(spec=spec, base_seed=seed, n_sweeps=n_sweeps, n_therm=n_therm)
         jid = ctypes.c_uint64()
         rc = _lib.load().gpumc_submit(self.h, ctypes.byref(job), ctypes.byref(jid))

@@ -33,7 +33,19 @@ CASES = [
     ("o3", [8, 6, 20], 0.69, 110, 3, {"alpha": 0.8}),
     ("msc", [66, 10], 0.4407, 111, 3, {}),
     ("msc", [34, 6, 20], 0.2216, 112, 2, {}),
+    # heat bath
+    ("ising", [64, 64], 0.4407, 121, 5, {"algorithm": "heat_bath"}),
+    ("ising", [34, 6, 20], 0.3, 122, 4, {"algorithm": "heat_bath", "J": -1.0}),
+    ("potts", [66, 10], 1.0, 123, 4, {"q": 3, "algorithm": "heat_bath"}),
+    ("potts", [18, 8, 10], 0.6, 124, 3, {"q": 6, "algorithm": "heat_bath"}),
+    ("o3", [66, 10], 0.7, 125, 3, {"algorithm": "heat_bath"}),
+    ("o3", [16, 8, 12], 0.69, 126, 3, {"algorithm": "heat_bath"}),
 ]
+
+
+def case_id(c):
+    suffix = "-hb" if c["extra"].get("algorithm") == "heat_bath" else ""
+    return f"{c['model']}-{'x'.join(map(str, c['shape']))}{suffix}"
 
 
 def omc(alpha):
@@ -46,8 +58,9 @@ def fingerprint(state):
 
 def run_case(oracle, model, shape, beta, seed, sweeps, extra):
     mid = {"ising": oracle.ISING, "potts": oracle.POTTS, "o3": oracle.O3, "msc": oracle.MSC}[model]
+    alg = oracle.HEAT_BATH if extra.get("algorithm") == "heat_bath" else oracle.METROPOLIS
     lat = oracle.Lattice(mid, tuple(shape), q=extra.get("q", 3), J=extra.get("J", 1.0), beta=beta,
-                         seed=seed, omc=omc(extra.get("alpha", 1.0)))
+                         seed=seed, omc=omc(extra.get("alpha", 1.0)), algorithm=alg)
     for _ in range(sweeps):
         lat.sweep(adapt=False)
     st = lat.state()

@@ -20,7 +20,7 @@ with open(os.path.join(HERE, "golden", "replay_fingerprints.json")) as f:
     CASES = json.load(f)["cases"]
 
 
-@pytest.mark.parametrize("case", CASES, ids=[f"{c['model']}-{'x'.join(map(str, c['shape']))}" for c in CASES])
+@pytest.mark.parametrize("case", CASES, ids=[make_golden.case_id(c) for c in CASES])
 def test_oracle_reproduces_golden_fingerprints(oracle, case):
     got = make_golden.run_case(oracle, case["model"], case["shape"], case["beta"], case["seed"],
                                case["sweeps"], case["extra"])

@@ -219,7 +219,9 @@ def _golden_cases():
 
 
 @pytest.mark.parametrize("case", _golden_cases(),
-                         ids=[f"{c['model']}-{'x'.join(map(str, c['shape']))}" for c in _golden_cases()])
+                         ids=[f"{c['model']}-{'x'.join(map(str, c['shape']))}"
+                              + ("-hb" if c["extra"].get("algorithm") == "heat_bath" else "")
+                              for c in _golden_cases()])
 def test_device_matches_committed_golden_fingerprints(gpumc, case):
     """The device against the committed fixtures, without the oracle."""
     import hashlib
@@ -230,7 +232,8 @@ def test_device_matches_committed_golden_fingerprints(gpumc, case):
     if case["model"] == "msc":
         mc = gpumc.MultiSpinIsing.from_params(params, case["seed"])
     else:
-        mc = gpumc.ClassicalMC.from_params(params, case["seed"], model=case["model"])
+        mc = gpumc.ClassicalMC.from_params(params, case["seed"], model=case["model"],
+                                           algorithm=extra.get("algorithm"))
     mc.on_phase_start(_lib.PHASE_MEASUREMENT)  # no cone adaptation (O(3))
     mc.sweep(case["sweeps"])
     st = np.ascontiguousarray(_gpu_state(mc))
