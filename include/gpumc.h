@@ -149,6 +149,25 @@ int gpumc_set_phase(gpumc_sim* sim, int32_t phase);
 int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps);
 /* Drains recorded measurements (oldest first); *n receives the count. */
 int gpumc_observables(gpumc_sim* sim, gpumc_obs* out, size_t cap, size_t* n);
+/* Device-side binning of the measured observables (the carlo-rs Accumulator,
+ * Carlo.rs/src/measurements.rs:60-183, fed on the device): while measuring,
+ * each sweep adds Energy, E2, Magnetization, M2, M4 (powi moments: e*e, m*m,
+ * (m*m)*(m*m)) of every slot to its open bin in sample order, and a full bin
+ * of `binsize` samples becomes one bin mean (sum / binsize) - the values a
+ * host Accumulator of the same bin size computes from the records.  A slot is
+ * a temperature index when the handle has one beta per replica (PT chains),
+ * else a replica index.  Per-sweep records are not written while binning is
+ * on.  binsize 0 switches back to records; enabling resets the bin state
+ * (records measured before stay available to gpumc_observables).
+ * bin_capacity = completed bins buffered on the device (drained by the host
+ * as needed).  Not for the multi-spin model or server jobs. */
+int gpumc_set_binning(gpumc_sim* sim, int32_t binsize, int32_t bin_capacity);
+/* Completed bins, oldest first: out[bin][slot][5] (slots = n_replicas);
+ * *n_bins receives the count (at most cap_bins). */
+int gpumc_drain_bins(gpumc_sim* sim, double* out, size_t cap_bins, size_t* n_bins);
+/* The open (partial) bin: sums[slot][5] of its samples and their count *fill
+ * (the reference's trailing partial bin, counted at finalize). */
+int gpumc_open_bin(gpumc_sim* sim, double* sums, int32_t* fill);
 /* Spin state of one replica in the reference's site order (x fastest,
  * CMC.rs/src/lattice/graph.rs:417-451): int8 (+-1 Ising, 0..q-1 Potts),
  * float32[3] per site (O(3)), uint64 per site (multi-spin). */

@@ -11,12 +11,14 @@ from ._lib import GpumcError, InvalidConfig
 from .measurements import Accumulator, Context, Estimate, binder_cumulant, specific_heat
 from .mc import (ClassicalMC, Engine, MultiSpinIsing, Params, Server, geometric_ladder_betas,
                  potts_beta_c, run_one)
+from .results import Metadata, Results
 from .snapshot import CheckpointCorrupted
 
 _lib.load()
 
 __all__ = [
     "Accumulator", "CheckpointCorrupted", "ClassicalMC", "Context", "Engine", "Estimate", "GpumcError", "InvalidConfig",
-    "MultiSpinIsing", "Params", "Server", "binder_cumulant", "geometric_ladder_betas", "potts_beta_c",
+    "Metadata", "MultiSpinIsing", "Params", "Results", "Server", "binder_cumulant", "geometric_ladder_betas",
+    "potts_beta_c",
     "run_one", "specific_heat",
 ]

@@ -111,6 +111,9 @@ SIGNATURES = {
     "gpumc_set_phase": [_vp, ctypes.c_int32],
     "gpumc_sweep": [_vp, ctypes.c_uint32],
     "gpumc_observables": [_vp, _P(Obs), ctypes.c_size_t, _P(ctypes.c_size_t)],
+    "gpumc_set_binning": [_vp, ctypes.c_int32, ctypes.c_int32],
+    "gpumc_drain_bins": [_vp, _P(ctypes.c_double), ctypes.c_size_t, _P(ctypes.c_size_t)],
+    "gpumc_open_bin": [_vp, _P(ctypes.c_double), _P(ctypes.c_int32)],
     "gpumc_get_spins": [_vp, ctypes.c_int32, _vp, ctypes.c_size_t],
     "gpumc_set_spins": [_vp, ctypes.c_int32, _vp, ctypes.c_size_t],
     "gpumc_energy": [_vp, _P(ctypes.c_double)],

@@ -854,12 +854,8 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
     // never outrun the smallest free record space of a measuring simulation
     uint32_t room = left;
     for (gpumc_sim* s : eng->sims) {
-      if (s->phase != GPUMC_PHASE_MEASUREMENT || s->device_schedule) continue;
-      if (s->rec_used >= s->rec_cap) {
-        rc = s->drain_records();
-        if (rc) return rc;
-      }
-      room = std::min<uint32_t>(room, (uint32_t)(s->rec_cap - s->rec_used));
+      rc = s->measure_room(room);
+      if (rc) return rc;
     }
     const uint32_t chunk = std::min<uint32_t>(room, 64);
     if (eng->has_per_sweep_work()) {
@@ -879,7 +875,7 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
     if (rc) return rc;
     for (gpumc_sim* s : eng->sims) {
       s->sweeps = std::min<uint64_t>(s->sweeps + chunk, s->target);
-      if (s->phase == GPUMC_PHASE_MEASUREMENT && !s->device_schedule) s->rec_used += (int)chunk;
+      s->note_measured(chunk);
     }
     left -= chunk;
   }

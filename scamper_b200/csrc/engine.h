@@ -34,6 +34,9 @@ enum Algorithm : int32_t { METROPOLIS = 0, HEAT_BATH = 1 };
 constexpr int kMaxClasses = 13;    // 2z+1 for z = 6 (Potts on the cubic lattice)
 constexpr int kMaxPottsCounts = 8; // fused order-parameter histogram (q <= 8)
 constexpr int kThreads = 256;      // CTA size of the sweep kernels
+// observables binned on the device, in this order: Energy, E2, Magnetization,
+// M2, M4 (DefaultObservableSet, CMC.rs/src/observables/common.rs:81-95)
+constexpr int kBinObs = 5;
 
 // Per-sweep accumulators, filled with atomics by the sweep kernels and
 // drained by the epilogue (last CTA of the launch).
@@ -100,6 +103,15 @@ struct GroupDesc {
   uint64_t pt_step;               // exchanges attempted so far
   unsigned long long pt_accepted; // accepted swaps (all pairs)
   Record* records;                // [rec_cap][n_rep]
+  // device-side binning of the measured observables (binsize 0: records)
+  int32_t binsize;                // samples per bin
+  int32_t bin_cap;                // completed bins the ring holds
+  int32_t bin_count;              // completed bins not yet drained
+  int32_t bin_fill;               // samples in the open bin (all slots alike)
+  int32_t bin_by_label;           // slot = temperature label (else replica index)
+  int32_t bin_overflow;
+  double* bin_open;               // [n_rep][kBinObs] sums of the open bin
+  double* bins;                   // [bin_cap][n_rep][kBinObs] completed bin means
 };
 
 struct TileItem {

@@ -36,7 +36,44 @@ __device__ __forceinline__ float o3_adapt(float omc, long long accepted, long lo
 }
 
 // Epilogue flags of a group for the sweep being finished (GroupDesc::epi).
-constexpr int32_t kEpiFinished = 1, kEpiMeasuring = 2, kEpiRecord = 4, kEpiMsc = 8, kEpiExchange = 16;
+constexpr int32_t kEpiFinished = 1, kEpiMeasuring = 2, kEpiRecord = 4, kEpiMsc = 8, kEpiExchange = 16,
+                  kEpiBin = 32;
+
+// One measured sample of a replica into the open bin of its slot: the values
+// Context::measure receives for Energy, E2, Magnetization, M2, M4 (the moments
+// as powi computes them: e*e, m*m, (m*m)*(m*m)), summed in sample order with
+// one rounding per operation, so that the bin means equal a host Accumulator's
+// (Carlo.rs/src/measurements.rs:60-183: sum of the bin's samples / binsize).
+// Magnetization as the records report it: |M|/N (Ising), (q max_s n_s - N) /
+// (N (q - 1)) (Potts), |sum s|/N (O(3)).
+static __device__ void bin_sample(const LatDesc* L, GroupDesc* G, int r, const Record& R) {
+  const int s = G->bin_by_label ? R.label : r;
+  double* acc = G->bin_open + (size_t)s * kBinObs;
+  const double n = (double)L->n_sites;
+  double m;
+  if (L->model == POTTS)
+    m = __ddiv_rn(__dsub_rn(__dmul_rn((double)L->q, R.m[0]), n), __dmul_rn(n, (double)(L->q - 1)));
+  else if (L->model == O3)
+    m = __ddiv_rn(__dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(R.m[0], R.m[0]), __dmul_rn(R.m[1], R.m[1])),
+                                       __dmul_rn(R.m[2], R.m[2]))),
+                  n);
+  else
+    m = __ddiv_rn(fabs(R.m[0]), n);
+  const double m2 = __dmul_rn(m, m);
+  const double v[kBinObs] = {R.energy, __dmul_rn(R.energy, R.energy), m, m2, __dmul_rn(m2, m2)};
+  const bool close = G->bin_fill + 1 >= G->binsize;
+  const bool room = G->bin_count < G->bin_cap;
+#pragma unroll
+  for (int k = 0; k < kBinObs; ++k) {
+    const double a = __dadd_rn(acc[k], v[k]);
+    if (close) {
+      if (room) G->bins[((size_t)G->bin_count * G->n_rep + s) * kBinObs + k] = __ddiv_rn(a, (double)G->binsize);
+      acc[k] = 0.0;
+    } else {
+      acc[k] = a;
+    }
+  }
+}
 
 // Per-replica part of the sweep epilogue: drain the accumulators of slot
 // `slot`, update the cached energy, write the record, advance the sweep.
@@ -75,6 +112,7 @@ static __device__ void finish_replica(LatDesc* lats, GroupDesc* G, int r, int32_
   R.pad = 0;
   R.sweep = L->sweep;
   if (flags & kEpiRecord) G->records[(size_t)G->rec_count * G->n_rep + r] = R;
+  if (flags & kEpiBin) bin_sample(L, G, r, R);
   L->sweep += 1;
 }
 
@@ -113,8 +151,10 @@ static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int
       } else {
         const bool msc = L0->model == MSC;
         const bool measuring = G->measure && L0->sweep >= G->measure_from;
+        const bool binning = !msc && G->binsize > 0;
         f = (msc ? kEpiMsc : 0) | (measuring ? kEpiMeasuring : 0) |
-            ((!msc && measuring && G->rec_count < G->rec_cap) ? kEpiRecord : 0);
+            ((!msc && !binning && measuring && G->rec_count < G->rec_cap) ? kEpiRecord : 0) |
+            ((binning && measuring) ? kEpiBin : 0);
         n = G->n_rep;
       }
       s_f[t] = f;
@@ -150,7 +190,13 @@ static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int
     if (G) {
       const int32_t f = s_f[t];
       if (!(f & kEpiFinished)) {
-        if ((f & kEpiMeasuring) && !(f & kEpiMsc)) {
+        if (f & kEpiBin) {
+          if (++G->bin_fill >= G->binsize) {
+            G->bin_fill = 0;
+            if (G->bin_count < G->bin_cap) G->bin_count += 1;
+            else G->bin_overflow = 1;
+          }
+        } else if ((f & kEpiMeasuring) && !(f & kEpiMsc)) {
           if (f & kEpiRecord) G->rec_count += 1;
           else G->overflow = 1;
         }

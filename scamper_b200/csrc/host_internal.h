@@ -159,8 +159,17 @@ struct gpumc_sim {
   int phase = GPUMC_PHASE_THERMALIZATION;
   uint32_t pt_interval = 0;
   std::vector<gpumc_obs> pending;
+  // device-side binning (gpumc_set_binning)
+  int binsize = 0, bin_cap = 0;
+  double* d_bin_open = nullptr;      // [n_rep][kBinObs]
+  double* d_bins = nullptr;          // [bin_cap][n_rep][kBinObs]
+  uint64_t bin_total = 0;            // measured sweeps in the device ring + open bin
+  std::vector<double> pending_bins;  // drained bins, [bin][n_rep][kBinObs]
 
   ~gpumc_sim();
+  int measure_room(uint32_t& room);
+  void note_measured(uint32_t chunk);
+  int drain_bins();
   int launch_one_sweep();
   int launch_msc_measurement();
   int run_graph(uint32_t n);

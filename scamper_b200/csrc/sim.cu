@@ -54,6 +54,8 @@ gpumc_sim::~gpumc_sim() {
   cudaFree(d_label);
   cudaFree(d_rep_at);
   cudaFree(d_records);
+  cudaFree(d_bin_open);
+  cudaFree(d_bins);
   cudaFree(d_msc_counters);
   cudaFree(d_tiles);
   cudaFree(d_gid);
@@ -167,6 +169,49 @@ int gpumc_sim::drain_records() {
   }
   rec_used = 0;
   return GPUMC_OK;
+}
+
+// Moves the completed bins of the device ring to pending_bins; the open bin
+// stays on the device.
+int gpumc_sim::drain_bins() {
+  CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  GroupDesc g;
+  CUDA_TRY(cudaMemcpy(&g, eng->d_groups + group, sizeof(GroupDesc), cudaMemcpyDeviceToHost));
+  if (g.bin_overflow) return fail(GPUMC_ESTATE, "bin buffer overflow (internal scheduling error)");
+  if (g.bin_count > 0) {
+    const size_t n = (size_t)g.bin_count * n_rep * kBinObs;
+    const size_t at = pending_bins.size();
+    pending_bins.resize(at + n);
+    CUDA_TRY(cudaMemcpy(pending_bins.data() + at, d_bins, n * sizeof(double), cudaMemcpyDeviceToHost));
+    const int32_t zero = 0;
+    RC_TRY(set_group_field(offsetof(GroupDesc, bin_count), zero));
+    CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  }
+  bin_total = (uint64_t)g.bin_fill;
+  return GPUMC_OK;
+}
+
+// Clamps `room` to the measured sweeps the device can take before its record
+// ring (or bin ring) is full, draining it first when it already is.
+int gpumc_sim::measure_room(uint32_t& room) {
+  if (phase != GPUMC_PHASE_MEASUREMENT || device_schedule) return GPUMC_OK;
+  if (binsize > 0) {
+    const uint64_t cap = (uint64_t)bin_cap * (uint64_t)binsize;
+    if (bin_total >= cap) RC_TRY(drain_bins());
+    room = (uint32_t)std::min<uint64_t>(room, cap - bin_total);
+  } else {
+    if (rec_used >= rec_cap) RC_TRY(drain_records());
+    room = std::min<uint32_t>(room, (uint32_t)(rec_cap - rec_used));
+  }
+  return GPUMC_OK;
+}
+
+void gpumc_sim::note_measured(uint32_t chunk) {
+  if (phase != GPUMC_PHASE_MEASUREMENT || device_schedule) return;
+  if (binsize > 0)
+    bin_total += chunk;
+  else
+    rec_used += (int)chunk;
 }
 
 // Launches the exact energy reduction of one buffer into d_e (int64 units of
@@ -443,10 +488,7 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
   uint32_t left = n_sweeps;
   while (left > 0) {
     uint32_t room = left;
-    if (sim->phase == GPUMC_PHASE_MEASUREMENT) {
-      if (sim->rec_used >= sim->rec_cap) RC_TRY(sim->drain_records());
-      room = std::min<uint32_t>(room, (uint32_t)(sim->rec_cap - sim->rec_used));
-    }
+    RC_TRY(sim->measure_room(room));
     const uint32_t chunk = std::min<uint32_t>(room, 64);
     if (sim->res.on && sim->blocking) {
       RC_TRY(launch_resident(sim->eng->stream, sim->d_tiles, sim->n_tiles, sim->eng->d_lats, sim->eng->d_groups,
@@ -459,9 +501,79 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
       sim->launches += (uint64_t)chunk * (uint64_t)lps;
     }
     sim->sweeps += chunk;
-    if (sim->phase == GPUMC_PHASE_MEASUREMENT) sim->rec_used += (int)chunk;
+    sim->note_measured(chunk);
     left -= chunk;
   }
+  return GPUMC_OK;
+}
+
+int gpumc_set_binning(gpumc_sim* sim, int32_t binsize, int32_t bin_capacity) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (binsize < 0) return fail(GPUMC_EINVAL, "binsize: must be >= 0 (0 = per-sweep records)");
+  if (binsize > 0 && bin_capacity < 1) return fail(GPUMC_EINVAL, "bin_capacity: must be >= 1");
+  if (binsize > 0 && sim->lay.model == MSC)
+    return fail(GPUMC_EINVAL, "binsize: the multi-spin model reports per-replica records only");
+  if (sim->device_schedule) return fail(GPUMC_ESTATE, "binning: not available for server jobs");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  RC_TRY(sim->drain_records());  // records measured so far stay available
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  cudaFree(sim->d_bin_open);
+  cudaFree(sim->d_bins);
+  sim->d_bin_open = sim->d_bins = nullptr;
+  sim->pending_bins.clear();
+  sim->bin_total = 0;
+  sim->binsize = 0;
+  sim->bin_cap = 0;
+  const size_t per = (size_t)sim->n_rep * kBinObs;
+  if (binsize > 0) {
+    CUDA_TRY(cudaMalloc(&sim->d_bin_open, per * sizeof(double)));
+    CUDA_TRY(cudaMemset(sim->d_bin_open, 0, per * sizeof(double)));
+    if (cudaMalloc(&sim->d_bins, per * (size_t)bin_capacity * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(sim->d_bin_open);
+      sim->d_bin_open = nullptr;
+      return fail(GPUMC_ENOMEM, "bin_capacity: device memory exhausted");
+    }
+    sim->binsize = binsize;
+    sim->bin_cap = bin_capacity;
+  }
+  const int32_t zero = 0, by_label = (sim->n_temps == sim->n_rep && sim->n_rep > 1) ? 1 : 0;
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, binsize), (int32_t)sim->binsize));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bin_cap), (int32_t)sim->bin_cap));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bin_count), zero));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bin_fill), zero));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bin_by_label), by_label));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bin_overflow), zero));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bin_open), sim->d_bin_open));
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, bins), sim->d_bins));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  return GPUMC_OK;
+}
+
+int gpumc_drain_bins(gpumc_sim* sim, double* out, size_t cap_bins, size_t* n_bins) {
+  if (!sim || !n_bins) return fail(GPUMC_EINVAL, "sim/n_bins: null");
+  if (sim->binsize <= 0) return fail(GPUMC_ESTATE, "binning: not enabled (gpumc_set_binning)");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  RC_TRY(sim->drain_bins());
+  const size_t per = (size_t)sim->n_rep * kBinObs;
+  const size_t k = std::min(cap_bins, sim->pending_bins.size() / per);
+  if (k && !out) return fail(GPUMC_EINVAL, "out: null");
+  std::copy(sim->pending_bins.begin(), sim->pending_bins.begin() + k * per, out);
+  sim->pending_bins.erase(sim->pending_bins.begin(), sim->pending_bins.begin() + k * per);
+  *n_bins = k;
+  return GPUMC_OK;
+}
+
+int gpumc_open_bin(gpumc_sim* sim, double* sums, int32_t* fill) {
+  if (!sim || !sums || !fill) return fail(GPUMC_EINVAL, "sim/sums/fill: null");
+  if (sim->binsize <= 0) return fail(GPUMC_ESTATE, "binning: not enabled (gpumc_set_binning)");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  GroupDesc g;
+  CUDA_TRY(cudaMemcpy(&g, sim->eng->d_groups + sim->group, sizeof(GroupDesc), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(sums, sim->d_bin_open, (size_t)sim->n_rep * kBinObs * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+  *fill = g.bin_fill;
   return GPUMC_OK;
 }
 

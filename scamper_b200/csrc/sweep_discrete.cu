@@ -45,8 +45,6 @@
 
 namespace gpumc {
 
-constexpr uint32_t kM2 = 0x02020202u;
-
 struct SiteTab {
   uint32_t head[kMaxClasses];
   unsigned long long tail[kMaxClasses];  // heat bath: the weights W[d]

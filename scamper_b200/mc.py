@@ -242,7 +242,10 @@ class ClassicalMC:
 
     def measure(self, ctx, namespace_by_chain=False):
         """Feeds every pending record into `ctx` with the reference's names
-        (DefaultObservableSet::measure_all, CMC.rs/src/observables/common.rs:81-95)."""
+        (DefaultObservableSet::measure_all, CMC.rs/src/observables/common.rs:81-95);
+        with device binning on, the completed device bins instead."""
+        if getattr(self, "binsize", 0):
+            return self._measure_bins(ctx)
         for r in self.observables():
             if namespace_by_chain or self.n_replicas > 1:
                 ctx.set_measurement_namespace(f"pt_chain_{r['temp_index']:04d}")
@@ -252,10 +255,93 @@ class ClassicalMC:
             ctx.measure("E2", e * e)
             ctx.measure("Magnetization", m)
             ctx.measure("M2", m * m)
-            ctx.measure("M4", m * m * m * m)
+            ctx.measure("M4", (m * m) * (m * m))  # powi(4): two squarings
             if namespace_by_chain or self.n_replicas > 1:
                 ctx.measure("_pt_parameter", r["beta"])
                 ctx.set_measurement_namespace(None)
+
+    # -- device-side binning --------------------------------------------------
+    BIN_NAMES = ("Energy", "E2", "Magnetization", "M2", "M4")
+
+    def enable_device_binning(self, binsize, capacity=4096):
+        """Bins Energy, E2, Magnetization, M2, M4 on the device (gpumc_set_binning):
+        measure(ctx) then feeds completed bins to ctx's accumulators, which must
+        use the same bin size; per-sweep records are not kept meanwhile.
+        binsize 0 switches back to records."""
+        _lib.call("gpumc_set_binning", self.h, int(binsize), int(capacity))
+        self.binsize = int(binsize)
+
+    def _bin_slot_name(self, slot):
+        if self.n_replicas == 1:
+            return None
+        if len(self.betas) == self.n_replicas:
+            return f"pt_chain_{slot:04d}"  # slot = temperature index
+        return f"replica_{slot:04d}"
+
+    def drain_bins(self):
+        """Completed bins, shape (n_bins, n_replicas, 5)."""
+        out = []
+        cap = 1024
+        buf = (ctypes.c_double * (cap * self.n_replicas * 5))()
+        while True:
+            n = ctypes.c_size_t()
+            _lib.call("gpumc_drain_bins", self.h, buf, cap, ctypes.byref(n))
+            if n.value == 0:
+                break
+            out.append(np.frombuffer(buf, dtype=np.float64, count=n.value * self.n_replicas * 5).copy())
+            if n.value < cap:
+                break
+        if not out:
+            return np.zeros((0, self.n_replicas, 5))
+        return np.concatenate(out).reshape(-1, self.n_replicas, 5)
+
+    def open_bin(self):
+        """(sums of the open bin, shape (n_replicas, 5), its sample count)."""
+        buf = (ctypes.c_double * (self.n_replicas * 5))()
+        fill = ctypes.c_int32()
+        _lib.call("gpumc_open_bin", self.h, buf, ctypes.byref(fill))
+        return np.array(buf[:]).reshape(self.n_replicas, 5), fill.value
+
+    def _measure_bins(self, ctx):
+        if ctx.binsize != self.binsize:
+            raise ValueError(f"device bins hold {self.binsize} samples, the context bins {ctx.binsize}")
+        bins = self.drain_bins()
+        if len(bins) == 0:
+            return
+        per_chain = len(self.betas) == self.n_replicas and self.n_replicas > 1
+        for slot in range(self.n_replicas):
+            ctx.set_measurement_namespace(self._bin_slot_name(slot))
+            for k, name in enumerate(self.BIN_NAMES):
+                ctx.accumulator(name).add_bins(bins[:, slot, k])
+            if per_chain:
+                # the chain's parameter is constant: the bin mean add() would
+                # produce from binsize equal samples
+                total = 0.0
+                for _ in range(self.binsize):
+                    total += self.betas[slot]
+                ctx.accumulator("_pt_parameter").add_bins(np.full(len(bins), total / self.binsize))
+        ctx.set_measurement_namespace(None)
+
+    def finish_measurements(self, ctx):
+        """Drains the last completed bins and hands the open bin to ctx as its
+        trailing partial bin (call once, before ctx.finalize_measurements())."""
+        if not getattr(self, "binsize", 0):
+            return self.measure(ctx)
+        self._measure_bins(ctx)
+        sums, fill = self.open_bin()
+        if fill == 0:
+            return
+        per_chain = len(self.betas) == self.n_replicas and self.n_replicas > 1
+        for slot in range(self.n_replicas):
+            ctx.set_measurement_namespace(self._bin_slot_name(slot))
+            for k, name in enumerate(self.BIN_NAMES):
+                ctx.accumulator(name).set_open_bin(sums[slot, k], fill)
+            if per_chain:
+                total = 0.0
+                for _ in range(fill):
+                    total += self.betas[slot]
+                ctx.accumulator("_pt_parameter").set_open_bin(total, fill)
+        ctx.set_measurement_namespace(None)
 
     # -- state ----------------------------------------------------------------
     def _site_dtype(self):
@@ -409,16 +495,17 @@ class MultiSpinIsing(ClassicalMC):
             row = recs[i:i + 64]
             e = np.array([r["energy"] for r in row])
             m = np.array([r["magnetization"] for r in row])
+            m4 = m * m * m * m  # left to right, as multi_spin.rs:268
             ctx.measure_array("Energy_replica", e)
             ctx.measure_array("Magnetization_replica", m)
             ctx.measure_array("E2_replica", e * e)
             ctx.measure_array("M2_replica", m * m)
-            ctx.measure_array("M4_replica", m ** 4)
+            ctx.measure_array("M4_replica", m4)
             ctx.measure("Energy", e[0])
             ctx.measure("Magnetization", m[0])
-            ctx.measure("E2", e[0] ** 2)
-            ctx.measure("M2", m[0] ** 2)
-            ctx.measure("M4", m[0] ** 4)
+            ctx.measure("E2", e[0] * e[0])
+            ctx.measure("M2", m[0] * m[0])
+            ctx.measure("M4", m4[0])
 
 
 def run_one(mc, thermalization_sweeps, measurement_sweeps, binsize=1):
@@ -435,6 +522,8 @@ def run_one(mc, thermalization_sweeps, measurement_sweeps, binsize=1):
         mc.sweep(k)
         mc.measure(ctx)
         left -= k
+    if getattr(mc, "binsize", 0):
+        mc.finish_measurements(ctx)
     return ctx.finalize_measurements()
 
 

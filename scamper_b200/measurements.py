@@ -69,6 +69,26 @@ class Accumulator:
         for x in np.asarray(values, dtype=np.float64).ravel():
             self.add(x)
 
+    def add_bins(self, means):
+        """Appends completed scalar bins computed elsewhere (the device's
+        binning: each mean is the sum of `bin_capacity` samples in order /
+        bin_capacity, the value add() would have produced).  Only valid at a
+        bin boundary."""
+        if self.filling:
+            raise ValueError("add_bins: the accumulator has an open bin")
+        for m in np.asarray(means, dtype=np.float64).ravel():
+            self.bins.append(np.array([m]))
+            self.total_count += self.bin_capacity
+
+    def set_open_bin(self, total, filling):
+        """The open (partial) bin: `filling` samples summing to `total`."""
+        if self.filling:
+            raise ValueError("set_open_bin: the accumulator has an open bin")
+        if filling > 0:
+            self.current = np.array([float(total)])
+            self.filling = int(filling)
+            self.total_count += int(filling)
+
     def autocorr_time(self):
         if len(self.bins) < 2:
             return 1.0
@@ -113,6 +133,14 @@ class Context:
         if key not in self.obs:
             self.obs[key] = Accumulator(self.binsize)
         self.obs[key].add(value)
+
+    def accumulator(self, name):
+        """The accumulator of `name` in the current namespace (created with
+        the context's bin size)."""
+        key = self._key(name)
+        if key not in self.obs:
+            self.obs[key] = Accumulator(self.binsize)
+        return self.obs[key]
 
     def measure_array(self, name, values):
         key = self._key(name)
