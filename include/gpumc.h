@@ -52,6 +52,12 @@ extern "C" {
  * model has Metropolis only. */
 #define GPUMC_METROPOLIS 0
 #define GPUMC_HEAT_BATH 1
+/* cluster updates, Ising and Potts with J >= 0: one Swendsen-Wang update of
+ * every cluster (SWCore, CMC.rs/src/algorithms/swendsen_wang.rs:73-138) or one
+ * Wolff cluster flip (WolffCore, CMC.rs/src/algorithms/wolff.rs:73-135) per
+ * sweep */
+#define GPUMC_SWENDSEN_WANG 2
+#define GPUMC_WOLFF 3
 
 #define GPUMC_INIT_HOT 0  /* "hot" / "random" initial_state */
 #define GPUMC_INIT_COLD 1 /* "cold" / "ordered" */
@@ -83,7 +89,7 @@ typedef struct {
   int32_t init;             /* GPUMC_INIT_HOT / GPUMC_INIT_COLD                */
   double cone_half_angle;   /* O(3): initial cap half-angle (radians), (0, pi] */
   int32_t record_capacity;  /* measured sweeps buffered on the device (>= 1)   */
-  int32_t algorithm;        /* GPUMC_METROPOLIS / GPUMC_HEAT_BATH              */
+  int32_t algorithm;        /* GPUMC_METROPOLIS / HEAT_BATH / SWENDSEN_WANG / WOLFF */
 } gpumc_spec;
 
 /* One measured sweep of one replica (Context::measure of Energy, E2,

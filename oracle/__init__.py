@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 ISING, POTTS, O3, MSC = 0, 1, 2, 3
-METROPOLIS, HEAT_BATH = 0, 1
+METROPOLIS, HEAT_BATH, SWENDSEN_WANG, WOLFF = 0, 1, 2, 3
 TAG_ACC, TAG_PROP, TAG_ACC_REFINE, TAG_PROP_REFINE, TAG_INIT, TAG_O3, TAG_MSC, TAG_PT = range(8)
 SUB_INIT, SUB_SWEEP = 0, 1
 
@@ -55,6 +55,9 @@ def lib():
             "orc_sweep_o3_hb": (ctypes.c_double, [_int, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float,
                                                   _u64, _u64, _f32p, _f32p, _f32p, _i64p]),
             "orc_one_minus_exp_neg": (ctypes.c_float, [ctypes.c_float]),
+            "orc_cluster_threshold": (_u64, [_int, ctypes.c_double, ctypes.c_double]),
+            "orc_sweep_cluster": (_i64, [_int, _int, _i64, _i64, _i64, _int, _int, _u64, _u64, _u64, _i8p,
+                                         _i64p]),
             "orc_log_one_minus": (ctypes.c_float, [ctypes.c_float]),
             "orc_init_discrete": (None, [_int, _int, _i64, _i64, _i64, _int, _u64, _u64, _int, _i8p]),
             "orc_sweep_discrete": (_i64, [_int, _int, _i64, _i64, _i64, _int, _u32p, _u64p, _u64, _u64,
@@ -178,14 +181,21 @@ class Lattice:
 
     def set_beta(self, beta):
         self.beta = beta
-        if self.model != O3:
+        if self.algorithm in (SWENDSEN_WANG, WOLFF):
+            self.thr = lib().orc_cluster_threshold(self.model, self.J, beta)
+        elif self.model != O3:
             tm = ISING if self.model == MSC else self.model
             self.head, self.tail = table(tm, self.dims, self.J, beta, self.algorithm)
 
     def sweep(self, adapt=False):
         L = lib()
         acc = ctypes.c_int64()
-        if self.model in (ISING, POTTS) and self.algorithm == HEAT_BATH:
+        if self.algorithm in (SWENDSEN_WANG, WOLFF):
+            d = L.orc_sweep_cluster(self.model, self.dims, self.lx, self.ly, self.lz, self.q,
+                                    1 if self.algorithm == WOLFF else 0, self.thr, self.key, self.sweeps,
+                                    _p(self.spins, _i8p), ctypes.byref(acc))
+            self.e_int += d
+        elif self.model in (ISING, POTTS) and self.algorithm == HEAT_BATH:
             d = L.orc_sweep_discrete_hb(self.model, self.dims, self.lx, self.ly, self.lz, self.q, self.J,
                                         _p(self.head, _u32p), _p(self.tail, _u64p), self.key,
                                         self.sweeps, _p(self.spins, _i8p), ctypes.byref(acc))

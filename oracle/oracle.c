@@ -506,6 +506,119 @@ int64_t orc_sweep_discrete_hb(int model, int dims, int64_t lx, int64_t ly, int64
     return dE;
 }
 
+uint64_t orc_cluster_threshold(int model, double J, double beta) {
+    double p = model == ORC_POTTS ? 1.0 - exp(-beta * J) : 1.0 - exp(-2.0 * beta * J);
+    p = p < 0.0 ? 0.0 : p;
+    return p >= 1.0 ? ~(uint64_t)0 : (uint64_t)ldexp(p, 64);
+}
+
+static uint32_t uf_find(uint32_t* par, uint32_t a) {
+    while (par[a] != a) {
+        par[a] = par[par[a]];
+        a = par[a];
+    }
+    return a;
+}
+
+/* the larger root under the smaller: every root is its component's minimum */
+static void uf_union(uint32_t* par, uint32_t a, uint32_t b) {
+    a = uf_find(par, a);
+    b = uf_find(par, b);
+    if (a < b) par[b] = a;
+    else if (b < a) par[a] = b;
+}
+
+/* integer in [0, n) by 32-bit multiply-shift with exact rejection over the
+ * four words of a block; 0 if all are rejected */
+static uint32_t uniform_below4(const uint32_t w[4], uint32_t n) {
+    uint32_t rej = (uint32_t)(0x100000000ull % n);
+    for (int i = 0; i < 4; ++i) {
+        uint64_t m = (uint64_t)w[i] * n;
+        if ((uint32_t)m >= rej) return (uint32_t)(m >> 32);
+    }
+    return 0;
+}
+
+int64_t orc_sweep_cluster(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q, int wolff,
+                          uint64_t thr, uint64_t key64, uint64_t sweep, int8_t* spins, int64_t* changed) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    int64_t n = lx * ly * g.lz;
+    uint32_t key[2];
+    key_of(key64, key);
+    uint32_t* par = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
+    int8_t* sn = (int8_t*)malloc((size_t)n);
+    for (int64_t i = 0; i < n; ++i) par[i] = (uint32_t)i;
+    /* bonds: Philox(site, TAG_SW, plane 0): +x words 0-1, +y words 2-3;
+     * plane 1: +z words 0-1 */
+    for (int64_t z = 0; z < g.lz; ++z)
+        for (int64_t y = 0; y < ly; ++y)
+            for (int64_t x = 0; x < lx; ++x) {
+                int64_t s = site_of(&g, x, y, z);
+                uint32_t ctr[4], o[4], o2[4];
+                make_ctr(ctr, (uint64_t)s, 0, ORC_TAG_SW, 0, sweep);
+                orc_philox4x32_10(ctr, key, o);
+                if (dims == 3) {
+                    make_ctr(ctr, (uint64_t)s, 0, ORC_TAG_SW, 1, sweep);
+                    orc_philox4x32_10(ctr, key, o2);
+                }
+                for (int d = 0; d < dims; ++d) {
+                    int64_t nb = d == 0 ? site_of(&g, x + 1 < lx ? x + 1 : 0, y, z)
+                               : d == 1 ? site_of(&g, x, y + 1 < ly ? y + 1 : 0, z)
+                                        : site_of(&g, x, y, z + 1 < g.lz ? z + 1 : 0);
+                    uint64_t u = d == 0 ? ((uint64_t)o[0] | ((uint64_t)o[1] << 32))
+                               : d == 1 ? ((uint64_t)o[2] | ((uint64_t)o[3] << 32))
+                                        : ((uint64_t)o2[0] | ((uint64_t)o2[1] << 32));
+                    if (spins[nb] == spins[s] && u < thr) uf_union(par, (uint32_t)s, (uint32_t)nb);
+                }
+            }
+    uint32_t seed_root = 0;
+    int8_t target = 0;
+    if (wolff) {
+        uint32_t ctr[4], o[4];
+        make_ctr(ctr, 0, 0, ORC_TAG_WOLFF, 0, sweep);
+        orc_philox4x32_10(ctr, key, o);
+        uint64_t nn = (uint64_t)n, rej = (0 - nn) % nn, seed = 0;
+        uint64_t u[2] = {(uint64_t)o[0] | ((uint64_t)o[1] << 32), (uint64_t)o[2] | ((uint64_t)o[3] << 32)};
+        for (int i = 0; i < 2; ++i)
+            if (u[i] * nn >= rej) {
+                seed = (uint64_t)(((unsigned __int128)u[i] * nn) >> 64);
+                break;
+            }
+        int8_t ss = spins[seed];
+        if (model == ORC_ISING) {
+            target = (int8_t)-ss;
+        } else {
+            make_ctr(ctr, 0, 0, ORC_TAG_WOLFF, 1, sweep);
+            orc_philox4x32_10(ctr, key, o);
+            uint32_t r = uniform_below4(o, (uint32_t)(q - 1));
+            target = (int8_t)((int)r < ss ? (int)r : (int)r + 1);
+        }
+        seed_root = uf_find(par, (uint32_t)seed);
+    }
+    int64_t nch = 0;
+    for (int64_t s = 0; s < n; ++s) {
+        uint32_t r = uf_find(par, (uint32_t)s);
+        int8_t v;
+        if (wolff) {
+            v = r == seed_root ? target : spins[s];
+        } else {
+            uint32_t ctr[4], o[4];
+            make_ctr(ctr, r, 0, ORC_TAG_SWFLIP, 0, sweep);
+            orc_philox4x32_10(ctr, key, o);
+            v = model == ORC_ISING ? ((o[0] >> 31) ? 1 : -1) : (int8_t)uniform_below4(o, (uint32_t)q);
+        }
+        sn[s] = v;
+        nch += v != spins[s];
+    }
+    int64_t e0 = orc_energy_int(model, dims, lx, ly, lz, spins);
+    memcpy(spins, sn, (size_t)n);
+    int64_t e1 = orc_energy_int(model, dims, lx, ly, lz, spins);
+    free(par);
+    free(sn);
+    if (changed) *changed = nch;
+    return e1 - e0;
+}
+
 int64_t orc_energy_int(int model, int dims, int64_t lx, int64_t ly, int64_t lz,
                        const int8_t* spins) {
     geom g = {dims, lx, ly, dims == 3 ? lz : 1};

@@ -44,7 +44,10 @@ enum {
     ORC_TAG_PACC = 10,      /* Potts (q <= 4) acceptance bit planes         */
     ORC_TAG_HBITS = 11,     /* heat bath: Ising bit planes                  */
     ORC_TAG_HB = 12,        /* heat bath: 64-bit uniforms of int8 Potts sites */
-    ORC_TAG_O3HB = 13       /* heat bath: O(3) (cos theta, phi) draws       */
+    ORC_TAG_O3HB = 13,      /* heat bath: O(3) (cos theta, phi) draws       */
+    ORC_TAG_SW = 14,        /* cluster updates: bond activations            */
+    ORC_TAG_SWFLIP = 15,    /* Swendsen-Wang: cluster decisions             */
+    ORC_TAG_WOLFF = 16      /* Wolff: seed site and target state            */
 };
 
 /* Substream ids used with RngStreamKey::with_substream. */
@@ -112,6 +115,16 @@ int64_t orc_sweep_discrete_hb(int model, int dims, int64_t lx, int64_t ly, int64
 double orc_sweep_o3_hb(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
                        uint64_t key64, uint64_t sweep, float* sx, float* sy, float* sz,
                        int64_t* changed);
+/* Cluster updates (SWCore, CMC.rs/src/algorithms/swendsen_wang.rs:73-138;
+ * WolffCore, CMC.rs/src/algorithms/wolff.rs:73-135) of an int8 Ising / Potts
+ * lattice in the engine's random streams: bonds between equal neighbours
+ * active iff a 64-bit uniform is below `thr` (orc_cluster_threshold),
+ * components by union-find with the minimum site as root, one decision per
+ * root (SW) or the seed's component flipped to the target (Wolff).  Returns
+ * dE in units of J; *changed = sites whose spin changed. */
+uint64_t orc_cluster_threshold(int model, double J, double beta);
+int64_t orc_sweep_cluster(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q, int wolff,
+                          uint64_t thr, uint64_t key64, uint64_t sweep, int8_t* spins, int64_t* changed);
 float orc_one_minus_exp_neg(float x);
 float orc_log_one_minus(float y);
 double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,

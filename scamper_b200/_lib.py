@@ -28,6 +28,8 @@ INIT_COLD = 1
 
 METROPOLIS = 0
 HEAT_BATH = 1
+SWENDSEN_WANG = 2
+WOLFF = 3
 PHASE_THERMALIZATION = 1
 PHASE_MEASUREMENT = 2
 

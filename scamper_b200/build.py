@@ -10,7 +10,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 SOURCES = ["capi.cu", "sim.cu", "server.cu", "sweep_discrete.cu", "sweep_o3.cu",
            "sweep_msc.cu", "lattice_ops.cu", "noalloc.cu",
-           "sweep_ising_bits.cu", "sweep_potts_bits.cu"]
+           "sweep_ising_bits.cu", "sweep_potts_bits.cu", "cluster.cu"]
 LIB = os.path.join(HERE, "libgpumc.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

@@ -39,6 +39,12 @@ template <int DIM>
 __global__ void k_sweep_potts_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int COLOUR, int ALG>
 __global__ void k_sweep_o3_march(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int MODEL, int WOLFF>
+__global__ void k_cluster_local(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int MODEL, int WOLFF>
+__global__ void k_cluster_global(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int MODEL, int WOLFF>
+__global__ void k_cluster_flip(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int ALG>
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
                                        uint2*, int, int);
@@ -137,6 +143,19 @@ void build_table(int model, int dims, double J, double beta, uint32_t* head,
                  unsigned long long* tail, int alg) {
   const int z = 2 * dims;
   const int n = n_classes(model, dims);
+  if (alg == SWENDSEN_WANG || alg == WOLFF) {
+    // cluster bond activation (ClusterModel::cluster_bond_probability,
+    // models.rs:130-147, :312-329): tail[0] = floor(p 2^64), active iff a
+    // 64-bit uniform is below it (p >= 1: all ones)
+    for (int c = 0; c < n; ++c) {
+      head[c] = 0;
+      tail[c] = 0;
+    }
+    double p = model == POTTS ? 1.0 - std::exp(-beta * J) : 1.0 - std::exp(-2.0 * beta * J);
+    p = p < 0.0 ? 0.0 : p;
+    tail[0] = p >= 1.0 ? ~0ull : (unsigned long long)std::ldexp(p, 64);
+    return;
+  }
   if (alg == HEAT_BATH) {
     for (int c = 0; c < n; ++c) {
       head[c] = 0;
@@ -202,10 +221,16 @@ int validate_spec(const gpumc_spec* s) {
   if (s->model == GPUMC_O3 && !(s->cone_half_angle > 0.0 && s->cone_half_angle <= M_PI))
     return fail(GPUMC_EINVAL, "cone_half_angle: must be in (0, pi]");
   if (s->record_capacity < 1) return fail(GPUMC_EINVAL, "record_capacity: must be >= 1");
-  if (s->algorithm != GPUMC_METROPOLIS && s->algorithm != GPUMC_HEAT_BATH)
-    return fail(GPUMC_EINVAL, "algorithm: expected metropolis or heat_bath");
-  if (s->algorithm == GPUMC_HEAT_BATH && s->model == GPUMC_ISING_MSC64)
+  if (s->algorithm < GPUMC_METROPOLIS || s->algorithm > GPUMC_WOLFF)
+    return fail(GPUMC_EINVAL, "algorithm: expected metropolis, heat_bath, swendsen_wang or wolff");
+  if (s->algorithm != GPUMC_METROPOLIS && s->model == GPUMC_ISING_MSC64)
     return fail(GPUMC_EINVAL, "algorithm: the multi-spin model has Metropolis sweeps only");
+  if (s->algorithm >= GPUMC_SWENDSEN_WANG) {
+    if (s->model != GPUMC_ISING && s->model != GPUMC_POTTS)
+      return fail(GPUMC_EINVAL, "algorithm: cluster updates are implemented for Ising and Potts");
+    if (s->J < 0.0)
+      return fail(GPUMC_EINVAL, "J: ferromagnetic cluster updates require J >= 0");
+  }
   if (!layout_ok(plan_layout(s)))
     return fail(GPUMC_EINVAL, "lattice: no tile plan fits this geometry (row too long for shared memory)");
   return GPUMC_OK;
@@ -233,9 +258,9 @@ static size_t bits_tile_smem(const Layout& L, const TileItem& t) {
 // every tile the plan enumerates.
 bool layout_ok(const Layout& L) {
   if (!(L.buf_bytes > 0 && L.tile_cx > 0 && L.tile_y > 0 && L.tile_z > 0 &&
-        (L.smem > 0 || L.model == O3) && L.smem <= 200 * 1024))
+        (L.smem > 0 || L.model == O3 || L.cluster) && L.smem <= 200 * 1024))
     return false;
-  if (L.model == ISING || (L.model == POTTS && L.bits)) {
+  if (!L.cluster && (L.model == ISING || (L.model == POTTS && L.bits))) {
     std::vector<TileItem> tiles;
     enumerate_tiles(L, 0, tiles);
     for (const TileItem& t : tiles)
@@ -278,7 +303,10 @@ int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots) {
 Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
   Layout L;
   L.model = s->model;
-  L.alg = s->algorithm == GPUMC_HEAT_BATH ? HEAT_BATH : METROPOLIS;
+  L.alg = s->algorithm == GPUMC_HEAT_BATH ? HEAT_BATH
+          : s->algorithm == GPUMC_SWENDSEN_WANG ? SWENDSEN_WANG
+          : s->algorithm == GPUMC_WOLFF ? WOLFF : METROPOLIS;
+  L.cluster = L.alg == SWENDSEN_WANG || L.alg == WOLFF;
   L.q = (int)s->q;
   L.dims = s->dims;
   L.lx = (int)s->lx;
@@ -436,10 +464,19 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
       L.smem = 4 * 8 * (size_t)(L.tile_y + 4) * (W + 4);
     }
   }
+  if (L.cluster) {
+    // cluster updates keep the model's buffer layout; their kernels take
+    // tiles of 16 x 16 (2D) or 8 x 8 x 4 (3D) sites, one thread per site
+    L.tile_cx = L.dims == 2 ? 16 : 8;  // sites
+    L.tile_y = L.dims == 2 ? 16 : 8;
+    L.tile_z = L.dims == 2 ? 1 : 4;
+    L.smem = 0;
+  }
   return L;
 }
 
 int tile_width_sites(const Layout& L) {
+  if (L.cluster) return L.tile_cx;
   if (L.model == ISING) return 64 * L.tile_cx;
   if (L.model == POTTS) return (L.bits ? 64 : 16) * L.tile_cx;
   if (L.model == O3) return 4 * L.tile_cx;
@@ -458,6 +495,7 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
 // runs the bit-sliced kernel (kinds 8 / 9); heat-bath layouts add
 // kKindHeatBath to the kind of the same model and geometry.
 int kernel_kind(const Layout& L) {
+  if (L.cluster) return kKindCluster + (L.model == POTTS ? 2 : 0) + (L.dims - 2) + (L.alg == WOLFF ? 4 : 0);
   const int hb = L.alg == HEAT_BATH ? kKindHeatBath : 0;
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
   if (L.model == O3 && L.march) return 10 + hb;
@@ -468,7 +506,8 @@ size_t footprint_bytes(const gpumc_spec* s) {
   const Layout L = plan_layout(s);
   const size_t per = (L.inplace ? 1 : 2) * L.buf_bytes;
   const size_t rec_entries = (size_t)s->record_capacity * s->n_replicas * (L.model == MSC ? 64 : 1);
-  return per * s->n_replicas + rec_entries * sizeof(Record) +
+  const size_t labels = L.cluster ? 4 * (size_t)L.n_sites : 0;
+  return (per + labels) * s->n_replicas + rec_entries * sizeof(Record) +
          (size_t)s->n_temps * kMaxClasses * 12 + 4096;
 }
 
@@ -531,6 +570,23 @@ static int prepare_kernels() {
 int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
                         LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem) {
   if (n_tiles <= 0) return GPUMC_OK;
+  if (is_cluster_kind(kind)) {
+    // local bonds + union, global union across tiles, flip (+ epilogue)
+    static const SweepKernel ck[8][3] = {
+        {k_cluster_local<2, ISING, 0>, k_cluster_global<2, ISING, 0>, k_cluster_flip<2, ISING, 0>},
+        {k_cluster_local<3, ISING, 0>, k_cluster_global<3, ISING, 0>, k_cluster_flip<3, ISING, 0>},
+        {k_cluster_local<2, POTTS, 0>, k_cluster_global<2, POTTS, 0>, k_cluster_flip<2, POTTS, 0>},
+        {k_cluster_local<3, POTTS, 0>, k_cluster_global<3, POTTS, 0>, k_cluster_flip<3, POTTS, 0>},
+        {k_cluster_local<2, ISING, 1>, k_cluster_global<2, ISING, 1>, k_cluster_flip<2, ISING, 1>},
+        {k_cluster_local<3, ISING, 1>, k_cluster_global<3, ISING, 1>, k_cluster_flip<3, ISING, 1>},
+        {k_cluster_local<2, POTTS, 1>, k_cluster_global<2, POTTS, 1>, k_cluster_flip<2, POTTS, 1>},
+        {k_cluster_local<3, POTTS, 1>, k_cluster_global<3, POTTS, 1>, k_cluster_flip<3, POTTS, 1>}};
+    const int c = kind - kKindCluster;
+    if (c < 0 || c >= 8) return fail(GPUMC_EINVAL, "internal: no cluster kernel for this layout");
+    for (int i = 0; i < 3; ++i) ck[c][i]<<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+    CUDA_TRY(cudaGetLastError());
+    return GPUMC_OK;
+  }
   const SweepKernel k = kernel_for(kind);
   if (!k) return fail(GPUMC_EINVAL, "internal: no sweep kernel for this layout");
   // O(3) sweeps in place: colour 0, then colour 1 (which runs the epilogue)
@@ -678,7 +734,7 @@ int gpumc_engine_launch_count(gpumc_engine* eng, uint64_t* n) {
 
 int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n) {
   if (!sim || !n) return fail(GPUMC_EINVAL, "null argument");
-  *n = (sim->lay.model == O3 ? 2 : 1) +
+  *n = (sim->lay.cluster ? 3 : sim->lay.model == O3 ? 2 : 1) +
        ((sim->lay.model == MSC && sim->phase == GPUMC_PHASE_MEASUREMENT) ? sim->n_rep + 1 : 0);
   return GPUMC_OK;
 }
@@ -800,7 +856,7 @@ int gpumc_engine::rebuild_batch() {
     c.n_groups = p.n_groups;
     c.group_ids = p.d_gids;
     CUDA_TRY(cudaMemcpy(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
-    if (p.kind % kKindHeatBath == 0) {  // 2D Ising, either algorithm
+    if (is_ising2d_bits_kind(p.kind)) {
       int rc = build_resident(device, tv, layout_of_lat, p.smem, p.res);
       if (rc) {
         p.release();
@@ -821,7 +877,7 @@ uint64_t gpumc_engine::launches_per_batch_sweep() const {
   for (const auto& p : batch_plans)
     if (!(p.res.on && blocking)) {
       const int base = p.kind % kKindHeatBath;  // O(3) sweeps are two colour launches
-      n += (base == 4 || base == 5 || base == 10) ? 2 : 1;
+      n += is_cluster_kind(p.kind) ? 3 : (base == 4 || base == 5 || base == 10) ? 2 : 1;
     }
   for (gpumc_sim* s : sims)
     if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) n += (uint64_t)s->n_rep + 1;

@@ -26,10 +26,13 @@ enum Tag : uint32_t {
   TAG_INIT = 4, TAG_O3 = 5, TAG_MSC = 6, TAG_PT = 7, TAG_BITS = 8, TAG_PBITS = 9, TAG_PACC = 10,
   TAG_HBITS = 11,  // heat bath: Ising bit planes
   TAG_HB = 12,     // heat bath: 64-bit uniforms of int8 Potts sites
-  TAG_O3HB = 13    // heat bath: O(3) (cos theta, phi) draws
+  TAG_O3HB = 13,   // heat bath: O(3) (cos theta, phi) draws
+  TAG_SW = 14,     // cluster updates: bond activations
+  TAG_SWFLIP = 15, // Swendsen-Wang: cluster decisions (counter = root site)
+  TAG_WOLFF = 16   // Wolff: seed site and target state
 };
 
-enum Algorithm : int32_t { METROPOLIS = 0, HEAT_BATH = 1 };
+enum Algorithm : int32_t { METROPOLIS = 0, HEAT_BATH = 1, SWENDSEN_WANG = 2, WOLFF = 3 };
 
 constexpr int kMaxClasses = 13;    // 2z+1 for z = 6 (Potts on the cubic lattice)
 constexpr int kMaxPottsCounts = 8; // fused order-parameter histogram (q <= 8)
@@ -68,6 +71,7 @@ struct LatDesc {
   int32_t pad0;
   int64_t n_sites;
   void* buf[2];
+  void* aux;                        // cluster updates: uint32 label per site
   uint64_t key;                     // Philox key of the sweep stream
   // mutable device state
   uint64_t sweep;                   // sweeps completed

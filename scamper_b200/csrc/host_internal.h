@@ -15,7 +15,8 @@ namespace gpumc {
 struct Layout {
   int model = 0, dims = 2, lx = 0, ly = 0, lz = 1, pitch = 0;
   int q = 2;             // Potts states
-  int alg = METROPOLIS;  // sweep algorithm (METROPOLIS / HEAT_BATH)
+  int alg = METROPOLIS;  // sweep algorithm (METROPOLIS / HEAT_BATH / SWENDSEN_WANG / WOLFF)
+  bool cluster = false;  // cluster update (label scratch per lattice, 3 launches per sweep)
   bool bits = false;     // Potts on the bit-sliced kernel (q <= 4, Metropolis)
   bool march = false;    // 3D O(3) on the shared-memory z-march kernel
   int64_t n_sites = 0;
@@ -34,6 +35,12 @@ void build_table(int model, int dims, double J, double beta, uint32_t* head,
 // kernel kinds of heat-bath layouts: the Metropolis kind of the same model and
 // geometry plus this offset
 constexpr int kKindHeatBath = 16;
+// kernel kinds of cluster layouts: kKindCluster + 2 (Potts) + (dims - 2) + 4 (Wolff)
+constexpr int kKindCluster = 32;
+inline bool is_cluster_kind(int kind) { return kind >= kKindCluster; }
+// 2D Ising on the bit-sliced kernel (either single-site algorithm): the kinds
+// the resident multi-sweep launch can take
+inline bool is_ising2d_bits_kind(int kind) { return kind == 0 || kind == kKindHeatBath; }
 int validate_spec(const gpumc_spec* s);
 // CTA slots of one B200 (148 SMs x 4 resident sweep CTAs); the engine
 // passes its device's own count.
@@ -135,6 +142,7 @@ struct gpumc_sim {
   int lat0 = -1, group = -1;
   uint64_t base_seed = 0;
   std::vector<void*> bufs;  // 2 per replica
+  std::vector<void*> aux;   // cluster updates: label array per replica
   uint32_t* d_head = nullptr;
   unsigned long long* d_tail = nullptr;
   double* d_betas = nullptr;

@@ -54,6 +54,7 @@ gpumc_sim::~gpumc_sim() {
   cudaFree(d_label);
   cudaFree(d_rep_at);
   cudaFree(d_records);
+  for (void* p : aux) cudaFree(p);
   cudaFree(d_bin_open);
   cudaFree(d_bins);
   cudaFree(d_msc_counters);
@@ -333,6 +334,10 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
     CUDA_CLEAN(cudaMalloc(&s->bufs[i], s->lay.buf_bytes));
     CUDA_CLEAN(cudaMemsetAsync(s->bufs[i], 0, s->lay.buf_bytes, eng->stream));
   }
+  if (s->lay.cluster) {  // union-find labels of the cluster updates, one array per replica
+    s->aux.assign(s->n_rep, nullptr);
+    for (int r = 0; r < s->n_rep; ++r) CUDA_CLEAN(cudaMalloc(&s->aux[r], 4 * (size_t)s->lay.n_sites));
+  }
   CUDA_CLEAN(cudaMalloc(&s->d_head, 4 * (size_t)s->n_temps * s->n_cls));
   CUDA_CLEAN(cudaMalloc(&s->d_tail, 8 * (size_t)s->n_temps * s->n_cls));
   CUDA_CLEAN(cudaMalloc(&s->d_betas, 8 * (size_t)s->n_temps));
@@ -363,7 +368,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   c.n_groups = 1;
   c.group_ids = s->d_gid;
   CUDA_CLEAN(cudaMemcpy(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
-  if (kernel_kind(s->lay) % kKindHeatBath == 0) {  // 2D Ising, either algorithm
+  if (is_ising2d_bits_kind(kernel_kind(s->lay))) {
     std::map<int, const Layout*> lay_of;
     for (int r = 0; r < s->n_rep; ++r) lay_of[s->lat0 + r] = &s->lay;
     rc = build_resident(eng->device, tiles, lay_of, s->lay.smem, s->res);
@@ -390,6 +395,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
     d.n_sites = s->lay.n_sites;
     d.buf[0] = s->bufs[2 * r];
     d.buf[1] = s->bufs[2 * r + 1];
+    d.aux = s->lay.cluster ? s->aux[r] : nullptr;
     const uint64_t rid = s->lay.model == MSC ? 64ull * r : (uint64_t)r;
     d.key = stream_key(base_seed, rid, 0, 1);
     d.sweep = 0;

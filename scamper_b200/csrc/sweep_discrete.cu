@@ -51,52 +51,52 @@ struct SiteTab {
   int32_t jneg;                          // heat bath: J < 0 (favoured = fewest neighbours)
 };
 
-// Heat-bath draw of one Potts site from its neighbour counts n[0..q-1], old
+// Heat-bath draw of one Potts site from its neighbour counts n[0..Q-1], old
 // state s and 64-bit uniform u; returns the new state t and sets dn = n[t] -
 // n[s] (dE = -J dn).  Exact integer arithmetic (restated by the oracle).
-__device__ __forceinline__ uint32_t potts_hb_pick(const int (&n)[kMaxPottsCounts], int q, uint32_t s,
+template <int Q>
+__device__ __forceinline__ uint32_t potts_hb_pick(const int (&n)[kMaxPottsCounts], uint32_t s,
                                                   unsigned long long u, const SiteTab& tab, int& dn) {
   int nmax = 0, nmin = 64;
 #pragma unroll
-  for (int k = 0; k < kMaxPottsCounts; ++k)
-    if (k < q) {
-      nmax = max(nmax, n[k]);
-      nmin = min(nmin, n[k]);
-    }
-  unsigned long long tot = 0;
+  for (int k = 0; k < Q; ++k) {
+    nmax = max(nmax, n[k]);
+    nmin = min(nmin, n[k]);
+  }
+  const int ref = tab.jneg ? nmin : nmax, sg = tab.jneg ? 1 : -1;  // d = |n - ref|
+  unsigned long long w[Q], tot = 0;
 #pragma unroll
-  for (int k = 0; k < kMaxPottsCounts; ++k)
-    if (k < q) tot += tab.tail[tab.jneg ? n[k] - nmin : nmax - n[k]];
+  for (int k = 0; k < Q; ++k) {
+    w[k] = tab.tail[sg * (n[k] - ref)];
+    tot += w[k];
+  }
   unsigned long long x = __umul64hi(u, tot);
-  uint32_t t = (uint32_t)(q - 1);
-  int nt = 0, ns = 0;
+  uint32_t t = (uint32_t)(Q - 1);
+  int nt = n[Q - 1], ns = 0;
   bool found = false;
 #pragma unroll
-  for (int k = 0; k < kMaxPottsCounts; ++k)
-    if (k < q) {
-      const unsigned long long w = tab.tail[tab.jneg ? n[k] - nmin : nmax - n[k]];
-      if (!found) {
-        if (x < w) {
-          t = (uint32_t)k;
-          nt = n[k];
-          found = true;
-        } else {
-          x -= w;
-        }
+  for (int k = 0; k < Q; ++k) {
+    if (!found) {
+      if (x < w[k]) {
+        t = (uint32_t)k;
+        nt = n[k];
+        found = true;
+      } else {
+        x -= w[k];
       }
-      if ((uint32_t)k == s) ns = n[k];
-      if (!found && k == q - 1) nt = n[k];  // unreachable: x < total
     }
+    if ((uint32_t)k == s) ns = n[k];
+  }
   dn = nt - ns;
   return t;
 }
 
 // Heat bath of the two pass-colour sites of one word (bytes 0 and 2 after the
 // pre-shift), from one Philox block r.
-template <int DIM>
+template <int DIM, int Q>
 __device__ __forceinline__ uint32_t potts_hb_word(uint32_t o, uint32_t lw, uint32_t rw, uint32_t u,
                                                   uint32_t d, uint32_t a, uint32_t b, int bsh,
-                                                  const uint4 r, const SiteTab& tab, int q,
+                                                  const uint4 r, const SiteTab& tab,
                                                   uint32_t own2, int& nacc, int& dsum) {
   constexpr int zc = 2 * DIM;
   const uint32_t os = o >> bsh;
@@ -104,23 +104,20 @@ __device__ __forceinline__ uint32_t potts_hb_word(uint32_t o, uint32_t lw, uint3
   const uint32_t nbw[6] = {lw >> bsh, rw >> bsh, u >> bsh, d >> bsh, a >> bsh, b >> bsh};
   int nA[kMaxPottsCounts], nB[kMaxPottsCounts];
 #pragma unroll
-  for (int k = 0; k < kMaxPottsCounts; ++k) {
-    nA[k] = nB[k] = 0;
-    if (k < q) {
-      const uint32_t pat = (uint32_t)k * 0x00010001u;
-      uint32_t c = 0;  // bytes 0 and 2: neighbours NOT in state k
+  for (int k = 0; k < Q; ++k) {
+    const uint32_t pat = (uint32_t)k * 0x00010001u;
+    uint32_t c = 0;  // bytes 0 and 2: neighbours NOT in state k
 #pragma unroll
-      for (int i = 0; i < zc; ++i) {
-        const uint32_t x = (nbw[i] ^ pat) & 0x00FF00FFu;
-        c += ((x + 0x00FF00FFu) >> 8) & 0x00010001u;
-      }
-      nA[k] = zc - (int)(c & 0xFFu);
-      nB[k] = zc - (int)(c >> 16);
+    for (int i = 0; i < zc; ++i) {
+      const uint32_t x = (nbw[i] ^ pat) & 0x00FF00FFu;
+      c += ((x + 0x00FF00FFu) >> 8) & 0x00010001u;
     }
+    nA[k] = zc - (int)(c & 0xFFu);
+    nB[k] = zc - (int)(c >> 16);
   }
   int dA, dB;
-  const uint32_t tA = potts_hb_pick(nA, q, sA, (unsigned long long)r.x | ((unsigned long long)r.y << 32), tab, dA);
-  const uint32_t tB = potts_hb_pick(nB, q, sB, (unsigned long long)r.z | ((unsigned long long)r.w << 32), tab, dB);
+  const uint32_t tA = potts_hb_pick<Q>(nA, sA, (unsigned long long)r.x | ((unsigned long long)r.y << 32), tab, dA);
+  const uint32_t tB = potts_hb_pick<Q>(nB, sB, (unsigned long long)r.z | ((unsigned long long)r.w << 32), tab, dB);
   const int oA = (int)((tA != sA) & (own2 & 1u)), oB = (int)((tB != sB) & ((own2 >> 1) & 1u));
   nacc += oA + oB;
   dsum += oA * dA + oB * dB;
@@ -278,7 +275,14 @@ __device__ __forceinline__ uint4 update_chunk_hb(const uint4 own, const uint4 up
     const uint32_t rw = __funnelshift_r(o[i], i == 3 ? wnext : o[i + 1], 8);
     const uint32_t own2 = ((owned16 >> (4 * i + bp)) & 1u) | (((owned16 >> (4 * i + bp + 2)) & 1u) << 1);
     const uint4 r = philox_fast(P, chunk, colour | (TAG_HB << 1) | ((uint32_t)i << 8));
-    res[i] = potts_hb_word<DIM>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, r, tab, q, own2, nacc, acc2);
+    // q is uniform over the launch's tile: one branch, loops of exactly q states
+    switch (q) {
+#define HB_CASE(QQ) \
+  case QQ: res[i] = potts_hb_word<DIM, QQ>(o[i], lw, rw, uu[i], dd[i], aa[i], bb[i], bsh, r, tab, own2, nacc, acc2); break;
+      HB_CASE(2) HB_CASE(3) HB_CASE(4) HB_CASE(5) HB_CASE(6) HB_CASE(7)
+      default: HB_CASE(8)
+#undef HB_CASE
+    }
   }
   return make_uint4(res[0], res[1], res[2], res[3]);
 }
@@ -307,13 +311,21 @@ __device__ __forceinline__ int8_t update_site(const int8_t* p, int S, const int8
     for (int k = 0; k < kMaxPottsCounts; ++k) {
       n[k] = 0;
 #pragma unroll
-      for (int i = 0; i < zc; ++i) n[k] += (k < q && nb[i] == k) ? 1 : 0;
+      for (int i = 0; i < zc; ++i) n[k] += nb[i] == k ? 1 : 0;
     }
     const uint4 hv = draw(key, chunk, colour, TAG_HB, (uint32_t)(slot >> 1), sweep);
     const unsigned long long u = (slot & 1) ? ((unsigned long long)hv.z | ((unsigned long long)hv.w << 32))
                                             : ((unsigned long long)hv.x | ((unsigned long long)hv.y << 32));
     int dn;
-    return (int8_t)potts_hb_pick(n, q, (uint32_t)s, u, tab, dn);
+    switch (q) {
+      case 2: return (int8_t)potts_hb_pick<2>(n, (uint32_t)s, u, tab, dn);
+      case 3: return (int8_t)potts_hb_pick<3>(n, (uint32_t)s, u, tab, dn);
+      case 4: return (int8_t)potts_hb_pick<4>(n, (uint32_t)s, u, tab, dn);
+      case 5: return (int8_t)potts_hb_pick<5>(n, (uint32_t)s, u, tab, dn);
+      case 6: return (int8_t)potts_hb_pick<6>(n, (uint32_t)s, u, tab, dn);
+      case 7: return (int8_t)potts_hb_pick<7>(n, (uint32_t)s, u, tab, dn);
+      default: return (int8_t)potts_hb_pick<8>(n, (uint32_t)s, u, tab, dn);
+    }
   }
   const uint4 rv = draw(key, chunk, colour, TAG_ACC, 0, sweep);
   const uint32_t w = (slot >> 1) == 0 ? rv.x : (slot >> 1) == 1 ? rv.y : (slot >> 1) == 2 ? rv.z : rv.w;

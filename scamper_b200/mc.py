@@ -51,11 +51,14 @@ class Params(dict):
 
 MODELS = {"ising": _lib.ISING, "potts": _lib.POTTS, "heisenberg": _lib.O3, "o3": _lib.O3}
 # the algorithm type parameter of ClassicalMC<H, A> (CMC.rs/src/classical_mc.rs:21-31):
-# MetropolisCore, or HeatBathCore / ContinuousHeatBathCore
-# (CMC.rs/src/algorithms/heat_bath.rs:12-134)
+# MetropolisCore, HeatBathCore / ContinuousHeatBathCore
+# (CMC.rs/src/algorithms/heat_bath.rs:12-134), SWCore
+# (CMC.rs/src/algorithms/swendsen_wang.rs) and WolffCore (CMC.rs/src/algorithms/wolff.rs)
 ALGORITHMS = {"metropolis": _lib.METROPOLIS, "metropolis-hastings": _lib.METROPOLIS,
               "heat_bath": _lib.HEAT_BATH, "heatbath": _lib.HEAT_BATH,
-              "continuous_heat_bath": _lib.HEAT_BATH}
+              "continuous_heat_bath": _lib.HEAT_BATH,
+              "swendsen_wang": _lib.SWENDSEN_WANG, "swendsen-wang": _lib.SWENDSEN_WANG, "sw": _lib.SWENDSEN_WANG,
+              "wolff": _lib.WOLFF}
 
 
 def algorithm_id(algorithm):
@@ -66,7 +69,7 @@ def algorithm_id(algorithm):
     a = str(algorithm).lower()
     if a not in ALGORITHMS:
         raise InvalidConfig(_lib.EINVAL, f"algorithm: unknown algorithm `{algorithm}` "
-                                         "(expected metropolis or heat_bath)")
+                                         "(expected metropolis, heat_bath, swendsen_wang or wolff)")
     return ALGORITHMS[a]
 
 
@@ -197,18 +200,24 @@ class ClassicalMC:
     @classmethod
     def from_params(cls, params, seed, model=None, n_replicas=1, betas=None, engine=None,
                     record_capacity=1024, algorithm=None):
-        """`algorithm`: "metropolis" (MetropolisCore, the default) or
+        """`algorithm`: "metropolis" (MetropolisCore, the default),
         "heat_bath" (HeatBathCore for Ising / Potts, ContinuousHeatBathCore
-        for O(3))."""
+        for O(3)), "swendsen_wang" (SWCore) or "wolff" (WolffCore; one cluster
+        per sweep), the cluster updates for Ising / Potts with J >= 0."""
         spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas,
                                       record_capacity=record_capacity, algorithm=algorithm)
         return cls(spec, seed, engine=engine, _keep=keep)
 
     # -- MonteCarlo -----------------------------------------------------------
     def name(self):
-        """Algorithm::name (CMC.rs/src/algorithms/heat_bath.rs:69-71, :131-133)."""
+        """Algorithm::name (CMC.rs/src/algorithms/heat_bath.rs:69-71, :131-133,
+        swendsen_wang.rs:141-143, wolff.rs:138-140)."""
         if self.algorithm == _lib.HEAT_BATH:
             return "ContinuousHeatBath" if self.model == _lib.O3 else "HeatBath"
+        if self.algorithm == _lib.SWENDSEN_WANG:
+            return "Swendsen-Wang"
+        if self.algorithm == _lib.WOLFF:
+            return "Wolff"
         return self.NAME
 
     def on_phase_start(self, phase):

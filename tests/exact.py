@@ -148,3 +148,20 @@ def kaufman_logz(m, n, beta, J=1.0):
 def kaufman_energy(L, beta, J=1.0, eps=1e-5):
     """Exact <E> (total) of the L x L periodic Ising model."""
     return -(kaufman_logz(L, L, beta + eps, J) - kaufman_logz(L, L, beta - eps, J)) / (2 * eps)
+
+
+def replicas_ok(series, ex, nbins=20):
+    """Independent chains against an exact mean: per-chain z (binned stderr)
+    below 4, mean z below 2, and the pooled mean within 4 standard errors of
+    the spread of the chain means (an unbiased error bar for independent
+    chains).  Raises AssertionError otherwise."""
+    zs, means = [], []
+    for e in series:
+        me, se = binned(e, nbins)
+        zs.append(zscore(me, se, ex))
+        means.append(me)
+    means = np.array(means)
+    pooled = (means.mean() - ex) / (means.std(ddof=1) / math.sqrt(len(means)))
+    assert max(abs(z) for z in zs) < 4.0, zs
+    assert abs(np.mean(zs)) < 2.0, zs
+    assert abs(pooled) < 4.0, (pooled, zs)

@@ -40,11 +40,18 @@ CASES = [
     ("potts", [18, 8, 10], 0.6, 124, 3, {"q": 6, "algorithm": "heat_bath"}),
     ("o3", [66, 10], 0.7, 125, 3, {"algorithm": "heat_bath"}),
     ("o3", [16, 8, 12], 0.69, 126, 3, {"algorithm": "heat_bath"}),
+    # cluster updates
+    ("ising", [66, 34], 0.4407, 131, 4, {"algorithm": "swendsen_wang"}),
+    ("ising", [18, 10, 6], 0.22, 132, 5, {"algorithm": "wolff"}),
+    ("potts", [34, 18], 1.0, 133, 3, {"q": 3, "algorithm": "swendsen_wang"}),
+    ("potts", [10, 8, 6], 0.55, 134, 4, {"q": 4, "algorithm": "wolff"}),
 ]
+
+_ALGS = {"heat_bath": "-hb", "swendsen_wang": "-sw", "wolff": "-wolff"}
 
 
 def case_id(c):
-    suffix = "-hb" if c["extra"].get("algorithm") == "heat_bath" else ""
+    suffix = _ALGS.get(c["extra"].get("algorithm"), "")
     return f"{c['model']}-{'x'.join(map(str, c['shape']))}{suffix}"
 
 
@@ -58,7 +65,8 @@ def fingerprint(state):
 
 def run_case(oracle, model, shape, beta, seed, sweeps, extra):
     mid = {"ising": oracle.ISING, "potts": oracle.POTTS, "o3": oracle.O3, "msc": oracle.MSC}[model]
-    alg = oracle.HEAT_BATH if extra.get("algorithm") == "heat_bath" else oracle.METROPOLIS
+    alg = {"heat_bath": oracle.HEAT_BATH, "swendsen_wang": oracle.SWENDSEN_WANG,
+           "wolff": oracle.WOLFF}.get(extra.get("algorithm"), oracle.METROPOLIS)
     lat = oracle.Lattice(mid, tuple(shape), q=extra.get("q", 3), J=extra.get("J", 1.0), beta=beta,
                          seed=seed, omc=omc(extra.get("alpha", 1.0)), algorithm=alg)
     for _ in range(sweeps):

@@ -220,7 +220,8 @@ def _golden_cases():
 
 @pytest.mark.parametrize("case", _golden_cases(),
                          ids=[f"{c['model']}-{'x'.join(map(str, c['shape']))}"
-                              + ("-hb" if c["extra"].get("algorithm") == "heat_bath" else "")
+                              + {"heat_bath": "-hb", "swendsen_wang": "-sw", "wolff": "-wolff"}.get(
+                                  c["extra"].get("algorithm"), "")
                               for c in _golden_cases()])
 def test_device_matches_committed_golden_fingerprints(gpumc, case):
     """The device against the committed fixtures, without the oracle."""

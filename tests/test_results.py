@@ -151,7 +151,9 @@ CASES = [
 def test_device_bins_equal_host_accumulator(gpumc, model, shape, kw, n_rep, betas, alg, binsize, sweeps):
     """Same seed, same trajectory: one handle records every sweep and feeds a
     host Context, the other bins on the device; the finalized estimates of
-    every observable and chain are identical (bit for bit)."""
+    every observable and chain are identical (bit for bit for the integer
+    models; O(3) energies carry the run-to-run rounding of the fp64 atomic
+    energy accumulation)."""
     from scamper_b200 import _lib
     out = []
     for device_bins in (False, True):
@@ -182,7 +184,14 @@ def test_device_bins_equal_host_accumulator(gpumc, model, shape, kw, n_rep, beta
         return
     assert set(host) == set(dev)
     for k in host:
-        assert host[k] == dev[k], k
+        if model == "o3":
+            # the O(3) energy cache sums fp64 warp partials with atomics, in an
+            # order that varies between the two runs: equal to ~1e-15
+            assert host[k].n_bins == dev[k].n_bins, k
+            assert dev[k].mean == pytest.approx(host[k].mean, rel=1e-9, abs=1e-12), k
+            assert dev[k].stderr == pytest.approx(host[k].stderr, rel=1e-6, abs=1e-12), k
+        else:
+            assert host[k] == dev[k], k
 
 
 @pytest.mark.gpu
