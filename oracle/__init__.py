@@ -56,6 +56,8 @@ def lib():
                                                   _u64, _u64, _f32p, _f32p, _f32p, _i64p]),
             "orc_one_minus_exp_neg": (ctypes.c_float, [ctypes.c_float]),
             "orc_cluster_threshold": (_u64, [_int, ctypes.c_double, ctypes.c_double]),
+            "orc_sweep_cluster_o3": (ctypes.c_double, [_int, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float, _int,
+                                                       _u64, _u64, _f32p, _f32p, _f32p, _i64p]),
             "orc_sweep_cluster": (_i64, [_int, _int, _i64, _i64, _i64, _int, _int, _u64, _u64, _u64, _i8p,
                                          _i64p]),
             "orc_log_one_minus": (ctypes.c_float, [ctypes.c_float]),
@@ -181,7 +183,7 @@ class Lattice:
 
     def set_beta(self, beta):
         self.beta = beta
-        if self.algorithm in (SWENDSEN_WANG, WOLFF):
+        if self.algorithm in (SWENDSEN_WANG, WOLFF) and self.model != O3:
             self.thr = lib().orc_cluster_threshold(self.model, self.J, beta)
         elif self.model != O3:
             tm = ISING if self.model == MSC else self.model
@@ -190,7 +192,13 @@ class Lattice:
     def sweep(self, adapt=False):
         L = lib()
         acc = ctypes.c_int64()
-        if self.algorithm in (SWENDSEN_WANG, WOLFF):
+        if self.algorithm in (SWENDSEN_WANG, WOLFF) and self.model == O3:
+            d = L.orc_sweep_cluster_o3(self.dims, self.lx, self.ly, self.lz, np.float32(self.J),
+                                       np.float32(self.beta), 1 if self.algorithm == WOLFF else 0, self.key,
+                                       self.sweeps, _p(self.sx, _f32p), _p(self.sy, _f32p), _p(self.sz, _f32p),
+                                       ctypes.byref(acc))
+            self.e += d
+        elif self.algorithm in (SWENDSEN_WANG, WOLFF):
             d = L.orc_sweep_cluster(self.model, self.dims, self.lx, self.ly, self.lz, self.q,
                                     1 if self.algorithm == WOLFF else 0, self.thr, self.key, self.sweeps,
                                     _p(self.spins, _i8p), ctypes.byref(acc))

@@ -929,6 +929,100 @@ double orc_sweep_o3_hb(int dims, int64_t lx, int64_t ly, int64_t lz, float J, fl
     return dEsum;
 }
 
+double orc_sweep_cluster_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta, int wolff,
+                            uint64_t key64, uint64_t sweep, float* sx, float* sy, float* sz, int64_t* changed) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    int64_t n = lx * ly * g.lz;
+    uint32_t key[2];
+    key_of(key64, key);
+    /* reflection axis of the sweep */
+    uint32_t ctr[4], o[4];
+    make_ctr(ctr, 0, 0, ORC_TAG_O3CL, 0, sweep);
+    orc_philox4x32_10(ctr, key, o);
+    float t = (float)(o[0] >> 8) * 0x1p-24f;
+    float rz = 1.0f - 2.0f * t;
+    float rho = sqrtf((1.0f - rz) * (1.0f + rz));
+    float c, s;
+    orc_sincos_turn(o[1], &c, &s);
+    float rx = rho * c, ry = rho * s;
+    float c2bj = (2.0f * beta) * J;
+    uint32_t* par = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
+    float* sig = (float*)malloc(sizeof(float) * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        par[i] = (uint32_t)i;
+        sig[i] = (sx[i] * rx + sy[i] * ry) + sz[i] * rz;
+    }
+    for (int64_t z = 0; z < g.lz; ++z)
+        for (int64_t y = 0; y < ly; ++y)
+            for (int64_t x = 0; x < lx; ++x) {
+                int64_t st = site_of(&g, x, y, z);
+                uint32_t o1[4], o2[4];
+                make_ctr(ctr, (uint64_t)st, 0, ORC_TAG_SW, 0, sweep);
+                orc_philox4x32_10(ctr, key, o1);
+                make_ctr(ctr, (uint64_t)st, 0, ORC_TAG_SW, 1, sweep);
+                orc_philox4x32_10(ctr, key, o2);
+                for (int d = 0; d < dims; ++d) {
+                    int64_t nb = d == 0 ? site_of(&g, x + 1 < lx ? x + 1 : 0, y, z)
+                               : d == 1 ? site_of(&g, x, y + 1 < ly ? y + 1 : 0, z)
+                                        : site_of(&g, x, y, z + 1 < g.lz ? z + 1 : 0);
+                    float prod = sig[st] * sig[nb];
+                    if (!(prod > 0.0f)) continue;
+                    float p = orc_one_minus_exp_neg(c2bj * prod);
+                    uint64_t thr = p >= 1.0f ? ~(uint64_t)0 : (uint64_t)((double)p * 18446744073709551616.0);
+                    uint64_t u = d == 0 ? ((uint64_t)o1[0] | ((uint64_t)o1[1] << 32))
+                               : d == 1 ? ((uint64_t)o1[2] | ((uint64_t)o1[3] << 32))
+                                        : ((uint64_t)o2[0] | ((uint64_t)o2[1] << 32));
+                    if (u < thr) uf_union(par, (uint32_t)st, (uint32_t)nb);
+                }
+            }
+    uint32_t seed_root = 0;
+    if (wolff) {
+        make_ctr(ctr, 0, 0, ORC_TAG_WOLFF, 0, sweep);
+        orc_philox4x32_10(ctr, key, o);
+        uint64_t nn = (uint64_t)n, rej = (0 - nn) % nn, seed = 0;
+        uint64_t u[2] = {(uint64_t)o[0] | ((uint64_t)o[1] << 32), (uint64_t)o[2] | ((uint64_t)o[3] << 32)};
+        for (int i = 0; i < 2; ++i)
+            if (u[i] * nn >= rej) {
+                seed = (uint64_t)(((unsigned __int128)u[i] * nn) >> 64);
+                break;
+            }
+        seed_root = uf_find(par, (uint32_t)seed);
+    }
+    float* nx = (float*)malloc(sizeof(float) * (size_t)n);
+    float* ny = (float*)malloc(sizeof(float) * (size_t)n);
+    float* nz = (float*)malloc(sizeof(float) * (size_t)n);
+    int64_t nch = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t r = uf_find(par, (uint32_t)i);
+        int refl;
+        if (wolff) {
+            refl = r == seed_root;
+        } else {
+            make_ctr(ctr, r, 0, ORC_TAG_SWFLIP, 0, sweep);
+            orc_philox4x32_10(ctr, key, o);
+            refl = (o[0] >> 31) != 0;
+        }
+        float vx = sx[i], vy = sy[i], vz = sz[i];
+        if (refl) {
+            float k = 2.0f * sig[i];
+            float px = vx - k * rx, py = vy - k * ry, pz = vz - k * rz;
+            float n2 = (px * px + py * py) + pz * pz;
+            float f = 1.5f - 0.5f * n2;
+            vx = px * f; vy = py * f; vz = pz * f;
+        }
+        nx[i] = vx; ny[i] = vy; nz[i] = vz;
+        nch += (vx != sx[i]) | (vy != sy[i]) | (vz != sz[i]);
+    }
+    double e0 = orc_energy_o3(dims, lx, ly, lz, (double)J, sx, sy, sz);
+    memcpy(sx, nx, sizeof(float) * (size_t)n);
+    memcpy(sy, ny, sizeof(float) * (size_t)n);
+    memcpy(sz, nz, sizeof(float) * (size_t)n);
+    double e1 = orc_energy_o3(dims, lx, ly, lz, (double)J, sx, sy, sz);
+    free(par); free(sig); free(nx); free(ny); free(nz);
+    if (changed) *changed = nch;
+    return e1 - e0;
+}
+
 double orc_energy_o3(int dims, int64_t lx, int64_t ly, int64_t lz, double J, const float* sx,
                      const float* sy, const float* sz) {
     geom g = {dims, lx, ly, dims == 3 ? lz : 1};

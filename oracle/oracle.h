@@ -47,7 +47,8 @@ enum {
     ORC_TAG_O3HB = 13,      /* heat bath: O(3) (cos theta, phi) draws       */
     ORC_TAG_SW = 14,        /* cluster updates: bond activations            */
     ORC_TAG_SWFLIP = 15,    /* Swendsen-Wang: cluster decisions             */
-    ORC_TAG_WOLFF = 16      /* Wolff: seed site and target state            */
+    ORC_TAG_WOLFF = 16,     /* Wolff: seed site and target state            */
+    ORC_TAG_O3CL = 17       /* O(3) cluster updates: reflection axis        */
 };
 
 /* Substream ids used with RngStreamKey::with_substream. */
@@ -125,6 +126,13 @@ double orc_sweep_o3_hb(int dims, int64_t lx, int64_t ly, int64_t lz, float J, fl
 uint64_t orc_cluster_threshold(int model, double J, double beta);
 int64_t orc_sweep_cluster(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q, int wolff,
                           uint64_t thr, uint64_t key64, uint64_t sweep, int8_t* spins, int64_t* changed);
+/* O(3) cluster updates (ClusterModel for ONModel, CMC.rs/src/lattice/
+ * models.rs:516-579): embedded Ising variables along a random axis per sweep,
+ * bonds p = 1 - exp(-2 beta J s_i.r s_j.r) for positive products, clusters
+ * reflected (SW: each with probability 1/2; Wolff: the seed's), in the
+ * engine's fp32 arithmetic; returns the exact fp64 dE. */
+double orc_sweep_cluster_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta, int wolff,
+                            uint64_t key64, uint64_t sweep, float* sx, float* sy, float* sz, int64_t* changed);
 float orc_one_minus_exp_neg(float x);
 float orc_log_one_minus(float y);
 double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,

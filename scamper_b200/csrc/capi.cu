@@ -45,6 +45,16 @@ template <int DIM, int MODEL, int WOLFF>
 __global__ void k_cluster_global(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM, int MODEL, int WOLFF>
 __global__ void k_cluster_flip(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int MODEL, int WOLFF>
+__global__ void k_cluster_account(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int WOLFF>
+__global__ void k_cluster_o3_local(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int WOLFF>
+__global__ void k_cluster_o3_global(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int WOLFF>
+__global__ void k_cluster_o3_flip(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+template <int DIM, int WOLFF>
+__global__ void k_cluster_o3_account(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int ALG>
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
                                        uint2*, int, int);
@@ -226,8 +236,8 @@ int validate_spec(const gpumc_spec* s) {
   if (s->algorithm != GPUMC_METROPOLIS && s->model == GPUMC_ISING_MSC64)
     return fail(GPUMC_EINVAL, "algorithm: the multi-spin model has Metropolis sweeps only");
   if (s->algorithm >= GPUMC_SWENDSEN_WANG) {
-    if (s->model != GPUMC_ISING && s->model != GPUMC_POTTS)
-      return fail(GPUMC_EINVAL, "algorithm: cluster updates are implemented for Ising and Potts");
+    if (s->model != GPUMC_ISING && s->model != GPUMC_POTTS && s->model != GPUMC_O3)
+      return fail(GPUMC_EINVAL, "algorithm: cluster updates are for Ising, Potts and O(3)");
     if (s->J < 0.0)
       return fail(GPUMC_EINVAL, "J: ferromagnetic cluster updates require J >= 0");
   }
@@ -471,6 +481,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     L.tile_y = L.dims == 2 ? 16 : 8;
     L.tile_z = L.dims == 2 ? 1 : 4;
     L.smem = 0;
+    L.inplace = false;  // O(3) too: the flip writes the other buffer
   }
   return L;
 }
@@ -495,6 +506,7 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
 // runs the bit-sliced kernel (kinds 8 / 9); heat-bath layouts add
 // kKindHeatBath to the kind of the same model and geometry.
 int kernel_kind(const Layout& L) {
+  if (L.cluster && L.model == O3) return kKindCluster + 8 + (L.dims - 2) + (L.alg == WOLFF ? 2 : 0);
   if (L.cluster) return kKindCluster + (L.model == POTTS ? 2 : 0) + (L.dims - 2) + (L.alg == WOLFF ? 4 : 0);
   const int hb = L.alg == HEAT_BATH ? kKindHeatBath : 0;
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
@@ -571,19 +583,24 @@ int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_
                         LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem) {
   if (n_tiles <= 0) return GPUMC_OK;
   if (is_cluster_kind(kind)) {
-    // local bonds + union, global union across tiles, flip (+ epilogue)
-    static const SweepKernel ck[8][3] = {
-        {k_cluster_local<2, ISING, 0>, k_cluster_global<2, ISING, 0>, k_cluster_flip<2, ISING, 0>},
-        {k_cluster_local<3, ISING, 0>, k_cluster_global<3, ISING, 0>, k_cluster_flip<3, ISING, 0>},
-        {k_cluster_local<2, POTTS, 0>, k_cluster_global<2, POTTS, 0>, k_cluster_flip<2, POTTS, 0>},
-        {k_cluster_local<3, POTTS, 0>, k_cluster_global<3, POTTS, 0>, k_cluster_flip<3, POTTS, 0>},
-        {k_cluster_local<2, ISING, 1>, k_cluster_global<2, ISING, 1>, k_cluster_flip<2, ISING, 1>},
-        {k_cluster_local<3, ISING, 1>, k_cluster_global<3, ISING, 1>, k_cluster_flip<3, ISING, 1>},
-        {k_cluster_local<2, POTTS, 1>, k_cluster_global<2, POTTS, 1>, k_cluster_flip<2, POTTS, 1>},
-        {k_cluster_local<3, POTTS, 1>, k_cluster_global<3, POTTS, 1>, k_cluster_flip<3, POTTS, 1>}};
+    // local bonds + union, global union across tiles, flip, account (+ epilogue)
+#define CLUSTER_ROW(D, M, W) \
+  {k_cluster_local<D, M, W>, k_cluster_global<D, M, W>, k_cluster_flip<D, M, W>, k_cluster_account<D, M, W>}
+#define CLUSTER_O3_ROW(D, W) \
+  {k_cluster_o3_local<D, W>, k_cluster_o3_global<D, W>, k_cluster_o3_flip<D, W>, k_cluster_o3_account<D, W>}
+    static const SweepKernel ck[12][4] = {CLUSTER_ROW(2, ISING, 0), CLUSTER_ROW(3, ISING, 0),
+                                          CLUSTER_ROW(2, POTTS, 0), CLUSTER_ROW(3, POTTS, 0),
+                                          CLUSTER_ROW(2, ISING, 1), CLUSTER_ROW(3, ISING, 1),
+                                          CLUSTER_ROW(2, POTTS, 1), CLUSTER_ROW(3, POTTS, 1),
+                                          CLUSTER_O3_ROW(2, 0),     CLUSTER_O3_ROW(3, 0),
+                                          CLUSTER_O3_ROW(2, 1),     CLUSTER_O3_ROW(3, 1)};
+#undef CLUSTER_ROW
+#undef CLUSTER_O3_ROW
     const int c = kind - kKindCluster;
-    if (c < 0 || c >= 8) return fail(GPUMC_EINVAL, "internal: no cluster kernel for this layout");
+    if (c < 0 || c >= 12) return fail(GPUMC_EINVAL, "internal: no cluster kernel for this layout");
     for (int i = 0; i < 3; ++i) ck[c][i]<<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+    // the accounting kernel strides over the tiles, about eight per CTA
+    ck[c][3]<<<std::max(1, std::min(n_tiles, (n_tiles + 7) / 8)), kThreads, 0, st>>>(tiles, lats, groups, ctl);
     CUDA_TRY(cudaGetLastError());
     return GPUMC_OK;
   }
@@ -734,7 +751,7 @@ int gpumc_engine_launch_count(gpumc_engine* eng, uint64_t* n) {
 
 int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n) {
   if (!sim || !n) return fail(GPUMC_EINVAL, "null argument");
-  *n = (sim->lay.cluster ? 3 : sim->lay.model == O3 ? 2 : 1) +
+  *n = (sim->lay.cluster ? 4 : sim->lay.model == O3 ? 2 : 1) +
        ((sim->lay.model == MSC && sim->phase == GPUMC_PHASE_MEASUREMENT) ? sim->n_rep + 1 : 0);
   return GPUMC_OK;
 }
@@ -855,6 +872,7 @@ int gpumc_engine::rebuild_batch() {
     c.done = 0;
     c.n_groups = p.n_groups;
     c.group_ids = p.d_gids;
+    c.n_tiles = p.n_tiles;
     CUDA_TRY(cudaMemcpy(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
     if (is_ising2d_bits_kind(p.kind)) {
       int rc = build_resident(device, tv, layout_of_lat, p.smem, p.res);
@@ -877,7 +895,7 @@ uint64_t gpumc_engine::launches_per_batch_sweep() const {
   for (const auto& p : batch_plans)
     if (!(p.res.on && blocking)) {
       const int base = p.kind % kKindHeatBath;  // O(3) sweeps are two colour launches
-      n += is_cluster_kind(p.kind) ? 3 : (base == 4 || base == 5 || base == 10) ? 2 : 1;
+      n += is_cluster_kind(p.kind) ? 4 : (base == 4 || base == 5 || base == 10) ? 2 : 1;
     }
   for (gpumc_sim* s : sims)
     if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) n += (uint64_t)s->n_rep + 1;

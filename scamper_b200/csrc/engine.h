@@ -29,7 +29,8 @@ enum Tag : uint32_t {
   TAG_O3HB = 13,   // heat bath: O(3) (cos theta, phi) draws
   TAG_SW = 14,     // cluster updates: bond activations
   TAG_SWFLIP = 15, // Swendsen-Wang: cluster decisions (counter = root site)
-  TAG_WOLFF = 16   // Wolff: seed site and target state
+  TAG_WOLFF = 16,  // Wolff: seed site and target state
+  TAG_O3CL = 17    // O(3) cluster updates: reflection axis of the sweep
 };
 
 enum Algorithm : int32_t { METROPOLIS = 0, HEAT_BATH = 1, SWENDSEN_WANG = 2, WOLFF = 3 };
@@ -131,6 +132,7 @@ struct LaunchCtl {
   unsigned int bar = 0;      // resident kernel: grid-barrier arrivals of this launch
   int32_t err = 0;           // resident kernel: 1 = a barrier wait gave up
   unsigned int epi = 0;      // resident kernel: launch-local sweeps whose epilogue is done
+  int32_t n_tiles = 0;       // tiles of the launch (kernels that stride over them)
 };
 
 }  // namespace gpumc

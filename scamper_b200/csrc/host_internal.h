@@ -16,7 +16,7 @@ struct Layout {
   int model = 0, dims = 2, lx = 0, ly = 0, lz = 1, pitch = 0;
   int q = 2;             // Potts states
   int alg = METROPOLIS;  // sweep algorithm (METROPOLIS / HEAT_BATH / SWENDSEN_WANG / WOLFF)
-  bool cluster = false;  // cluster update (label scratch per lattice, 3 launches per sweep)
+  bool cluster = false;  // cluster update (label scratch per lattice, 4 launches per sweep)
   bool bits = false;     // Potts on the bit-sliced kernel (q <= 4, Metropolis)
   bool march = false;    // 3D O(3) on the shared-memory z-march kernel
   int64_t n_sites = 0;
@@ -35,7 +35,8 @@ void build_table(int model, int dims, double J, double beta, uint32_t* head,
 // kernel kinds of heat-bath layouts: the Metropolis kind of the same model and
 // geometry plus this offset
 constexpr int kKindHeatBath = 16;
-// kernel kinds of cluster layouts: kKindCluster + 2 (Potts) + (dims - 2) + 4 (Wolff)
+// kernel kinds of cluster layouts: kKindCluster + 2 (Potts) + (dims - 2) + 4 (Wolff);
+// O(3): kKindCluster + 8 + (dims - 2) + 2 (Wolff)
 constexpr int kKindCluster = 32;
 inline bool is_cluster_kind(int kind) { return kind >= kKindCluster; }
 // 2D Ising on the bit-sliced kernel (either single-site algorithm): the kinds

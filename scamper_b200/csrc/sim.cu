@@ -367,6 +367,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   c.done = 0;
   c.n_groups = 1;
   c.group_ids = s->d_gid;
+  c.n_tiles = s->n_tiles;
   CUDA_CLEAN(cudaMemcpy(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
   if (is_ising2d_bits_kind(kernel_kind(s->lay))) {
     std::map<int, const Layout*> lay_of;

@@ -9,7 +9,7 @@ for Potts q = 3, 4 against exact enumeration, and its beta = 0 limit
 transfer matrix); its cached energy equals recomputation; invalid specs
 (J < 0, O(3), multi-spin) are rejected as the reference's asserts do.
 
-GPU: the three-launch device sweep (tile union-find, global union, flip)
+GPU: the four-launch device sweep (tile union-find, global union, flip, account)
 against the oracle bit for bit (spins, energies, changed counts) on 2D and
 3D lattices whose extents are and are not multiples of the tile, alone,
 with several replicas and ladders, and batched with other models in one
@@ -111,16 +111,62 @@ def _params(shape, **kw):
 
 
 def test_cluster_specs_validated(gpumc):
-    for model, kw in [("ising", dict(J=-1.0)), ("potts", dict(J=-0.5, q=3)), ("o3", {}),
+    for model, kw in [("ising", dict(J=-1.0)), ("potts", dict(J=-0.5, q=3)), ("o3", dict(J=-1.0)),
                       (_lib.ISING_MSC64, {})]:
         for alg in ("swendsen_wang", "wolff"):
             with pytest.raises(gpumc.InvalidConfig):
                 gpumc.ClassicalMC.validate_params(_params((8, 8), beta=0.4, **kw), model=model, algorithm=alg)
     gpumc.ClassicalMC.validate_params(_params((8, 8), beta=0.4), model="ising", algorithm="sw")
     gpumc.ClassicalMC.validate_params(_params((6, 8, 10), beta=0.4, q=5), model="potts", algorithm="wolff")
+    gpumc.ClassicalMC.validate_params(_params((6, 8, 10), beta=0.7), model="o3", algorithm="swendsen_wang")
+
+
+@pytest.mark.parametrize("alg", ["sw", "wolff"])
+def test_o3_cluster_matches_heat_bath_4x4(oracle, alg):
+    """O(3) cluster updates (embedded Ising reflections, models.rs:516-579)
+    against the heat bath (itself pinned to the Langevin moments) on the 4x4
+    torus: pooled <E> of independent chains agree (cross-solver z, cf.
+    CMC.rs/tests/physics/continuous_cross_solver.rs)."""
+    a = oracle.SWENDSEN_WANG if alg == "sw" else oracle.WOLFF
+    beta = 0.9
+    means = {}
+    for name, algo in (("cluster", a), ("hb", oracle.HEAT_BATH)):
+        ms = []
+        for seed in range(1, 13):
+            lat = oracle.Lattice(oracle.O3, (4, 4), beta=beta, seed=seed + (0 if name == "cluster" else 100),
+                                 algorithm=algo)
+            es, _ = _chain(lat, 200, 3000)
+            ms.append(np.mean(es))
+            st = lat.state().astype(np.float64)
+            assert np.abs((st ** 2).sum(axis=1) - 1.0).max() < 1e-5
+            assert lat.cached_energy() == pytest.approx(lat.energy(), rel=1e-9, abs=1e-9)
+        means[name] = (np.mean(ms), np.std(ms, ddof=1) / math.sqrt(len(ms)))
+    (m1, s1), (m2, s2) = means["cluster"], means["hb"]
+    assert abs(m1 - m2) < 4.0 * math.hypot(s1, s2), means
 
 
 SHAPES = [(16, 16), (34, 18), (4, 4), (64, 64), (6, 6, 6), (8, 8, 8), (18, 10, 6), (130, 6, 4)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(16, 16), (34, 18), (6, 6, 6), (18, 10, 6)])
+@pytest.mark.parametrize("alg", ["swendsen_wang", "wolff"])
+def test_gpu_o3_cluster_matches_oracle(gpumc, oracle, shape, alg):
+    a = oracle.SWENDSEN_WANG if alg == "swendsen_wang" else oracle.WOLFF
+    beta = 0.8 if len(shape) == 2 else 0.6
+    mc = gpumc.ClassicalMC.from_params(_params(shape, beta=beta), 67, model="o3", algorithm=alg)
+    ref = oracle.Lattice(oracle.O3, shape, beta=beta, seed=67, algorithm=a)
+    mc.on_phase_start(_lib.PHASE_MEASUREMENT)
+    changed = []
+    for _ in range(3):
+        mc.sweep(2)
+        changed += [ref.sweep(), ref.sweep()]
+        np.testing.assert_array_equal(mc.spins(), ref.state().reshape(mc.spins().shape))
+        assert mc.energy()[0] == pytest.approx(ref.cached_energy(), rel=1e-12, abs=1e-9)
+    obs = mc.observables()
+    assert [round(o["acceptance"] * ref.n) for o in obs] == changed
+    assert mc.launches_per_sweep() == 4
+    mc.close()
 
 
 @pytest.mark.gpu
@@ -146,7 +192,7 @@ def test_gpu_cluster_matches_oracle(gpumc, oracle, shape, model, q, beta, alg):
     obs = mc.observables()
     assert [round(o["acceptance"] * ref.n) for o in obs] == changed
     assert mc.name() == ("Swendsen-Wang" if alg == "swendsen_wang" else "Wolff")
-    assert mc.launches_per_sweep() == 3
+    assert mc.launches_per_sweep() == 4
     mc.close()
 
 
