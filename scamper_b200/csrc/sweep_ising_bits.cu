@@ -146,6 +146,20 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
   const int cprev = g.xh ? cc - 1 : (cc == 0 ? g.NC - 1 : cc - 1);
   const int cnext = g.xh ? cc + 1 : (cc == g.NC - 1 ? 0 : cc + 1);
   const bool has_prev = cprev >= 0, has_next = cnext < g.NC;
+  // the class patterns of the pass in registers: the loop stores to the
+  // shared plane, so reads of the shared table would be repeated per word
+  constexpr int kPend = DIM == 2 ? 2 : 3;  // pending slots: z/2
+  const int npend = tab.npend;
+  uint32_t pn[kPend][3], qn[kPend][3], hn[3];
+#pragma unroll
+  for (int i = 0; i < kPend; ++i)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      pn[i][b] = tab.pend_neg[i][b];
+      qn[i][b] = ALG ? tab.pair_neg[i][b] : 0u;
+    }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) hn[b] = ALG ? tab.half_neg[b] : 0u;
   for (int it = 0; it < iters; ++it) {
     const int r = rlo + g.row0 + it * g.rstep;
     const bool active = col_ok && r < rlo + nrows;
@@ -205,19 +219,18 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       }
       // masks of the pending classes (class index k = b2 b1 b0 in bits)
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        if (i < tab.npend) {
-          m[i] = (b0 ^ tab.pend_neg[i][0]) & (b1 ^ tab.pend_neg[i][1]) & (b2 ^ tab.pend_neg[i][2]) & valid;
+      for (int i = 0; i < kPend; ++i) {
+        if (i < npend) {
+          m[i] = (b0 ^ pn[i][0]) & (b1 ^ pn[i][1]) & (b2 ^ pn[i][2]) & valid;
           if (ALG) {
-            const uint32_t mn =
-                (b0 ^ tab.pair_neg[i][0]) & (b1 ^ tab.pair_neg[i][1]) & (b2 ^ tab.pair_neg[i][2]) & valid;
+            const uint32_t mn = (b0 ^ qn[i][0]) & (b1 ^ qn[i][1]) & (b2 ^ qn[i][2]) & valid;
             m[i] |= mn;
             negm |= mn;
           }
           pending |= m[i];
         }
       }
-      if (ALG) half = (b0 ^ tab.half_neg[0]) & (b1 ^ tab.half_neg[1]) & (b2 ^ tab.half_neg[2]) & valid;
+      if (ALG) half = (b0 ^ hn[0]) & (b1 ^ hn[1]) & (b2 ^ hn[2]) & valid;
       always = valid & ~pending;
       segid = (uint32_t)(y + g.ly * z) * (uint32_t)g.nseg + (uint32_t)gs;
     }

@@ -45,6 +45,8 @@ CASES = [
     ("ising", [18, 10, 6], 0.22, 132, 5, {"algorithm": "wolff"}),
     ("potts", [34, 18], 1.0, 133, 3, {"q": 3, "algorithm": "swendsen_wang"}),
     ("potts", [10, 8, 6], 0.55, 134, 4, {"q": 4, "algorithm": "wolff"}),
+    ("o3", [34, 18], 0.8, 135, 3, {"algorithm": "swendsen_wang"}),
+    ("o3", [10, 8, 6], 0.6, 136, 4, {"algorithm": "wolff"}),
 ]
 
 _ALGS = {"heat_bath": "-hb", "swendsen_wang": "-sw", "wolff": "-wolff"}
