@@ -59,6 +59,14 @@ extern "C" {
 #define GPUMC_SWENDSEN_WANG 2
 #define GPUMC_WOLFF 3
 
+/* O(3) Metropolis proposals: the engine's cap around the current spin
+ * (adapted half-angle), the reference's StandardStrategy (independent uniform
+ * unit vector, CMC.rs/src/lattice/proposal.rs:45-63) and OPSSStrategy (random
+ * plane rotation with adapted bound, proposal.rs:72-167) */
+#define GPUMC_O3_CAP 0
+#define GPUMC_O3_UNIFORM 1
+#define GPUMC_O3_OPSS 2
+
 #define GPUMC_INIT_HOT 0  /* "hot" / "random" initial_state */
 #define GPUMC_INIT_COLD 1 /* "cold" / "ordered" */
 
@@ -87,9 +95,11 @@ typedef struct {
   int32_t n_temps;          /* entries in betas: 1 (shared) or n_replicas      */
   const double* betas;      /* inverse temperatures, finite and >= 0           */
   int32_t init;             /* GPUMC_INIT_HOT / GPUMC_INIT_COLD                */
-  double cone_half_angle;   /* O(3): initial cap half-angle (radians), (0, pi] */
+  double cone_half_angle;   /* O(3): initial cap half-angle, or the OPSS bound  */
+                            /* sigma (radians), (0, pi]                        */
   int32_t record_capacity;  /* measured sweeps buffered on the device (>= 1)   */
   int32_t algorithm;        /* GPUMC_METROPOLIS / HEAT_BATH / SWENDSEN_WANG / WOLFF */
+  int32_t o3_proposal;      /* GPUMC_O3_CAP / UNIFORM / OPSS (O(3) Metropolis) */
 } gpumc_spec;
 
 /* One measured sweep of one replica (Context::measure of Energy, E2,
@@ -190,6 +200,8 @@ int gpumc_recompute_energy(gpumc_sim* sim, double* energies);
 int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* energy64,
                                   double* mag64);
 int gpumc_sweep_count(gpumc_sim* sim, uint64_t* out);
+/* O(3) proposal step of a replica: the cap half-angle (cap proposal) or the
+ * rotation bound sigma (OPSS, OPSSStrategy::sigma). */
 int gpumc_acceptance(gpumc_sim* sim, int32_t replica, double* cone_half_angle);
 /* Resume support for state snapshots (the cmc-rs-snapshot-v2 format of
  * ClassicalMC::save_snapshot / load_snapshot, CMC.rs/src/classical_mc.rs:

@@ -71,6 +71,9 @@ def lib():
             "orc_energy_o3": (ctypes.c_double, [_int, _i64, _i64, _i64, ctypes.c_double, _f32p, _f32p,
                                                 _f32p]),
             "orc_o3_adapt": (ctypes.c_float, [ctypes.c_float, _i64, _i64]),
+            "orc_opss_adapt": (ctypes.c_float, [ctypes.c_float, _i64, _i64]),
+            "orc_sweep_o3_prop": (ctypes.c_double, [_int, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float,
+                                                    ctypes.c_float, _int, _u64, _u64, _f32p, _f32p, _f32p, _i64p]),
             "orc_exp_neg": (ctypes.c_float, [ctypes.c_float]),
             "orc_sincos_turn": (None, [ctypes.c_uint32, _f32p, _f32p]),
             "orc_init_msc": (None, [_int, _i64, _i64, _i64, _u64, _int, _u64p]),
@@ -143,9 +146,10 @@ class Lattice:
     """Oracle replica of one lattice under the engine's checkerboard method."""
 
     def __init__(self, model, shape, q=3, J=1.0, beta=0.44, seed=1, replica=0, hot=True,
-                 omc=None, algorithm=METROPOLIS):
+                 omc=None, algorithm=METROPOLIS, prop=0):
         self.model = model
         self.algorithm = algorithm
+        self.prop = prop  # O(3) Metropolis proposal: 0 cap, 1 uniform, 2 OPSS (omc = sigma)
         self.dims = len(shape)
         self.lx, self.ly = shape[0], shape[1]
         self.lz = shape[2] if self.dims == 3 else 1
@@ -219,12 +223,14 @@ class Lattice:
                                      self.sweeps, _p(self.spins, _i8p), ctypes.byref(acc))
             self.e_int += d
         elif self.model == O3:
-            d = L.orc_sweep_o3(self.dims, self.lx, self.ly, self.lz, np.float32(self.J),
-                               np.float32(self.beta), self.omc, self.key, self.sweeps,
-                               _p(self.sx, _f32p), _p(self.sy, _f32p), _p(self.sz, _f32p),
-                               ctypes.byref(acc))
+            d = L.orc_sweep_o3_prop(self.dims, self.lx, self.ly, self.lz, np.float32(self.J),
+                                    np.float32(self.beta), self.omc, self.prop, self.key, self.sweeps,
+                                    _p(self.sx, _f32p), _p(self.sy, _f32p), _p(self.sz, _f32p),
+                                    ctypes.byref(acc))
             self.e += d
-            if adapt:
+            if adapt and self.prop == 2:
+                self.omc = np.float32(L.orc_opss_adapt(self.omc, acc.value, self.n))
+            elif adapt and self.prop == 0:
                 self.omc = np.float32(L.orc_o3_adapt(self.omc, acc.value, self.n))
         else:
             L.orc_sweep_msc(self.dims, self.lx, self.ly, self.lz, _p(self.head, _u32p),

@@ -720,6 +720,18 @@ void orc_init_o3(int dims, int64_t lx, int64_t ly, int64_t lz, uint64_t base_see
 double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
                     float omc, uint64_t key64, uint64_t sweep, float* sx, float* sy,
                     float* sz, int64_t* accepted) {
+    return orc_sweep_o3_prop(dims, lx, ly, lz, J, beta, omc, 0, key64, sweep, sx, sy, sz, accepted);
+}
+
+static void o3_newton(float* px, float* py, float* pz) {
+    float n2 = (*px * *px + *py * *py) + *pz * *pz;
+    float f = 1.5f - 0.5f * n2;
+    *px = *px * f; *py = *py * f; *pz = *pz * f;
+}
+
+double orc_sweep_o3_prop(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
+                         float omc, int prop, uint64_t key64, uint64_t sweep, float* sx, float* sy,
+                         float* sz, int64_t* accepted) {
     geom g = {dims, lx, ly, dims == 3 ? lz : 1};
     uint32_t key[2];
     key_of(key64, key);
@@ -744,28 +756,55 @@ double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float
                     uint32_t ctr[4], o[4];
                     make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_O3, 0, sweep);
                     orc_philox4x32_10(ctr, key, o);
-                    float w = ((float)(o[0] >> 8) * 0x1p-24f) * omc;
-                    float ct = 1.0f - w;
-                    float st = sqrtf(w * (2.0f - w));
-                    float cp, sp;
-                    orc_sincos_turn(o[1], &cp, &sp);
-                    /* cap sample through the Duff et al. (2017) orthonormal basis */
-                    float vx = st * cp, vy = st * sp;
-                    float sg = az >= 0.0f ? 1.0f : -1.0f;
-                    float k = -1.0f / (sg + az);
-                    float b = (ax * ay) * k;
-                    float e1x = 1.0f + (sg * (ax * ax)) * k;
-                    float e1y = sg * b;
-                    float e1z = -(sg * ax);
-                    float e2x = b;
-                    float e2y = sg + (ay * ay) * k;
-                    float e2z = -ay;
-                    float nx = (vx * e1x + vy * e2x) + ct * ax;
-                    float ny = (vx * e1y + vy * e2y) + ct * ay;
-                    float nz = (vx * e1z + vy * e2z) + ct * az;
-                    float n2 = (nx * nx + ny * ny) + nz * nz;
-                    float f = 1.5f - 0.5f * n2;      /* one Newton step of 1/sqrt(n2) from 1 */
-                    nx = nx * f; ny = ny * f; nz = nz * f;
+                    float nx, ny, nz;
+                    if (prop == 0) {
+                        float w = ((float)(o[0] >> 8) * 0x1p-24f) * omc;
+                        float ct = 1.0f - w;
+                        float st = sqrtf(w * (2.0f - w));
+                        float cp, sp;
+                        orc_sincos_turn(o[1], &cp, &sp);
+                        /* cap sample through the Duff et al. (2017) orthonormal basis */
+                        float vx = st * cp, vy = st * sp;
+                        float sg = az >= 0.0f ? 1.0f : -1.0f;
+                        float k = -1.0f / (sg + az);
+                        float b = (ax * ay) * k;
+                        float e1x = 1.0f + (sg * (ax * ax)) * k;
+                        float e1y = sg * b;
+                        float e1z = -(sg * ax);
+                        float e2x = b;
+                        float e2y = sg + (ay * ay) * k;
+                        float e2z = -ay;
+                        nx = (vx * e1x + vy * e2x) + ct * ax;
+                        ny = (vx * e1y + vy * e2y) + ct * ay;
+                        nz = (vx * e1z + vy * e2z) + ct * az;
+                        o3_newton(&nx, &ny, &nz);   /* one Newton step of 1/sqrt(n2) from 1 */
+                    } else if (prop == 1) {
+                        /* StandardStrategy: a uniform unit vector */
+                        nz = 1.0f - 2.0f * ((float)(o[0] >> 8) * 0x1p-24f);
+                        float rho = sqrtf((1.0f - nz) * (1.0f + nz));
+                        float cp, sp;
+                        orc_sincos_turn(o[1], &cp, &sp);
+                        nx = rho * cp;
+                        ny = rho * sp;
+                        o3_newton(&nx, &ny, &nz);
+                    } else {
+                        /* OPSSStrategy: rotation by theta in (-sigma, sigma) in
+                         * plane floor(3 w0 / 2^32) of (x,y), (y,z), (z,x) */
+                        uint32_t plane = (uint32_t)(((uint64_t)o[0] * 3u) >> 32);
+                        float u = ((float)(o[1] >> 8) + 0.5f) * 0x1p-24f;
+                        float theta = omc * (2.0f * u - 1.0f);
+                        float turns = theta * 0x1.45f306p-3f;
+                        uint32_t tu = (uint32_t)(int64_t)llrintf(turns * 0x1p32f);
+                        float c, s;
+                        orc_sincos_turn(tu, &c, &s);
+                        float a0 = plane == 0 ? ax : (plane == 1 ? ay : az);
+                        float a1 = plane == 0 ? ay : (plane == 1 ? az : ax);
+                        float r0 = c * a0 - s * a1, r1 = s * a0 + c * a1;
+                        nx = plane == 0 ? r0 : (plane == 1 ? ax : r1);
+                        ny = plane == 0 ? r1 : (plane == 1 ? r0 : ay);
+                        nz = plane == 0 ? az : (plane == 1 ? r1 : r0);
+                        o3_newton(&nx, &ny, &nz);
+                    }
                     float dot = ((nx - ax) * hx + (ny - ay) * hy) + (nz - az) * hz;
                     float dE = mJ * dot;
                     int ok;
@@ -1038,6 +1077,17 @@ double orc_energy_o3(int dims, int64_t lx, int64_t ly, int64_t lz, double J, con
                               (double)sz[s] * sz[nb[i]]);
             }
     return e;
+}
+
+float orc_opss_adapt(float sigma, int64_t accepted, int64_t attempted) {
+    if (attempted <= 0) return sigma;
+    float rate = (float)accepted / (float)attempted;
+    float x = 0.08f * (rate - 0.5f);
+    float f = x <= 0.0f ? orc_exp_neg(x) : 1.0f / orc_exp_neg(-x);
+    float s = sigma * f;
+    s = s < 1e-4f ? 1e-4f : s;
+    s = s > 0x1.921fb6p+1f ? 0x1.921fb6p+1f : s;
+    return s;
 }
 
 float orc_o3_adapt(float omc, int64_t accepted, int64_t attempted) {

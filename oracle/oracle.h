@@ -135,6 +135,14 @@ double orc_sweep_cluster_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float 
                             uint64_t key64, uint64_t sweep, float* sx, float* sy, float* sz, int64_t* changed);
 float orc_one_minus_exp_neg(float x);
 float orc_log_one_minus(float y);
+/* O(3) Metropolis with proposal prop: 0 the cap (omc = 1 - cos(alpha)), 1
+ * StandardStrategy's uniform unit vector, 2 OPSSStrategy's plane rotation
+ * (omc = sigma); CMC.rs/src/lattice/proposal.rs:45-167. */
+double orc_sweep_o3_prop(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
+                         float omc, int prop, uint64_t key64, uint64_t sweep, float* sx, float* sy,
+                         float* sz, int64_t* accepted);
+/* OPSSStrategy::finish_sweep (proposal.rs:156-167) in fp32 */
+float orc_opss_adapt(float sigma, int64_t accepted, int64_t attempted);
 double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
                     float omc, uint64_t key64, uint64_t sweep, float* sx, float* sy,
                     float* sz, int64_t* accepted);

@@ -30,6 +30,9 @@ METROPOLIS = 0
 HEAT_BATH = 1
 SWENDSEN_WANG = 2
 WOLFF = 3
+O3_CAP = 0
+O3_UNIFORM = 1
+O3_OPSS = 2
 PHASE_THERMALIZATION = 1
 PHASE_MEASUREMENT = 2
 
@@ -51,6 +54,7 @@ class Spec(ctypes.Structure):
         ("cone_half_angle", ctypes.c_double),
         ("record_capacity", ctypes.c_int32),
         ("algorithm", ctypes.c_int32),
+        ("o3_proposal", ctypes.c_int32),
     ]
 
 

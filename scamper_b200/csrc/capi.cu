@@ -230,6 +230,8 @@ int validate_spec(const gpumc_spec* s) {
     return fail(GPUMC_EINVAL, "initial_state: expected hot/random or cold/ordered");
   if (s->model == GPUMC_O3 && !(s->cone_half_angle > 0.0 && s->cone_half_angle <= M_PI))
     return fail(GPUMC_EINVAL, "cone_half_angle: must be in (0, pi]");
+  if (s->o3_proposal < GPUMC_O3_CAP || s->o3_proposal > GPUMC_O3_OPSS)
+    return fail(GPUMC_EINVAL, "o3_proposal: expected cap, uniform (standard) or opss");
   if (s->record_capacity < 1) return fail(GPUMC_EINVAL, "record_capacity: must be >= 1");
   if (s->algorithm < GPUMC_METROPOLIS || s->algorithm > GPUMC_WOLFF)
     return fail(GPUMC_EINVAL, "algorithm: expected metropolis, heat_bath, swendsen_wang or wolff");
@@ -317,6 +319,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
           : s->algorithm == GPUMC_SWENDSEN_WANG ? SWENDSEN_WANG
           : s->algorithm == GPUMC_WOLFF ? WOLFF : METROPOLIS;
   L.cluster = L.alg == SWENDSEN_WANG || L.alg == WOLFF;
+  L.prop = (L.model == O3 && L.alg == METROPOLIS) ? s->o3_proposal : 0;
   L.q = (int)s->q;
   L.dims = s->dims;
   L.lx = (int)s->lx;
@@ -508,7 +511,9 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
 int kernel_kind(const Layout& L) {
   if (L.cluster && L.model == O3) return kKindCluster + 8 + (L.dims - 2) + (L.alg == WOLFF ? 2 : 0);
   if (L.cluster) return kKindCluster + (L.model == POTTS ? 2 : 0) + (L.dims - 2) + (L.alg == WOLFF ? 4 : 0);
-  const int hb = L.alg == HEAT_BATH ? kKindHeatBath : 0;
+  const int hb = L.alg == HEAT_BATH ? kKindHeatBath
+                 : L.prop == GPUMC_O3_UNIFORM ? kKindO3Uniform
+                 : L.prop == GPUMC_O3_OPSS ? kKindO3Opss : 0;
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
   if (L.model == O3 && L.march) return 10 + hb;
   return L.model * 2 + (L.dims - 2) + hb;
@@ -547,6 +552,12 @@ static SweepKernel kernel_for(int kind) {
     case kKindHeatBath + 4: return k_sweep_o3<2, 1, 1>;
     case kKindHeatBath + 5: return k_sweep_o3<3, 1, 1>;
     case kKindHeatBath + 10: return k_sweep_o3_march<1, 1>;
+    case kKindO3Uniform + 4: return k_sweep_o3<2, 1, 2>;
+    case kKindO3Uniform + 5: return k_sweep_o3<3, 1, 2>;
+    case kKindO3Uniform + 10: return k_sweep_o3_march<1, 2>;
+    case kKindO3Opss + 4: return k_sweep_o3<2, 1, 3>;
+    case kKindO3Opss + 5: return k_sweep_o3<3, 1, 3>;
+    case kKindO3Opss + 10: return k_sweep_o3_march<1, 3>;
     default: return nullptr;
   }
 }
@@ -557,7 +568,7 @@ static int prepare_kernels() {
   static std::once_flag once;
   static cudaError_t status = cudaSuccess;
   std::call_once(once, [] {
-    for (int k = 0; k < 2 * kKindHeatBath; ++k) {
+    for (int k = 0; k < kKindO3Opss + 16; ++k) {
       if (!kernel_for(k)) continue;
       cudaError_t e = cudaFuncSetAttribute(kernel_for(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kMaxDynSmem);
@@ -568,7 +579,8 @@ static int prepare_kernels() {
       cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kIsingTileSmem);
       if (e != cudaSuccess) status = e;
     }
-    const void* colour0[] = {(const void*)k_sweep_o3_march<0, 0>, (const void*)k_sweep_o3_march<0, 1>};
+    const void* colour0[] = {(const void*)k_sweep_o3_march<0, 0>, (const void*)k_sweep_o3_march<0, 1>,
+                             (const void*)k_sweep_o3_march<0, 2>, (const void*)k_sweep_o3_march<0, 3>};
     for (const void* f : colour0) {
       cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
@@ -614,6 +626,14 @@ int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_
   if (kind == kKindHeatBath + 5) k_sweep_o3<3, 0, 1><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindHeatBath + 10)
     k_sweep_o3_march<0, 1><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Uniform + 4) k_sweep_o3<2, 0, 2><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Uniform + 5) k_sweep_o3<3, 0, 2><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Uniform + 10)
+    k_sweep_o3_march<0, 2><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Opss + 4) k_sweep_o3<2, 0, 3><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Opss + 5) k_sweep_o3<3, 0, 3><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Opss + 10)
+    k_sweep_o3_march<0, 3><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   k<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   CUDA_TRY(cudaGetLastError());
   return GPUMC_OK;

@@ -69,7 +69,7 @@ struct LatDesc {
   int32_t tile_cx, tile_y, tile_z;  // tile shape: chunks (16 sites) x rows x planes
   int32_t group;                    // index into the group array (PT / records)
   int32_t replica;                  // replica index within its group
-  int32_t pad0;
+  int32_t prop;                     // O(3) Metropolis proposal: 0 cap, 1 uniform, 2 OPSS
   int64_t n_sites;
   void* buf[2];
   void* aux;                        // cluster updates: uint32 label per site
@@ -79,7 +79,7 @@ struct LatDesc {
   uint64_t target;                  // stop once sweep reaches this count (serving)
   long long e_int;                  // discrete: energy in units of J
   double e_f;                       // O(3): running energy
-  float omc;                        // O(3): 1 - cos(cone half-angle)
+  float omc;                        // O(3): 1 - cos(cap half-angle); OPSS: rotation bound sigma
   int32_t adapt;                    // O(3): adapt omc during this sweep
   Accum acc;
   Accum acc2;                       // resident kernel: accumulators of odd launch-local sweeps

@@ -35,6 +35,20 @@ __device__ __forceinline__ float o3_adapt(float omc, long long accepted, long lo
   return w;
 }
 
+__device__ __forceinline__ float opss_adapt(float sigma, long long accepted, long long attempted) {
+  // OPSSStrategy::finish_sweep (CMC.rs/src/lattice/proposal.rs:156-167):
+  // sigma *= exp(0.08 (rate - 0.5)), clamped to [1e-4, pi]; |x| <= 0.04, so
+  // exp(x) is exp_neg(x) or 1 / exp_neg(-x)
+  if (attempted <= 0) return sigma;
+  const float rate = __fdiv_rn((float)accepted, (float)attempted);
+  const float x = __fmul_rn(0.08f, __fsub_rn(rate, 0.5f));
+  const float f = x <= 0.0f ? exp_neg(x) : __fdiv_rn(1.0f, exp_neg(-x));
+  float s = __fmul_rn(sigma, f);
+  s = s < 1e-4f ? 1e-4f : s;
+  s = s > 0x1.921fb6p+1f ? 0x1.921fb6p+1f : s;
+  return s;
+}
+
 // Epilogue flags of a group for the sweep being finished (GroupDesc::epi).
 constexpr int32_t kEpiFinished = 1, kEpiMeasuring = 2, kEpiRecord = 4, kEpiMsc = 8, kEpiExchange = 16,
                   kEpiBin = 32;
@@ -92,7 +106,8 @@ static __device__ void finish_replica(LatDesc* lats, GroupDesc* G, int r, int32_
     R.m[0] = take_f64(&A->mx);
     R.m[1] = take_f64(&A->my);
     R.m[2] = take_f64(&A->mz);
-    if (L->adapt && L->sweep < G->adapt_until) L->omc = o3_adapt(L->omc, nacc, L->n_sites);
+    if (L->adapt && L->sweep < G->adapt_until)
+      L->omc = L->prop == 2 ? opss_adapt(L->omc, nacc, L->n_sites) : o3_adapt(L->omc, nacc, L->n_sites);
   } else {
     L->e_int += dE;
     R.energy = G->J * (double)L->e_int;

@@ -17,6 +17,7 @@ struct Layout {
   int q = 2;             // Potts states
   int alg = METROPOLIS;  // sweep algorithm (METROPOLIS / HEAT_BATH / SWENDSEN_WANG / WOLFF)
   bool cluster = false;  // cluster update (label scratch per lattice, 4 launches per sweep)
+  int prop = 0;          // O(3) Metropolis proposal (GPUMC_O3_*)
   bool bits = false;     // Potts on the bit-sliced kernel (q <= 4, Metropolis)
   bool march = false;    // 3D O(3) on the shared-memory z-march kernel
   int64_t n_sites = 0;
@@ -38,7 +39,9 @@ constexpr int kKindHeatBath = 16;
 // kernel kinds of cluster layouts: kKindCluster + 2 (Potts) + (dims - 2) + 4 (Wolff);
 // O(3): kKindCluster + 8 + (dims - 2) + 2 (Wolff)
 constexpr int kKindCluster = 32;
-inline bool is_cluster_kind(int kind) { return kind >= kKindCluster; }
+inline bool is_cluster_kind(int kind) { return kind >= kKindCluster && kind < kKindCluster + 16; }
+// O(3) Metropolis with the uniform / OPSS proposal: the cap kind plus these
+constexpr int kKindO3Uniform = 48, kKindO3Opss = 64;
 // 2D Ising on the bit-sliced kernel (either single-site algorithm): the kinds
 // the resident multi-sweep launch can take
 inline bool is_ising2d_bits_kind(int kind) { return kind == 0 || kind == kKindHeatBath; }

@@ -132,7 +132,8 @@ static int admit(gpumc_server* srv, JobState* js) {
   if (!rc) rc = s->set_group_field(offsetof(GroupDesc, adapt_until), (uint64_t)js->job.n_therm);
   for (int r = 0; r < s->n_rep && !rc; ++r) {
     rc = s->set_lat_field(r, offsetof(LatDesc, target), js->target);
-    if (!rc && s->lay.model == O3 && s->lay.alg == METROPOLIS) rc = s->set_lat_field(r, offsetof(LatDesc, adapt), one);
+    if (!rc && s->lay.model == O3 && s->lay.alg == METROPOLIS && s->lay.prop != GPUMC_O3_UNIFORM)
+      rc = s->set_lat_field(r, offsetof(LatDesc, adapt), one);
   }
   if (!rc && cudaStreamSynchronize(srv->eng->stream) != cudaSuccess)
     rc = fail(GPUMC_ECUDA, "job admission: stream synchronize failed");

@@ -91,7 +91,8 @@ int gpumc_sim::push_phase_flags() {
   RC_TRY(set_group_field(offsetof(GroupDesc, measure), measure));
   if (lay.model == O3) {
     // the cone adapts during thermalization; the heat bath has no cone
-    const int32_t adapt = phase == GPUMC_PHASE_THERMALIZATION && lay.alg == METROPOLIS ? 1 : 0;
+    const int32_t adapt =
+        phase == GPUMC_PHASE_THERMALIZATION && lay.alg == METROPOLIS && lay.prop != GPUMC_O3_UNIFORM ? 1 : 0;
     for (int r = 0; r < n_rep; ++r) RC_TRY(set_lat_field(r, offsetof(LatDesc, adapt), adapt));
   }
   CUDA_TRY(cudaStreamSynchronize(eng->stream));
@@ -401,8 +402,12 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
     d.key = stream_key(base_seed, rid, 0, 1);
     d.sweep = 0;
     d.target = ~0ull;
-    d.omc = omc;
-    d.adapt = s->lay.alg == METROPOLIS ? 1 : 0;
+    d.prop = s->lay.prop;
+    // OPSS keeps its bound sigma where the cap keeps 1 - cos(alpha)
+    d.omc = s->lay.prop == GPUMC_O3_OPSS ? (float)spec->cone_half_angle : omc;
+    // the cap and OPSS adapt while thermalizing; the uniform proposal and the
+    // heat bath have nothing to adapt
+    d.adapt = (s->lay.alg == METROPOLIS && s->lay.prop != GPUMC_O3_UNIFORM) ? 1 : 0;
     CUDA_CLEAN(cudaMemcpy(eng->d_lats + s->lat0 + r, &d, sizeof(d), cudaMemcpyHostToDevice));
   }
   GroupDesc g;
@@ -761,8 +766,10 @@ int gpumc_acceptance(gpumc_sim* sim, int32_t replica, double* cone_half_angle) {
   CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
   LatDesc d;
   CUDA_TRY(cudaMemcpy(&d, sim->eng->d_lats + sim->lat0 + replica, sizeof(d), cudaMemcpyDeviceToHost));
-  // omc = 1 - cos(alpha) = 2 sin^2(alpha / 2)
-  *cone_half_angle = 2.0 * std::asin(std::sqrt(std::min(1.0, 0.5 * (double)d.omc)));
+  if (sim->lay.prop == GPUMC_O3_OPSS)
+    *cone_half_angle = (double)d.omc;  // the rotation bound sigma itself
+  else  // cap: omc = 1 - cos(alpha) = 2 sin^2(alpha / 2)
+    *cone_half_angle = 2.0 * std::asin(std::sqrt(std::min(1.0, 0.5 * (double)d.omc)));
   return GPUMC_OK;
 }
 
@@ -801,7 +808,8 @@ int gpumc_get_cone_omc(gpumc_sim* sim, int32_t replica, float* omc) {
 int gpumc_set_cone_omc(gpumc_sim* sim, int32_t replica, float omc) {
   if (!sim) return fail(GPUMC_EINVAL, "sim: null");
   if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
-  if (!(omc > 0.0f && omc <= 2.0f)) return fail(GPUMC_EINVAL, "omc: must be in (0, 2]");
+  if (sim->lay.prop == GPUMC_O3_OPSS ? !(omc >= 1e-4f && omc <= 0x1.921fb6p+1f) : !(omc > 0.0f && omc <= 2.0f))
+    return fail(GPUMC_EINVAL, "omc: must be in (0, 2] (cap) or [1e-4, pi] (OPSS sigma)");
   CUDA_TRY(cudaSetDevice(sim->eng->device));
   RC_TRY(sim->set_lat_field(replica, offsetof(LatDesc, omc), omc));
   CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));

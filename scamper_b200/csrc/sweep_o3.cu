@@ -17,6 +17,18 @@
 // dE = -J (s' - s) . h, h the sum of the neighbour spins
 // (ONModel::bond_energy, CMC.rs/src/lattice/models.rs:440-452).
 //
+// Other proposals of the Metropolis step (ALG = 2, 3): the reference's
+// StandardStrategy (an independent uniform unit vector, ONModel::propose_from,
+// CMC.rs/src/lattice/proposal.rs:45-63; here z = 1 - 2u, phi from word 1, one
+// Newton renormalisation) and OPSSStrategy (proposal.rs:72-167: a rotation by
+// theta uniform in (-sigma, sigma) in a random coordinate plane, then
+// normalised; sigma adapted during thermalisation by exp(0.08 (rate - 0.5)),
+// clamped to [1e-4, pi]).  OPSS takes the plane floor(3 w0 / 2^32) of
+// {(x,y), (y,z), (z,x)} (rotating in (j,i) by theta is rotating in (i,j) by
+// -theta, so unordered planes with a symmetric angle are the reference's
+// ordered pairs) and theta = sigma (2u - 1), u from word 1, its sine and
+// cosine by the engine's own turn polynomials; sigma is the lattice's `omc`.
+//
 // Heat bath (ALG = 1; ContinuousHeatBathCore, CMC.rs/src/algorithms/
 // heat_bath.rs:75-134, with ContinuousHeatBathable for ONModel<3>,
 // CMC.rs/src/lattice/models.rs:617-663): the new spin is drawn from
@@ -67,18 +79,55 @@ __device__ __forceinline__ void o3_place(float ax, float ay, float az, float ct,
   pz = fmul(pz, f);
 }
 
-// Metropolis step with the cap proposal: returns the decision and the
-// proposed spin and its fp32 dE.
+// Renormalisation by one Newton step of 1/sqrt(n2) from 1.
+__device__ __forceinline__ void o3_renorm(float& px, float& py, float& pz) {
+  const float n2 = fadd(fadd(fmul(px, px), fmul(py, py)), fmul(pz, pz));
+  const float f = fsub(1.5f, fmul(0.5f, n2));
+  px = fmul(px, f);
+  py = fmul(py, f);
+  pz = fmul(pz, f);
+}
+
+// Metropolis step: PROP 0 cap proposal (w = 1 - cos(alpha) in omc), 1
+// uniform unit vector, 2 OPSS plane rotation (sigma in omc).  Returns the
+// decision and the proposed spin and its fp32 dE.
+template <int PROP>
 __device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx, float hy,
                                           float hz, uint4 o, float omc, float mJ, float beta,
                                           float& nx, float& ny, float& nz, float& dE) {
-  const float w = fmul(fmul((float)(o.x >> 8), 0x1p-24f), omc);
-  const float ct = fsub(1.0f, w);
-  const float st = fsqrt(fmul(w, fsub(2.0f, w)));
-  float cp, sp;
-  sincos_turn(o.y, cp, sp);
   float px, py, pz;
-  o3_place(ax, ay, az, ct, st, cp, sp, px, py, pz);
+  if (PROP == 0) {
+    const float w = fmul(fmul((float)(o.x >> 8), 0x1p-24f), omc);
+    const float ct = fsub(1.0f, w);
+    const float st = fsqrt(fmul(w, fsub(2.0f, w)));
+    float cp, sp;
+    sincos_turn(o.y, cp, sp);
+    o3_place(ax, ay, az, ct, st, cp, sp, px, py, pz);
+  } else if (PROP == 1) {
+    pz = fsub(1.0f, fmul(2.0f, fmul((float)(o.x >> 8), 0x1p-24f)));
+    const float rho = fsqrt(fmul(fsub(1.0f, pz), fadd(1.0f, pz)));
+    float cp, sp;
+    sincos_turn(o.y, cp, sp);
+    px = fmul(rho, cp);
+    py = fmul(rho, sp);
+    o3_renorm(px, py, pz);
+  } else {
+    const uint32_t plane = __umulhi(o.x, 3u);
+    const float u = fmul(fadd((float)(o.y >> 8), 0.5f), 0x1p-24f);
+    const float theta = fmul(omc, fsub(fmul(2.0f, u), 1.0f));
+    // theta as a signed fraction of a turn, 32-bit fixed point
+    const float turns = fmul(theta, 0x1.45f306p-3f);  // 1 / (2 pi)
+    const uint32_t tu = (uint32_t)(long long)__float2ll_rn(fmul(turns, 0x1p32f));
+    float c, s;
+    sincos_turn(tu, c, s);
+    const float a0 = plane == 0 ? ax : (plane == 1 ? ay : az);
+    const float a1 = plane == 0 ? ay : (plane == 1 ? az : ax);
+    const float r0 = fsub(fmul(c, a0), fmul(s, a1)), r1 = fadd(fmul(s, a0), fmul(c, a1));
+    px = plane == 0 ? r0 : (plane == 1 ? ax : r1);
+    py = plane == 0 ? r1 : (plane == 1 ? r0 : ay);
+    pz = plane == 0 ? az : (plane == 1 ? r1 : r0);
+    o3_renorm(px, py, pz);
+  }
   const float dot =
       fadd(fadd(fmul(fsub(px, ax), hx), fmul(fsub(py, ay), hy)), fmul(fsub(pz, az), hz));
   const float de = fmul(mJ, dot);
@@ -229,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   const float mJ = -G->Jf;
   const double Jd = G->J;
   const float omc = L->omc;
-  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG ? TAG_O3HB : TAG_O3) << 1));
+  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(L->tile_y, ly - t.y0);
   const int dv = DIM == 3 ? min(L->tile_z, lz - t.z0) : 1;
   const int half = lx >> 1;
@@ -274,11 +323,12 @@ __global__ void __launch_bounds__(kThreads, 4)
   auto update = [&](const O3Site& q) {
     float nx, ny, nz, de;
     bool ok;
-    if (ALG) {
+    if (ALG == 1) {
       o3_heat_bath(q.hx, q.hy, q.hz, o3_philox(P, q.site), -mJ, beta, nx, ny, nz);
       ok = (nx != q.ax) | (ny != q.ay) | (nz != q.az);
     } else {
-      ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx, ny, nz, de);
+      ok = o3_update<ALG == 2 ? 1 : (ALG == 3 ? 2 : 0)>(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site),
+                                                         omc, mJ, beta, nx, ny, nz, de);
     }
     float fx = q.ax, fy = q.ay, fz = q.az;
     if (ok) {
@@ -369,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   const float mJ = -G->Jf;
   const double Jd = G->J;
   const float omc = L->omc;
-  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG ? TAG_O3HB : TAG_O3) << 1));
+  const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(L->tile_y, ly - t.y0);
   const int dv = min(L->tile_z, lz - t.z0);
   const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
@@ -395,11 +445,12 @@ __global__ void __launch_bounds__(kThreads, 4)
   auto update = [&](const O3Site& q) {
     float nx, ny, nz, de;
     bool ok;
-    if (ALG) {
+    if (ALG == 1) {
       o3_heat_bath(q.hx, q.hy, q.hz, o3_philox(P, q.site), -mJ, beta, nx, ny, nz);
       ok = (nx != q.ax) | (ny != q.ay) | (nz != q.az);
     } else {
-      ok = o3_update(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site), omc, mJ, beta, nx, ny, nz, de);
+      ok = o3_update<ALG == 2 ? 1 : (ALG == 3 ? 2 : 0)>(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site),
+                                                         omc, mJ, beta, nx, ny, nz, de);
     }
     float fx = q.ax, fy = q.ay, fz = q.az;
     if (ok) {
@@ -518,5 +569,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   template __global__ void k_sweep_o3<3, 1, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 O3_INSTANTIATE(0)
 O3_INSTANTIATE(1)
+O3_INSTANTIATE(2)
+O3_INSTANTIATE(3)
 
 }  // namespace gpumc

@@ -106,7 +106,15 @@ def lattice_from_params(params):
                         "engine (square, cubic, hypercubic)")
 
 
-def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capacity=1024, algorithm=None):
+# O(3) Metropolis proposals: the engine's adapted cap, the reference's
+# StandardStrategy (uniform unit vector) and OPSSStrategy (plane rotation),
+# CMC.rs/src/lattice/proposal.rs:45-167
+O3_PROPOSALS = {"cap": _lib.O3_CAP, "cone": _lib.O3_CAP, "standard": _lib.O3_UNIFORM,
+                "uniform": _lib.O3_UNIFORM, "opss": _lib.O3_OPSS}
+
+
+def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capacity=1024, algorithm=None,
+                     o3_proposal=None):
     params = params if isinstance(params, Params) else Params(params)
     mname = model if model is not None else str(params.get("model", "ising")).lower()
     if isinstance(mname, int):
@@ -127,12 +135,19 @@ def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capaci
         init_id = _lib.INIT_COLD
     else:
         raise InvalidConfig(_lib.EINVAL, "initial_state: expected hot/random or cold/ordered")
+    prop = "cap" if o3_proposal is None else str(o3_proposal).lower()
+    if prop not in O3_PROPOSALS:
+        raise InvalidConfig(_lib.EINVAL, f"o3_proposal: unknown proposal `{o3_proposal}` "
+                                         "(expected cap, standard or opss)")
+    # the OPSS bound starts at OPSSStrategy's default sigma = 0.5 unless given
+    step = params.get_as("opss_sigma", float, 0.5) if O3_PROPOSALS[prop] == _lib.O3_OPSS else \
+        params.get_as("cone_half_angle", float, 1.0)
     arr = (ctypes.c_double * len(betas))(*betas)
     spec = _lib.Spec(model=mid, dims=dims, lx=lx, ly=ly, lz=lz, pbc=1 if pbc else 0,
                      q=params.get_as("q", int, 3), J=params.get_as("J", float, 1.0),
                      n_replicas=n_replicas, n_temps=len(betas), betas=arr, init=init_id,
-                     cone_half_angle=params.get_as("cone_half_angle", float, 1.0),
-                     record_capacity=record_capacity, algorithm=algorithm_id(algorithm))
+                     cone_half_angle=step, record_capacity=record_capacity,
+                     algorithm=algorithm_id(algorithm), o3_proposal=O3_PROPOSALS[prop])
     return spec, arr
 
 
@@ -193,19 +208,24 @@ class ClassicalMC:
 
     # -- FromParams -----------------------------------------------------------
     @staticmethod
-    def validate_params(params, model=None, algorithm=None):
-        spec, _keep = spec_from_params(params, model=model, algorithm=algorithm)
+    def validate_params(params, model=None, algorithm=None, o3_proposal=None):
+        spec, _keep = spec_from_params(params, model=model, algorithm=algorithm, o3_proposal=o3_proposal)
         _lib.call("gpumc_validate", ctypes.byref(spec))
 
     @classmethod
     def from_params(cls, params, seed, model=None, n_replicas=1, betas=None, engine=None,
-                    record_capacity=1024, algorithm=None):
+                    record_capacity=1024, algorithm=None, o3_proposal=None):
         """`algorithm`: "metropolis" (MetropolisCore, the default),
         "heat_bath" (HeatBathCore for Ising / Potts, ContinuousHeatBathCore
         for O(3)), "swendsen_wang" (SWCore) or "wolff" (WolffCore; one cluster
-        per sweep), the cluster updates for Ising / Potts with J >= 0."""
+        per sweep), the cluster updates for Ising / Potts / O(3) with J >= 0.
+        `o3_proposal` (O(3) Metropolis): "cap" (default: a cap around the
+        current spin, half-angle adapted), "standard" (StandardStrategy:
+        uniform unit vector) or "opss" (OPSSStrategy: plane rotation, bound
+        from params["opss_sigma"], default 0.5, adapted)."""
         spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas,
-                                      record_capacity=record_capacity, algorithm=algorithm)
+                                      record_capacity=record_capacity, algorithm=algorithm,
+                                      o3_proposal=o3_proposal)
         return cls(spec, seed, engine=engine, _keep=keep)
 
     # -- MonteCarlo -----------------------------------------------------------
