@@ -692,6 +692,16 @@ int gpumc_engine_create(int32_t device, gpumc_engine** out) {
     delete e;
     return fail(GPUMC_ECUDA, std::string("engine allocation: ") + cudaGetErrorString(err));
   }
+  // Simulations allocate from the device's stream-ordered pool: keep freed
+  // memory pooled (no release to the driver at synchronisation points), so
+  // admitting a job after another retired reuses its memory without mapping
+  // pages or synchronising the device.  The pool setting belongs to this
+  // process; destroying the engine trims the pool again.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   int n_sm = 0, per_sm = 0;
   err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
   if (err == cudaSuccess)
@@ -717,7 +727,10 @@ int gpumc_engine_create(int32_t device, gpumc_engine** out) {
 gpumc_engine::~gpumc_engine() {
   cudaSetDevice(device);
   drop_graphs();
-  for (auto& p : batch_plans) p.release();
+  for (auto& p : batch_plans) p.release(stream);
+  if (stream) cudaStreamSynchronize(stream);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   if (d_lats) cudaFree(d_lats);
   if (d_groups) cudaFree(d_groups);
   if (stream) cudaStreamDestroy(stream);
@@ -776,27 +789,27 @@ int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n) {
   return GPUMC_OK;
 }
 
-void BatchPlan::release() {
-  if (d_tiles) cudaFree(d_tiles);
-  if (d_gids) cudaFree(d_gids);
-  if (d_ctl) cudaFree(d_ctl);
+void BatchPlan::release(cudaStream_t st) {
+  dev_free(d_tiles, st);
+  dev_free(d_gids, st);
+  dev_free(d_ctl, st);
   d_tiles = nullptr;
   d_gids = nullptr;
   d_ctl = nullptr;
-  res.release();
+  res.release(st);
 }
 
-void ResidentPlan::release() {
-  if (d_nbr) cudaFree(d_nbr);
-  if (d_xchg) cudaFree(d_xchg);
+void ResidentPlan::release(cudaStream_t st) {
+  dev_free(d_nbr, st);
+  dev_free(d_xchg, st);
   d_nbr = nullptr;
   d_xchg = nullptr;
   on = false;
 }
 
-int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
+int gpumc::build_resident(int device, cudaStream_t st, const std::vector<TileItem>& tiles,
                           const std::map<int, const Layout*>& layout_of_lat, size_t smem, ResidentPlan& rp) {
-  rp.release();
+  rp.release(st);
   if (tiles.empty() || smem > kIsingTileSmem) return GPUMC_OK;
   // every tile a whole-row 2D Ising tile of >= 2 rows; a lattice's tiles are
   // consecutive in y order (enumerate_tiles), so its neighbours are the
@@ -828,9 +841,9 @@ int gpumc::build_resident(int device, const std::vector<TileItem>& tiles,
       &per_sm, rp.alg == HEAT_BATH ? k_sweep_ising_resident<1> : k_sweep_ising_resident<0>, kThreads, smem));
   if (!coop || (int64_t)per_sm * n_sm < (int64_t)tiles.size()) return GPUMC_OK;
   rp.xstride = 2 * 4 * wmax;
-  CUDA_TRY(cudaMalloc(&rp.d_nbr, sizeof(int2) * nbr.size()));
-  CUDA_TRY(cudaMemcpy(rp.d_nbr, nbr.data(), sizeof(int2) * nbr.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&rp.d_xchg, sizeof(uint2) * (size_t)rp.xstride * tiles.size()));
+  CUDA_TRY(cudaMallocAsync(&rp.d_nbr, sizeof(int2) * nbr.size(), st));
+  CUDA_TRY(cudaMemcpyAsync(rp.d_nbr, nbr.data(), sizeof(int2) * nbr.size(), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMallocAsync(&rp.d_xchg, sizeof(uint2) * (size_t)rp.xstride * tiles.size(), st));
   rp.on = true;
   return GPUMC_OK;
 }
@@ -860,7 +873,7 @@ int gpumc::launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, 
 int gpumc_engine::rebuild_batch() {
   if (!batch_dirty) return GPUMC_OK;
   drop_graphs();
-  for (auto& p : batch_plans) p.release();
+  for (auto& p : batch_plans) p.release(stream);
   batch_plans.clear();
   std::map<int, BatchPlan> plans;
   std::map<int, std::vector<TileItem>> tiles;
@@ -883,21 +896,21 @@ int gpumc_engine::rebuild_batch() {
     auto& gv = gids[kv.first];
     p.n_tiles = (int)tv.size();
     p.n_groups = (int)gv.size();
-    CUDA_TRY(cudaMalloc(&p.d_tiles, sizeof(TileItem) * tv.size()));
-    CUDA_TRY(cudaMalloc(&p.d_gids, sizeof(int32_t) * gv.size()));
-    CUDA_TRY(cudaMalloc(&p.d_ctl, sizeof(LaunchCtl)));
-    CUDA_TRY(cudaMemcpy(p.d_tiles, tv.data(), sizeof(TileItem) * tv.size(), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(p.d_gids, gv.data(), sizeof(int32_t) * gv.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMallocAsync(&p.d_tiles, sizeof(TileItem) * tv.size(), stream));
+    CUDA_TRY(cudaMallocAsync(&p.d_gids, sizeof(int32_t) * gv.size(), stream));
+    CUDA_TRY(cudaMallocAsync(&p.d_ctl, sizeof(LaunchCtl), stream));
+    CUDA_TRY(cudaMemcpyAsync(p.d_tiles, tv.data(), sizeof(TileItem) * tv.size(), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(p.d_gids, gv.data(), sizeof(int32_t) * gv.size(), cudaMemcpyHostToDevice, stream));
     LaunchCtl c;
     c.done = 0;
     c.n_groups = p.n_groups;
     c.group_ids = p.d_gids;
     c.n_tiles = p.n_tiles;
-    CUDA_TRY(cudaMemcpy(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
     if (is_ising2d_bits_kind(p.kind)) {
-      int rc = build_resident(device, tv, layout_of_lat, p.smem, p.res);
+      int rc = build_resident(device, stream, tv, layout_of_lat, p.smem, p.res);
       if (rc) {
-        p.release();
+        p.release(stream);
         return rc;
       }
     }

@@ -28,6 +28,11 @@ struct Layout {
 };
 
 int fail(int code, const std::string& msg);
+// Stream-ordered release into the device's memory pool (no device-wide
+// synchronisation; the engine keeps freed memory pooled for reuse).
+inline void dev_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
 uint64_t stream_key(uint64_t base, uint64_t replica, uint64_t phase, uint64_t substream);
 void threshold80(double p, uint32_t& head, unsigned long long& tail);
 int n_classes(int model, int dims);
@@ -76,7 +81,7 @@ struct ResidentPlan {
   int2* d_nbr = nullptr;
   uint2* d_xchg = nullptr;
   int xstride = 0;  // uint2 words of exchange space per tile
-  void release();
+  void release(cudaStream_t st);
 };
 
 struct BatchPlan {
@@ -88,14 +93,14 @@ struct BatchPlan {
   int n_groups = 0;
   LaunchCtl* d_ctl = nullptr;
   ResidentPlan res;
-  void release();
+  void release(cudaStream_t st);
 };
 
 // Qualifies a tile list for the resident Ising kernel (every tile a
 // whole-row 2D Ising tile of at least two rows, all tiles co-resident on the
 // device) and allocates its neighbour table and exchange buffer; leaves
 // rp.on false when the list does not qualify.
-int build_resident(int device, const std::vector<TileItem>& tiles,
+int build_resident(int device, cudaStream_t st, const std::vector<TileItem>& tiles,
                    const std::map<int, const Layout*>& layout_of_lat, size_t smem, ResidentPlan& rp);
 // n_sweeps sweeps of every tile in one cooperative launch; waits for it and
 // reports a barrier timeout as an error.

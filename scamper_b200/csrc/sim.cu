@@ -45,23 +45,26 @@ gpumc_sim::~gpumc_sim() {
   cudaSetDevice(eng->device);
   cudaStreamSynchronize(eng->stream);
   drop_graphs();
+  // stream-ordered frees: no device-wide synchronisation, the memory goes
+  // back to the pool for the next simulation
+  const cudaStream_t st = eng->stream;
   for (size_t i = 0; i < bufs.size(); ++i)
-    if (bufs[i] && (i % 2 == 0 || bufs[i] != bufs[i - 1])) cudaFree(bufs[i]);
-  cudaFree(d_head);
-  cudaFree(d_tail);
-  cudaFree(d_betas);
-  cudaFree(d_betas_f);
-  cudaFree(d_label);
-  cudaFree(d_rep_at);
-  cudaFree(d_records);
-  for (void* p : aux) cudaFree(p);
-  cudaFree(d_bin_open);
-  cudaFree(d_bins);
-  cudaFree(d_msc_counters);
-  cudaFree(d_tiles);
-  cudaFree(d_gid);
-  cudaFree(d_ctl);
-  res.release();
+    if (bufs[i] && (i % 2 == 0 || bufs[i] != bufs[i - 1])) dev_free(bufs[i], st);
+  dev_free(d_head, st);
+  dev_free(d_tail, st);
+  dev_free(d_betas, st);
+  dev_free(d_betas_f, st);
+  dev_free(d_label, st);
+  dev_free(d_rep_at, st);
+  dev_free(d_records, st);
+  for (void* p : aux) dev_free(p, st);
+  dev_free(d_bin_open, st);
+  dev_free(d_bins, st);
+  dev_free(d_msc_counters, st);
+  dev_free(d_tiles, st);
+  dev_free(d_gid, st);
+  dev_free(d_ctl, st);
+  res.release(st);
 }
 
 void gpumc_sim::drop_graphs() {
@@ -244,7 +247,7 @@ int gpumc_sim::launch_energy(const void* buf, unsigned long long* d_e, unsigned 
 int gpumc_sim::recompute(std::vector<double>& out, bool store) {
   out.assign(n_rep, 0.0);
   unsigned long long* d_acc = nullptr;
-  CUDA_TRY(cudaMalloc(&d_acc, 8 * (size_t)n_rep));
+  CUDA_TRY(cudaMallocAsync(&d_acc, 8 * (size_t)n_rep, eng->stream));
   int rc = GPUMC_OK;
   cudaError_t e = cudaMemsetAsync(d_acc, 0, 8 * (size_t)n_rep, eng->stream);
   for (int r = 0; r < n_rep && e == cudaSuccess && rc == GPUMC_OK; ++r)
@@ -252,8 +255,8 @@ int gpumc_sim::recompute(std::vector<double>& out, bool store) {
   std::vector<unsigned long long> h(n_rep);
   if (e == cudaSuccess && rc == GPUMC_OK)
     e = cudaMemcpyAsync(h.data(), d_acc, 8 * (size_t)n_rep, cudaMemcpyDeviceToHost, eng->stream);
+  dev_free(d_acc, eng->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
-  cudaFree(d_acc);
   if (rc != GPUMC_OK) return rc;
   if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("energy recompute: ") + cudaGetErrorString(e));
   for (int r = 0; r < n_rep; ++r) {
@@ -332,48 +335,48 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
       s->bufs[i] = s->bufs[i - 1];
       continue;
     }
-    CUDA_CLEAN(cudaMalloc(&s->bufs[i], s->lay.buf_bytes));
+    CUDA_CLEAN(cudaMallocAsync(&s->bufs[i], s->lay.buf_bytes, eng->stream));
     CUDA_CLEAN(cudaMemsetAsync(s->bufs[i], 0, s->lay.buf_bytes, eng->stream));
   }
   if (s->lay.cluster) {  // union-find labels of the cluster updates, one array per replica
     s->aux.assign(s->n_rep, nullptr);
-    for (int r = 0; r < s->n_rep; ++r) CUDA_CLEAN(cudaMalloc(&s->aux[r], 4 * (size_t)s->lay.n_sites));
+    for (int r = 0; r < s->n_rep; ++r) CUDA_CLEAN(cudaMallocAsync(&s->aux[r], 4 * (size_t)s->lay.n_sites, eng->stream));
   }
-  CUDA_CLEAN(cudaMalloc(&s->d_head, 4 * (size_t)s->n_temps * s->n_cls));
-  CUDA_CLEAN(cudaMalloc(&s->d_tail, 8 * (size_t)s->n_temps * s->n_cls));
-  CUDA_CLEAN(cudaMalloc(&s->d_betas, 8 * (size_t)s->n_temps));
-  CUDA_CLEAN(cudaMalloc(&s->d_betas_f, 4 * (size_t)s->n_temps));
-  CUDA_CLEAN(cudaMalloc(&s->d_label, 4 * (size_t)s->n_rep));
-  CUDA_CLEAN(cudaMalloc(&s->d_rep_at, 4 * (size_t)s->n_rep));
-  CUDA_CLEAN(cudaMalloc(&s->d_records, sizeof(Record) * (size_t)s->rec_cap * s->rec_stride));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_head, 4 * (size_t)s->n_temps * s->n_cls, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_tail, 8 * (size_t)s->n_temps * s->n_cls, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_betas, 8 * (size_t)s->n_temps, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_betas_f, 4 * (size_t)s->n_temps, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_label, 4 * (size_t)s->n_rep, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_rep_at, 4 * (size_t)s->n_rep, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_records, sizeof(Record) * (size_t)s->rec_cap * s->rec_stride, eng->stream));
   if (s->lay.model == MSC) {
-    CUDA_CLEAN(cudaMalloc(&s->d_msc_counters, 8 * 128 * (size_t)s->n_rep));
+    CUDA_CLEAN(cudaMallocAsync(&s->d_msc_counters, 8 * 128 * (size_t)s->n_rep, eng->stream));
     CUDA_CLEAN(cudaMemsetAsync(s->d_msc_counters, 0, 8 * 128 * (size_t)s->n_rep, eng->stream));
   }
   rc = s->upload_tables();
   if (rc) return cleanup(rc);
   std::vector<int32_t> labels(s->n_rep);
   for (int r = 0; r < s->n_rep; ++r) labels[r] = s->n_temps == 1 ? 0 : r;
-  CUDA_CLEAN(cudaMemcpy(s->d_label, labels.data(), 4 * (size_t)s->n_rep, cudaMemcpyHostToDevice));
+  CUDA_CLEAN(cudaMemcpyAsync(s->d_label, labels.data(), 4 * (size_t)s->n_rep, cudaMemcpyHostToDevice, eng->stream));
   // tiles and launch control of the plain path
   std::vector<TileItem> tiles;
   for (int r = 0; r < s->n_rep; ++r) enumerate_tiles(s->lay, s->lat0 + r, tiles);
   s->n_tiles = (int)tiles.size();
-  CUDA_CLEAN(cudaMalloc(&s->d_tiles, sizeof(TileItem) * tiles.size()));
-  CUDA_CLEAN(cudaMemcpy(s->d_tiles, tiles.data(), sizeof(TileItem) * tiles.size(), cudaMemcpyHostToDevice));
-  CUDA_CLEAN(cudaMalloc(&s->d_gid, sizeof(int32_t)));
-  CUDA_CLEAN(cudaMemcpy(s->d_gid, &s->group, sizeof(int32_t), cudaMemcpyHostToDevice));
-  CUDA_CLEAN(cudaMalloc(&s->d_ctl, sizeof(LaunchCtl)));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_tiles, sizeof(TileItem) * tiles.size(), eng->stream));
+  CUDA_CLEAN(cudaMemcpyAsync(s->d_tiles, tiles.data(), sizeof(TileItem) * tiles.size(), cudaMemcpyHostToDevice, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_gid, sizeof(int32_t), eng->stream));
+  CUDA_CLEAN(cudaMemcpyAsync(s->d_gid, &s->group, sizeof(int32_t), cudaMemcpyHostToDevice, eng->stream));
+  CUDA_CLEAN(cudaMallocAsync(&s->d_ctl, sizeof(LaunchCtl), eng->stream));
   LaunchCtl c;
   c.done = 0;
   c.n_groups = 1;
   c.group_ids = s->d_gid;
   c.n_tiles = s->n_tiles;
-  CUDA_CLEAN(cudaMemcpy(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  CUDA_CLEAN(cudaMemcpyAsync(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, eng->stream));
   if (is_ising2d_bits_kind(kernel_kind(s->lay))) {
     std::map<int, const Layout*> lay_of;
     for (int r = 0; r < s->n_rep; ++r) lay_of[s->lat0 + r] = &s->lay;
-    rc = build_resident(eng->device, tiles, lay_of, s->lay.smem, s->res);
+    rc = build_resident(eng->device, eng->stream, tiles, lay_of, s->lay.smem, s->res);
     if (rc) return cleanup(rc);
   }
   // descriptors
@@ -408,7 +411,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
     // the cap and OPSS adapt while thermalizing; the uniform proposal and the
     // heat bath have nothing to adapt
     d.adapt = (s->lay.alg == METROPOLIS && s->lay.prop != GPUMC_O3_UNIFORM) ? 1 : 0;
-    CUDA_CLEAN(cudaMemcpy(eng->d_lats + s->lat0 + r, &d, sizeof(d), cudaMemcpyHostToDevice));
+    CUDA_CLEAN(cudaMemcpyAsync(eng->d_lats + s->lat0 + r, &d, sizeof(d), cudaMemcpyHostToDevice, eng->stream));
   }
   GroupDesc g;
   std::memset(&g, 0, sizeof(g));
@@ -430,12 +433,12 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   g.adapt_until = ~0ull;
   g.pt_key = stream_key(base_seed, 0, 3, 0);
   g.records = s->d_records;
-  CUDA_CLEAN(cudaMemcpy(eng->d_groups + s->group, &g, sizeof(g), cudaMemcpyHostToDevice));
+  CUDA_CLEAN(cudaMemcpyAsync(eng->d_groups + s->group, &g, sizeof(g), cudaMemcpyHostToDevice, eng->stream));
   // initial state
   const int blocks = (int)std::min<int64_t>(kInitBlocks, (s->lay.n_sites + 255) / 256);
   const int hot = spec->init == GPUMC_INIT_HOT;
   uint64_t* d_keys = nullptr;
-  if (s->lay.model == MSC) CUDA_CLEAN(cudaMalloc(&d_keys, 8 * 64));
+  if (s->lay.model == MSC) CUDA_CLEAN(cudaMallocAsync(&d_keys, 8 * 64, eng->stream));
   for (int r = 0; r < s->n_rep; ++r) {
     const uint64_t kinit = stream_key(base_seed, (uint64_t)r, 0, 0);
     if (s->lay.model == ISING || s->lay.model == POTTS) {
@@ -448,7 +451,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
     } else {
       uint64_t keys[64];
       for (int b = 0; b < 64; ++b) keys[b] = stream_key(base_seed, 64ull * r + b, 0, 0);
-      CUDA_CLEAN(cudaMemcpy(d_keys, keys, sizeof(keys), cudaMemcpyHostToDevice));
+      CUDA_CLEAN(cudaMemcpyAsync(d_keys, keys, sizeof(keys), cudaMemcpyHostToDevice, eng->stream));
       k_init_msc<<<blocks, 256, 0, eng->stream>>>((unsigned long long*)s->bufs[2 * r], s->lay.lx,
                                                    s->lay.ly, s->lay.lz, s->lay.pitch, d_keys, hot);
       CUDA_CLEAN(cudaStreamSynchronize(eng->stream));
@@ -456,7 +459,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   }
   CUDA_CLEAN(cudaGetLastError());
   CUDA_CLEAN(cudaStreamSynchronize(eng->stream));
-  if (d_keys) cudaFree(d_keys);
+  if (d_keys) dev_free(d_keys, eng->stream);
   std::vector<double> e0;
   rc = s->recompute(e0, true);
   if (rc) return cleanup(rc);
@@ -529,8 +532,8 @@ int gpumc_set_binning(gpumc_sim* sim, int32_t binsize, int32_t bin_capacity) {
   CUDA_TRY(cudaSetDevice(sim->eng->device));
   RC_TRY(sim->drain_records());  // records measured so far stay available
   CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
-  cudaFree(sim->d_bin_open);
-  cudaFree(sim->d_bins);
+  dev_free(sim->d_bin_open, sim->eng->stream);
+  dev_free(sim->d_bins, sim->eng->stream);
   sim->d_bin_open = sim->d_bins = nullptr;
   sim->pending_bins.clear();
   sim->bin_total = 0;
@@ -538,11 +541,12 @@ int gpumc_set_binning(gpumc_sim* sim, int32_t binsize, int32_t bin_capacity) {
   sim->bin_cap = 0;
   const size_t per = (size_t)sim->n_rep * kBinObs;
   if (binsize > 0) {
-    CUDA_TRY(cudaMalloc(&sim->d_bin_open, per * sizeof(double)));
-    CUDA_TRY(cudaMemset(sim->d_bin_open, 0, per * sizeof(double)));
-    if (cudaMalloc(&sim->d_bins, per * (size_t)bin_capacity * sizeof(double)) != cudaSuccess) {
+    CUDA_TRY(cudaMallocAsync(&sim->d_bin_open, per * sizeof(double), sim->eng->stream));
+    CUDA_TRY(cudaMemsetAsync(sim->d_bin_open, 0, per * sizeof(double), sim->eng->stream));
+    if (cudaMallocAsync(&sim->d_bins, per * (size_t)bin_capacity * sizeof(double), sim->eng->stream) !=
+        cudaSuccess) {
       cudaGetLastError();
-      cudaFree(sim->d_bin_open);
+      dev_free(sim->d_bin_open, sim->eng->stream);
       sim->d_bin_open = nullptr;
       return fail(GPUMC_ENOMEM, "bin_capacity: device memory exhausted");
     }
@@ -650,15 +654,15 @@ int gpumc_set_spins(gpumc_sim* sim, int32_t replica, const void* host, size_t nb
     // :238-252); only a valid state replaces the current one.
     void* stage = sim->bufs[2 * replica + ((sim->sweeps & 1) ^ 1)];
     unsigned long long* d_acc = nullptr;
-    CUDA_TRY(cudaMalloc(&d_acc, 16));
     cudaStream_t st = sim->eng->stream;
+    CUDA_TRY(cudaMallocAsync(&d_acc, 16, st));
     unsigned long long h[2] = {0, 0};
     cudaError_t e = cudaMemcpy2DAsync(stage, L.pitch, host, L.lx, L.lx, rows, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_acc, 0, 16, st);
     int rc = e == cudaSuccess ? sim->launch_energy(stage, d_acc, (unsigned int*)(d_acc + 1)) : GPUMC_OK;
     if (e == cudaSuccess && rc == GPUMC_OK) e = cudaMemcpyAsync(h, d_acc, 16, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && rc == GPUMC_OK) e = cudaStreamSynchronize(st);
-    cudaFree(d_acc);
+    dev_free(d_acc, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (rc != GPUMC_OK) return rc;
     if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("set_spins: ") + cudaGetErrorString(e));
     if ((unsigned int)h[1] != 0)
@@ -723,13 +727,13 @@ int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* 
   CUDA_TRY(cudaSetDevice(sim->eng->device));
   CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
   unsigned long long* d = nullptr;
-  CUDA_TRY(cudaMalloc(&d, 8 * 128));
-  CUDA_TRY(cudaMemset(d, 0, 8 * 128));
+  CUDA_TRY(cudaMallocAsync(&d, 8 * 128, sim->eng->stream));
+  CUDA_TRY(cudaMemsetAsync(d, 0, 8 * 128, sim->eng->stream));
   int rc = launch_msc_measure(sim->eng->stream, sim->lay, sim->eng->d_lats, sim->lat0 + word_lattice, d);
   unsigned long long h[128];
   cudaError_t e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, sim->eng->stream);
+  dev_free(d, sim->eng->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(sim->eng->stream);
-  cudaFree(d);
   if (rc) return rc;
   if (e != cudaSuccess) return fail(GPUMC_ECUDA, cudaGetErrorString(e));
   const double n = (double)sim->lay.n_sites;
