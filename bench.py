@@ -489,7 +489,9 @@ def bench_serving(gpumc, torch, args):
                     "p50_s": float(np.percentile(lat, 50)),
                     "p99_s": float(np.percentile(lat, 99)), "wall_s": wall,
                     "attempts_per_ns": total_att / (wall * 1e9),
-                    "busy_attempts_per_ns": st["attempts"] / (st["busy_s"] * 1e9)})
+                    "busy_attempts_per_ns": st["attempts"] / (st["busy_s"] * 1e9),
+                    "host_s": {"admit": round(st["admit_s"], 4), "sweep": round(st["sweep_s"], 4),
+                               "retire": round(st["retire_s"], 4)}})
     return out
 
 

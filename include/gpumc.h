@@ -144,6 +144,17 @@ int gpumc_launches_per_sweep(gpumc_sim* sim, int32_t* n);
  * reference has no counterpart: its sweep is one CPU loop per chain.) */
 int gpumc_set_temporal_blocking(gpumc_sim* sim, int32_t enable);
 int gpumc_engine_set_temporal_blocking(gpumc_engine* eng, int32_t enable);
+/* Tile refinement (default on): a launch with fewer tiles than half the
+ * device's CTA slots (a lone lattice, a few serving jobs) splits its 3D
+ * Ising, Potts and O(3) tiles, largest first, until it fills them; off =
+ * every lattice keeps the tiles sized for a full launch.  Both give identical
+ * spins, energies and records.  The _engine_ form applies to the batches of
+ * gpumc_engine_sweep, the other to gpumc_sweep of one handle; `n_tiles` of
+ * gpumc_tile_count is the CTA count of one sweep launch of the handle's own
+ * path.  (No counterpart in the reference: its sweep is one CPU loop.) */
+int gpumc_set_tile_refinement(gpumc_sim* sim, int32_t enable);
+int gpumc_engine_set_tile_refinement(gpumc_engine* eng, int32_t enable);
+int gpumc_tile_count(gpumc_sim* sim, int32_t* n_tiles);
 /* Kernel launches issued so far by gpumc_sweep of this handle / by
  * gpumc_engine_sweep of this engine (sweep, measurement and resident
  * launches; host copies excluded). */
@@ -257,6 +268,12 @@ int gpumc_cancel(gpumc_server* srv, uint64_t job_id);
 /* Final spins of a finished job's replica (kept until polled). */
 int gpumc_job_spins(gpumc_server* srv, uint64_t job_id, int32_t replica, void* host, size_t nbytes);
 int gpumc_server_stats(gpumc_server* srv, double* attempts_total, double* busy_s, size_t* bytes_in_use);
+/* Host seconds the server's steps spent admitting jobs, sweeping (launches
+ * and the wait for them) and retiring jobs, summed over all steps. */
+int gpumc_server_timing(gpumc_server* srv, double* admit_s, double* sweep_s, double* retire_s);
+/* Final spins are kept for gpumc_job_spins for jobs of at most this many
+ * sites over all replicas (default 2^20); larger jobs skip the copy. */
+int gpumc_server_set_keep_spins(gpumc_server* srv, size_t max_sites);
 int gpumc_server_destroy(gpumc_server* srv);
 
 /* ---- diagnostics ------------------------------------------------------- */
@@ -266,6 +283,11 @@ int gpumc_philox_probe(const uint32_t* ctr4, const uint32_t* key2, uint32_t* out
 /* Bytes of device memory a spec needs (both ping-pong buffers, tables,
  * records): the admission footprint. */
 int gpumc_footprint(const gpumc_spec* spec, size_t* bytes);
+/* Host-side tile plan of a spec's own sweep launch on a device with `slots`
+ * CTA slots (`slots3` for the 3D bit-sliced kernels): the CTA count and the
+ * kernel kind, with or without tile refinement.  Needs no device. */
+int gpumc_plan_tiles(const gpumc_spec* spec, int32_t slots, int32_t slots3, int32_t refine,
+                     int64_t* n_tiles, int32_t* kind);
 
 /* ---- allocation-free exact energy ---------------------------------------
  * No counterpart in the reference: an engine-specific entry point for callers

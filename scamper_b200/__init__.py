@@ -10,7 +10,7 @@ from . import _lib
 from ._lib import GpumcError, InvalidConfig
 from .measurements import Accumulator, Context, Estimate, binder_cumulant, specific_heat
 from .mc import (ClassicalMC, Engine, MultiSpinIsing, Params, Server, geometric_ladder_betas,
-                 potts_beta_c, run_one)
+                 plan_tiles, potts_beta_c, run_one)
 from .results import Metadata, Results
 from .snapshot import CheckpointCorrupted
 
@@ -19,6 +19,6 @@ _lib.load()
 __all__ = [
     "Accumulator", "CheckpointCorrupted", "ClassicalMC", "Context", "Engine", "Estimate", "GpumcError", "InvalidConfig",
     "Metadata", "MultiSpinIsing", "Params", "Results", "Server", "binder_cumulant", "geometric_ladder_betas",
-    "potts_beta_c",
+    "plan_tiles", "potts_beta_c",
     "run_one", "specific_heat",
 ]

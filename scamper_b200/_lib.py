@@ -109,6 +109,9 @@ SIGNATURES = {
     "gpumc_get_cone_omc": [_vp, ctypes.c_int32, _P(ctypes.c_float)],
     "gpumc_set_cone_omc": [_vp, ctypes.c_int32, ctypes.c_float],
     "gpumc_engine_set_temporal_blocking": [_vp, ctypes.c_int32],
+    "gpumc_set_tile_refinement": [_vp, ctypes.c_int32],
+    "gpumc_engine_set_tile_refinement": [_vp, ctypes.c_int32],
+    "gpumc_tile_count": [_vp, _P(ctypes.c_int32)],
     "gpumc_launch_count": [_vp, _P(ctypes.c_uint64)],
     "gpumc_engine_launch_count": [_vp, _P(ctypes.c_uint64)],
     "gpumc_create": [_vp, _P(Spec), ctypes.c_uint64, _P(_vp)],
@@ -139,10 +142,14 @@ SIGNATURES = {
     "gpumc_cancel": [_vp, ctypes.c_uint64],
     "gpumc_job_spins": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_size_t],
     "gpumc_server_stats": [_vp, _P(ctypes.c_double), _P(ctypes.c_double), _P(ctypes.c_size_t)],
+    "gpumc_server_timing": [_vp, _P(ctypes.c_double), _P(ctypes.c_double), _P(ctypes.c_double)],
+    "gpumc_server_set_keep_spins": [_vp, ctypes.c_size_t],
     "gpumc_server_destroy": [_vp],
     "gpumc_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "gpumc_philox_probe": [_P(ctypes.c_uint32), _P(ctypes.c_uint32), _P(ctypes.c_uint32), ctypes.c_int32],
     "gpumc_footprint": [_P(Spec), _P(ctypes.c_size_t)],
+    "gpumc_plan_tiles": [_P(Spec), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P(ctypes.c_int64),
+                         _P(ctypes.c_int32)],
     "gpumc_energy_int8_noalloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
                                   ctypes.c_int64, _vp, ctypes.c_int32, _vp, _vp],
 }

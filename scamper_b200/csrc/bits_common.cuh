@@ -66,13 +66,13 @@ __device__ __forceinline__ BitsGeom make_bits_geom(const TileItem& t, const LatD
   g.pitch = L->pitch;
   g.nseg = L->pitch >> 6;
   g.s0 = t.x0 >> 6;
-  g.ns = min(L->tile_cx, g.nseg - g.s0);
+  g.ns = min(t.cx, g.nseg - g.s0);
   g.xh = g.ns < g.nseg ? 1 : 0;
   g.NC = g.ns + 2 * g.xh;
   g.y0 = t.y0;
-  g.hv = min(L->tile_y, g.ly - t.y0);
+  g.hv = min(t.ty, g.ly - t.y0);
   // a 3D tile that spans whole planes needs no y halo: its rows wrap
-  g.yw = L->dims == 3 && t.y0 == 0 && L->tile_y >= g.ly && g.xh == 0;
+  g.yw = L->dims == 3 && t.y0 == 0 && t.ty >= g.ly && g.xh == 0;
   g.yo = g.yw ? 0 : 2;
   g.R = g.yw ? g.hv : g.hv + 4;
   g.hlast = (g.lx - 64 * (g.nseg - 1)) >> 1;

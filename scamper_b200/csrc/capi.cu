@@ -502,7 +502,7 @@ void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out) {
   if (tw <= 0 || L.tile_y <= 0 || L.tile_z <= 0) return;  // rejected by layout_ok()
   for (int z0 = 0; z0 < L.lz; z0 += L.tile_z)
     for (int y0 = 0; y0 < L.ly; y0 += L.tile_y)
-      for (int x0 = 0; x0 < L.lx; x0 += tw) out.push_back(TileItem{lat, x0, y0, z0});
+      for (int x0 = 0; x0 < L.lx; x0 += tw) out.push_back(TileItem{lat, x0, y0, z0, L.tile_cx, L.tile_y, L.tile_z, 0});
 }
 
 // Kernel of a layout: model x dims; Potts planned on bit planes (q <= 4)
@@ -517,6 +517,108 @@ int kernel_kind(const Layout& L) {
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
   if (L.model == O3 && L.march) return 10 + hb;
   return L.model * 2 + (L.dims - 2) + hb;
+}
+
+// ---------------------------------------------------------------------------
+// Launch-dependent tile shapes.  plan_layout sizes a lattice's tiles for a
+// launch with plenty of tiles (halo and staging work amortised over large
+// tiles).  A launch with far fewer tiles than the device has CTA slots (a
+// lone lattice, a few serving jobs) would run on a fraction of the SMs with
+// each CTA stepping through a large tile, so refine_layouts splits tiles,
+// the simulation whose tiles hold the most sites first, until the launch has
+// at least half a wave of CTAs or nothing can be split further.  Results do
+// not depend on tile shapes: a colour pass reads only the other colour, and
+// every draw is keyed by site or row segment, not by tile.
+// ---------------------------------------------------------------------------
+int64_t count_tiles(const Layout& L) {
+  const int tw = tile_width_sites(L);
+  if (tw <= 0 || L.tile_y <= 0 || L.tile_z <= 0) return 0;
+  return (int64_t)((L.lx + tw - 1) / tw) * ((L.ly + L.tile_y - 1) / L.tile_y) *
+         ((L.lz + L.tile_z - 1) / L.tile_z);
+}
+
+// One step of refinement (about halving the tile volume); false when the
+// layout's tiles cannot be split further.  2D Ising tiles are already sized
+// against the device's slots (ising_tile_rows) and feed the resident kernel;
+// multi-spin and cluster layouts keep their shapes.
+static bool split_tiles(Layout& L) {
+  if (L.cluster || L.model == MSC || (L.model == ISING && L.dims == 2)) return false;
+  if (L.model == O3) {
+    if (L.march && L.tile_z >= 8) {
+      L.tile_z = (L.tile_z + 1) / 2;
+      return true;
+    }
+    if (L.march) {
+      // the plain kernel with its own full-launch tiles (about 2048 sites of
+      // each colour), split further by the steps below
+      L.march = false;
+      L.smem = 0;
+      L.tile_y = std::max(1, std::min(L.ly, 4096 / L.lx));
+      L.tile_z = L.tile_y < L.ly ? 1 : std::max(1, std::min(L.lz, 4096 / (L.lx * L.ly)));
+      return true;
+    }
+    if (L.tile_z > 1) {
+      L.tile_z = (L.tile_z + 1) / 2;
+      return true;
+    }
+    if (L.tile_y > 1 && (int64_t)L.tile_y * L.lx > 256) {
+      L.tile_y = (L.tile_y + 1) / 2;
+      return true;
+    }
+    return false;
+  }
+  // bit-sliced Ising / Potts and int8 Potts: tiles with two-row y halos
+  const bool bits = L.model == ISING || L.bits;
+  if (bits && L.dims == 3 && L.tile_y >= L.ly) {
+    if (L.ly < 8) return false;
+    L.tile_y = (L.ly + 1) / 2;  // whole-plane tiles -> row bands with halos
+  } else if (L.tile_y > 4) {
+    L.tile_y = (L.tile_y + 1) / 2;
+  } else if (L.dims == 3 && L.tile_z > 2) {
+    L.tile_z = (L.tile_z + 1) / 2;
+  } else {
+    return false;
+  }
+  if (bits) {
+    L.smem = bits_tile_smem(L, TileItem{0, 0, 0, 0, L.tile_cx, L.tile_y, L.tile_z, 0});
+  } else {
+    L.smem = (L.dims == 2 ? 2 : 6) * (size_t)(L.tile_y + 4) * (16 * L.tile_cx + 32);
+  }
+  return true;
+}
+
+void refine_layouts(std::vector<Layout>& lays, const std::vector<int>& reps, int slots) {
+  const size_t n = lays.size();
+  std::vector<bool> fixed(n, false);
+  int64_t total = 0;
+  for (size_t i = 0; i < n; ++i) total += count_tiles(lays[i]) * reps[i];
+  const int64_t target = std::max(1, slots / 2);
+  while (total < target) {
+    size_t best = n;
+    double most = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      if (fixed[i]) continue;
+      const double per = (double)lays[i].n_sites / (double)std::max<int64_t>(1, count_tiles(lays[i]));
+      if (per > most) {
+        most = per;
+        best = i;
+      }
+    }
+    if (best == n) break;
+    Layout t = lays[best];
+    if (!split_tiles(t) || !layout_ok(t)) {
+      fixed[best] = true;
+      continue;
+    }
+    total += (count_tiles(t) - count_tiles(lays[best])) * reps[best];
+    lays[best] = t;
+  }
+}
+
+// CTA slots a launch of this layout's family fills: the 3D bit-sliced
+// kernels run fewer CTAs per SM.
+int family_slots(const Layout& L, int slots, int slots3) {
+  return (L.dims == 3 && (L.model == ISING || L.bits)) ? slots3 : slots;
 }
 
 size_t footprint_bytes(const gpumc_spec* s) {
@@ -776,6 +878,15 @@ int gpumc_engine_set_temporal_blocking(gpumc_engine* eng, int32_t enable) {
   return GPUMC_OK;
 }
 
+int gpumc_engine_set_tile_refinement(gpumc_engine* eng, int32_t enable) {
+  if (!eng) return fail(GPUMC_EINVAL, "engine: null");
+  if (eng->refine != (enable != 0)) {
+    eng->refine = enable != 0;
+    eng->batch_dirty = true;  // the next engine sweep re-plans the batch
+  }
+  return GPUMC_OK;
+}
+
 int gpumc_engine_launch_count(gpumc_engine* eng, uint64_t* n) {
   if (!eng || !n) return fail(GPUMC_EINVAL, "null argument");
   *n = eng->launches;
@@ -879,14 +990,28 @@ int gpumc_engine::rebuild_batch() {
   std::map<int, std::vector<TileItem>> tiles;
   std::map<int, std::vector<int32_t>> gids;
   std::map<int, const Layout*> layout_of_lat;
+  // tile shapes for this batch: the simulations of one kernel family (kind
+  // of the creation-time plan) share its launch and are refined together
+  std::map<int, std::vector<gpumc_sim*>> family;
+  for (gpumc_sim* s : sims) family[kernel_kind(s->base)].push_back(s);
+  for (auto& kv : family) {
+    std::vector<Layout> lays;
+    std::vector<int> reps;
+    for (gpumc_sim* s : kv.second) {
+      lays.push_back(s->base);
+      reps.push_back(s->n_rep);
+    }
+    if (refine) refine_layouts(lays, reps, family_slots(lays[0], slots, slots3));
+    for (size_t i = 0; i < kv.second.size(); ++i) kv.second[i]->blay = lays[i];
+  }
   for (gpumc_sim* s : sims) {
-    const int kind = kernel_kind(s->lay);
+    const int kind = kernel_kind(s->blay);
     BatchPlan& p = plans[kind];
     p.kind = kind;
-    p.smem = std::max(p.smem, s->lay.smem);
+    p.smem = std::max(p.smem, s->blay.smem);
     for (int r = 0; r < s->n_rep; ++r) {
-      enumerate_tiles(s->lay, s->lat0 + r, tiles[kind]);
-      layout_of_lat[s->lat0 + r] = &s->lay;
+      enumerate_tiles(s->blay, s->lat0 + r, tiles[kind]);
+      layout_of_lat[s->lat0 + r] = &s->blay;
     }
     gids[kind].push_back(s->group);
   }

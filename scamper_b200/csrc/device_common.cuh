@@ -187,4 +187,29 @@ __device__ __forceinline__ void atomic_add_i64(unsigned long long* p, long long 
   atomicAdd(p, (unsigned long long)v);
 }
 
+// CTA-wide sums of N per-thread values (long long or double): a shuffle tree
+// per warp, then thread 0 adds the other warps' totals in warp order and
+// returns with the CTA's totals in v.  Every thread of the CTA must call it.
+// The caller then issues one atomic per accumulator per CTA instead of one
+// per warp: same-address atomics serialise in L2, which launches of many
+// small tiles would otherwise wait on.
+template <typename T, int N>
+__device__ __forceinline__ void cta_sum(T (&v)[N]) {
+  __shared__ T part[kThreads / 32][N];
+  const unsigned full = 0xFFFFFFFFu;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(full, v[i], o);
+  __syncthreads();  // a previous call's reads of `part` are over
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int i = 0; i < N; ++i) part[threadIdx.x >> 5][i] = v[i];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < kThreads / 32; ++w)
+#pragma unroll
+      for (int i = 0; i < N; ++i) v[i] += part[w][i];
+}
+
 }  // namespace gpumc

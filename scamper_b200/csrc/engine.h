@@ -66,7 +66,7 @@ struct Record {
 struct LatDesc {
   // geometry / model (immutable after creation)
   int32_t model, dims, lx, ly, lz, pitch, q, z;
-  int32_t tile_cx, tile_y, tile_z;  // tile shape: chunks (16 sites) x rows x planes
+  int32_t tile_cx, tile_y, tile_z;  // creation-time tile shape (kernels read TileItem's)
   int32_t group;                    // index into the group array (PT / records)
   int32_t replica;                  // replica index within its group
   int32_t prop;                     // O(3) Metropolis proposal: 0 cap, 1 uniform, 2 OPSS
@@ -119,8 +119,13 @@ struct GroupDesc {
   double* bins;                   // [bin_cap][n_rep][kBinObs] completed bin means
 };
 
+// One CTA's work: the tile's origin and the tile shape of its lattice in the
+// launch (chunks x rows x planes, the units of LatDesc's tile fields).  The
+// shape travels with the tile because it depends on the launch: a batch that
+// leaves CTA slots idle splits its lattices into smaller tiles.
 struct TileItem {
   int32_t lat, x0, y0, z0;
+  int32_t cx, ty, tz, pad;
 };
 
 // Device-side bookkeeping of one launch (last-CTA epilogue; grid barrier of

@@ -62,6 +62,11 @@ int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);
 bool layout_ok(const Layout& L);
 void enumerate_tiles(const Layout& L, int lat, std::vector<TileItem>& out);
 int kernel_kind(const Layout& L);
+int64_t count_tiles(const Layout& L);
+// Split the tiles of the layouts of one launch (n_rep lattices each) until the
+// launch has at least half of `slots` CTAs or no tile can be split further.
+void refine_layouts(std::vector<Layout>& lays, const std::vector<int>& reps, int slots);
+int family_slots(const Layout& L, int slots, int slots3);
 size_t footprint_bytes(const gpumc_spec* s);
 int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_tiles,
                         LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, size_t smem);
@@ -124,6 +129,7 @@ struct gpumc_engine {
   bool batch_dirty = true;
   bool use_graphs = true;
   bool blocking = true;       // temporal blocking of qualifying Ising plans
+  bool refine = true;         // split tiles of batches that leave CTA slots idle
   uint64_t launches = 0;      // kernel launches issued by gpumc_engine_sweep
   int slots = gpumc::kDefaultSlots;  // resident sweep CTAs of the device (tile planning)
   int slots3 = gpumc::kDefaultSlots3;  // the same for the 3D Ising kernel
@@ -146,7 +152,9 @@ struct gpumc_sim {
   bool private_engine = false;
   gpumc_spec spec{};
   std::vector<double> betas;
-  gpumc::Layout lay;
+  gpumc::Layout base;  // creation-time plan (tiles sized for a full launch)
+  gpumc::Layout lay;   // plan of the simulation's own launches (base refined for it alone)
+  gpumc::Layout blay;  // plan inside the engine's current batch (base refined for the batch)
   int n_rep = 1, n_temps = 1, n_cls = 0;
   int lat0 = -1, group = -1;
   uint64_t base_seed = 0;
@@ -193,6 +201,7 @@ struct gpumc_sim {
   int drain_records();
   int push_phase_flags();
   int upload_tables();
+  int upload_own_tiles(std::vector<gpumc::TileItem>& tiles);
   void drop_graphs();
   int recompute(std::vector<double>& out, bool store);
   int launch_energy(const void* buf, unsigned long long* d_e, unsigned int* d_bad);

@@ -62,8 +62,11 @@ struct gpumc_server {
   std::map<uint64_t, JobState*> finished;
   std::vector<gpumc_job_result> results;
   double attempts_total = 0.0, busy_s = 0.0;
+  double admit_s = 0.0, sweep_s = 0.0, retire_s = 0.0;  // host time of the step's phases
   size_t max_waiting = 1u << 20;
-  size_t keep_spins_sites = 1u << 22;
+  // final spins of jobs up to this many sites (all replicas) are kept for
+  // gpumc_job_spins; larger jobs skip the device-to-host copy at retirement
+  size_t keep_spins_sites = 1u << 20;
 };
 
 static int retire(gpumc_server* srv, JobState* js) {
@@ -200,6 +203,8 @@ int gpumc_server_step(gpumc_server* srv, int32_t* active) {
     srv->in_use += js->bytes;
     srv->active.push_back(js);
   }
+  const double t1 = now_s();
+  srv->admit_s += t1 - t0;
   // 2. one chunk of batched sweeps over every active job
   if (!srv->active.empty()) {
     int rc = gpumc_engine_sweep(srv->eng, srv->chunk);
@@ -207,6 +212,8 @@ int gpumc_server_step(gpumc_server* srv, int32_t* active) {
     if (cudaStreamSynchronize(srv->eng->stream) != cudaSuccess)
       return fail(GPUMC_ECUDA, "server step: stream synchronize failed");
   }
+  const double t2 = now_s();
+  srv->sweep_s += t2 - t1;
   // 3. retire finished jobs
   std::vector<JobState*> still;
   for (JobState* js : srv->active) {
@@ -218,7 +225,9 @@ int gpumc_server_step(gpumc_server* srv, int32_t* active) {
     }
   }
   srv->active.swap(still);
-  srv->busy_s += now_s() - t0;
+  const double t3 = now_s();
+  srv->retire_s += t3 - t2;
+  srv->busy_s += t3 - t0;
   if (active) *active = (int32_t)(srv->active.size() + srv->waiting.size());
   return GPUMC_OK;
 }
@@ -289,6 +298,20 @@ int gpumc_server_stats(gpumc_server* srv, double* attempts_total, double* busy_s
   if (attempts_total) *attempts_total = srv->attempts_total;
   if (busy_s) *busy_s = srv->busy_s;
   if (bytes_in_use) *bytes_in_use = srv->in_use;
+  return GPUMC_OK;
+}
+
+int gpumc_server_timing(gpumc_server* srv, double* admit_s, double* sweep_s, double* retire_s) {
+  if (!srv) return fail(GPUMC_EINVAL, "server: null");
+  if (admit_s) *admit_s = srv->admit_s;
+  if (sweep_s) *sweep_s = srv->sweep_s;
+  if (retire_s) *retire_s = srv->retire_s;
+  return GPUMC_OK;
+}
+
+int gpumc_server_set_keep_spins(gpumc_server* srv, size_t max_sites) {
+  if (!srv) return fail(GPUMC_EINVAL, "server: null");
+  srv->keep_spins_sites = max_sites;
   return GPUMC_OK;
 }
 

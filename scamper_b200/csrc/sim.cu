@@ -67,6 +67,25 @@ gpumc_sim::~gpumc_sim() {
   res.release(st);
 }
 
+// The tile list of the simulation's own launches, from `lay`; a launch
+// control block that exists already gets the new tile count.
+int gpumc_sim::upload_own_tiles(std::vector<TileItem>& tiles) {
+  tiles.clear();
+  for (int r = 0; r < n_rep; ++r) enumerate_tiles(lay, lat0 + r, tiles);
+  TileItem* d = nullptr;
+  CUDA_TRY(cudaMallocAsync(&d, sizeof(TileItem) * tiles.size(), eng->stream));
+  CUDA_TRY(cudaMemcpyAsync(d, tiles.data(), sizeof(TileItem) * tiles.size(), cudaMemcpyHostToDevice, eng->stream));
+  dev_free(d_tiles, eng->stream);
+  d_tiles = d;
+  n_tiles = (int)tiles.size();
+  if (d_ctl) {
+    const int32_t n = n_tiles;
+    CUDA_TRY(cudaMemcpyAsync(&d_ctl->n_tiles, &n, sizeof(n), cudaMemcpyHostToDevice, eng->stream));
+    CUDA_TRY(cudaStreamSynchronize(eng->stream));  // `n` lives on this stack frame
+  }
+  return GPUMC_OK;
+}
+
 void gpumc_sim::drop_graphs() {
   for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
   graphs.clear();
@@ -287,6 +306,19 @@ int gpumc_footprint(const gpumc_spec* spec, size_t* bytes) {
   return GPUMC_OK;
 }
 
+int gpumc_plan_tiles(const gpumc_spec* spec, int32_t slots, int32_t slots3, int32_t refine,
+                     int64_t* n_tiles, int32_t* kind) {
+  RC_TRY(validate_spec(spec));
+  if (!n_tiles || !kind) return fail(GPUMC_EINVAL, "null argument");
+  if (slots < 1 || slots3 < 1) return fail(GPUMC_EINVAL, "slots: must be >= 1");
+  std::vector<Layout> one{plan_layout(spec, slots, slots3)};
+  const int n_rep = std::max<int>(1, (int)spec->n_replicas);
+  if (refine) refine_layouts(one, {n_rep}, family_slots(one[0], slots, slots3));
+  *n_tiles = count_tiles(one[0]) * n_rep;
+  *kind = kernel_kind(one[0]);
+  return GPUMC_OK;
+}
+
 int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, gpumc_sim** out) {
   RC_TRY(validate_spec(spec));
   if (!out) return fail(GPUMC_EINVAL, "out: null pointer");
@@ -302,7 +334,15 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   s->spec = *spec;
   s->betas.assign(spec->betas, spec->betas + spec->n_temps);
   s->spec.betas = nullptr;
-  s->lay = plan_layout(spec, eng->slots, eng->slots3);
+  s->base = plan_layout(spec, eng->slots, eng->slots3);
+  {
+    // the simulation's own launches: tiles split until they fill the device
+    std::vector<Layout> one{s->base};
+    refine_layouts(one, {std::max<int>(1, (int)spec->n_replicas)},
+                   family_slots(s->base, eng->slots, eng->slots3));
+    s->lay = one[0];
+  }
+  s->blay = s->lay;
   s->n_rep = spec->n_replicas;
   s->n_temps = spec->n_temps;
   s->n_cls = n_classes(s->lay.model == MSC ? ISING : s->lay.model, s->lay.dims);
@@ -360,10 +400,8 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   CUDA_CLEAN(cudaMemcpyAsync(s->d_label, labels.data(), 4 * (size_t)s->n_rep, cudaMemcpyHostToDevice, eng->stream));
   // tiles and launch control of the plain path
   std::vector<TileItem> tiles;
-  for (int r = 0; r < s->n_rep; ++r) enumerate_tiles(s->lay, s->lat0 + r, tiles);
-  s->n_tiles = (int)tiles.size();
-  CUDA_CLEAN(cudaMallocAsync(&s->d_tiles, sizeof(TileItem) * tiles.size(), eng->stream));
-  CUDA_CLEAN(cudaMemcpyAsync(s->d_tiles, tiles.data(), sizeof(TileItem) * tiles.size(), cudaMemcpyHostToDevice, eng->stream));
+  rc = s->upload_own_tiles(tiles);
+  if (rc) return cleanup(rc);
   CUDA_CLEAN(cudaMallocAsync(&s->d_gid, sizeof(int32_t), eng->stream));
   CUDA_CLEAN(cudaMemcpyAsync(s->d_gid, &s->group, sizeof(int32_t), cudaMemcpyHostToDevice, eng->stream));
   CUDA_CLEAN(cudaMallocAsync(&s->d_ctl, sizeof(LaunchCtl), eng->stream));
@@ -495,6 +533,33 @@ int gpumc_set_phase(gpumc_sim* sim, int32_t phase) {
   sim->drop_graphs();
   sim->eng->drop_graphs();
   return sim->push_phase_flags();
+}
+
+int gpumc_set_tile_refinement(gpumc_sim* sim, int32_t enable) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  std::vector<Layout> one{sim->base};
+  if (enable) refine_layouts(one, {sim->n_rep}, family_slots(sim->base, sim->eng->slots, sim->eng->slots3));
+  const Layout& want = one[0];
+  if (want.tile_cx == sim->lay.tile_cx && want.tile_y == sim->lay.tile_y && want.tile_z == sim->lay.tile_z &&
+      want.march == sim->lay.march)
+    return GPUMC_OK;
+  const Layout old = sim->lay;
+  sim->lay = want;
+  std::vector<TileItem> tiles;
+  const int rc = sim->upload_own_tiles(tiles);
+  if (rc) {
+    sim->lay = old;
+    return rc;
+  }
+  sim->drop_graphs();
+  return GPUMC_OK;
+}
+
+int gpumc_tile_count(gpumc_sim* sim, int32_t* n_tiles) {
+  if (!sim || !n_tiles) return fail(GPUMC_EINVAL, "null argument");
+  *n_tiles = sim->n_tiles;
+  return GPUMC_OK;
 }
 
 int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {

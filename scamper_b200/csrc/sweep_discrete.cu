@@ -577,31 +577,21 @@ __device__ __forceinline__ void flush_accumulators(LatDesc* L, int nacc, int acc
   constexpr int zc = 2 * DIM;
   // Ising: dE = sum over accepted owned flips of 2(z - 2k) = 2 z n - 4 sum k;
   // Potts: dE = -sum d.
-  long long dE = MODEL == ISING ? 2LL * zc * nacc - 4LL * acc2 : -(long long)acc2;
-  const unsigned full = 0xFFFFFFFFu;
+  long long v[3 + kMaxPottsCounts];
+  v[0] = MODEL == ISING ? 2LL * zc * nacc - 4LL * acc2 : -(long long)acc2;
+  v[1] = nacc;
+  v[2] = mag;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dE += __shfl_xor_sync(full, dE, o);
-    nacc += __shfl_xor_sync(full, nacc, o);
-    mag += __shfl_xor_sync(full, mag, o);
-  }
-  int c[kMaxPottsCounts];
-#pragma unroll
-  for (int s = 0; s < kMaxPottsCounts; ++s) {
-    c[s] = cnt[s];
-    if (MODEL == POTTS) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) c[s] += __shfl_xor_sync(full, c[s], o);
-    }
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (dE) atomic_add_i64(&L->acc.dE, dE);
-    if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
+  for (int s = 0; s < kMaxPottsCounts; ++s) v[3 + s] = MODEL == POTTS ? cnt[s] : 0;
+  cta_sum(v);
+  if (threadIdx.x == 0) {
+    if (v[0]) atomic_add_i64(&L->acc.dE, v[0]);
+    if (v[1]) atomic_add_i64(&L->acc.accepted, v[1]);
     if (MODEL == ISING) {
-      if (mag) atomic_add_i64(&L->acc.mag, mag);
+      if (v[2]) atomic_add_i64(&L->acc.mag, v[2]);
     } else {
       for (int s = 0; s < kMaxPottsCounts && s < q; ++s)
-        if (c[s]) atomic_add_i64(&L->acc.counts[s], c[s]);
+        if (v[3 + s]) atomic_add_i64(&L->acc.counts[s], v[3 + s]);
     }
   }
 }
@@ -623,11 +613,11 @@ __device__ __forceinline__ TileGeom make_geom(const TileItem& t, const LatDesc* 
   g.ly = L->ly;
   g.pitch = L->pitch;
   g.pc = L->pitch >> 4;
-  g.W = L->tile_cx * 16;
+  g.W = t.cx * 16;
   g.S = g.W + 32;
   g.Wv = min(g.W, g.lx - t.x0);
   g.ncv = (g.Wv + 15) >> 4;
-  g.hv = min(L->tile_y, g.ly - t.y0);
+  g.hv = min(t.ty, g.ly - t.y0);
   g.R = g.hv + 4;
   g.rstep = kThreads / g.ncv;
   g.col = threadIdx.x % g.ncv;
@@ -700,7 +690,7 @@ __global__ void __launch_bounds__(kThreads)
   const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
   int8_t* nxt = (int8_t*)L->buf[(sweep & 1) ^ 1];
   const TileGeom g = make_geom(t, L);
-  const int dv = min(L->tile_z, lz - t.z0);
+  const int dv = min(t.tz, lz - t.z0);
   const int pb = g.R * g.S;  // bytes per plane
   uint8_t* Aring = smem;          // 3 planes
   uint8_t* Bring = smem + 3 * pb; // 3 planes

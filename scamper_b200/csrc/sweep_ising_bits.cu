@@ -354,20 +354,12 @@ __device__ __forceinline__ void load_bits_table(BitsTab& tab, const LatDesc* L, 
 }
 
 __device__ __forceinline__ void flush_bits(Accum* A, const PassAcc& a, int zc) {
-  long long dE = 2LL * zc * a.nacc - 4LL * a.ksum;
-  long long mag = (long long)a.owned_sites - 2LL * a.down;
-  long long nacc = a.nacc;
-  const unsigned full = 0xFFFFFFFFu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dE += __shfl_xor_sync(full, dE, o);
-    mag += __shfl_xor_sync(full, mag, o);
-    nacc += __shfl_xor_sync(full, nacc, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (dE) atomic_add_i64(&A->dE, dE);
-    if (mag) atomic_add_i64(&A->mag, mag);
-    if (nacc) atomic_add_i64(&A->accepted, nacc);
+  long long v[3] = {2LL * zc * a.nacc - 4LL * a.ksum, (long long)a.owned_sites - 2LL * a.down, a.nacc};
+  cta_sum(v);
+  if (threadIdx.x == 0) {
+    if (v[0]) atomic_add_i64(&A->dE, v[0]);
+    if (v[1]) atomic_add_i64(&A->mag, v[1]);
+    if (v[2]) atomic_add_i64(&A->accepted, v[2]);
   }
 }
 
@@ -399,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
     bits_pass<2, ALG>(bsm, bsm, bsm, g, 0, 1, 2, g.hv, g.iters_white, true, 1, nxt, tab, P, acc);
   } else {
     const int lz = L->lz;
-    const int dv = min(L->tile_z, lz - t.z0);
+    const int dv = min(t.tz, lz - t.z0);
     const int pw = g.R * g.NC;
     for (int s = 0; s < dv + 4; ++s) {
       const int zl = t.z0 - 2 + s;

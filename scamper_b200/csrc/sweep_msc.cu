@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(kThreads)
       tab.tail[i] = G->tail[label * G->n_cls + i];
     }
   }
-  const int Wv = min(L->tile_cx * 2, lx - t.x0);
-  const int hv = min(L->tile_y, ly - t.y0);
+  const int Wv = min(t.cx * 2, lx - t.x0);
+  const int hv = min(t.ty, ly - t.y0);
   const int S = Wv + 4, R = hv + 4;
   const int plane = R * S;
   long long dE = 0;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kThreads)
     pass(wsm, wsm, wsm, 0, 0, true);
     pass(wsm, wsm, wsm, 1, 0, true);
   } else {
-    const int dv = min(L->tile_z, lz - t.z0);
+    const int dv = min(t.tz, lz - t.z0);
     for (int s = 0; s < dv + 4; ++s) {
       const int zl = t.z0 - 2 + s;
       unsigned long long* pl = wsm + (s & 3) * plane;
@@ -205,10 +205,9 @@ __global__ void __launch_bounds__(kThreads)
       __syncthreads();
     }
   }
-  const unsigned full = 0xFFFFFFFFu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) dE += __shfl_xor_sync(full, dE, o);
-  if ((threadIdx.x & 31) == 0 && dE) atomic_add_i64(&L->acc.dE, dE);
+  long long v[1] = {dE};
+  cta_sum(v);
+  if (threadIdx.x == 0 && v[0]) atomic_add_i64(&L->acc.dE, v[0]);
   launch_epilogue(lats, groups, ctl);
 }
 

@@ -279,8 +279,8 @@ __global__ void __launch_bounds__(kThreads, 4)
   const double Jd = G->J;
   const float omc = L->omc;
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
-  const int hv = min(L->tile_y, ly - t.y0);
-  const int dv = DIM == 3 ? min(L->tile_z, lz - t.z0) : 1;
+  const int hv = min(t.ty, ly - t.y0);
+  const int dv = DIM == 3 ? min(t.tz, lz - t.z0) : 1;
   const int half = lx >> 1;
   const int rows = hv * dv;
   // thread mapping: fixed column (or column stride) per thread, rows strided
@@ -361,21 +361,16 @@ __global__ void __launch_bounds__(kThreads, 4)
     update(qa);
     if (two) update(qb);
   }
-  const unsigned full = 0xFFFFFFFFu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dE += __shfl_xor_sync(full, dE, o);
-    nacc += __shfl_xor_sync(full, nacc, o);
-    mx += __shfl_xor_sync(full, mx, o);
-    my += __shfl_xor_sync(full, my, o);
-    mz += __shfl_xor_sync(full, mz, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&L->acc.dEf, dE);
-    atomicAdd(&L->acc.mx, mx);
-    atomicAdd(&L->acc.my, my);
-    atomicAdd(&L->acc.mz, mz);
-    if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
+  double v[4] = {dE, mx, my, mz};
+  long long n[1] = {nacc};
+  cta_sum(v);
+  cta_sum(n);
+  if (threadIdx.x == 0) {
+    atomicAdd(&L->acc.dEf, v[0]);
+    atomicAdd(&L->acc.mx, v[1]);
+    atomicAdd(&L->acc.my, v[2]);
+    atomicAdd(&L->acc.mz, v[3]);
+    if (n[0]) atomic_add_i64(&L->acc.accepted, n[0]);
   }
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
@@ -420,8 +415,8 @@ __global__ void __launch_bounds__(kThreads, 4)
   const double Jd = G->J;
   const float omc = L->omc;
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
-  const int hv = min(L->tile_y, ly - t.y0);
-  const int dv = min(L->tile_z, lz - t.z0);
+  const int hv = min(t.ty, ly - t.y0);
+  const int dv = min(t.tz, lz - t.z0);
   const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
   const size_t slot = (size_t)3 * RW * pitch;  // floats per ring slot
   const int nvec = pitch >> 2;              // 16-byte chunks per row
@@ -541,21 +536,16 @@ __global__ void __launch_bounds__(kThreads, 4)
     __syncthreads();  // the next copy overwrites the z-1 slot read above
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  const unsigned full = 0xFFFFFFFFu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dE += __shfl_xor_sync(full, dE, o);
-    nacc += __shfl_xor_sync(full, nacc, o);
-    mx += __shfl_xor_sync(full, mx, o);
-    my += __shfl_xor_sync(full, my, o);
-    mz += __shfl_xor_sync(full, mz, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&L->acc.dEf, dE);
-    atomicAdd(&L->acc.mx, mx);
-    atomicAdd(&L->acc.my, my);
-    atomicAdd(&L->acc.mz, mz);
-    if (nacc) atomic_add_i64(&L->acc.accepted, nacc);
+  double v[4] = {dE, mx, my, mz};
+  long long n[1] = {nacc};
+  cta_sum(v);
+  cta_sum(n);
+  if (threadIdx.x == 0) {
+    atomicAdd(&L->acc.dEf, v[0]);
+    atomicAdd(&L->acc.mx, v[1]);
+    atomicAdd(&L->acc.my, v[2]);
+    atomicAdd(&L->acc.mz, v[3]);
+    if (n[0]) atomic_add_i64(&L->acc.accepted, n[0]);
   }
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }

@@ -360,23 +360,16 @@ __device__ __forceinline__ void potts_pass(uint4* pl, const uint4* pm, const uin
 }
 
 __device__ __forceinline__ void flush_potts(Accum* A, const PottsAcc& a, int zc) {
-  long long dE = -((long long)a.clsum - (long long)zc * a.nacc);  // -(sum of d), d = cls - z
-  long long nacc = a.nacc;
-  long long c[4] = {a.counts[0], a.counts[1], a.counts[2], a.counts[3]};
-  const unsigned full = 0xFFFFFFFFu;
+  // dE = -(sum of d), d = cls - z
+  long long v[6] = {-((long long)a.clsum - (long long)zc * a.nacc), a.nacc, a.counts[0], a.counts[1],
+                    a.counts[2], a.counts[3]};
+  cta_sum(v);
+  if (threadIdx.x == 0) {
+    if (v[0]) atomic_add_i64(&A->dE, v[0]);
+    if (v[1]) atomic_add_i64(&A->accepted, v[1]);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dE += __shfl_xor_sync(full, dE, o);
-    nacc += __shfl_xor_sync(full, nacc, o);
-#pragma unroll
-    for (int v = 0; v < 4; ++v) c[v] += __shfl_xor_sync(full, c[v], o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (dE) atomic_add_i64(&A->dE, dE);
-    if (nacc) atomic_add_i64(&A->accepted, nacc);
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      if (c[v]) atomic_add_i64(&A->counts[v], c[v]);
+    for (int k = 0; k < 4; ++k)
+      if (v[2 + k]) atomic_add_i64(&A->counts[k], v[2 + k]);
   }
 }
 
@@ -409,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 3 : 2)
     potts_pass<2>(psm, psm, psm, g, 0, 1, 2, g.hv, g.iters_white, true, 1, nxt, q, tab, P, acc);
   } else {
     const int lz = L->lz;
-    const int dv = min(L->tile_z, lz - t.z0);
+    const int dv = min(t.tz, lz - t.z0);
     const int pw = g.R * g.NC;
     for (int s = 0; s < dv + 4; ++s) {
       const int zl = t.z0 - 2 + s;

@@ -151,6 +151,18 @@ def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capaci
     return spec, arr
 
 
+def plan_tiles(params, model=None, n_replicas=1, algorithm=None, refine=True, slots=148 * 4, slots3=148 * 3):
+    """(CTAs, kernel kind) of one sweep launch of a handle's own path on a
+    device with `slots` CTA slots (`slots3` for the 3D bit-sliced kernels),
+    with or without tile refinement; host-side planning, no device needed."""
+    spec, _keep = spec_from_params(params, model=model, n_replicas=n_replicas, algorithm=algorithm)
+    n = ctypes.c_int64()
+    kind = ctypes.c_int32()
+    _lib.call("gpumc_plan_tiles", ctypes.byref(spec), int(slots), int(slots3), 1 if refine else 0,
+              ctypes.byref(n), ctypes.byref(kind))
+    return n.value, kind.value
+
+
 class Engine:
     """A device context whose simulations can be swept together in one
     batched launch per sweep (gpumc_engine_sweep)."""
@@ -172,6 +184,11 @@ class Engine:
 
     def set_temporal_blocking(self, enable):
         _lib.call("gpumc_engine_set_temporal_blocking", self.h, 1 if enable else 0)
+
+    def set_tile_refinement(self, enable):
+        """Split the tiles of batches that leave CTA slots idle (default) or
+        keep every lattice's full-launch tiles; results identical."""
+        _lib.call("gpumc_engine_set_tile_refinement", self.h, 1 if enable else 0)
 
     def launch_count(self):
         v = ctypes.c_uint64()
@@ -419,6 +436,17 @@ class ClassicalMC:
         (default) or as one streaming launch per sweep; results identical."""
         _lib.call("gpumc_set_temporal_blocking", self.h, 1 if enable else 0)
 
+    def set_tile_refinement(self, enable):
+        """Split this handle's tiles until one sweep launch fills the device
+        (default) or keep the tiles sized for a full batch; results identical."""
+        _lib.call("gpumc_set_tile_refinement", self.h, 1 if enable else 0)
+
+    def tile_count(self):
+        """CTAs of one sweep launch of this handle's own path."""
+        v = ctypes.c_int32()
+        _lib.call("gpumc_tile_count", self.h, ctypes.byref(v))
+        return v.value
+
     def launch_count(self):
         """Kernel launches issued so far by this handle's sweeps."""
         v = ctypes.c_uint64()
@@ -622,7 +650,14 @@ class Server:
         busy = ctypes.c_double()
         used = ctypes.c_size_t()
         _lib.call("gpumc_server_stats", self.h, ctypes.byref(att), ctypes.byref(busy), ctypes.byref(used))
-        return dict(attempts=att.value, busy_s=busy.value, bytes_in_use=used.value)
+        adm, swp, ret = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _lib.call("gpumc_server_timing", self.h, ctypes.byref(adm), ctypes.byref(swp), ctypes.byref(ret))
+        return dict(attempts=att.value, busy_s=busy.value, bytes_in_use=used.value, admit_s=adm.value,
+                    sweep_s=swp.value, retire_s=ret.value)
+
+    def set_keep_spins(self, max_sites):
+        """Keep final spins (gpumc_job_spins) of jobs up to `max_sites` sites."""
+        _lib.call("gpumc_server_set_keep_spins", self.h, int(max_sites))
 
     def close(self):
         if self.h:
