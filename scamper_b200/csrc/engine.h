@@ -49,8 +49,11 @@ struct Accum {
   unsigned long long mag;       // int64 sum of spins (Ising)
   unsigned long long accepted;  // accepted moves
   unsigned long long counts[kMaxPottsCounts];
-  double dEf;                   // O(3): accumulated fp32 dE
+  double dEf;                   // O(3) cluster updates: accumulated energy change
   double mx, my, mz;            // O(3): magnetisation components
+  double ebond;                 // O(3) sweeps: sum over colour-1 sites of s . h (fp64)
+  int32_t fresh;                // set when ebond holds the full bond sum of a sweep
+  int32_t pad;
 };
 
 // One measured sweep of one lattice, as recorded on the device.

@@ -101,7 +101,14 @@ static __device__ void finish_replica(LatDesc* lats, GroupDesc* G, int r, int32_
   R.m[0] = R.m[1] = R.m[2] = 0.0;
   if (L->model == O3) {
     const double dEf = take_f64(&A->dEf);
-    L->e_f += dEf;
+    if (A->fresh) {
+      // sweeps: every bond has exactly one colour-1 end, so the energy after
+      // the sweep is -J times the colour-1 pass's sum of s . h
+      A->fresh = 0;
+      L->e_f = -G->J * take_f64(&A->ebond);
+    } else {
+      L->e_f += dEf;  // cluster updates: exact change of the flipped clusters
+    }
     R.energy = L->e_f;
     R.m[0] = take_f64(&A->mx);
     R.m[1] = take_f64(&A->my);

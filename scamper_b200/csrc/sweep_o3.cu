@@ -9,6 +9,13 @@
 // and neighbour reads are served by L1/L2.  The colour-1 launch ends with the
 // sweep epilogue.
 //
+// Energy: on the bipartite periodic lattice every bond has exactly one
+// colour-1 end, so the colour-1 pass sums s . h over its sites with their
+// final spins (fp64 neighbour sums of the fp32 components, exact products)
+// and the epilogue sets E = -J times that sum: the energy after each sweep is
+// computed afresh rather than carried by a cache of per-move changes, so it
+// cannot drift, and the colour-0 pass does no fp64 work.
+//
 // Proposal: a uniform point on the spherical cap of half-angle alpha around
 // the current spin (w = 1 - cos(alpha) stored per lattice, adapted toward 50 %
 // acceptance during thermalisation only, mirroring the adaptation contract of
@@ -173,8 +180,8 @@ __device__ __forceinline__ void o3_heat_bath(float hx, float hy, float hz, uint4
 
 // Philox4x32-10 of counter (site, colour | TAG_O3 << 1, sweep) with the
 // sweep-uniform part of round 1 precomputed; the round keys are bumped on the
-// fly (two adds per round instead of twenty live registers: this kernel is
-// bound by load latency, so registers, i.e. resident warps, matter more).
+// fly (two adds per round instead of twenty live registers: resident warps
+// matter more here), and each round multiply is one 32x32->64 wide product.
 struct O3Philox {
   uint32_t a, b, c, k0, k1;
 };
@@ -189,29 +196,32 @@ __device__ __forceinline__ O3Philox make_o3_philox(uint64_t key, uint64_t sweep,
   return P;
 }
 __device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
-  uint4 c = make_uint4(P.a, P.b, __umulhi(0xD2511F53u, index) ^ P.c, 0xD2511F53u * index);
+  const uint64_t p00 = (uint64_t)0xD2511F53u * index;
+  uint4 c = make_uint4(P.a, P.b, (uint32_t)(p00 >> 32) ^ P.c, (uint32_t)p00);
   uint32_t k0 = P.k0, k1 = P.k1;
 #pragma unroll
   for (int r = 1; r < 10; ++r) {
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
-    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1,
+                   (uint32_t)p0);
   }
   return c;
 }
 
-// One site of a colour pass: its own spin and the fp32 (decision) and exact
-// fp64 (energy cache) sums of its neighbours, loaded before any update of
-// the thread's sites so that the loads of two sites overlap.
+// One site of a colour pass: its own spin and the fp32 sum of its
+// neighbours (the decision), plus, in the colour-1 pass, their exact fp64 sum
+// (the sweep's bond sum), loaded before any update of the thread's sites so
+// that the loads of two sites overlap.
 struct O3Site {
   uint32_t me, site;
   float ax, ay, az, hx, hy, hz;
   double hxd, hyd, hzd;
 };
 
-template <int DIM>
+template <int DIM, bool EXACT>
 __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const float* S1, const float* S2,
                                              int x, int y, int z, int lx, int ly, int lz, int pitch) {
   const uint32_t rowoff = ((uint32_t)z * ly + y) * (uint32_t)pitch;
@@ -227,16 +237,23 @@ __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const fl
   const uint32_t nb[6] = {rowoff + xm, rowoff + xp, ((uint32_t)z * ly + ym) * (uint32_t)pitch + x,
                           ((uint32_t)z * ly + yp) * (uint32_t)pitch + x, zmo, zpo};
   float hx = __ldg(S + nb[0]), hy = __ldg(S1 + nb[0]), hz = __ldg(S2 + nb[0]);
-  double hxd = (double)hx, hyd = (double)hy, hzd = (double)hz;
+  double hxd = 0.0, hyd = 0.0, hzd = 0.0;
+  if (EXACT) {
+    hxd = (double)hx;
+    hyd = (double)hy;
+    hzd = (double)hz;
+  }
 #pragma unroll
   for (int i = 1; i < 2 * DIM; ++i) {
     const float vx = __ldg(S + nb[i]), vy = __ldg(S1 + nb[i]), vz = __ldg(S2 + nb[i]);
     hx = fadd(hx, vx);
     hy = fadd(hy, vy);
     hz = fadd(hz, vz);
-    hxd += (double)vx;
-    hyd += (double)vy;
-    hzd += (double)vz;
+    if (EXACT) {
+      hxd += (double)vx;
+      hyd += (double)vy;
+      hzd += (double)vz;
+    }
   }
   q.me = rowoff + x;
   q.ax = S[q.me];
@@ -276,7 +293,6 @@ __global__ void __launch_bounds__(kThreads, 4)
   const int label = G->label[L->replica];
   const float beta = G->betas_f[label];
   const float mJ = -G->Jf;
-  const double Jd = G->J;
   const float omc = L->omc;
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(t.ty, ly - t.y0);
@@ -296,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     r0 = threadIdx.x / half;
     rstep = kThreads / half;
   }
-  double dE = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  double eb = 0.0, mx = 0.0, my = 0.0, mz = 0.0;  // eb: colour 1's sum of s . h
   int nacc = 0;
   // this thread's sites, row-major: rows r0, r0 + rstep, ... of the tile's
   // rows (y fastest, then z), columns col0, col0 + cstep, ...; taken two at a
@@ -332,10 +348,6 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
     float fx = q.ax, fy = q.ay, fz = q.az;
     if (ok) {
-      // energy cache: exact fp64 change of the fp32 configuration (the
-      // decision used the fp32 dE)
-      dE += -Jd * (((double)nx - (double)q.ax) * q.hxd + ((double)ny - (double)q.ay) * q.hyd +
-                   ((double)nz - (double)q.az) * q.hzd);
       ++nacc;
       fx = nx;
       fy = ny;
@@ -347,26 +359,33 @@ __global__ void __launch_bounds__(kThreads, 4)
     mx += (double)fx;
     my += (double)fy;
     mz += (double)fz;
+    // every bond has one colour-1 end: the sweep's energy is -J times the
+    // colour-1 pass's sum of s . h over the final spins (exact products of
+    // fp32 components and fp64 neighbour sums)
+    if (COLOUR == 1) eb += ((double)fx * q.hxd + (double)fy * q.hyd) + (double)fz * q.hzd;
   };
   for (int k = 0; k < n_items; k += 2) {
     int x, y, z;
     O3Site qa, qb;
     next_site(x, y, z);
-    o3_load_site<DIM>(qa, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
+    o3_load_site<DIM, COLOUR == 1>(qa, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
     const bool two = k + 1 < n_items;
     if (two) {
       next_site(x, y, z);
-      o3_load_site<DIM>(qb, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
+      o3_load_site<DIM, COLOUR == 1>(qb, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
     }
     update(qa);
     if (two) update(qb);
   }
-  double v[4] = {dE, mx, my, mz};
+  double v[4] = {eb, mx, my, mz};
   long long n[1] = {nacc};
   cta_sum(v);
   cta_sum(n);
   if (threadIdx.x == 0) {
-    atomicAdd(&L->acc.dEf, v[0]);
+    if (COLOUR == 1) {
+      atomicAdd(&L->acc.ebond, v[0]);
+      L->acc.fresh = 1;
+    }
     atomicAdd(&L->acc.mx, v[1]);
     atomicAdd(&L->acc.my, v[2]);
     atomicAdd(&L->acc.mz, v[3]);
@@ -393,8 +412,11 @@ __device__ __forceinline__ void o3_cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
+// Colour 1 also carries the sweep epilogue's shared memory, so three CTAs
+// fit an SM: its register budget is that of three CTAs (no spills of the fp64
+// neighbour sums).
 template <int COLOUR, int ALG>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                      GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
   extern __shared__ __align__(16) float osm[];
@@ -412,27 +434,45 @@ __global__ void __launch_bounds__(kThreads, 4)
   const int label = G->label[L->replica];
   const float beta = G->betas_f[label];
   const float mJ = -G->Jf;
-  const double Jd = G->J;
   const float omc = L->omc;
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(t.ty, ly - t.y0);
   const int dv = min(t.tz, lz - t.z0);
   const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
-  const size_t slot = (size_t)3 * RW * pitch;  // floats per ring slot
+  const int cstr = RW * pitch;              // floats per component in a slot
+  const int slot = 3 * cstr;                // floats per ring slot
   const int nvec = pitch >> 2;              // 16-byte chunks per row
+  // Plane copies: thread k copies chunks k, k + kThreads, ... of the
+  // 3 x RW x nvec chunks (component c, slot row r, chunk v), walked by a
+  // division-free cursor that advances kThreads chunks per step.
+  const int cv0 = threadIdx.x % nvec, ccr0 = threadIdx.x / nvec;
+  const int cc0 = ccr0 / RW, cr0 = ccr0 - cc0 * RW;
+  const int step_v = kThreads % nvec, step_r = kThreads / nvec;
+  float* S1 = S + cs;
+  float* S2 = S + 2 * cs;
   auto copy_plane = [&](int sl, int z) {
     const int zz = z < 0 ? z + lz : (z >= lz ? z - lz : z);
     float* dst = osm + sl * slot;
-    for (int i = threadIdx.x; i < 3 * RW * nvec; i += kThreads) {
-      const int cr = i / nvec, v = i - cr * nvec;
-      const int c = cr / RW, r = cr - c * RW;
+    const float* src = S + (size_t)zz * ly * pitch;
+    int v = cv0, r = cr0, c = cc0;
+    while (c < 3) {
       int y = t.y0 - 1 + r;
       y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
-      o3_cp_async16(dst + (size_t)cr * pitch + 4 * v, S + c * cs + ((size_t)zz * ly + y) * pitch + 4 * v);
+      o3_cp_async16(dst + c * cstr + r * pitch + 4 * v, src + c * cs + y * pitch + 4 * v);
+      v += step_v;
+      r += step_r;
+      if (v >= nvec) {
+        v -= nvec;
+        ++r;
+      }
+      while (r >= RW) {
+        r -= RW;
+        ++c;
+      }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  double dE = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  double eb = 0.0, mx = 0.0, my = 0.0, mz = 0.0;  // eb: colour 1's sum of s . h
   int nacc = 0;
   const int half = lx >> 1;
   const int n_items = hv * half;  // colour sites of the tile's rows in one plane
@@ -449,20 +489,18 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
     float fx = q.ax, fy = q.ay, fz = q.az;
     if (ok) {
-      // energy cache: exact fp64 change of the fp32 configuration
-      dE += -Jd * (((double)nx - (double)q.ax) * q.hxd + ((double)ny - (double)q.ay) * q.hyd +
-                   ((double)nz - (double)q.az) * q.hzd);
       ++nacc;
       fx = nx;
       fy = ny;
       fz = nz;
       S[q.me] = fx;
-      S[cs + q.me] = fy;
-      S[2 * cs + q.me] = fz;
+      S1[q.me] = fy;
+      S2[q.me] = fz;
     }
     mx += (double)fx;
     my += (double)fy;
     mz += (double)fz;
+    if (COLOUR == 1) eb += ((double)fx * q.hxd + (double)fy * q.hyd) + (double)fz * q.hzd;
   };
   copy_plane(0, t.z0 - 1);
   copy_plane(1, t.z0);
@@ -485,32 +523,36 @@ __global__ void __launch_bounds__(kThreads, 4)
       const int y = t.y0 + rl;
       const int x = 2 * j + ((y + z + COLOUR) & 1);
       const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
-      const int r = rl + 1;  // slot row of y
+      const int oc = (rl + 1) * pitch;  // slot row of y
       // neighbour order x-1, x+1, y-1, y+1, z-1, z+1 (as k_sweep_o3)
       float h[3];
       double hd[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float* row = pc + (size_t)(c * RW + r) * pitch;
-        const float v0 = row[xm], v1 = row[xp];
-        const float v2 = pc[(size_t)(c * RW + r - 1) * pitch + x];
-        const float v3 = pc[(size_t)(c * RW + r + 1) * pitch + x];
-        const float v4 = pm[(size_t)(c * RW + r) * pitch + x];
-        const float v5 = pp[(size_t)(c * RW + r) * pitch + x];
+        const float* P = pc + c * cstr;
+        const float v0 = P[oc + xm], v1 = P[oc + xp];
+        const float v2 = P[oc - pitch + x];
+        const float v3 = P[oc + pitch + x];
+        const float v4 = pm[c * cstr + oc + x];
+        const float v5 = pp[c * cstr + oc + x];
         h[c] = fadd(fadd(fadd(fadd(fadd(v0, v1), v2), v3), v4), v5);
-        hd[c] = (((((double)v0 + (double)v1) + (double)v2) + (double)v3) + (double)v4) + (double)v5;
+        hd[c] = COLOUR == 1
+                    ? (((((double)v0 + (double)v1) + (double)v2) + (double)v3) + (double)v4) + (double)v5
+                    : 0.0;
       }
-      q.ax = pc[(size_t)(0 * RW + r) * pitch + x];
-      q.ay = pc[(size_t)(1 * RW + r) * pitch + x];
-      q.az = pc[(size_t)(2 * RW + r) * pitch + x];
+      q.ax = pc[oc + x];
+      q.ay = pc[cstr + oc + x];
+      q.az = pc[2 * cstr + oc + x];
       q.hx = h[0];
       q.hy = h[1];
       q.hz = h[2];
       q.hxd = hd[0];
       q.hyd = hd[1];
       q.hzd = hd[2];
-      q.me = (uint32_t)(((size_t)z * ly + y) * pitch + x);
-      q.site = (uint32_t)((size_t)(z * ly + y) * lx + x);
+      // 32-bit index arithmetic: the same values as the 64-bit products
+      // truncated to the 32-bit fields
+      q.me = ((uint32_t)z * (uint32_t)ly + (uint32_t)y) * (uint32_t)pitch + (uint32_t)x;
+      q.site = ((uint32_t)z * (uint32_t)ly + (uint32_t)y) * (uint32_t)lx + (uint32_t)x;
     };
     // items i = threadIdx.x, + kThreads, ... as (row, column) cursors
     int ra = threadIdx.x / half, ja = threadIdx.x - ra * half;
@@ -536,12 +578,15 @@ __global__ void __launch_bounds__(kThreads, 4)
     __syncthreads();  // the next copy overwrites the z-1 slot read above
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  double v[4] = {dE, mx, my, mz};
+  double v[4] = {eb, mx, my, mz};
   long long n[1] = {nacc};
   cta_sum(v);
   cta_sum(n);
   if (threadIdx.x == 0) {
-    atomicAdd(&L->acc.dEf, v[0]);
+    if (COLOUR == 1) {
+      atomicAdd(&L->acc.ebond, v[0]);
+      L->acc.fresh = 1;
+    }
     atomicAdd(&L->acc.mx, v[1]);
     atomicAdd(&L->acc.my, v[2]);
     atomicAdd(&L->acc.mz, v[3]);
