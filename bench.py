@@ -337,6 +337,37 @@ def bench_heat_bath(gpumc, torch, args):
     return out
 
 
+def bench_o3_proposals(gpumc, torch, args):
+    """O(3) Metropolis proposals on 3D L=64 x 8 replicas at beta=0.7: the
+    engine's adapted cap, the reference's StandardStrategy (uniform unit
+    vector) and OPSSStrategy (plane rotation, sigma adapted), measured in the
+    measurement phase after 20 adapting sweeps."""
+    from scamper_b200 import _lib
+    out = {}
+    for prop in ("cap", "standard", "opss"):
+        mc = gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 64}, 37, model="o3", n_replicas=8,
+                                           betas=[0.7], o3_proposal=prop, record_capacity=64)
+        mc.sweep(20)
+        mc.on_phase_start(_lib.PHASE_MEASUREMENT)
+        mc.sweep(3)
+        mc.observables()
+        steps = args.aux_steps
+        ms = 0.0
+        done = 0
+        mc.sweep(min(50, steps))  # CUDA graphs of the chunk size, untimed
+        acc = [r["acceptance"] for r in mc.observables()]
+        while done < steps:
+            k = min(50, steps - done)
+            ms += time_sweeps(torch, mc, mc.stream_ptr(), k, mc.sweep, warm=k != min(50, steps))
+            acc += [r["acceptance"] for r in mc.observables()]
+            done += k
+        v = float(mc.n_sites) * 8 * steps / (ms * 1e6)
+        out[prop] = {"value": v, "unit": "spin-flip attempts/ns", "ms_per_sweep": ms / steps,
+                     "acceptance": float(np.mean(acc)), "hbm_gbs_algorithmic": v * BYTES_PER_ATTEMPT["o3"]}
+        mc.close()
+    return out
+
+
 def bench_cluster(gpumc, torch, args):
     """Cluster updates (SWCore / WolffCore) at the critical point: 2D Ising
     L=4096 (Swendsen-Wang and Wolff), 3D Ising L=128 (Swendsen-Wang, beta
@@ -569,7 +600,8 @@ def main():
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only-headline", action="store_true")
-    ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving", "heat_bath", "cluster"], default=None,
+    ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving", "heat_bath", "cluster", "o3_proposals"],
+                    default=None,
                     help="run one extra workload alone (profiling)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 100.0, 1000.0])
     ap.add_argument("--serve-jobs", type=int, default=64)
@@ -589,7 +621,7 @@ def main():
 
     if args.only:
         fn = {"msc": bench_msc, "pt": bench_pt, "mixed": bench_mixed, "serving": bench_serving,
-              "heat_bath": bench_heat_bath, "cluster": bench_cluster}[args.only]
+              "heat_bath": bench_heat_bath, "cluster": bench_cluster, "o3_proposals": bench_o3_proposals}[args.only]
         print(json.dumps({"workload": args.only, "result": fn(gpumc, torch, args)}), flush=True)
         return 0
     h = headline(gpumc, torch, args, dist, rank, world)
@@ -611,7 +643,8 @@ def main():
     workloads = {}
     if rank == 0 and not args.only_headline:
         for name, fn in [("msc", bench_msc), ("pt", bench_pt), ("mixed", bench_mixed),
-                         ("heat_bath", bench_heat_bath), ("cluster", bench_cluster), ("serving", bench_serving)]:
+                         ("heat_bath", bench_heat_bath), ("o3_proposals", bench_o3_proposals),
+                         ("cluster", bench_cluster), ("serving", bench_serving)]:
             try:
                 workloads[name] = fn(gpumc, torch, args)
             except Exception as exc:  # report, never hide
