@@ -496,6 +496,7 @@ def bench_serving(gpumc, torch, args):
             att = float(L ** (2 if lt == "square" else 3)) * sweeps
             jobs.append((t, model, p, sweeps, att))
         srv = gpumc.Server(hbm_budget=int(args.serve_budget_gb * (1 << 30)), chunk=args.serve_chunk)
+        srv.set_keep_spins(0)  # a job's product is its observables (the reference's task results)
         t0 = time.perf_counter()
         pending = list(jobs)
         done = {}
