@@ -154,6 +154,12 @@ int gpumc_engine_set_temporal_blocking(gpumc_engine* eng, int32_t enable);
  * path.  (No counterpart in the reference: its sweep is one CPU loop.) */
 int gpumc_set_tile_refinement(gpumc_sim* sim, int32_t enable);
 int gpumc_engine_set_tile_refinement(gpumc_engine* eng, int32_t enable);
+/* Concurrent kernel kinds (default on): the plans of an engine batch (one
+ * per kernel kind) touch disjoint lattices, so gpumc_engine_sweep runs each
+ * plan's sweeps on a stream of its own, forked from and joined back into the
+ * engine stream; off = all plans in sequence on the engine stream.  Both
+ * give identical results. */
+int gpumc_engine_set_concurrent_kinds(gpumc_engine* eng, int32_t enable);
 int gpumc_tile_count(gpumc_sim* sim, int32_t* n_tiles);
 /* Kernel launches issued so far by gpumc_sweep of this handle / by
  * gpumc_engine_sweep of this engine (sweep, measurement and resident

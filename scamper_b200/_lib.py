@@ -111,6 +111,7 @@ SIGNATURES = {
     "gpumc_engine_set_temporal_blocking": [_vp, ctypes.c_int32],
     "gpumc_set_tile_refinement": [_vp, ctypes.c_int32],
     "gpumc_engine_set_tile_refinement": [_vp, ctypes.c_int32],
+    "gpumc_engine_set_concurrent_kinds": [_vp, ctypes.c_int32],
     "gpumc_tile_count": [_vp, _P(ctypes.c_int32)],
     "gpumc_launch_count": [_vp, _P(ctypes.c_uint64)],
     "gpumc_engine_launch_count": [_vp, _P(ctypes.c_uint64)],

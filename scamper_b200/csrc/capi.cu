@@ -831,6 +831,12 @@ gpumc_engine::~gpumc_engine() {
   drop_graphs();
   for (auto& p : batch_plans) p.release(stream);
   if (stream) cudaStreamSynchronize(stream);
+  for (cudaStream_t s2 : side) {
+    cudaStreamSynchronize(s2);
+    cudaStreamDestroy(s2);
+  }
+  for (cudaEvent_t ev : side_done) cudaEventDestroy(ev);
+  if (fork) cudaEventDestroy(fork);
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   if (d_lats) cudaFree(d_lats);
@@ -874,6 +880,15 @@ int gpumc_engine_set_temporal_blocking(gpumc_engine* eng, int32_t enable) {
   if (eng->blocking != (enable != 0)) {
     eng->blocking = enable != 0;
     eng->drop_graphs();  // captured sweeps depend on which plans run resident
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_engine_set_concurrent_kinds(gpumc_engine* eng, int32_t enable) {
+  if (!eng) return fail(GPUMC_EINVAL, "engine: null");
+  if (eng->concurrent != (enable != 0)) {
+    eng->concurrent = enable != 0;
+    eng->drop_graphs();  // captured sweeps depend on the stream layout
   }
   return GPUMC_OK;
 }
@@ -1091,11 +1106,7 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
     }
     const uint32_t chunk = std::min<uint32_t>(room, 64);
     if (eng->has_per_sweep_work()) {
-      if (eng->use_graphs) {
-        rc = eng->run_graph(chunk);
-      } else {
-        for (uint32_t i = 0; i < chunk && rc == GPUMC_OK; ++i) rc = eng->launch_batch_sweep();
-      }
+      rc = eng->use_graphs ? eng->run_graph(chunk) : eng->launch_batch_sweeps(chunk);
       eng->launches += (uint64_t)chunk * eng->launches_per_batch_sweep();
     }
     for (auto& p : eng->batch_plans)
@@ -1114,13 +1125,84 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
   return GPUMC_OK;
 }
 
+int gpumc_engine::ensure_side(size_t n) {
+  if (!fork) CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  while (side.size() < n) {
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(s2);
+      return fail(GPUMC_ECUDA, std::string("event create: ") + cudaGetErrorString(e));
+    }
+    side.push_back(s2);
+    side_done.push_back(ev);
+  }
+  return GPUMC_OK;
+}
+
+static bool is_msc_kind(int kind) { return kind == MSC * 2 || kind == MSC * 2 + 1; }
+
+// n sweeps of every plan that runs per sweep.  The plans of a batch touch
+// disjoint lattices (one kernel kind each, each with its own launch control
+// and groups), so with `concurrent` every plan runs its n sweeps on a stream
+// of its own, forked from and joined back into the engine stream by events
+// (the same inside graph capture), and the kinds fill each other's idle SMs.
+// Multi-spin plans and their measurement kernels stay on the engine stream,
+// in sweep order.
+int gpumc_engine::launch_batch_sweeps(uint32_t n) {
+  std::vector<size_t> fan;
+  for (size_t i = 0; i < batch_plans.size(); ++i) {
+    const BatchPlan& p = batch_plans[i];
+    if (!(p.res.on && blocking) && !is_msc_kind(p.kind)) fan.push_back(i);
+  }
+  if (!concurrent || fan.size() < 2) {
+    for (uint32_t k = 0; k < n; ++k) {
+      const int rc = launch_batch_sweep();
+      if (rc) return rc;
+    }
+    return GPUMC_OK;
+  }
+  int rc = ensure_side(fan.size());
+  if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(fork, stream));
+  for (size_t j = 0; j < fan.size(); ++j) {
+    const BatchPlan& p = batch_plans[fan[j]];
+    CUDA_TRY(cudaStreamWaitEvent(side[j], fork, 0));
+    for (uint32_t k = 0; k < n; ++k) {
+      rc = launch_sweep_kernel(side[j], p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
+      if (rc) return rc;
+    }
+    CUDA_TRY(cudaEventRecord(side_done[j], side[j]));
+  }
+  for (uint32_t k = 0; k < n; ++k) {
+    for (const BatchPlan& p : batch_plans) {
+      if (!is_msc_kind(p.kind) || (p.res.on && blocking)) continue;
+      rc = launch_sweep_kernel(stream, p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
+      if (rc) return rc;
+    }
+    for (gpumc_sim* s : sims) {
+      if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) {
+        rc = s->launch_msc_measurement();
+        if (rc) return rc;
+      }
+    }
+  }
+  for (size_t j = 0; j < fan.size(); ++j) CUDA_TRY(cudaStreamWaitEvent(stream, side_done[j], 0));
+  return GPUMC_OK;
+}
+
 int gpumc_engine::run_graph(uint32_t n) {
   auto it = batch_graphs.find(n);
   if (it == batch_graphs.end()) {
     cudaGraph_t g;
+    if (concurrent) {  // create the side streams outside the capture
+      const int rs = ensure_side(batch_plans.size());
+      if (rs) return rs;
+    }
     CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    int rc = GPUMC_OK;
-    for (uint32_t i = 0; i < n && rc == GPUMC_OK; ++i) rc = launch_batch_sweep();
+    const int rc = launch_batch_sweeps(n);
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(GPUMC_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));

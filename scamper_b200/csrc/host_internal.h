@@ -130,6 +130,10 @@ struct gpumc_engine {
   bool use_graphs = true;
   bool blocking = true;       // temporal blocking of qualifying Ising plans
   bool refine = true;         // split tiles of batches that leave CTA slots idle
+  bool concurrent = true;     // each plan's sweeps on a stream of its own (disjoint lattices)
+  std::vector<cudaStream_t> side;     // per-plan streams, created on first use
+  std::vector<cudaEvent_t> side_done; // per-plan join events
+  cudaEvent_t fork = nullptr;         // fork point on the engine stream
   uint64_t launches = 0;      // kernel launches issued by gpumc_engine_sweep
   int slots = gpumc::kDefaultSlots;  // resident sweep CTAs of the device (tile planning)
   int slots3 = gpumc::kDefaultSlots3;  // the same for the 3D Ising kernel
@@ -139,6 +143,8 @@ struct gpumc_engine {
   ~gpumc_engine();
   int rebuild_batch();
   int launch_batch_sweep();
+  int launch_batch_sweeps(uint32_t n);
+  int ensure_side(size_t n);
   bool has_per_sweep_work() const;
   uint64_t launches_per_batch_sweep() const;
   int run_graph(uint32_t n);

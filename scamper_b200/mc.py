@@ -190,6 +190,11 @@ class Engine:
         keep every lattice's full-launch tiles; results identical."""
         _lib.call("gpumc_engine_set_tile_refinement", self.h, 1 if enable else 0)
 
+    def set_concurrent_kinds(self, enable):
+        """Run each kernel kind's sweeps on a stream of its own (default) or
+        all kinds in sequence on the engine stream; results identical."""
+        _lib.call("gpumc_engine_set_concurrent_kinds", self.h, 1 if enable else 0)
+
     def launch_count(self):
         v = ctypes.c_uint64()
         _lib.call("gpumc_engine_launch_count", self.h, ctypes.byref(v))
