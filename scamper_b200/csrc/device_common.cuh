@@ -33,6 +33,44 @@ __device__ __forceinline__ uint4 draw(uint64_t key, uint64_t index, uint32_t col
   return philox10(c, (uint32_t)key, (uint32_t)(key >> 32));
 }
 
+// Philox4x32-10 of counter (index, ctrl, sweep) with the sweep-uniform part
+// of round 1 precomputed and the round keys bumped on the fly: five
+// registers, for kernels where resident warps matter more than two adds per
+// round.  ctrl0 (given once) and ctrl (per call) are XORed into word 1, so a
+// call equals draw() with word 1 = ctrl0 ^ ctrl.  Each round multiply is one
+// 32x32->64 wide product.
+struct RunPhilox {
+  uint32_t a, b, c, k0, k1;
+};
+__device__ __forceinline__ RunPhilox make_run_philox(uint64_t key, uint64_t sweep, uint32_t ctrl0) {
+  RunPhilox P;
+  P.k0 = (uint32_t)key;
+  P.k1 = (uint32_t)(key >> 32);
+  const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
+  P.a = __umulhi(0xCD9E8D57u, c2) ^ P.k0 ^ ctrl0;
+  P.b = 0xCD9E8D57u * c2;
+  P.c = c3 ^ P.k1;
+  return P;
+}
+__device__ __forceinline__ uint4 run_philox(const RunPhilox& P, uint32_t index, uint32_t ctrl) {
+  const uint64_t p00 = (uint64_t)0xD2511F53u * index;
+  uint4 c = make_uint4(P.a ^ ctrl, P.b, (uint32_t)(p00 >> 32) ^ P.c, (uint32_t)p00);
+  uint32_t k0 = P.k0, k1 = P.k1;
+#pragma unroll
+  for (int r = 1; r < 10; ++r) {
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1,
+                   (uint32_t)p0);
+  }
+  return c;
+}
+
+// v wrapped into [0, n) for v in [-n, 2n) (halo coordinates): no division
+__device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
 __device__ __forceinline__ int wrapi(int v, int n) {
   v %= n;
   return v < 0 ? v + n : v;

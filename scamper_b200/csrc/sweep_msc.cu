@@ -22,27 +22,53 @@ namespace gpumc {
 
 constexpr int kMscMaxItems = 4;
 
+// Acceptance table of a sweep in the comparator's form.  Classes with p < 1
+// ("pending") are those with dE > 0: at most z/2 of them for the Ising table
+// (k < z/2 anti-aligned neighbours for J > 0, k > z/2 for J < 0); every other
+// class is accepted outright.  pneg[i][b] = ~0 where bit b of pending class
+// i is 0; tw[j] bit i = bit j (most significant first) of the 80-bit
+// threshold of pending class i.
 struct MscTab {
-  uint32_t head[7];
-  unsigned long long tail[7];
-  int ncls;
+  int npend;
+  uint32_t pneg[3][3];
+  unsigned char tw[80];
 };
 
-__device__ __forceinline__ unsigned long long t_plane(const MscTab& tab, int k, int j) {
-  // bit j (0 = most significant) of the 80-bit threshold of class k, as a mask
-  const uint32_t h = tab.head[k];
-  const unsigned long long b =
-      j < 16 ? (unsigned long long)((h >> (15 - j)) & 1u) : ((tab.tail[k] >> (79 - j)) & 1ull);
-  return 0ull - b;
+__device__ __forceinline__ void load_msc_table(MscTab& tab, const LatDesc* L, const GroupDesc* G) {
+  if (threadIdx.x != 0) return;
+  const int label = G->label[L->replica];
+  const int n = min(G->n_cls, 7);
+  const uint32_t* head = G->head + label * G->n_cls;
+  const unsigned long long* tail = G->tail + label * G->n_cls;
+  int pc[3] = {0, 0, 0}, np = 0;
+  for (int k = 0; k < n; ++k)
+    if (head[k] < 65536u && np < 3) pc[np++] = k;
+  tab.npend = np;
+  for (int i = 0; i < 3; ++i)
+    for (int b = 0; b < 3; ++b) tab.pneg[i][b] = (i < np && ((pc[i] >> b) & 1)) ? 0u : 0xFFFFFFFFu;
+  for (int j = 0; j < 80; ++j) {
+    unsigned int v = 0;
+    for (int i = 0; i < np; ++i) {
+      const uint32_t h = head[pc[i]];
+      const unsigned long long t = tail[pc[i]];
+      const unsigned int bit = j < 16 ? (h >> (15 - j)) & 1u : (unsigned int)((t >> (79 - j)) & 1ull);
+      v |= bit << i;
+    }
+    tab.tw[j] = (unsigned char)v;
+  }
+}
+
+__device__ __forceinline__ unsigned long long rep64(uint32_t v) {
+  return (unsigned long long)v | ((unsigned long long)v << 32);
 }
 
 template <int DIM>
 __device__ __forceinline__ unsigned long long msc_site(unsigned long long w,
                                                        const unsigned long long* nb,
-                                                       const MscTab& tab, uint64_t key,
-                                                       uint64_t site, uint32_t colour,
-                                                       uint64_t sweep, long long& dE) {
+                                                       const MscTab& tab, const RunPhilox& P,
+                                                       uint64_t site, uint32_t colour, long long& dE) {
   constexpr int zc = 2 * DIM;
+  constexpr int kPend = DIM;  // z / 2
   unsigned long long x[6];
 #pragma unroll
   for (int i = 0; i < zc; ++i) x[i] = w ^ nb[i];
@@ -64,40 +90,46 @@ __device__ __forceinline__ unsigned long long msc_site(unsigned long long w,
     b1 = c0 ^ c1 ^ c2;
     b2 = (c0 & c1) | (c2 & (c0 ^ c1));
   }
-  unsigned long long mask[7];
-  unsigned long long always = 0, pending = 0;
+  // replicas of each pending class (class k = b2 b1 b0 in bits)
+  unsigned long long m[kPend], pending = 0;
 #pragma unroll
-  for (int k = 0; k <= zc; ++k) {
-    const unsigned long long m = ((k & 1) ? b0 : ~b0) & ((k & 2) ? b1 : ~b1) & ((k & 4) ? b2 : ~b2);
-    mask[k] = m;
-    if (tab.head[k] >= 65536u) always |= m;
-    else pending |= m;
+  for (int i = 0; i < kPend; ++i) {
+    m[i] = 0;
+    if (i < tab.npend) {
+      m[i] = (b0 ^ rep64(tab.pneg[i][0])) & (b1 ^ rep64(tab.pneg[i][1])) & (b2 ^ rep64(tab.pneg[i][2]));
+      pending |= m[i];
+    }
   }
+  // bit-serial comparison of the 64 uniforms, two planes per draw
+  const uint32_t ctrl = (uint32_t)(site >> 32) << 16;
   unsigned long long lt = 0, eq = pending;
   for (int pair = 0; pair < 40 && eq; ++pair) {
-    const uint4 o = draw(key, site, colour, TAG_MSC, (uint32_t)pair, sweep);
+    const uint4 o = run_philox(P, (uint32_t)site, ctrl | ((uint32_t)pair << 8));
     const unsigned long long u0 = (unsigned long long)o.x | ((unsigned long long)o.y << 32);
     const unsigned long long u1 = (unsigned long long)o.z | ((unsigned long long)o.w << 32);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int j = 2 * pair + h;
       const unsigned long long u = h ? u1 : u0;
+      const unsigned int tb = tab.tw[2 * pair + h];
       unsigned long long tj = 0;
 #pragma unroll
-      for (int k = 0; k <= zc; ++k)
-        if (tab.head[k] < 65536u) tj |= mask[k] & t_plane(tab, k, j);
+      for (int i = 0; i < kPend; ++i)
+        if ((tb >> i) & 1u) tj |= m[i];
       lt |= eq & tj & ~u;
       eq &= ~(tj ^ u);
     }
   }
-  const unsigned long long flip = always | lt;
-#pragma unroll
-  for (int k = 0; k <= zc; ++k) dE += (long long)__popcll(flip & mask[k]) * (2 * (zc - 2 * k));
+  const unsigned long long flip = ~pending | lt;
+  // dE = sum over flipped replicas of 2 (z - 2 k)
+  dE += 2LL * zc * __popcll(flip) -
+        4LL * (__popcll(flip & b0) + 2LL * __popcll(flip & b1) + 4LL * __popcll(flip & b2));
   return w ^ flip;
 }
 
+// four CTAs per SM in 2D (64 registers, a few spilled words) measured 3 %
+// faster than three at 80 registers
 template <int DIM>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
     k_sweep_msc(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                 GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
   extern __shared__ __align__(16) unsigned long long wsm[];
@@ -114,26 +146,28 @@ __global__ void __launch_bounds__(kThreads)
   const uint64_t key = L->key;
   const unsigned long long* cur = (const unsigned long long*)L->buf[sweep & 1];
   unsigned long long* nxt = (unsigned long long*)L->buf[(sweep & 1) ^ 1];
-  if (threadIdx.x == 0) {
-    const int label = G->label[L->replica];
-    tab.ncls = G->n_cls;
-    for (int i = 0; i < G->n_cls && i < 7; ++i) {
-      tab.head[i] = G->head[label * G->n_cls + i];
-      tab.tail[i] = G->tail[label * G->n_cls + i];
-    }
-  }
+  load_msc_table(tab, L, G);
   const int Wv = min(t.cx * 2, lx - t.x0);
   const int hv = min(t.ty, ly - t.y0);
   const int S = Wv + 4, R = hv + 4;
   const int plane = R * S;
   long long dE = 0;
+  // words k, k + kThreads, ... of the R x S staged rows, walked by a
+  // division-free (row, column) cursor
+  const int lc0 = threadIdx.x % S, lr0 = threadIdx.x / S;
+  const int lstep_c = kThreads % S, lstep_r = kThreads / S;
   auto load = [&](unsigned long long* pl, int z) {
-    const int cols = Wv + 4;
-    for (int i = threadIdx.x; i < R * cols; i += kThreads) {
-      const int r = i / cols, c = i - r * cols;
-      const int y = wrapi(t.y0 - 2 + r, ly);
-      const int x = wrapi(t.x0 - 2 + c, lx);
+    int r = lr0, c = lc0;
+    while (r < R) {
+      const int y = wrap1(t.y0 - 2 + r, ly);
+      const int x = wrap1(t.x0 - 2 + c, lx);
       pl[r * S + c] = cur[((size_t)z * ly + y) * (size_t)pitch + x];
+      c += lstep_c;
+      r += lstep_r;
+      if (c >= S) {
+        c -= S;
+        ++r;
+      }
     }
   };
   auto pass = [&](unsigned long long* pl, const unsigned long long* pm,
@@ -145,14 +179,23 @@ __global__ void __launch_bounds__(kThreads)
     const int nitems = nrows * half;
     unsigned long long res[kMscMaxItems];
     int roff[kMscMaxItems];
+    const RunPhilox P = make_run_philox(key, sweep, (uint32_t)colour | (TAG_MSC << 1));
+    // items threadIdx.x, + kThreads, ... as (row, column) cursors
+    const int dr = kThreads / half, dk = kThreads - dr * half;
+    int ir = threadIdx.x / half, ik = threadIdx.x - ir * half;
 #pragma unroll
     for (int it = 0; it < kMscMaxItems; ++it) {
       roff[it] = -1;
       const int i = threadIdx.x + it * kThreads;
+      const int r = rlo + ir, k = ik;
+      ik += dk;
+      ir += dr;
+      if (ik >= half) {
+        ik -= half;
+        ++ir;
+      }
       if (i < nitems) {
-        const int r = rlo + i / half;
-        const int k = i - (r - rlo) * half;
-        const int y = wrapi(t.y0 - 2 + r, ly);
+        const int y = wrap1(t.y0 - 2 + r, ly);
         const int pos = xlo + 2 * k + ((xlo + y + z + colour) & 1);
         const int off = r * S + (pos - t.x0 + 2);
         unsigned long long nb[6] = {pl[off - 1], pl[off + 1], pl[off - S], pl[off + S], 0, 0};
@@ -160,12 +203,11 @@ __global__ void __launch_bounds__(kThreads)
           nb[4] = pm[off];
           nb[5] = pp[off];
         }
-        const int xr = wrapi(pos, lx);
+        const int xr = wrap1(pos, lx);
         const uint64_t site = ((uint64_t)z * ly + y) * (uint64_t)lx + (uint64_t)xr;
         const bool owned = owned_plane && r >= 2 && r < 2 + hv && pos >= t.x0 && pos < t.x0 + Wv;
         long long de = 0;
-        const unsigned long long nw = msc_site<DIM>(pl[off], nb, tab, key, site, (uint32_t)colour,
-                                                    sweep, de);
+        const unsigned long long nw = msc_site<DIM>(pl[off], nb, tab, P, site, (uint32_t)colour, de);
         res[it] = nw;
         roff[it] = off;
         if (owned) {
