@@ -199,6 +199,28 @@ def test_server_results_identical_alone_and_in_mix(gpumc):
     srv.close()
 
 
+def test_server_timing_and_spin_retention(gpumc):
+    """gpumc_server_timing splits the steps' host time into admit / sweep /
+    retire; gpumc_server_set_keep_spins bounds which finished jobs keep their
+    final spins for gpumc_job_spins."""
+    srv = gpumc.Server(hbm_budget=1 << 30, chunk=5)
+    srv.set_keep_spins(32 * 32)
+    small = srv.submit(_params((32, 32), beta=0.44), 11, 12)
+    large = srv.submit(_params((64, 64), beta=0.44), 12, 12)
+    for _ in range(20):
+        if srv.step() == 0:
+            break
+    res = {r["job_id"]: r for r in srv.poll()}
+    assert res[small]["status"] == 0 and res[large]["status"] == 0
+    assert srv.job_spins(small, 32 * 32).size == 32 * 32
+    with pytest.raises(gpumc.GpumcError):
+        srv.job_spins(large, 64 * 64)
+    st = srv.stats()
+    assert st["admit_s"] > 0 and st["sweep_s"] > 0 and st["retire_s"] > 0
+    assert st["admit_s"] + st["sweep_s"] + st["retire_s"] == pytest.approx(st["busy_s"], rel=1e-9, abs=1e-9)
+    srv.close()
+
+
 def test_server_admission_by_footprint(gpumc):
     srv = gpumc.Server(hbm_budget=3 << 20, chunk=5)
     big = _params((1024, 1024), beta=0.4)  # 2 MiB of ping-pong buffers + records
