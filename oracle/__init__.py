@@ -1,8 +1,8 @@
 """ctypes wrapper of the CPU oracle (oracle/liboracle.so).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
-the checker, and by bench.py's CPU-baseline leg.  Nothing on the product path
-imports it.
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() to
+check the device result, and by bench.py's CPU-baseline leg.  Nothing on the
+product path imports it.
 """
 import ctypes
 import os

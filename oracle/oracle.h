@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the lattice Metropolis engine.  TEST INFRASTRUCTURE ONLY:
- * it is the checker the parity tests and the CPU baseline of the benchmark
- * use, never a product code path.
+ * the parity tests compare the device against it and the benchmark times it
+ * as the CPU baseline; it is never a product code path.
  *
  * Two parts:
  *  1. A bit-exact replay of the engine's method (checkerboard colour order,
