@@ -445,14 +445,17 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     L.tile_cx = (lx + 3) / 4;
     // 3D: tiles of whole rows marched along z through a ring of four shared
     // planes (3 components x (rows + 2 halo rows) x pitch floats each) of at
-    // most 56 KB (three CTAs per SM), up to 16 rows x 22 planes per tile (for
-    // 32 lattices of 64^3: 384 tiles, one wave of 148 x 3 CTAs)
+    // most 56 KB (three CTAs per SM), up to 16 rows x 8 planes per tile (for
+    // 32 lattices of 64^3: 1024 tiles, 2.3 waves of 148 x 3 CTAs).  Deeper
+    // tiles re-read fewer halo planes but leave the last wave ragged: on
+    // that mix 22 planes ran at 41.2 attempts/ns, 11 at 42.7, 8 at 47.5,
+    // 6 at 44.1 and 4 at 45.2.
     const int ty_max = (int)(kO3MarchSmem / (48 * (size_t)L.pitch)) - 2;
     if (L.dims == 3 && ty_max >= 1) {
       L.march = true;
       const int nty = (ly + std::min(16, ty_max) - 1) / std::min(16, ty_max);
       L.tile_y = (ly + nty - 1) / nty;
-      const int ntz = (lz + 21) / 22;
+      const int ntz = (lz + 7) / 8;
       L.tile_z = (lz + ntz - 1) / ntz;
       L.smem = 48 * (size_t)(L.tile_y + 2) * L.pitch;
     } else {
