@@ -1170,30 +1170,34 @@ int gpumc_engine::launch_batch_sweeps(uint32_t n) {
   int rc = ensure_side(fan.size());
   if (rc) return rc;
   CUDA_TRY(cudaEventRecord(fork, stream));
-  for (size_t j = 0; j < fan.size(); ++j) {
+  size_t forked = 0;  // side streams that wait on the fork and must be joined
+  for (size_t j = 0; j < fan.size() && rc == GPUMC_OK; ++j) {
     const BatchPlan& p = batch_plans[fan[j]];
-    CUDA_TRY(cudaStreamWaitEvent(side[j], fork, 0));
-    for (uint32_t k = 0; k < n; ++k) {
+    if (cudaStreamWaitEvent(side[j], fork, 0) != cudaSuccess) {
+      rc = fail(GPUMC_ECUDA, "stream fork failed");
+      break;
+    }
+    ++forked;
+    for (uint32_t k = 0; k < n && rc == GPUMC_OK; ++k)
       rc = launch_sweep_kernel(side[j], p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
-      if (rc) return rc;
-    }
-    CUDA_TRY(cudaEventRecord(side_done[j], side[j]));
   }
-  for (uint32_t k = 0; k < n; ++k) {
+  for (uint32_t k = 0; k < n && rc == GPUMC_OK; ++k) {
     for (const BatchPlan& p : batch_plans) {
-      if (!is_msc_kind(p.kind) || (p.res.on && blocking)) continue;
+      if (!is_msc_kind(p.kind) || (p.res.on && blocking) || rc) continue;
       rc = launch_sweep_kernel(stream, p.kind, p.d_tiles, p.n_tiles, d_lats, d_groups, p.d_ctl, p.smem);
-      if (rc) return rc;
     }
-    for (gpumc_sim* s : sims) {
-      if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) {
-        rc = s->launch_msc_measurement();
-        if (rc) return rc;
-      }
+    for (gpumc_sim* s : sims)
+      if (!rc && s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) rc = s->launch_msc_measurement();
+  }
+  // join every forked stream, on success and on error alike, so that the
+  // engine stream (and a capture in progress) never leaves work behind
+  for (size_t j = 0; j < forked; ++j) {
+    if (cudaEventRecord(side_done[j], side[j]) != cudaSuccess ||
+        cudaStreamWaitEvent(stream, side_done[j], 0) != cudaSuccess) {
+      if (!rc) rc = fail(GPUMC_ECUDA, "stream join failed");
     }
   }
-  for (size_t j = 0; j < fan.size(); ++j) CUDA_TRY(cudaStreamWaitEvent(stream, side_done[j], 0));
-  return GPUMC_OK;
+  return rc;
 }
 
 int gpumc_engine::run_graph(uint32_t n) {
