@@ -605,7 +605,7 @@ def main():
     ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving", "heat_bath", "cluster", "o3_proposals"],
                     default=None,
                     help="run one extra workload alone (profiling)")
-    ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 100.0, 1000.0])
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 30.0, 100.0, 300.0, 1000.0])
     ap.add_argument("--serve-jobs", type=int, default=64)
     ap.add_argument("--serve-sweep-scale", type=float, default=0.1)
     ap.add_argument("--serve-chunk", type=int, default=20)
