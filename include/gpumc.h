@@ -240,6 +240,14 @@ int gpumc_change_parameter(gpumc_sim* sim, int32_t replica, double new_beta);
 int gpumc_pt_configure(gpumc_sim* sim, uint32_t interval);
 /* labels[r] = ladder index held by replica r (always a permutation). */
 int gpumc_pt_labels(gpumc_sim* sim, int32_t* labels);
+/* Restores the labels of a resumed ensemble (labels[r] = ladder index held
+ * by replica r; a permutation), the parameter-chain indices that
+ * ParallelTemperingCompatible chains carry across a checkpoint
+ * (set_chain_idx, Carlo.rs/src/parallel_tempering.rs:159-163).  Each
+ * exchange's step and pairing follow from the sweep count (sweep / interval,
+ * parallel_tempering.rs:372-373), so restoring the sweep count with
+ * gpumc_set_sweep_count and the labels continues the same exchanges. */
+int gpumc_pt_set_labels(gpumc_sim* sim, const int32_t* labels);
 int gpumc_pt_stats(gpumc_sim* sim, uint64_t* exchange_steps, uint64_t* accepted_swaps);
 
 /* ---- serving: continuous batching of simulation jobs ------------------ */
@@ -308,13 +316,19 @@ int gpumc_plan_tiles(const gpumc_spec* spec, int32_t slots, int32_t slots3, int3
  *   energy_out device pointer: n_lattices int64 results
  *   stream     cudaStream_t to run on (NULL = default stream); the call is
  *              asynchronous with respect to the host
+ * Extents are 1..2^20 (any parity); bonds follow the reference's periodic
+ * hypercubic builder (CMC.rs/src/lattice/graph.rs:417-451): one +1 bond per
+ * axis and site, wrapping at the far face, and none along an axis of extent 1
+ * (extent 2 gives the two parallel bonds the builder makes).
  * Limits: 1 <= n_lattices <= 64, at most 4e9 sites per lattice; larger
  * requests return GPUMC_EINVAL.  Its reduction scratch is one file-scope
  * device array of 128 KiB (64 lattices x 256 partial sums) that every GPU
- * which loads the library holds until exit.  The first call on a device looks
- * up that array's device address; make it before any stream capture.  All
- * calls on a device share the array: calls that overlap on the GPU (different
- * streams without ordering between them) race and must not be issued. */
+ * which loads the library holds until exit.  The first call in a context
+ * (per device, and again after cudaDeviceReset) looks up that array's device
+ * address; make it before any stream capture.  All calls on a device share
+ * the array: calls that overlap on the GPU (different streams without
+ * ordering between them) race and must not be issued.  A CUDA error already
+ * pending when the call starts is returned as GPUMC_ECUDA and left pending. */
 int gpumc_energy_int8_noalloc(int32_t model, int32_t dims, int64_t lx, int64_t ly, int64_t lz,
                               const int8_t* spins, int32_t n_lattices, long long* energy_out,
                               void* stream);

@@ -135,6 +135,7 @@ SIGNATURES = {
     "gpumc_change_parameter": [_vp, ctypes.c_int32, ctypes.c_double],
     "gpumc_pt_configure": [_vp, ctypes.c_uint32],
     "gpumc_pt_labels": [_vp, _P(ctypes.c_int32)],
+    "gpumc_pt_set_labels": [_vp, _P(ctypes.c_int32)],
     "gpumc_pt_stats": [_vp, _P(ctypes.c_uint64), _P(ctypes.c_uint64)],
     "gpumc_server_create": [ctypes.c_int32, ctypes.c_size_t, ctypes.c_uint32, _P(_vp)],
     "gpumc_submit": [_vp, _P(Job), _P(ctypes.c_uint64)],

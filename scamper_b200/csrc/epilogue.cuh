@@ -235,7 +235,10 @@ static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int
     for (int i = 0; i < ndue; ++i) {
       GroupDesc* H = &groups[ids[s_due[i]]];
       const int m = H->n_rep;
-      const uint64_t step = H->pt_step;
+      // exchange step = sweep count / interval, as PtExchange::try_exchange
+      // derives it (Carlo.rs/src/parallel_tempering.rs:372-373), so a handle
+      // resumed at a sweep count continues the pairing and the stream
+      const uint64_t step = lats[H->first_lat].sweep / (uint64_t)H->pt_interval;
       int32_t* at = H->rep_at;
       if (t == 0) s_acc = 0;
       for (int r = t; r < m; r += kThreads) at[H->label[r]] = r;

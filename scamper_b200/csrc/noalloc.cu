@@ -10,6 +10,7 @@
 // gpumc_energy_int8_noalloc: the same exact bond-sum reduction, with its
 // scratch (per-block partial sums) in a file-scope __device__ array instead
 // of allocated memory.  The caller passes the spins and the output.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -46,20 +47,23 @@ __global__ void __launch_bounds__(256)
     const long long rho = i / lx;
     const int y = (int)(rho % ly);
     const int z = (int)(rho / ly);
-    const int xp = x + 1 < lx ? x + 1 : 0;
-    const int yp = y + 1 < ly ? y + 1 : 0;
     const int8_t a = s[i];
-    const int8_t bx = s[rho * lx + xp];
-    const int8_t by = s[((long long)z * ly + yp) * lx + x];
-    if (model == ISING) {
-      e -= (long long)a * bx + (long long)a * by;
-    } else {
-      e -= (long long)(a == bx) + (long long)(a == by);
+    // one +1 bond per axis, wrapping at the far face; an axis of extent 1 has
+    // no bond at all (a site is not its own neighbour)
+    if (lx > 1) {
+      const int xp = x + 1 < lx ? x + 1 : 0;
+      const int8_t b = s[rho * lx + xp];
+      e -= model == ISING ? (long long)a * b : (long long)(a == b);
     }
-    if (dims == 3) {
+    if (ly > 1) {
+      const int yp = y + 1 < ly ? y + 1 : 0;
+      const int8_t b = s[((long long)z * ly + yp) * lx + x];
+      e -= model == ISING ? (long long)a * b : (long long)(a == b);
+    }
+    if (dims == 3 && lz > 1) {
       const int zp = z + 1 < lz ? z + 1 : 0;
-      const int8_t bz = s[((long long)zp * ly + y) * lx + x];
-      e -= model == ISING ? (long long)a * bz : (long long)(a == bz);
+      const int8_t b = s[((long long)zp * ly + y) * lx + x];
+      e -= model == ISING ? (long long)a * b : (long long)(a == b);
     }
   }
   __shared__ long long red[256 / 32];
@@ -89,25 +93,53 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (the array's host-side name is not a device address).
-static long long* g_scratch_ptr[kNoAllocMaxDevices];
+// Device address of the scratch array, looked up with the device current
+// (the array's host-side name is not a device address).  The address belongs
+// to the device's current context: it is cached together with that context's
+// unique id and looked up again when the id changes (after cudaDeviceReset the
+// runtime creates a new primary context and reloads the module).
+struct ScratchSlot {
+  long long* ptr = nullptr;
+  unsigned long long ctx_id = 0;
+};
+static ScratchSlot g_scratch[kNoAllocMaxDevices];
 static std::mutex g_scratch_mu;
+
+// Unique id of the calling thread's current context (cuCtxGetId through the
+// runtime's driver entry point, so the library needs no link to libcuda).
+static bool current_context_id(unsigned long long* id) {
+  typedef CUresult (*CtxGetId)(CUcontext, unsigned long long*);
+  static CtxGetId fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return (CtxGetId)p;
+  }();
+  return fn && fn(nullptr, id) == CUDA_SUCCESS;
+}
 
 static int scratch_for_current_device(long long** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(GPUMC_ENODEV, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(GPUMC_ENODEV, "device index beyond 64");
+  unsigned long long ctx = 0;
+  const bool have_ctx = current_context_id(&ctx);
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  ScratchSlot& slot = g_scratch[dev];
+  if (!have_ctx || !slot.ptr || slot.ctx_id != ctx) {
     long long* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_noalloc_partials);
+    e = cudaGetSymbolAddress((void**)&p, g_noalloc_partials);  // creates the context if needed
     if (e != cudaSuccess)
       return fail(GPUMC_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_scratch_ptr[dev] = p;
+    if (!current_context_id(&ctx))
+      return fail(GPUMC_ECUDA, "no current CUDA context after looking up the scratch array");
+    slot.ptr = p;
+    slot.ctx_id = ctx;
   }
-  *out = g_scratch_ptr[dev];
+  *out = slot.ptr;
   return GPUMC_OK;
 }
 
@@ -134,6 +166,11 @@ int gpumc_energy_int8_noalloc(int32_t model, int32_t dims, int64_t lx, int64_t l
   long long* scratch = nullptr;
   int rc = scratch_for_current_device(&scratch);
   if (rc) return rc;
+  // An error left pending by the caller's earlier work is reported as such
+  // (and left pending), so the check after the launches sees only their own.
+  cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return fail(GPUMC_ECUDA, std::string("CUDA error pending before the call: ") + cudaGetErrorString(pending));
   cudaStream_t st = (cudaStream_t)stream;
   const dim3 grid(kNoAllocBlocksPerLattice, (unsigned)n_lattices);
   k_noalloc_energy_partials<<<grid, 256, 0, st>>>(model, dims, (int)lx, (int)ly, (int)lzz, spins, scratch);

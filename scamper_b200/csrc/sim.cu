@@ -859,6 +859,10 @@ int gpumc_set_sweep_count(gpumc_sim* sim, uint64_t sweeps) {
     }
     RC_TRY(sim->set_lat_field(r, offsetof(LatDesc, sweep), sweeps));
   }
+  // exchange steps attempted up to this count (the device derives each
+  // exchange's step from the sweep count; this keeps gpumc_pt_stats in line)
+  const uint64_t steps = sim->pt_interval > 0 ? sweeps / sim->pt_interval : 0;
+  RC_TRY(sim->set_group_field(offsetof(GroupDesc, pt_step), steps));
   CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
   sim->sweeps = sweeps;
   return GPUMC_OK;
@@ -930,6 +934,22 @@ int gpumc_pt_labels(gpumc_sim* sim, int32_t* labels) {
   CUDA_TRY(cudaSetDevice(sim->eng->device));
   CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
   CUDA_TRY(cudaMemcpy(labels, sim->d_label, 4 * (size_t)sim->n_rep, cudaMemcpyDeviceToHost));
+  return GPUMC_OK;
+}
+
+int gpumc_pt_set_labels(gpumc_sim* sim, const int32_t* labels) {
+  if (!sim || !labels) return fail(GPUMC_EINVAL, "null argument");
+  if (sim->n_temps != sim->n_rep)
+    return fail(GPUMC_EINVAL, "labels: the handle needs one ladder entry per replica (n_temps = n_replicas)");
+  std::vector<char> seen(sim->n_rep, 0);
+  for (int r = 0; r < sim->n_rep; ++r) {
+    if (labels[r] < 0 || labels[r] >= sim->n_rep || seen[labels[r]])
+      return fail(GPUMC_EINVAL, "labels: must be a permutation of 0..n_replicas-1");
+    seen[labels[r]] = 1;
+  }
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  CUDA_TRY(cudaMemcpy(sim->d_label, labels, 4 * (size_t)sim->n_rep, cudaMemcpyHostToDevice));
   return GPUMC_OK;
 }
 

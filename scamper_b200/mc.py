@@ -515,6 +515,13 @@ class ClassicalMC:
         _lib.call("gpumc_pt_labels", self.h, a)
         return np.array(a[:], dtype=np.int32)
 
+    def set_pt_labels(self, labels):
+        """Restores the ladder index held by each replica (a resumed
+        ensemble's parameter-chain indices, set_chain_idx,
+        Carlo.rs/src/parallel_tempering.rs:159-163)."""
+        a = (ctypes.c_int32 * self.n_replicas)(*[int(v) for v in labels])
+        _lib.call("gpumc_pt_set_labels", self.h, a)
+
     def pt_stats(self):
         s = ctypes.c_uint64()
         a = ctypes.c_uint64()

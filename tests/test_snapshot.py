@@ -129,3 +129,64 @@ def test_snapshot_load_recomputes_energy_and_restores_beta(gpumc):
     assert b.log_weight_ratio("beta", 0.5) == pytest.approx((0.3 - 0.5) * a.energy()[0])
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model,shape,n1,n2", [
+    ("ising", (16, 8), 25, 23),
+    ("ising", (64, 64), 37, 40),
+    ("potts", (8, 6, 6), 22, 20),
+    ("o3", (6, 4, 4), 13, 17),
+])
+def test_parallel_tempering_resumes_mid_run(gpumc, model, shape, n1, n2):
+    """A PT ensemble stopped after n1 sweeps and restored into a fresh handle
+    (spins, sweep count, labels) continues exactly as the uninterrupted run:
+    each exchange's pairing and random stream follow from the sweep count
+    (exchange_step = sweep_count / interval, Carlo.rs/src/parallel_tempering.rs:
+    372-373), not from how many exchanges the handle itself has made."""
+    from scamper_b200 import _lib
+    R, interval = 8, 3
+    betas = gpumc.geometric_ladder_betas(1.5, 3.5, R) if model != "o3" else \
+        gpumc.geometric_ladder_betas(0.9, 2.0, R)
+    kw = dict(q=3) if model == "potts" else {}
+
+    def make():
+        mc = gpumc.ClassicalMC.from_params(_params(shape, **kw), 77, model=model, n_replicas=R, betas=betas)
+        mc.on_phase_start(_lib.PHASE_MEASUREMENT)  # no O(3) cone adaptation
+        mc.pt_configure(interval)
+        return mc
+
+    cont = make()
+    cont.sweep(n1 + n2)
+    split = make()
+    split.sweep(n1)
+    spins = [split.spins(r).copy() for r in range(R)]
+    labels = split.pt_labels()
+    assert split.pt_stats()[0] == n1 // interval
+    split.close()
+    fresh = make()
+    fresh.set_sweep_count(n1)
+    fresh.set_pt_labels(labels)
+    for r in range(R):
+        fresh.set_spins(r, spins[r])
+    assert fresh.pt_stats()[0] == n1 // interval
+    fresh.sweep(n2)
+    np.testing.assert_array_equal(fresh.pt_labels(), cont.pt_labels())
+    for r in range(R):
+        np.testing.assert_array_equal(fresh.spins(r), cont.spins(r))
+    assert fresh.pt_stats()[0] == cont.pt_stats()[0] == (n1 + n2) // interval
+    fresh.close()
+    cont.close()
+
+
+@pytest.mark.gpu
+def test_pt_set_labels_rejects_non_permutations(gpumc):
+    mc = gpumc.ClassicalMC.from_params(_params((8, 8)), 3, n_replicas=4,
+                                       betas=gpumc.geometric_ladder_betas(1.5, 3.5, 4))
+    mc.pt_configure(2)
+    for bad in ([0, 1, 2, 2], [0, 1, 2, 4], [-1, 0, 1, 2]):
+        with pytest.raises(gpumc.InvalidConfig):
+            mc.set_pt_labels(bad)
+    mc.set_pt_labels([3, 2, 1, 0])
+    assert mc.pt_labels().tolist() == [3, 2, 1, 0]
+    mc.close()

@@ -54,6 +54,53 @@ def test_noalloc_energy_matches_allocating_entry_point(gpumc, model, shape, q):
     mc.close()
 
 
+def _edge_list_energy(spins, shape, potts):
+    """Energy in units of J from the reference's periodic hypercubic edge list
+    (CMC.rs/src/lattice/graph.rs:417-451): one +1 bond per axis and site, no
+    bond along an axis of extent 1."""
+    from scamper_b200.snapshot import lattice_topology
+    _, _, _, src, dst, kinds = lattice_topology(shape)
+    keep = np.array([shape[k] > 1 for k in kinds], dtype=bool) if len(kinds) else np.zeros(0, bool)
+    a, b = spins[src[keep]].astype(np.int64), spins[dst[keep]].astype(np.int64)
+    return -int((a == b).sum()) if potts else -int((a * b).sum())
+
+
+@pytest.mark.parametrize("model,shape,q", [
+    ("ising", (5, 3), 2),
+    ("potts", (2, 6), 3),
+    ("ising", (3, 3, 5), 2),
+    ("ising", (7, 1), 2),
+    ("potts", (1, 1), 4),
+    ("ising", (4, 1, 3), 2),
+    ("potts", (1, 9, 2), 5),
+    ("ising", (2, 2, 2), 2),
+])
+def test_noalloc_energy_small_and_odd_extents_match_the_edge_list(gpumc, model, shape, q):
+    """Extents the allocating path does not accept (odd, 1, 2) against the
+    reference builder's edge list: an axis of extent 1 has no bond, extent 2
+    has the builder's two parallel bonds."""
+    import torch
+    from scamper_b200 import _lib
+    rng = np.random.default_rng(sum(shape) * 7 + q)
+    n_rep = 3
+    n = int(np.prod(shape))
+    if model == "ising":
+        host = rng.choice(np.array([-1, 1], dtype=np.int8), size=(n_rep, n))
+    else:
+        host = rng.integers(0, q, size=(n_rep, n), dtype=np.int8)
+    expect = [_edge_list_energy(host[r], shape, model == "potts") for r in range(n_rep)]
+    dev = torch.from_numpy(host.ravel().copy()).to("cuda")
+    out = torch.zeros(n_rep, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    mid = _lib.ISING if model == "ising" else _lib.POTTS
+    for call in range(2):
+        out.fill_(12345)
+        rc = _noalloc(gpumc, mid, len(shape), shape, dev.data_ptr(), n_rep, out.data_ptr(), stream)
+        assert rc == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        assert out.cpu().numpy().tolist() == expect, f"call {call}"
+
+
 def test_noalloc_rejects_requests_beyond_its_scratch(gpumc):
     import torch
     from scamper_b200 import _lib
