@@ -3,9 +3,10 @@
 
 Headline workload (spin-flip attempts per ns on one B200): 2D square-lattice
 Ising, L = 8192 (67,108,864 int8 spins per lattice), J = 1, one lattice per
-beta in {0.35, 0.4407, 0.5}, hot start, checkerboard sweeps.  The three
-lattices are resident together (2 x 3 x 64 MiB ping-pong buffers, larger than
-the 126 MB L2), and one step is one sweep of all three in one launch.
+beta in {0.35, 0.4407, 0.5}, hot start, checkerboard sweeps, observables
+recorded every sweep.  The three lattices are resident together (2 x 3 x 64
+MiB ping-pong buffers, larger than the 126 MB L2), and one step is one run of
+the configured job: 1000 sweeps of all three lattices (--sweeps-per-step).
 
 Printed as one JSON line (rank 0).  Extra workloads (multi-spin L = 2048 x 64
 replicas, batched parallel tempering, the uneven Potts / O(3) mix batched vs
@@ -140,15 +141,39 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/traffic.json), if present."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def profiled_counters():
+    """Per-launch ncu counters of the dominant kernels (warp instructions,
+    DRAM bytes, the attempts and sweeps of the captured launch), from the
+    committed summary profiles/kernel_counters.json."""
+    path = os.path.join(ROOT, "profiles", "kernel_counters.json")
     try:
         with open(path) as f:
             return json.load(f)
     except (OSError, ValueError):
         return {}
+
+
+RESIDENT_KEY = "k_sweep_ising_resident<0>: 2D Ising L=8192 x3, 64 sweeps per launch"
+STREAMING_KEY = "k_sweep_ising_bits<2,0>: 2D Ising L=8192 x3, one sweep per launch"
+MSC_KEY = "k_sweep_msc<2>: multi-spin Ising L=2048 x 64 bit-replicas, one sweep per launch"
+
+
+def issue_roofline(counters, key, attempts_per_ns, sm_count, clock_mhz):
+    """Integer-issue roofline of a kernel that is bound by instruction issue:
+    achieved = (warp instructions per attempt, from the ncu capture of the
+    same kernel on the same workload) x the live attempts/ns; peak = SMs x 4
+    schedulers x 1 warp instruction per cycle x the SM clock sampled during
+    the timed region."""
+    c = counters.get(key)
+    if not c or not clock_mhz:
+        return None
+    per_attempt = c["warp_inst"] / c["attempts"]
+    achieved = per_attempt * attempts_per_ns  # G warp instructions / s
+    peak = sm_count * 4 * clock_mhz * 1e-3
+    return {"bound": "int_issue", "achieved": achieved, "peak": peak, "unit": "Gwarp-inst/s",
+            "frac": achieved / peak, "warp_inst_per_attempt": per_attempt,
+            "thread_inst_per_attempt": 32 * per_attempt, "clock_mhz": clock_mhz, "sm_count": sm_count,
+            "counters": f"profiles/kernel_counters.json[{key}]"}
 
 
 def time_sweeps(torch, mc_or_engine, stream_ptr, steps, sweep_fn, warm=True):
@@ -174,23 +199,25 @@ def time_sweeps(torch, mc_or_engine, stream_ptr, steps, sweep_fn, warm=True):
 def headline(gpumc, torch, args, dist, rank, world):
     from scamper_b200 import _lib
     params = {"lattice_type": "square", "Lx": HEADLINE_L, "Ly": HEADLINE_L}
+    spp = args.sweeps_per_step
+    n_sweeps = args.steps * spp
     mc = gpumc.ClassicalMC.from_params(params, 1000 + rank, model="ising",
                                        n_replicas=len(HEADLINE_BETAS), betas=HEADLINE_BETAS,
-                                       record_capacity=max(64, args.steps + args.warmup))
+                                       record_capacity=max(64, n_sweeps, args.warmup * spp))
     mc.on_phase_start(_lib.PHASE_MEASUREMENT)  # observables recorded every sweep
     sp = mc.stream_ptr()
-    mc.sweep(args.warmup)
+    mc.sweep(args.warmup * spp)
     mc.observables()
     barrier(dist)
     n0 = mc.launch_count()
     with ClockSampler(torch.cuda.current_device()) as clk:
-        ms = time_sweeps(torch, mc, sp, args.steps, mc.sweep, warm=False)
+        ms = time_sweeps(torch, mc, sp, n_sweeps, mc.sweep, warm=False)
     launches = mc.launch_count() - n0
     barrier(dist)
     ms_max = max_over_ranks(dist, ms)
-    attempts = float(mc.n_sites) * len(HEADLINE_BETAS) * args.steps
+    attempts = float(mc.n_sites) * len(HEADLINE_BETAS) * n_sweeps
     recs = mc.observables()
-    assert len(recs) == len(HEADLINE_BETAS) * args.steps
+    assert len(recs) == len(HEADLINE_BETAS) * n_sweeps
     # the same workload on the streaming kernel (one launch per sweep, int8
     # read and written every sweep), for the per-sweep HBM roofline
     mc.set_temporal_blocking(False)
@@ -267,22 +294,31 @@ def bench_pt(gpumc, torch, args):
     """Batched parallel tempering: 2D L=512 x 64 replicas (T 1.5..3.5) plus 3D
     L=128 x 32 replicas (T 3.5..5.5), exchange every 10 sweeps on the device,
     both ensembles in one engine launch per sweep."""
-    from scamper_b200 import _lib
+    from scamper_b200 import _lib, autotune
+
+    def build(eng, measure=False):
+        a = gpumc.ClassicalMC.from_params({"lattice_type": "square", "L": 512}, 11, model="ising",
+                                          n_replicas=64, betas=gpumc.geometric_ladder_betas(1.5, 3.5, 64),
+                                          engine=eng, record_capacity=64)
+        b = gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 128}, 12, model="ising",
+                                          n_replicas=32, betas=gpumc.geometric_ladder_betas(3.5, 5.5, 32),
+                                          engine=eng, record_capacity=64)
+        for m in (a, b):
+            m.pt_configure(10)
+            if measure:
+                m.on_phase_start(_lib.PHASE_MEASUREMENT)
+        return [a, b]
+
+    knobs, source, tuning = tuned_knobs(autotune, torch, args, PT_WORKLOAD, build, PT_SPACE)
     eng = gpumc.Engine()
-    a = gpumc.ClassicalMC.from_params({"lattice_type": "square", "L": 512}, 11, model="ising",
-                                      n_replicas=64, betas=gpumc.geometric_ladder_betas(1.5, 3.5, 64),
-                                      engine=eng, record_capacity=64)
-    b = gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 128}, 12, model="ising",
-                                      n_replicas=32, betas=gpumc.geometric_ladder_betas(3.5, 5.5, 32),
-                                      engine=eng, record_capacity=64)
-    for m in (a, b):
-        m.pt_configure(10)
-        m.on_phase_start(_lib.PHASE_MEASUREMENT)
+    a, b = build(eng, measure=True)
     eng.sweep(10)
     a.observables()
     b.observables()
     steps = args.aux_steps
+    n0 = eng.launch_count()
     ms = time_sweeps(torch, eng, eng.stream_ptr(), steps, eng.sweep)
+    launches = (eng.launch_count() - n0) / 2  # time_sweeps runs the same count untimed first
     att = (64 * 512 * 512 + 32 * 128 ** 3) * float(steps)
     s1, acc1 = a.pt_stats()
     s2, acc2 = b.pt_stats()
@@ -292,10 +328,18 @@ def bench_pt(gpumc, torch, args):
         m.close()
     eng.close()
     v = att / (ms * 1e6)
-    return {"config": "PT 2D L=512x64 + 3D L=128x32, exchange every 10 sweeps, FP64 records",
-            "value": v, "unit": "spin-flip attempts/ns", "ms_per_sweep": ms / steps,
-            "hbm_frac_algorithmic": None, "pt_exchange_steps": [s1, s2],
-            "pt_accepted_swaps": [acc1, acc2]}
+    ms_t = autotune.time_workload(build, knobs, steps, 3, torch)
+    ms_a = autotune.time_workload(build, {}, steps, 3, torch)
+    out = {"config": "PT 2D L=512x64 + 3D L=128x32, exchange every 10 sweeps, FP64 records",
+           "value": v, "unit": "spin-flip attempts/ns", "ms_per_sweep": ms / steps,
+           "launches_per_sweep": launches / steps, "pt_exchange_steps": [s1, s2],
+           "pt_accepted_swaps": [acc1, acc2],
+           "tuned": {"knobs": knobs, "source": source, "value": att / (ms_t * steps * 1e6), "ms_per_sweep": ms_t,
+                     "analytic_value": att / (ms_a * steps * 1e6),
+                     "note": "tuned and analytic plans both measured without records (thermalization phase)"}}
+    if tuning is not None:
+        out["tuned"]["table"] = tuning["table"]
+    return out
 
 
 def bench_heat_bath(gpumc, torch, args):
@@ -418,11 +462,35 @@ def mixed_specs(seed=2024, n_potts=256, n_o3=32):
     return out
 
 
+MIX_WORKLOAD = "uneven mix: 256 2D Potts + 32 3D O(3) L=64"
+MIX_SPACE = {"potts_segments": [768, 1024, 2048, 3072], "o3_rows": [8, 12], "o3_planes": [4, 6, 12, 16]}
+PT_WORKLOAD = "PT: 2D Ising L=512 x64 + 3D Ising L=128 x32"
+PT_SPACE = {"ising3d_planes": [4, 6, 8, 16, 32], "ising2d_rows": [16, 32, 64]}
+
+
+def tuned_knobs(autotune, torch, args, workload, build, space):
+    """Tile knobs for a workload: the committed cache entry for this device,
+    or (--tune, or no entry) a live coordinate-descent tuning run."""
+    name = torch.cuda.get_device_name()
+    cache = autotune.TileCache()
+    knobs = cache.get(name, workload)
+    if knobs is not None and not args.tune:
+        return knobs, "cache (scamper_b200/tuned_tiles.json)", None
+    res = autotune.tune(build, space, sweeps=10, warm=3, torch=torch)
+    return res["knobs"], "tuned in this run", res
+
+
 def bench_mixed(gpumc, torch, args):
+    from scamper_b200 import autotune
     specs = mixed_specs()
+
+    def build(eng):
+        return [gpumc.ClassicalMC.from_params(p, 300 + i, model=m, engine=eng, record_capacity=8)
+                for i, (m, p, _) in enumerate(specs)]
+
+    knobs, source, tuning = tuned_knobs(autotune, torch, args, MIX_WORKLOAD, build, MIX_SPACE)
     eng = gpumc.Engine()
-    sims = [gpumc.ClassicalMC.from_params(p, 300 + i, model=m, engine=eng, record_capacity=8)
-            for i, (m, p, _) in enumerate(specs)]
+    sims = build(eng)
     eng.sweep(3)
     steps = args.aux_steps
     ms_b = time_sweeps(torch, eng, eng.stream_ptr(), steps, eng.sweep)
@@ -460,11 +528,21 @@ def bench_mixed(gpumc, torch, args):
     v_b = att / (ms_b * 1e6)
     v_p = (att_potts + att_o3) * plain_steps / (dt_plain * 1e9)
     bytes_per_sweep = att_potts * 2.0 + att_o3 * 24.0
-    return {"config": "256 2D Potts (q 2..4, L 32..2048 log-uniform) + 32 3D O(3) L=64, one launch "
-                      "per model kind per sweep", "value": v_b, "unit": "spin-flip attempts/ns",
-            "plain_value": v_p, "batched_over_plain": v_b / v_p, "by_kind": kinds,
-            "hbm_gbs_algorithmic": bytes_per_sweep * steps / (ms_b * 1e6),
-            "ms_per_sweep": ms_b / steps}
+    ms_t = autotune.time_workload(build, knobs, steps, 3, torch)
+    v_t = att / (ms_t * steps * 1e6)
+    peak, _ = measured_peak_hbm()
+    out = {"config": "256 2D Potts (q 2..4, L 32..2048 log-uniform) + 32 3D O(3) L=64, one launch "
+                     "per model kind per sweep", "value": v_b, "unit": "spin-flip attempts/ns",
+           "plain_value": v_p, "batched_over_plain": v_b / v_p, "by_kind": kinds,
+           "hbm_gbs_algorithmic": bytes_per_sweep * steps / (ms_b * 1e6),
+           "hbm_frac_algorithmic": bytes_per_sweep * steps / (ms_b * 1e6) / peak,
+           "ms_per_sweep": ms_b / steps,
+           "tuned": {"knobs": knobs, "source": source, "value": v_t, "ms_per_sweep": ms_t,
+                     "over_analytic": v_t / v_b, "tuned_over_plain": v_t / v_p,
+                     "hbm_frac_algorithmic": bytes_per_sweep / (ms_t * 1e6) / peak}}
+    if tuning is not None:
+        out["tuned"]["table"] = tuning["table"]
+    return out
 
 
 def bench_serving(gpumc, torch, args):
@@ -527,9 +605,55 @@ def bench_serving(gpumc, torch, args):
     return out
 
 
+def headline_config(world, args):
+    """The workload description both arms print (same dict, so the two lines
+    name the same configuration)."""
+    return {"workload": f"2D square Ising L={HEADLINE_L}, J=1, one lattice per beta in "
+                        f"{HEADLINE_BETAS}, single-site Metropolis sweeps, observables recorded every sweep",
+            "global_batch": len(HEADLINE_BETAS) * world, "sites_per_lattice": HEADLINE_L ** 2,
+            "sweeps_per_step": args.sweeps_per_step,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (2 x 3 x 64 MiB resident)"}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline (the reference's algorithm restated in C; bounded sample)
 # ---------------------------------------------------------------------------
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            return next((ln.split(":", 1)[1].strip() for ln in f if ln.startswith("model name")), "")
+    except OSError:
+        return ""
+
+
+def cpu_baseline_config1(args):
+    """The plain CPU configuration of the reference (2D Ising L=64, J=1,
+    beta=0.4407, hot start, 10^3 thermalization + 10^4 measured sweeps,
+    E/N and |M| measured every sweep) on the restated reference sampler:
+    one chain on one core, and one chain per core on every core (the
+    reference's Scheduler::run_parallel with its Rayon backend); plus the
+    restated MultiSpinIsing (64 replicas in one u64 word per site, one shared
+    visit order and stream, replica 0 extraction and exact energy per sweep,
+    the 64-replica measurement every sweep) on the same lattice."""
+    import oracle
+    oracle.build()
+    nproc = os.cpu_count() or 1
+    L, beta = 64, 0.4407
+    one = oracle.ref_run_parallel(oracle.ISING, (L, L), beta, 1, 1, 1, args.cpu1_therm, args.cpu1_meas)
+    allc = oracle.ref_run_parallel(oracle.ISING, (L, L), beta, 1, nproc, nproc, args.cpu1_therm, args.cpu1_meas)
+    msc = oracle.ref_msc_run((L, L), beta, 1, args.cpu1_msc_sweeps, measure=True)
+    return {"workload": f"2D Ising L={L}, J=1, beta={beta}, {args.cpu1_therm} thermalization + "
+                        f"{args.cpu1_meas} measured sweeps, E/N and |M| every sweep",
+            "single_core": one["attempts"] / (one["seconds"] * 1e9),
+            "all_cores": allc["attempts"] / (allc["seconds"] * 1e9), "cores": nproc,
+            "all_cores_chains": nproc, "mean_e_per_site": allc["mean_e"], "mean_abs_m": allc["mean_m"],
+            "msc_single_core": msc["attempts"] / (msc["seconds"] * 1e9),
+            "msc_sweeps": args.cpu1_msc_sweeps, "unit": "spin-flip attempts/ns",
+            "cpu_model": _cpu_model(), "kind": "port",
+            "seconds": {"single_core": one["seconds"], "all_cores": allc["seconds"], "msc": msc["seconds"]}}
+
+
 def cpu_baseline(args, threads=None):
     import oracle
     oracle.build()
@@ -541,16 +665,11 @@ def cpu_baseline(args, threads=None):
                                 cores, 0, args.cpu_sweeps)
     v = r["attempts"] / (r["seconds"] * 1e9)
     n_chains = len(HEADLINE_BETAS)
-    cpu_model = ""
-    try:
-        with open("/proc/cpuinfo") as f:
-            cpu_model = next((ln.split(":", 1)[1].strip() for ln in f if ln.startswith("model name")), "")
-    except OSError:
-        pass
     return {"value": v, "unit": "spin-flip attempts/ns", "cores": min(cores, n_chains),
-            "single_core_value": v / min(cores, n_chains), "nproc": os.cpu_count(), "cpu_model": cpu_model,
+            "single_core_value": v / min(cores, n_chains), "nproc": os.cpu_count(), "cpu_model": _cpu_model(),
             "kind": "port",
-            "sample": f"{len(HEADLINE_BETAS)} chains (one per beta) of 2D Ising L={L}, "
+            "sample": f"{len(HEADLINE_BETAS)} chains (one per beta, one thread each: the reference runs one "
+                      f"chain per task, so 3 chains use 3 cores) of 2D Ising L={L}, "
                       f"{args.cpu_sweeps} sweep(s) each, restated cmc-rs MetropolisCore "
                       f"(CSR, Fisher-Yates order, f64, log-space acceptance, |M| per sweep)",
             "seconds": r["seconds"]}
@@ -575,8 +694,7 @@ def run_reference(args):
             "unit": "spin-flip attempts/ns", "n_gpus": args.gpus, "steps": len(vals),
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (hot random start from seed)",
-            "config": {"workload": f"2D Ising L={args.cpu_L}, J=1, beta in {HEADLINE_BETAS}, "
-                                   "one chain per beta"},
+            "config": headline_config(args.gpus, args),
             "cpu_baseline": {"kind": out["kind"], "cores": out["cores"], "sample": out["sample"],
                              "value": v},
             "e2e": {"value": v, "unit": "spin-flip attempts/ns", "h2d_bytes_per_step": 0,
@@ -590,17 +708,24 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--sweeps-per-step", type=int, default=1000,
+                    help="sweeps of the three headline lattices in one step (the configured run: 10^3)")
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--aux-steps", type=int, default=100)
     ap.add_argument("--stream-steps", type=int, default=300,
                     help="sweeps timed on the streaming (per-sweep) kernel for roofline_streaming")
-    ap.add_argument("--e2e-sweeps", type=int, default=1000)
-    ap.add_argument("--e2e-calls", type=int, default=1)
+    ap.add_argument("--e2e-sweeps", type=int, default=None, help="default: --sweeps-per-step")
+    ap.add_argument("--e2e-calls", type=int, default=3)
     ap.add_argument("--cpu-L", type=int, default=HEADLINE_L)
     ap.add_argument("--cpu-sweeps", type=int, default=1)
+    ap.add_argument("--cpu1-therm", type=int, default=1000)
+    ap.add_argument("--cpu1-meas", type=int, default=10000)
+    ap.add_argument("--cpu1-msc-sweeps", type=int, default=300)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tune", action="store_true",
+                    help="tune the tile knobs of the mixed and PT workloads live instead of using the cache")
     ap.add_argument("--only-headline", action="store_true")
     ap.add_argument("--only", choices=["msc", "pt", "mixed", "serving", "heat_bath", "cluster", "o3_proposals"],
                     default=None,
@@ -613,6 +738,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.e2e_sweeps is None:
+        args.e2e_sweeps = args.sweeps_per_step
     if args.impl == "reference":
         return run_reference(args)
 
@@ -628,20 +755,55 @@ def main():
         return 0
     h = headline(gpumc, torch, args, dist, rank, world)
     value = h["attempts"] / (h["ms"] * 1e6)
+    n_sweeps = args.steps * args.sweeps_per_step
     peak, peak_kind = measured_peak_hbm()
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    sm_count = props.multi_processor_count
+    counters = profiled_counters()
     # dominant kernel: the resident (temporally blocked) kernel when the
     # sweeps ran as multi-sweep launches, else the streaming kernel
-    resident = h["launches"] < args.steps
-    sweeps_per_launch = args.steps / max(1, h["launches"])
+    resident = h["launches"] < n_sweeps
+    sweeps_per_launch = n_sweeps / max(1, h["launches"])
     per_launch_ms = h["ms"] / max(1, h["launches"])
-    alg_bytes_sweep = BYTES_PER_ATTEMPT["int8"] * h["attempts_rank"] / args.steps
+    alg_bytes_sweep = BYTES_PER_ATTEMPT["int8"] * h["attempts_rank"] / n_sweeps
     alg_bytes_launch = alg_bytes_sweep * sweeps_per_launch
-    achieved = alg_bytes_launch / (per_launch_ms * 1e6)  # GB/s
-    prof = profiled_traffic()
-    traffic = prof.get("k_sweep_ising_resident 2D Ising L=8192 x3, 64 sweeps per launch" if resident
-                       else "k_sweep_ising_bits<2> 2D Ising L=8192 x3")
+    achieved_hbm_equiv = alg_bytes_launch / (per_launch_ms * 1e6)  # GB/s
+    clock = h["clocks"].get("sm_mhz") or h["clocks"].get("sm_max_mhz") or 1965.0
+    rank_value = h["attempts_rank"] / (h["ms"] * 1e6)
     stream_ms = h["ms_stream"] / args.stream_steps
     stream_achieved = alg_bytes_sweep / (stream_ms * 1e6)
+    stream_value = h["attempts_rank"] / n_sweeps * args.stream_steps / (h["ms_stream"] * 1e6)
+    sc = counters.get(STREAMING_KEY, {})
+    roofline_streaming = {"bound": "hbm", "kernel": "k_sweep_ising_bits<2,0>", "value": stream_value,
+                          "achieved": stream_achieved, "peak": peak, "unit": "GB/s",
+                          "frac": stream_achieved / peak, "peak_source": peak_kind, "steps": args.stream_steps,
+                          "traffic": sc.get("dram_bytes"),
+                          "algorithmic_bytes_per_launch": alg_bytes_sweep,
+                          "note": "one launch per sweep: the int8 state read and written every sweep "
+                                  "(2 B per attempt), the honest HBM fraction of this workload"}
+    if resident:
+        rc = counters.get(RESIDENT_KEY, {})
+        # per-launch DRAM traffic of the captured 64-sweep launch, scaled to
+        # this run's sweeps per launch (the state moves once per launch, edge
+        # rows once per sweep)
+        traffic = None
+        if rc:
+            fixed = rc.get("dram_bytes_fixed", 0.0)
+            per_sweep = (rc["dram_bytes"] - fixed) / rc["sweeps"]
+            traffic = fixed + per_sweep * sweeps_per_launch
+        roofline = issue_roofline(counters, RESIDENT_KEY, rank_value, sm_count, clock) or {}
+        roofline.update({"kernel": "k_sweep_ising_resident<0>", "temporal_blocking": True,
+                         "traffic": traffic, "sweeps_per_launch": sweeps_per_launch,
+                         "hbm_equivalent": {"achieved": achieved_hbm_equiv, "peak": peak, "unit": "GB/s",
+                                            "frac": achieved_hbm_equiv / peak, "peak_source": peak_kind,
+                                            "algorithmic_bytes_per_launch": alg_bytes_launch},
+                         "note": "the resident kernel keeps the packed lattices in shared memory across the "
+                                 "sweeps of a launch (DRAM sees the int8 state once per launch plus edge "
+                                 "rows: traffic), so it is bound by integer instruction issue; "
+                                 "hbm_equivalent counts the 2 B/attempt a per-sweep kernel must move, and "
+                                 "roofline_streaming is the per-sweep kernel's HBM fraction"})
+    else:
+        roofline = dict(roofline_streaming)
     workloads = {}
     if rank == 0 and not args.only_headline:
         for name, fn in [("msc", bench_msc), ("pt", bench_pt), ("mixed", bench_mixed),
@@ -654,33 +816,18 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args)
+        cpu["config1"] = cpu_baseline_config1(args)
+    if isinstance(workloads.get("msc"), dict) and "value" in workloads["msc"]:
+        workloads["msc"]["roofline"] = issue_roofline(counters, MSC_KEY, workloads["msc"]["value"], sm_count, clock)
     line = {
         "metric": "spin-flip attempts/ns", "value": value, "unit": "spin-flip attempts/ns",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": h["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8",
         "data": "synthetic (hot random start from seed)",
-        "config": {"workload": f"2D square Ising L={HEADLINE_L}, J=1, one lattice per beta in "
-                               f"{HEADLINE_BETAS}, checkerboard sweeps, observables recorded every sweep",
-                   "global_batch": len(HEADLINE_BETAS) * world, "sites_per_lattice": HEADLINE_L ** 2,
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (2 x 3 x 64 MiB resident)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes_launch,
-                     "sweeps_per_launch": sweeps_per_launch,
-                     "kernel": "k_sweep_ising_resident" if resident else "k_sweep_ising_bits<2>",
-                     "temporal_blocking": resident,
-                     "note": ("achieved counts the 2 B/attempt a per-sweep formulation must move; the "
-                              "resident kernel keeps the packed lattice on chip between its sweeps, so its "
-                              "DRAM traffic (traffic) is the int8 state once per launch plus edge rows, and "
-                              "it is bound by integer issue, not HBM; roofline_streaming is the per-sweep "
-                              "kernel on the same workload") if resident else None},
-        "roofline_streaming": {"bound": "hbm", "kernel": "k_sweep_ising_bits<2>",
-                               "value": h["attempts_rank"] / args.steps * args.stream_steps / (h["ms_stream"] * 1e6),
-                               "achieved": stream_achieved, "peak": peak, "unit": "GB/s",
-                               "frac": stream_achieved / peak, "steps": args.stream_steps,
-                               "traffic": prof.get("k_sweep_ising_bits<2> 2D Ising L=8192 x3")},
+        "config": headline_config(world, args),
+        "roofline": roofline,
+        "roofline_streaming": roofline_streaming,
         "clocks": h["clocks"], "gpu_launches": h["launches"], "e2e": h["e2e"],
         "energy_cache_audit": h["audit_ok"], "workloads": workloads,
     }

@@ -160,7 +160,29 @@ int gpumc_engine_set_tile_refinement(gpumc_engine* eng, int32_t enable);
  * engine stream; off = all plans in sequence on the engine stream.  Both
  * give identical results. */
 int gpumc_engine_set_concurrent_kinds(gpumc_engine* eng, int32_t enable);
+/* Polls (128 ns apart) after which an inter-CTA wait of the resident Ising
+ * kernel (its per-sweep grid barrier, the wait for a PT exchange) gives up
+ * (default 2^22, about half a second; 0 = give up at the first unsuccessful
+ * poll).  A wait that gives up makes every CTA leave, the sweep call returns
+ * GPUMC_ECUDA, and the handles of that launch must be restored (spins, sweep
+ * count) before they continue: the failure path of a lost CTA, where the
+ * reference's sweep panics (CMC.rs/src/classical_mc.rs:181-184). */
+int gpumc_engine_set_wait_limit(gpumc_engine* eng, int64_t polls);
 int gpumc_tile_count(gpumc_sim* sim, int32_t* n_tiles);
+/* Tile knobs of the planner, for the autotuner (scamper_b200/autotune.py):
+ * 0 keeps the analytic choice, a positive value replaces it in every layout
+ * planned afterwards (simulations created, batches rebuilt): rows of the
+ * whole-row 2D Ising tiles, planes of the whole-plane 3D Ising tiles, packed
+ * 64-site segments per bit-sliced 2D Potts tile (at most 3072), planes per
+ * whole-plane 3D Potts tile, and the rows / planes of the O(3) z-march tiles.
+ * Results never depend on tiles (a colour pass reads only the other colour
+ * and every draw is keyed by site or segment).  Process-wide.  (The
+ * reference has no counterpart: its sweep is one CPU loop.) */
+typedef struct {
+  int32_t ising2d_rows, ising3d_planes, potts_segments, potts3d_planes, o3_rows, o3_planes;
+} gpumc_tile_knobs;
+int gpumc_set_tile_knobs(const gpumc_tile_knobs* knobs);
+int gpumc_get_tile_knobs(gpumc_tile_knobs* knobs);
 /* Kernel launches issued so far by gpumc_sweep of this handle / by
  * gpumc_engine_sweep of this engine (sweep, measurement and resident
  * launches; host copies excluded). */
@@ -216,6 +238,14 @@ int gpumc_recompute_energy(gpumc_sim* sim, double* energies);
  * (MultiSpinIsing::measure, CMC.rs/src/multi_spin.rs:220-286). */
 int gpumc_msc_replica_observables(gpumc_sim* sim, int32_t word_lattice, double* energy64,
                                   double* mag64);
+/* Periodic cache audit (should_audit_cache / audit_lattice_cache,
+ * CMC.rs/src/audit.rs:35-52, which the reference runs every 1024 completed
+ * sweeps in debug builds): after every `interval`-th completed sweep,
+ * gpumc_sweep and gpumc_engine_sweep compare each replica's cached energy with
+ * an exact recomputation (tolerance 1e-10 (1 + |exact|)) and return
+ * GPUMC_ESTATE with both values on a mismatch (the reference panics).  0 = off
+ * (default).  Not for server jobs. */
+int gpumc_set_audit_interval(gpumc_sim* sim, uint64_t interval);
 int gpumc_sweep_count(gpumc_sim* sim, uint64_t* out);
 /* O(3) proposal step of a replica: the cap half-angle (cap proposal) or the
  * rotation bound sigma (OPSS, OPSSStrategy::sigma). */
@@ -292,6 +322,18 @@ int gpumc_server_destroy(gpumc_server* srv);
 
 /* ---- diagnostics ------------------------------------------------------- */
 int gpumc_last_error(char* buf, size_t cap);
+/* Adds `delta` to a replica's cached energy (integer models: a whole number
+ * of J) without touching its spins: a host-made cache fault for testing the
+ * audit.  gpumc_set_spins or gpumc_change_parameter restores the cache. */
+int gpumc_perturb_energy_cache(gpumc_sim* sim, int32_t replica, double delta);
+/* Bounds-checked builds (libgpumc_bounds.so, compiled with
+ * -DGPUMC_DEBUG_BOUNDS): every checked global and shared-memory access of the
+ * sweep, cluster and lattice kernels that falls outside its buffer is
+ * skipped and counted.  Returns the violations counted since the last call
+ * (and clears them), the module (0 O(3) sweep, 1 Ising bits, 2 Potts bits,
+ * 3 int8 Potts, 4 multi-spin, 5 cluster, 6 lattice ops) and source line of
+ * the first, and compiled = 0 for a release library (no checks). */
+int gpumc_debug_bounds(uint64_t* hits, int32_t* first_module, int32_t* first_line, int32_t* compiled);
 /* Device Philox4x32-10 outputs for n (counter, key) pairs (4 + 2 words each). */
 int gpumc_philox_probe(const uint32_t* ctr4, const uint32_t* key2, uint32_t* out4, int32_t n);
 /* Bytes of device memory a spec needs (both ping-pong buffers, tables,

@@ -44,6 +44,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         sig = {
             "orc_philox4x32_10": (None, [_u32p, _u32p, _u32p]),
+            "orc_set_threads": (None, [_int]),
             "orc_stream_seed": (_u64, [_u64] * 8),
             "orc_replica_key": (_u64, [_u64, _u64, _u64]),
             "orc_exchange_key": (_u64, [_u64]),
@@ -75,6 +76,12 @@ def lib():
             "orc_sweep_o3_prop": (ctypes.c_double, [_int, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float,
                                                     ctypes.c_float, _int, _u64, _u64, _f32p, _f32p, _f32p, _i64p]),
             "orc_exp_neg": (ctypes.c_float, [ctypes.c_float]),
+            "orc_exp_neg2": (ctypes.c_float, [ctypes.c_float]),
+            "orc_unit23": (ctypes.c_float, [ctypes.c_uint32]),
+            "orc_half23": (ctypes.c_float, [ctypes.c_uint32]),
+            "orc_sincos23": (None, [ctypes.c_uint32, _f32p, _f32p]),
+            "orc_o3_fixed_observables": (None, [_int, _i64, _i64, _i64, ctypes.c_double, _f32p, _f32p, _f32p,
+                                                _f64p, _f64p]),
             "orc_sincos_turn": (None, [ctypes.c_uint32, _f32p, _f32p]),
             "orc_init_msc": (None, [_int, _i64, _i64, _i64, _u64, _int, _u64p]),
             "orc_sweep_msc": (None, [_int, _i64, _i64, _i64, _u32p, _u64p, _u64, _u64, _u64p, _i64p]),
@@ -87,6 +94,7 @@ def lib():
             "orc_ref_sweep": (None, [ctypes.c_void_p, _int]),
             "orc_ref_measure": (None, [ctypes.c_void_p, _f64p, _f64p]),
             "orc_ref_recompute_energy": (ctypes.c_double, [ctypes.c_void_p]),
+            "orc_ref_series": (None, [ctypes.c_void_p, _int, _int, _f64p, _f64p]),
             "orc_ref_set_beta": (None, [ctypes.c_void_p, ctypes.c_double]),
             "orc_ref_n_sites": (_i64, [ctypes.c_void_p]),
             "orc_ref_run_parallel": (ctypes.c_double, [_int, _int, _i64, _i64, _i64, _int,
@@ -101,6 +109,12 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def set_threads(n):
+    """Threads of the discrete and multi-spin replays (same results for any
+    count)."""
+    lib().orc_set_threads(int(n))
 
 
 def _p(a, t):
@@ -251,6 +265,15 @@ class Lattice:
         e, m = self.msc_observables()
         return float(e.sum())
 
+    def fixed_observables(self):
+        """O(3): (energy, magnetisation vector) as the sweep kernels record
+        them (fixed-point sums of the fp32 configuration)."""
+        e = ctypes.c_double()
+        m = np.zeros(3, dtype=np.float64)
+        lib().orc_o3_fixed_observables(self.dims, self.lx, self.ly, self.lz, self.J, _p(self.sx, _f32p),
+                                       _p(self.sy, _f32p), _p(self.sz, _f32p), ctypes.byref(e), _p(m, _f64p))
+        return e.value, m
+
     def cached_energy(self):
         if self.model in (ISING, POTTS):
             return self.J * self.e_int
@@ -315,6 +338,14 @@ class RefSampler:
 
     def recompute_energy(self):
         return lib().orc_ref_recompute_energy(self.h)
+
+    def series(self, therm, meas):
+        """therm sweeps, then meas measured sweeps: (E/N, |M|) per sweep.  The
+        C call releases the GIL, so chains can run on Python threads."""
+        e = np.zeros(meas, dtype=np.float64)
+        m = np.zeros(meas, dtype=np.float64)
+        lib().orc_ref_series(self.h, therm, meas, _p(e, _f64p), _p(m, _f64p))
+        return e, m
 
     def set_beta(self, beta):
         lib().orc_ref_set_beta(self.h, beta)

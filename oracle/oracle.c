@@ -20,6 +20,7 @@
  */
 #include "oracle.h"
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -147,6 +148,57 @@ int orc_build_table_hb(int model, int dims, double J, double beta, uint32_t* hea
         orc_threshold(p, &head[k], &tail[k]);
     }
     return n;
+}
+
+/* ------------------------------------------------------------------------ */
+/* row-parallel colour passes                                                */
+/* ------------------------------------------------------------------------ */
+/* Within one checkerboard colour every site reads only sites of the other
+ * colour and writes only itself, and every draw is keyed by site or row
+ * segment, so the rows of a colour pass can be split across threads without
+ * changing any result (integer sums are order-free).  orc_set_threads sets
+ * the thread count of the discrete and multi-spin replays (default 1). */
+static int g_threads = 1;
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+
+typedef void (*rows_fn)(void* ctx, uint32_t colour, int64_t r0, int64_t r1, int64_t* dE,
+                        int64_t* acc);
+typedef struct {
+    rows_fn fn;
+    void* ctx;
+    uint32_t colour;
+    int64_t r0, r1, dE, acc;
+} rows_job;
+
+static void* rows_worker(void* p) {
+    rows_job* j = (rows_job*)p;
+    j->fn(j->ctx, j->colour, j->r0, j->r1, &j->dE, &j->acc);
+    return NULL;
+}
+
+static void run_rows(rows_fn fn, void* ctx, uint32_t colour, int64_t nrows, int64_t* dE,
+                     int64_t* acc) {
+    int nt = g_threads;
+    if (nt > nrows) nt = (int)nrows;
+    if (nt <= 1) {
+        int64_t d = 0, a = 0;
+        fn(ctx, colour, 0, nrows, &d, &a);
+        *dE += d;
+        *acc += a;
+        return;
+    }
+    rows_job jobs[256];
+    pthread_t th[256];
+    for (int t = 0; t < nt; ++t) {
+        rows_job j = {fn, ctx, colour, nrows * t / nt, nrows * (t + 1) / nt, 0, 0};
+        jobs[t] = j;
+        pthread_create(&th[t], NULL, rows_worker, &jobs[t]);
+    }
+    for (int t = 0; t < nt; ++t) {
+        pthread_join(th[t], NULL);
+        *dE += jobs[t].dE;
+        *acc += jobs[t].acc;
+    }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -356,70 +408,100 @@ void orc_init_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t lz, 
     }
 }
 
+typedef struct {
+    int model, q, zc, potts_bits;
+    geom g;
+    const uint32_t* head;
+    const uint64_t* tail;
+    uint32_t key[2];
+    uint64_t sweep;
+    int8_t* spins;
+} discrete_ctx;
+
+static void discrete_rows(void* p, uint32_t colour, int64_t r0, int64_t r1, int64_t* dE_out,
+                          int64_t* acc_out) {
+    const discrete_ctx* c = (const discrete_ctx*)p;
+    const geom* g = &c->g;
+    const int model = c->model, q = c->q, zc = c->zc;
+    const uint32_t* head = c->head;
+    const uint64_t* tail = c->tail;
+    const uint32_t* key = c->key;
+    const uint64_t sweep = c->sweep;
+    int8_t* spins = c->spins;
+    int64_t dE = 0, acc = 0;
+    for (int64_t rho = r0; rho < r1; ++rho) {
+        const int64_t z = rho / g->ly, y = rho % g->ly;
+        for (int64_t x = 0; x < g->lx; ++x) {
+            if ((uint32_t)((x + y + z) & 1) != colour) continue;
+            int64_t site = site_of(g, x, y, z);
+            int64_t nb[6];
+            int nn = neighbours(g, x, y, z, nb);
+            int8_t s = spins[site];
+            if (model == ORC_ISING) {
+                int k = 0;
+                for (int i = 0; i < nn; ++i) k += spins[nb[i]] != s;
+                if (accept_bits(g, x, y, z, head[k], tail[k], colour, key, sweep)) {
+                    spins[site] = (int8_t)-s;
+                    dE += 2 * (zc - 2 * k);
+                    ++acc;
+                }
+            } else if (c->potts_bits) {
+                uint32_t v = potts_bits_proposal(g, x, y, z, q, colour, key, sweep);
+                int8_t t = (int8_t)((int)v < s ? (int)v : (int)v + 1);
+                int nold = 0, nnew = 0;
+                for (int i = 0; i < nn; ++i) {
+                    nold += spins[nb[i]] == s;
+                    nnew += spins[nb[i]] == t;
+                }
+                int d = nnew - nold;
+                if (potts_bits_accept(g, x, y, z, head[d + zc], tail[d + zc], colour, key, sweep)) {
+                    spins[site] = t;
+                    dE += -d;
+                    ++acc;
+                }
+            } else {
+                uint32_t u = chunk_u16(g, x, y, z, colour, ORC_TAG_ACC, key, sweep);
+                uint32_t pu = chunk_u16(g, x, y, z, colour, ORC_TAG_PROP, key, sweep);
+                uint32_t r = potts_draw(pu, (uint32_t)(q - 1), (uint64_t)site, colour, key, sweep);
+                int8_t t = (int8_t)((int)r < s ? (int)r : (int)r + 1);
+                int nold = 0, nnew = 0;
+                for (int i = 0; i < nn; ++i) {
+                    nold += spins[nb[i]] == s;
+                    nnew += spins[nb[i]] == t;
+                }
+                int d = nnew - nold;
+                if (accept_discrete(u, head[d + zc], tail[d + zc], (uint64_t)site, colour, key, sweep)) {
+                    spins[site] = t;
+                    dE += -d;
+                    ++acc;
+                }
+            }
+        }
+    }
+    *dE_out = dE;
+    *acc_out = acc;
+}
+
 int64_t orc_sweep_discrete(int model, int dims, int64_t lx, int64_t ly, int64_t lz, int q,
                            const uint32_t* head, const uint64_t* tail, uint64_t key64,
                            uint64_t sweep, int8_t* spins, int64_t* accepted) {
+    discrete_ctx c;
     geom g = {dims, lx, ly, dims == 3 ? lz : 1};
-    int zc = 2 * dims;
-    uint32_t key[2];
-    key_of(key64, key);
-    int64_t dE = 0, acc = 0;
+    c.model = model;
+    c.q = q;
+    c.zc = 2 * dims;
     /* Potts on bit planes when q <= 4 and rows are at most 128 segments of 64
      * sites or a whole number of segments; else the 16-bit chunk method */
-    int potts_bits = q <= 4 && ((lx + 63) / 64 <= 128 || lx % 64 == 0);
-    for (uint32_t colour = 0; colour < 2; ++colour) {
-        for (int64_t z = 0; z < g.lz; ++z)
-            for (int64_t y = 0; y < g.ly; ++y)
-                for (int64_t x = 0; x < g.lx; ++x) {
-                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
-                    int64_t site = site_of(&g, x, y, z);
-                    int64_t nb[6];
-                    int nn = neighbours(&g, x, y, z, nb);
-                    int8_t s = spins[site];
-                    if (model == ORC_ISING) {
-                        int k = 0;
-                        for (int i = 0; i < nn; ++i) k += spins[nb[i]] != s;
-                        if (accept_bits(&g, x, y, z, head[k], tail[k], colour, key, sweep)) {
-                            spins[site] = (int8_t)-s;
-                            dE += 2 * (zc - 2 * k);
-                            ++acc;
-                        }
-                    } else if (potts_bits) {
-                        uint32_t v = potts_bits_proposal(&g, x, y, z, q, colour, key, sweep);
-                        int8_t t = (int8_t)((int)v < s ? (int)v : (int)v + 1);
-                        int nold = 0, nnew = 0;
-                        for (int i = 0; i < nn; ++i) {
-                            nold += spins[nb[i]] == s;
-                            nnew += spins[nb[i]] == t;
-                        }
-                        int d = nnew - nold;
-                        if (potts_bits_accept(&g, x, y, z, head[d + zc], tail[d + zc], colour, key,
-                                              sweep)) {
-                            spins[site] = t;
-                            dE += -d;
-                            ++acc;
-                        }
-                    } else {
-                        uint32_t u = chunk_u16(&g, x, y, z, colour, ORC_TAG_ACC, key, sweep);
-                        uint32_t pu = chunk_u16(&g, x, y, z, colour, ORC_TAG_PROP, key, sweep);
-                        uint32_t r = potts_draw(pu, (uint32_t)(q - 1), (uint64_t)site, colour, key,
-                                                sweep);
-                        int8_t t = (int8_t)((int)r < s ? (int)r : (int)r + 1);
-                        int nold = 0, nnew = 0;
-                        for (int i = 0; i < nn; ++i) {
-                            nold += spins[nb[i]] == s;
-                            nnew += spins[nb[i]] == t;
-                        }
-                        int d = nnew - nold;
-                        if (accept_discrete(u, head[d + zc], tail[d + zc], (uint64_t)site,
-                                            colour, key, sweep)) {
-                            spins[site] = t;
-                            dE += -d;
-                            ++acc;
-                        }
-                    }
-                }
-    }
+    c.potts_bits = q <= 4 && ((lx + 63) / 64 <= 128 || lx % 64 == 0);
+    c.g = g;
+    c.head = head;
+    c.tail = tail;
+    key_of(key64, c.key);
+    c.sweep = sweep;
+    c.spins = spins;
+    int64_t dE = 0, acc = 0;
+    for (uint32_t colour = 0; colour < 2; ++colour)
+        run_rows(discrete_rows, &c, colour, g.ly * g.lz, &dE, &acc);
     if (accepted) *accepted = acc;
     return dE;
 }
@@ -723,10 +805,162 @@ double orc_sweep_o3(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float
     return orc_sweep_o3_prop(dims, lx, ly, lz, J, beta, omc, 0, key64, sweep, sx, sy, sz, accepted);
 }
 
-static void o3_newton(float* px, float* py, float* pz) {
-    float n2 = (*px * *px + *py * *py) + *pz * *pz;
-    float f = 1.5f - 0.5f * n2;
+/* ---- O(3) Metropolis arithmetic of the sweep kernels ----------------------
+ * Uniforms are built from bits, not by integer-to-float conversion:
+ * unit23(u) = 1.m - 1 with the top 23 bits of u as m (multiples of 2^-23 in
+ * [0, 1)), half23(u) = unit23(u) + 2^-24 (in (0, 1)); both exact.  Products
+ * are fused where the kernel fuses them (fmaf: one rounding, as the device's
+ * fma.rn), every other operation is one IEEE rounding. */
+static inline float bits_f(uint32_t b) { float f; memcpy(&f, &b, 4); return f; }
+static inline uint32_t f_bits(float f) { uint32_t b; memcpy(&b, &f, 4); return b; }
+float orc_unit23(uint32_t u) { return bits_f(0x3F800000u | (u >> 9)) - 1.0f; }
+float orc_half23(uint32_t u) { return bits_f(0x3F800000u | (u >> 9)) - 0x1.fffffep-1f; }
+
+/* (cos, sin) of 2 pi u / 2^32: octant from the top 3 bits, the next 23 bits
+ * as the fraction t of the octant, Taylor polynomials of degree 9 / 10 on
+ * [0, pi/4] (Horner, fused), swaps and signs by octant. */
+void orc_sincos23(uint32_t u, float* c, float* s) {
+    uint32_t octant = u >> 29;
+    float t = bits_f(0x3F800000u | ((u >> 6) & 0x7FFFFFu)) - 1.0f;
+    if (octant & 1u) t = 1.0f - t;
+    float th = t * 0x1.921fb6p-1f;          /* pi / 4 */
+    float t2 = th * th;
+    float sp = 0x1.71de3ap-19f;
+    sp = fmaf(sp, t2, -0x1.a01a02p-13f);
+    sp = fmaf(sp, t2, 0x1.111112p-7f);
+    sp = fmaf(sp, t2, -0x1.555556p-3f);
+    sp = fmaf(sp, t2, 1.0f);
+    float sn = th * sp;
+    float cp = -0x1.27e4fcp-22f;
+    cp = fmaf(cp, t2, 0x1.a01a02p-16f);
+    cp = fmaf(cp, t2, -0x1.6c16c2p-10f);
+    cp = fmaf(cp, t2, 0x1.555556p-5f);
+    cp = fmaf(cp, t2, -0.5f);
+    float cs = fmaf(cp, t2, 1.0f);
+    int sw = ((octant + 1u) & 2u) != 0u;
+    float a = sw ? sn : cs, b = sw ? cs : sn;
+    *c = ((octant + 2u) & 4u) ? -a : a;
+    *s = (octant & 4u) ? -b : b;
+}
+
+/* exp(x) for -87 <= x <= 0 (smaller x are clamped to -87, where the result is
+ * below every acceptance draw): x log2(e) = n + f with n = rint by the
+ * 1.5 * 2^23 shifter, f in [-1/2, 1/2], e^(f ln 2) by the degree-7 Taylor
+ * polynomial (fused Horner), times 2^n. */
+float orc_exp_neg2(float x) {
+    if (x < -87.0f) x = -87.0f;
+    float y = x * 0x1.715476p+0f;
+    float r = y + 0x1.8p23f;
+    float n = r - 0x1.8p23f;
+    int ni = (int)f_bits(r) - 0x4B400000;
+    float t = (y - n) * 0x1.62e430p-1f;
+    float p = 0x1.a01a02p-13f;
+    p = fmaf(p, t, 0x1.6c16c2p-10f);
+    p = fmaf(p, t, 0x1.111112p-7f);
+    p = fmaf(p, t, 0x1.555556p-5f);
+    p = fmaf(p, t, 0x1.555556p-3f);
+    p = fmaf(p, t, 0.5f);
+    p = fmaf(p, t, 1.0f);
+    p = fmaf(p, t, 1.0f);
+    return p * bits_f((uint32_t)(ni + 127) << 23);
+}
+
+static void o3_renorm2(float* px, float* py, float* pz) {
+    float n2 = fmaf(*pz, *pz, fmaf(*py, *py, *px * *px));
+    float f = fmaf(-0.5f, n2, 1.5f);
     *px = *px * f; *py = *py * f; *pz = *pz * f;
+}
+
+/* Proposal of the Metropolis step from the site's draw o: 0 the cap of
+ * 1 - cos(alpha) = omc around a (Duff et al. 2017 basis), 1 a uniform unit
+ * vector (StandardStrategy), 2 a rotation by theta = omc (2u - 1) in plane
+ * floor(3 o0 / 2^32) (OPSSStrategy). */
+void orc_o3_propose(int prop, float ax, float ay, float az, const uint32_t o[4], float omc,
+                    float* nx, float* ny, float* nz) {
+    float px, py, pz;
+    if (prop == 0) {
+        float w = orc_unit23(o[0]) * omc;
+        float ct = 1.0f - w;
+        float st = sqrtf(fmaf(-w, w, w + w));
+        float cp, sp;
+        orc_sincos23(o[1], &cp, &sp);
+        float vx = st * cp, vy = st * sp;
+        float sg = az >= 0.0f ? 1.0f : -1.0f;
+        float k = -1.0f / (sg + az);
+        float axk = ax * k;
+        float b = ay * axk;
+        float sax = sg * ax;
+        float e1x = fmaf(sax, axk, 1.0f), e1y = sg * b, e1z = -sax;
+        float e2x = b, e2y = fmaf(ay * k, ay, sg), e2z = -ay;
+        px = fmaf(ct, ax, fmaf(vy, e2x, vx * e1x));
+        py = fmaf(ct, ay, fmaf(vy, e2y, vx * e1y));
+        pz = fmaf(ct, az, fmaf(vy, e2z, vx * e1z));
+    } else if (prop == 1) {
+        pz = fmaf(-2.0f, orc_unit23(o[0]), 1.0f);
+        float rho = sqrtf(fmaf(-pz, pz, 1.0f));
+        float cp, sp;
+        orc_sincos23(o[1], &cp, &sp);
+        px = rho * cp;
+        py = rho * sp;
+    } else {
+        uint32_t plane = (uint32_t)(((uint64_t)o[0] * 3u) >> 32);
+        float theta = omc * fmaf(2.0f, orc_half23(o[1]), -1.0f);
+        float turns = theta * 0x1.45f306p-3f;
+        uint32_t tu = (uint32_t)(int64_t)llrintf(turns * 0x1p32f);
+        float c, sn;
+        orc_sincos23(tu, &c, &sn);
+        float a0 = plane == 0 ? ax : (plane == 1 ? ay : az);
+        float a1 = plane == 0 ? ay : (plane == 1 ? az : ax);
+        float r0 = fmaf(c, a0, -(sn * a1)), r1 = fmaf(sn, a0, c * a1);
+        px = plane == 0 ? r0 : (plane == 1 ? ax : r1);
+        py = plane == 0 ? r1 : (plane == 1 ? r0 : ay);
+        pz = plane == 0 ? az : (plane == 1 ? r1 : r0);
+    }
+    o3_renorm2(&px, &py, &pz);
+    *nx = px; *ny = py; *nz = pz;
+}
+
+/* Decision: dE = -J (p - a) . h (fused); accept when dE <= 0, else when
+ * half23(o2) < exp(-beta dE). */
+int orc_o3_accept(float ax, float ay, float az, float px, float py, float pz, float hx, float hy,
+                  float hz, float mJ, float beta, uint32_t o2) {
+    float dot = fmaf(pz - az, hz, fmaf(py - ay, hy, (px - ax) * hx));
+    float de = mJ * dot;
+    if (de <= 0.0f) return 1;
+    return orc_half23(o2) < orc_exp_neg2(-(beta * de));
+}
+
+/* Fixed-point observables of an O(3) configuration as the sweep kernels
+ * accumulate them: every site's components as rint(s 2^21), and for every
+ * site of colour 1 the bond sum rint(2^19 s . h) with h its fp32 neighbour
+ * sum (order x-1, x+1, y-1, y+1, z-1, z+1) and the dot fused; integer sums,
+ * so the order of accumulation does not matter.  Every bond has exactly one
+ * colour-1 end: energy = -J 2^-19 sum. */
+void orc_o3_fixed_observables(int dims, int64_t lx, int64_t ly, int64_t lz, double J, const float* sx,
+                              const float* sy, const float* sz, double* energy, double m[3]) {
+    geom g = {dims, lx, ly, dims == 3 ? lz : 1};
+    int64_t eq = 0, mq[3] = {0, 0, 0};
+    for (int64_t z = 0; z < g.lz; ++z)
+        for (int64_t y = 0; y < g.ly; ++y)
+            for (int64_t x = 0; x < g.lx; ++x) {
+                int64_t site = site_of(&g, x, y, z);
+                float v[3] = {sx[site], sy[site], sz[site]};
+                for (int c = 0; c < 3; ++c)
+                    mq[c] += (int32_t)(f_bits(fmaf(v[c], 0x1p21f, 0x1.8p23f)) - 0x4B400000u);
+                if (((x + y + z) & 1) != 1) continue;
+                int64_t nb[6];
+                int nn = neighbours(&g, x, y, z, nb);
+                float hx = sx[nb[0]], hy = sy[nb[0]], hz = sz[nb[0]];
+                for (int i = 1; i < nn; ++i) {
+                    hx = hx + sx[nb[i]];
+                    hy = hy + sy[nb[i]];
+                    hz = hz + sz[nb[i]];
+                }
+                float e = fmaf(v[2], hz, fmaf(v[1], hy, v[0] * hx));
+                eq += (int32_t)(f_bits(fmaf(e, 0x1p19f, 0x1.8p23f)) - 0x4B400000u);
+            }
+    *energy = -J * ((double)eq * 0x1p-19);
+    for (int c = 0; c < 3; ++c) m[c] = (double)mq[c] * 0x1p-21;
 }
 
 double orc_sweep_o3_prop(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
@@ -757,66 +991,10 @@ double orc_sweep_o3_prop(int dims, int64_t lx, int64_t ly, int64_t lz, float J, 
                     make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_O3, 0, sweep);
                     orc_philox4x32_10(ctr, key, o);
                     float nx, ny, nz;
-                    if (prop == 0) {
-                        float w = ((float)(o[0] >> 8) * 0x1p-24f) * omc;
-                        float ct = 1.0f - w;
-                        float st = sqrtf(w * (2.0f - w));
-                        float cp, sp;
-                        orc_sincos_turn(o[1], &cp, &sp);
-                        /* cap sample through the Duff et al. (2017) orthonormal basis */
-                        float vx = st * cp, vy = st * sp;
-                        float sg = az >= 0.0f ? 1.0f : -1.0f;
-                        float k = -1.0f / (sg + az);
-                        float b = (ax * ay) * k;
-                        float e1x = 1.0f + (sg * (ax * ax)) * k;
-                        float e1y = sg * b;
-                        float e1z = -(sg * ax);
-                        float e2x = b;
-                        float e2y = sg + (ay * ay) * k;
-                        float e2z = -ay;
-                        nx = (vx * e1x + vy * e2x) + ct * ax;
-                        ny = (vx * e1y + vy * e2y) + ct * ay;
-                        nz = (vx * e1z + vy * e2z) + ct * az;
-                        o3_newton(&nx, &ny, &nz);   /* one Newton step of 1/sqrt(n2) from 1 */
-                    } else if (prop == 1) {
-                        /* StandardStrategy: a uniform unit vector */
-                        nz = 1.0f - 2.0f * ((float)(o[0] >> 8) * 0x1p-24f);
-                        float rho = sqrtf((1.0f - nz) * (1.0f + nz));
-                        float cp, sp;
-                        orc_sincos_turn(o[1], &cp, &sp);
-                        nx = rho * cp;
-                        ny = rho * sp;
-                        o3_newton(&nx, &ny, &nz);
-                    } else {
-                        /* OPSSStrategy: rotation by theta in (-sigma, sigma) in
-                         * plane floor(3 w0 / 2^32) of (x,y), (y,z), (z,x) */
-                        uint32_t plane = (uint32_t)(((uint64_t)o[0] * 3u) >> 32);
-                        float u = ((float)(o[1] >> 8) + 0.5f) * 0x1p-24f;
-                        float theta = omc * (2.0f * u - 1.0f);
-                        float turns = theta * 0x1.45f306p-3f;
-                        uint32_t tu = (uint32_t)(int64_t)llrintf(turns * 0x1p32f);
-                        float c, s;
-                        orc_sincos_turn(tu, &c, &s);
-                        float a0 = plane == 0 ? ax : (plane == 1 ? ay : az);
-                        float a1 = plane == 0 ? ay : (plane == 1 ? az : ax);
-                        float r0 = c * a0 - s * a1, r1 = s * a0 + c * a1;
-                        nx = plane == 0 ? r0 : (plane == 1 ? ax : r1);
-                        ny = plane == 0 ? r1 : (plane == 1 ? r0 : ay);
-                        nz = plane == 0 ? az : (plane == 1 ? r1 : r0);
-                        o3_newton(&nx, &ny, &nz);
-                    }
-                    float dot = ((nx - ax) * hx + (ny - ay) * hy) + (nz - az) * hz;
-                    float dE = mJ * dot;
-                    int ok;
-                    if (dE <= 0.0f) {
-                        ok = 1;
-                    } else {
-                        float p = orc_exp_neg(-(beta * dE));
-                        float u = ((float)(o[2] >> 8) + 0.5f) * 0x1p-24f;
-                        ok = u < p;
-                    }
-                    if (ok) {
-                        /* energy cache: exact fp64 change of the fp32 configuration */
+                    orc_o3_propose(prop, ax, ay, az, o, omc, &nx, &ny, &nz);
+                    if (orc_o3_accept(ax, ay, az, nx, ny, nz, hx, hy, hz, mJ, beta, o[2])) {
+                        /* the reference's energy cache: exact fp64 change of
+                         * the fp32 configuration */
                         double hxd = 0.0, hyd = 0.0, hzd = 0.0;
                         for (int i = 0; i < nn; ++i) {
                             hxd += (double)sx[nb[i]];
@@ -1128,49 +1306,78 @@ static int t_bit(uint32_t head, uint64_t tail, int j) {
     return j < 16 ? (int)((head >> (15 - j)) & 1u) : (int)((tail >> (79 - j)) & 1u);
 }
 
+typedef struct {
+    geom g;
+    const uint32_t* head;
+    const uint64_t* tail;
+    uint32_t key[2];
+    uint64_t sweep;
+    uint64_t* words;
+} msc_ctx;
+
+static void msc_rows(void* p, uint32_t colour, int64_t r0, int64_t r1, int64_t* dE_out,
+                     int64_t* acc_out) {
+    const msc_ctx* c = (const msc_ctx*)p;
+    const geom* g = &c->g;
+    const uint32_t* head = c->head;
+    const uint64_t* tail = c->tail;
+    const uint32_t* key = c->key;
+    const uint64_t sweep = c->sweep;
+    uint64_t* words = c->words;
+    int64_t acc = 0;
+    for (int64_t rho = r0; rho < r1; ++rho) {
+        const int64_t z = rho / g->ly, y = rho % g->ly;
+        for (int64_t x = 0; x < g->lx; ++x) {
+            if ((uint32_t)((x + y + z) & 1) != colour) continue;
+            int64_t site = site_of(g, x, y, z);
+            int64_t nb[6];
+            int nn = neighbours(g, x, y, z, nb);
+            uint64_t w = words[site];
+            uint64_t planes[80];
+            int have = 0;
+            uint64_t flip = 0;
+            for (int r = 0; r < 64; ++r) {
+                int k = 0;
+                for (int i = 0; i < nn; ++i) k += (int)(((w ^ words[nb[i]]) >> r) & 1u);
+                if (head[k] >= 65536u) { flip |= 1ull << r; continue; }
+                int decided = 0, less = 0;
+                for (int j = 0; j < 80 && !decided; ++j) {
+                    while (have <= j) {
+                        uint32_t ctr[4], out[4];
+                        make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_MSC, (uint32_t)(have >> 1), sweep);
+                        orc_philox4x32_10(ctr, key, out);
+                        planes[have] = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
+                        planes[have + 1] = (uint64_t)out[2] | ((uint64_t)out[3] << 32);
+                        have += 2;
+                    }
+                    int ub = (int)((planes[j] >> r) & 1u);
+                    int tb = t_bit(head[k], tail[k], j);
+                    if (ub != tb) { decided = 1; less = ub < tb; }
+                }
+                if (less) flip |= 1ull << r;
+            }
+            words[site] = w ^ flip;
+            acc += __builtin_popcountll(flip);
+        }
+    }
+    *dE_out = 0;
+    *acc_out = acc;
+}
+
 void orc_sweep_msc(int dims, int64_t lx, int64_t ly, int64_t lz, const uint32_t* head,
                    const uint64_t* tail, uint64_t key64, uint64_t sweep, uint64_t* words,
                    int64_t* accepted) {
+    msc_ctx c;
     geom g = {dims, lx, ly, dims == 3 ? lz : 1};
-    uint32_t key[2];
-    key_of(key64, key);
-    int64_t acc = 0;
+    c.g = g;
+    c.head = head;
+    c.tail = tail;
+    key_of(key64, c.key);
+    c.sweep = sweep;
+    c.words = words;
+    int64_t dE = 0, acc = 0;
     for (uint32_t colour = 0; colour < 2; ++colour)
-        for (int64_t z = 0; z < g.lz; ++z)
-            for (int64_t y = 0; y < g.ly; ++y)
-                for (int64_t x = 0; x < g.lx; ++x) {
-                    if ((uint32_t)((x + y + z) & 1) != colour) continue;
-                    int64_t site = site_of(&g, x, y, z);
-                    int64_t nb[6];
-                    int nn = neighbours(&g, x, y, z, nb);
-                    uint64_t w = words[site];
-                    uint64_t planes[80];
-                    int have = 0;
-                    uint64_t flip = 0;
-                    for (int r = 0; r < 64; ++r) {
-                        int k = 0;
-                        for (int i = 0; i < nn; ++i) k += (int)(((w ^ words[nb[i]]) >> r) & 1u);
-                        if (head[k] >= 65536u) { flip |= 1ull << r; continue; }
-                        int decided = 0, less = 0;
-                        for (int j = 0; j < 80 && !decided; ++j) {
-                            while (have <= j) {
-                                uint32_t ctr[4], out[4];
-                                make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_MSC,
-                                         (uint32_t)(have >> 1), sweep);
-                                orc_philox4x32_10(ctr, key, out);
-                                planes[have] = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
-                                planes[have + 1] = (uint64_t)out[2] | ((uint64_t)out[3] << 32);
-                                have += 2;
-                            }
-                            int ub = (int)((planes[j] >> r) & 1u);
-                            int tb = t_bit(head[k], tail[k], j);
-                            if (ub != tb) { decided = 1; less = ub < tb; }
-                        }
-                        if (less) flip |= 1ull << r;
-                    }
-                    words[site] = w ^ flip;
-                    acc += __builtin_popcountll(flip);
-                }
+        run_rows(msc_rows, &c, colour, g.ly * g.lz, &dE, &acc);
     if (accepted) *accepted = acc;
 }
 

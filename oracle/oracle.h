@@ -54,6 +54,10 @@ enum {
 /* Substream ids used with RngStreamKey::with_substream. */
 enum { ORC_SUB_INIT = 0, ORC_SUB_SWEEP = 1 };
 
+/* Threads of the discrete and multi-spin replays (rows of a colour pass are
+ * split; results do not depend on the count).  Default 1. */
+void orc_set_threads(int n);
+
 /* --- RNG ---------------------------------------------------------------- */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 uint64_t orc_stream_seed(uint64_t base_seed, uint64_t task, uint64_t run, uint64_t chain,
@@ -138,6 +142,20 @@ float orc_log_one_minus(float y);
 /* O(3) Metropolis with proposal prop: 0 the cap (omc = 1 - cos(alpha)), 1
  * StandardStrategy's uniform unit vector, 2 OPSSStrategy's plane rotation
  * (omc = sigma); CMC.rs/src/lattice/proposal.rs:45-167. */
+/* O(3) Metropolis arithmetic of the sweep kernels (bit-identical): 23-bit
+ * uniforms from bits, (cos, sin) of a turn, exp(x) for x <= 0, the proposal
+ * and the decision of one site, and the fixed-point observables (energy from
+ * colour-1 bond sums at 2^-19, magnetisation components at 2^-21). */
+float orc_unit23(uint32_t u);
+float orc_half23(uint32_t u);
+void orc_sincos23(uint32_t u, float* c, float* s);
+float orc_exp_neg2(float x);
+void orc_o3_propose(int prop, float ax, float ay, float az, const uint32_t o[4], float omc,
+                    float* nx, float* ny, float* nz);
+int orc_o3_accept(float ax, float ay, float az, float px, float py, float pz, float hx, float hy,
+                  float hz, float mJ, float beta, uint32_t o2);
+void orc_o3_fixed_observables(int dims, int64_t lx, int64_t ly, int64_t lz, double J, const float* sx,
+                              const float* sy, const float* sz, double* energy, double m[3]);
 double orc_sweep_o3_prop(int dims, int64_t lx, int64_t ly, int64_t lz, float J, float beta,
                          float omc, int prop, uint64_t key64, uint64_t sweep, float* sx, float* sy,
                          float* sz, int64_t* accepted);
@@ -179,6 +197,9 @@ void orc_ref_sweep(orc_ref* r, int adapt);
 /* observables of the current state: E (total), |M|/N (order parameter for
  * Potts), energy from cache */
 void orc_ref_measure(const orc_ref* r, double* energy, double* mag);
+/* therm sweeps, then meas measured sweeps: per-sweep E/N and |M| (or the
+ * Potts order parameter) into the caller's arrays */
+void orc_ref_series(orc_ref* r, int therm, int meas, double* e_per_site, double* mag);
 double orc_ref_recompute_energy(const orc_ref* r);
 void orc_ref_set_beta(orc_ref* r, double beta);
 int64_t orc_ref_n_sites(const orc_ref* r);

@@ -262,6 +262,19 @@ void orc_ref_measure(const orc_ref* r, double* energy, double* mag) {
     }
 }
 
+/* One chain's run: `therm` sweeps, then `meas` sweeps each followed by a
+ * measurement (Energy per site and Magnetization, ClassicalMC::measure). */
+void orc_ref_series(orc_ref* r, int therm, int meas, double* e_per_site, double* mag) {
+    for (int s = 0; s < therm; ++s) orc_ref_sweep(r, 1);
+    for (int s = 0; s < meas; ++s) {
+        orc_ref_sweep(r, 0);
+        double e, m;
+        orc_ref_measure(r, &e, &m);
+        e_per_site[s] = e / (double)r->n;
+        mag[s] = m;
+    }
+}
+
 /* ---- one chain per thread (Scheduler::run_parallel + RayonBackend) ------ */
 typedef struct {
     int model, dims, q, therm, meas, tid, n_threads, n_chains;

@@ -7,6 +7,7 @@ The CUDA library (libgpumc.so, sm_100a) is the only compute path: importing
 the package fails loudly if it has not been built.
 """
 from . import _lib
+from . import autotune
 from ._lib import GpumcError, InvalidConfig
 from .measurements import Accumulator, Context, Estimate, binder_cumulant, specific_heat
 from .mc import (ClassicalMC, Engine, MultiSpinIsing, Params, Server, geometric_ladder_betas,

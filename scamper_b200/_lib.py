@@ -7,7 +7,12 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgpumc.so")
+# GPUMC_LIBRARY=bounds loads the bounds-checked build (libgpumc_bounds.so,
+# python scamper_b200/build.py --bounds) instead of the release library.
+# GPUMC_LIBRARY=<absolute path> loads that build of the library instead.
+_choice = os.environ.get("GPUMC_LIBRARY", "")
+LIB_PATH = (_choice if os.path.isabs(_choice) else
+            os.path.join(HERE, "libgpumc_bounds.so" if _choice == "bounds" else "libgpumc.so"))
 
 OK = 0
 EINVAL = -1
@@ -94,6 +99,12 @@ class JobResult(ctypes.Structure):
 
 
 # (name, argtypes) of every exported entry point declared in include/gpumc.h
+class TileKnobs(ctypes.Structure):
+    """gpumc_tile_knobs: 0 = the planner's analytic choice."""
+    _fields_ = [(name, ctypes.c_int32) for name in
+                ("ising2d_rows", "ising3d_planes", "potts_segments", "potts3d_planes", "o3_rows", "o3_planes")]
+
+
 _vp = ctypes.c_void_p
 _P = ctypes.POINTER
 SIGNATURES = {
@@ -134,6 +145,12 @@ SIGNATURES = {
     "gpumc_log_weight_ratio": [_vp, ctypes.c_int32, ctypes.c_double, _P(ctypes.c_double)],
     "gpumc_change_parameter": [_vp, ctypes.c_int32, ctypes.c_double],
     "gpumc_pt_configure": [_vp, ctypes.c_uint32],
+    "gpumc_engine_set_wait_limit": [_vp, ctypes.c_int64],
+    "gpumc_set_audit_interval": [_vp, ctypes.c_uint64],
+    "gpumc_set_tile_knobs": [_P(TileKnobs)],
+    "gpumc_get_tile_knobs": [_P(TileKnobs)],
+    "gpumc_debug_bounds": [_P(ctypes.c_uint64), _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_int32)],
+    "gpumc_perturb_energy_cache": [_vp, ctypes.c_int32, ctypes.c_double],
     "gpumc_pt_labels": [_vp, _P(ctypes.c_int32)],
     "gpumc_pt_set_labels": [_vp, _P(ctypes.c_int32)],
     "gpumc_pt_stats": [_vp, _P(ctypes.c_uint64), _P(ctypes.c_uint64)],
@@ -180,7 +197,7 @@ def load():
         return _lib
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python scamper_b200/build.py` "
+            f"{LIB_PATH} is missing: build it with `python scamper_b200/build.py` (--bounds for the checked build) "
             "(there is no CPU fallback)")
     lib = ctypes.CDLL(LIB_PATH)
     for name, args in SIGNATURES.items():
@@ -189,6 +206,14 @@ def load():
         fn.restype = ctypes.c_int
     _lib = lib
     return lib
+
+
+def debug_bounds():
+    """(violations since the last call, first module, first line, compiled)
+    of a bounds-checked library; compiled is False for a release library."""
+    h, m, ln, c = ctypes.c_uint64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    check(load().gpumc_debug_bounds(ctypes.byref(h), ctypes.byref(m), ctypes.byref(ln), ctypes.byref(c)))
+    return h.value, m.value, ln.value, bool(c.value)
 
 
 def last_error():

@@ -12,6 +12,7 @@ SOURCES = ["capi.cu", "sim.cu", "server.cu", "sweep_discrete.cu", "sweep_o3.cu",
            "sweep_msc.cu", "lattice_ops.cu", "noalloc.cu",
            "sweep_ising_bits.cu", "sweep_potts_bits.cu", "cluster.cu"]
 LIB = os.path.join(HERE, "libgpumc.so")
+LIB_BOUNDS = os.path.join(HERE, "libgpumc_bounds.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr", "-static-global-template-stub=false",
@@ -25,18 +26,23 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_library(force=False, verbose=False, jobs=None):
+def build_library(force=False, verbose=False, jobs=None, bounds=False):
+    """Builds libgpumc.so, or with bounds=True the bounds-checked
+    libgpumc_bounds.so (-DGPUMC_DEBUG_BOUNDS: out-of-range accesses of the
+    kernels are skipped and counted, gpumc_debug_bounds reports them)."""
+    lib = LIB_BOUNDS if bounds else LIB
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "gpumc.h")]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    objdir = os.path.join(HERE, "_build")
+    if not force and not _stale(lib, deps):
+        return lib
+    objdir = os.path.join(HERE, "_build_bounds" if bounds else "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
+    extra = ["-DGPUMC_DEBUG_BOUNDS"] if bounds else []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
         objs.append(obj)
-        cmd = [NVCC, *FLAGS, "-rdc=false", "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [NVCC, *FLAGS, *extra, "-rdc=false", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
@@ -50,10 +56,10 @@ def build_library(force=False, verbose=False, jobs=None):
     if failed:
         msg = "\n".join(f"--- {s}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
-    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs,
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib, *objs,
            "-Xcompiler", "-fPIC", "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
     subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 def build_oracle():
@@ -62,6 +68,6 @@ def build_oracle():
 
 
 if __name__ == "__main__":
-    build_library(force="--force" in sys.argv, verbose=True)
+    build_library(force="--force" in sys.argv, verbose=True, bounds="--bounds" in sys.argv)
     if "--oracle" in sys.argv:
         build_oracle()

@@ -55,6 +55,8 @@ struct BitsGeom {
   bool yw;                      // whole-plane 3D tile: rows wrap inside the tile
   int hlast;                    // valid site pairs of the last segment of a row
   int col, row0, rstep, iters_load, iters_black, iters_white;
+  long long gbytes;             // bytes of one int8 buffer of the lattice (bounds checks)
+  int pw;                       // words of one shared plane (R x NC)
 };
 
 __device__ __forceinline__ int wrap_i(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
@@ -82,6 +84,8 @@ __device__ __forceinline__ BitsGeom make_bits_geom(const TileItem& t, const LatD
   g.iters_load = (g.R + g.rstep - 1) / g.rstep;
   g.iters_black = (g.R - 2 + 2 * (g.yo == 0) + g.rstep - 1) / g.rstep;
   g.iters_white = (g.hv + g.rstep - 1) / g.rstep;
+  g.gbytes = (long long)L->pitch * L->ly * (L->dims == 3 ? L->lz : 1);
+  g.pw = g.R * g.NC;
   return g;
 }
 

@@ -57,7 +57,10 @@ template <int DIM, int WOLFF>
 __global__ void k_cluster_o3_account(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int ALG>
 __global__ void k_sweep_ising_resident(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
-                                       uint2*, int, int);
+                                       uint2*, int, int, long long);
+template <int ALG>
+__global__ void k_sweep_ising_resident3(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*, const int2*,
+                                        uint2*, int, int, long long);
 template <int DIM>
 __global__ void k_msc_measure(const LatDesc*, int, unsigned long long*);
 __global__ void k_msc_record(LatDesc*, GroupDesc*, int, unsigned long long*);
@@ -312,7 +315,18 @@ int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots) {
   return best;
 }
 
+// Tile knobs of the planner (gpumc_set_tile_knobs): 0 = the analytic
+// choice; a positive value replaces it for layouts planned afterwards.
+static gpumc_tile_knobs g_knobs = {0, 0, 0, 0, 0, 0};
+static std::mutex g_knobs_mu;
+
+static gpumc_tile_knobs current_knobs() {
+  std::lock_guard<std::mutex> lock(g_knobs_mu);
+  return g_knobs;
+}
+
 Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
+  const gpumc_tile_knobs kn = current_knobs();
   Layout L;
   L.model = s->model;
   L.alg = s->algorithm == GPUMC_HEAT_BATH ? HEAT_BATH
@@ -341,7 +355,8 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     if (L.dims == 2 && nseg <= 256) {
       L.tile_cx = nseg;
       const int hv_max = std::max(1, (int)(kIsingTileSmem / (8 * (size_t)nseg)) - 4);
-      L.tile_y = ising_tile_rows(ly, std::max<int>(1, (int)s->n_replicas), nseg, hv_max, slots);
+      L.tile_y = kn.ising2d_rows > 0 ? std::min({kn.ising2d_rows, hv_max, ly})
+                                     : ising_tile_rows(ly, std::max<int>(1, (int)s->n_replicas), nseg, hv_max, slots);
       L.tile_z = 1;
       L.smem = 8 * (size_t)(L.tile_y + 4) * nseg;
     } else if (L.dims == 3 && nseg <= 256 && (size_t)ly * nseg * 8 * 4 <= kIsingTileSmem) {
@@ -364,7 +379,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
           best = dv;
         }
       }
-      L.tile_z = best;
+      L.tile_z = kn.ising3d_planes > 0 ? std::min(kn.ising3d_planes, lz) : best;
       L.smem = 4 * 8 * (size_t)ly * nseg;
     } else {
       const bool xsplit = (lx % 64 == 0) && nseg > 32;
@@ -396,14 +411,15 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     if (L.dims == 3 && nseg <= 128 && (size_t)ly * nseg * 16 * 4 <= kIsingTileSmem) {
       L.tile_cx = nseg;
       L.tile_y = ly;
-      const int ntz = (lz + 15) / 16;
+      const int zmax = kn.potts3d_planes > 0 ? kn.potts3d_planes : 16;
+      const int ntz = (lz + zmax - 1) / zmax;
       L.tile_z = (lz + ntz - 1) / ntz;
       L.smem = 4 * 16 * (size_t)ly * nseg;
     } else {
       const bool xsplit = (lx % 64 == 0) && nseg > 128;
       L.tile_cx = xsplit ? 32 : nseg;
       const int nc = L.tile_cx + (xsplit ? 2 : 0);
-      const int items = L.dims == 2 ? 1536 : 768;
+      const int items = L.dims == 2 ? (kn.potts_segments > 0 ? std::min(kn.potts_segments, 3072) : 1536) : 768;
       const int hv_max = std::max(1, items / nc - 4);
       const int nty = (ly + hv_max - 1) / hv_max;
       L.tile_y = (ly + nty - 1) / nty;
@@ -453,9 +469,11 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     const int ty_max = (int)(kO3MarchSmem / (48 * (size_t)L.pitch)) - 2;
     if (L.dims == 3 && ty_max >= 1) {
       L.march = true;
-      const int nty = (ly + std::min(16, ty_max) - 1) / std::min(16, ty_max);
+      const int rows = std::min(kn.o3_rows > 0 ? kn.o3_rows : 16, ty_max);
+      const int nty = (ly + rows - 1) / rows;
       L.tile_y = (ly + nty - 1) / nty;
-      const int ntz = (lz + 7) / 8;
+      const int planes = kn.o3_planes > 0 ? kn.o3_planes : 8;
+      const int ntz = (lz + planes - 1) / planes;
       L.tile_z = (lz + ntz - 1) / ntz;
       L.smem = 48 * (size_t)(L.tile_y + 2) * L.pitch;
     } else {
@@ -682,6 +700,11 @@ static int prepare_kernels() {
     const void* extra[] = {(const void*)k_sweep_ising_resident<0>, (const void*)k_sweep_ising_resident<1>};
     for (const void* f : extra) {
       cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kIsingTileSmem);
+      if (e != cudaSuccess) status = e;
+    }
+    const void* extra3[] = {(const void*)k_sweep_ising_resident3<0>, (const void*)k_sweep_ising_resident3<1>};
+    for (const void* f : extra3) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
     }
     const void* colour0[] = {(const void*)k_sweep_o3_march<0, 0>, (const void*)k_sweep_o3_march<0, 1>,
@@ -936,10 +959,62 @@ void ResidentPlan::release(cudaStream_t st) {
   on = false;
 }
 
+// 3D path of build_resident: whole-plane slabs of at least two planes, each
+// lattice's slabs consecutive in z order (enumerate_tiles), neighbours the
+// previous and next slab of its run, cyclically.
+static int build_resident3(int device, cudaStream_t st, const std::vector<TileItem>& tiles,
+                           const std::map<int, const Layout*>& layout_of_lat, ResidentPlan& rp) {
+  int pwmax = 0;
+  size_t smem = 0;
+  std::vector<int2> nbr(tiles.size());
+  for (size_t i = 0; i < tiles.size();) {
+    auto it = layout_of_lat.find(tiles[i].lat);
+    if (it == layout_of_lat.end()) return GPUMC_OK;
+    const Layout& L = *it->second;
+    const int nseg = L.pitch / 64;
+    if (L.model != ISING || L.dims != 3 || L.tile_cx != nseg || L.tile_y != L.ly) return GPUMC_OK;
+    if (i == 0) rp.alg = L.alg;
+    if (L.alg != rp.alg) return GPUMC_OK;
+    size_t j = i;
+    while (j < tiles.size() && tiles[j].lat == tiles[i].lat) ++j;
+    const int n = (int)(j - i);
+    for (int k = 0; k < n; ++k) {
+      const TileItem& t = tiles[i + k];
+      if (t.x0 != 0 || t.y0 != 0 || t.ty < L.ly || t.cx != nseg || t.z0 != k * t.tz ||
+          std::min(t.tz, L.lz - t.z0) < 2)
+        return GPUMC_OK;
+      smem = std::max(smem, (size_t)8 * (size_t)(std::min(t.tz, L.lz) + 4) * L.ly * nseg);
+      nbr[i + k] = make_int2((int)i + (k + n - 1) % n, (int)i + (k + 1) % n);
+    }
+    pwmax = std::max(pwmax, L.ly * nseg);
+    i = j;
+  }
+  if (smem > kMaxDynSmem) return GPUMC_OK;
+  int coop = 0, n_sm = 0, per_sm = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, rp.alg == HEAT_BATH ? k_sweep_ising_resident3<1> : k_sweep_ising_resident3<0>, kThreads, smem));
+  if (!coop || (int64_t)per_sm * n_sm < (int64_t)tiles.size()) return GPUMC_OK;
+  rp.dims = 3;
+  rp.smem = smem;
+  rp.xstride = 2 * 4 * pwmax;
+  CUDA_TRY(cudaMallocAsync(&rp.d_nbr, sizeof(int2) * nbr.size(), st));
+  CUDA_TRY(cudaMemcpyAsync(rp.d_nbr, nbr.data(), sizeof(int2) * nbr.size(), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMallocAsync(&rp.d_xchg, sizeof(uint2) * (size_t)rp.xstride * tiles.size(), st));
+  rp.on = true;
+  return GPUMC_OK;
+}
+
 int gpumc::build_resident(int device, cudaStream_t st, const std::vector<TileItem>& tiles,
                           const std::map<int, const Layout*>& layout_of_lat, size_t smem, ResidentPlan& rp) {
   rp.release(st);
-  if (tiles.empty() || smem > kIsingTileSmem) return GPUMC_OK;
+  if (tiles.empty()) return GPUMC_OK;
+  {
+    auto it = layout_of_lat.find(tiles[0].lat);
+    if (it != layout_of_lat.end() && it->second->dims == 3) return build_resident3(device, st, tiles, layout_of_lat, rp);
+  }
+  if (smem > kIsingTileSmem) return GPUMC_OK;
   // every tile a whole-row 2D Ising tile of >= 2 rows; a lattice's tiles are
   // consecutive in y order (enumerate_tiles), so its neighbours are the
   // previous and next tile of its run, cyclically
@@ -969,6 +1044,8 @@ int gpumc::build_resident(int device, cudaStream_t st, const std::vector<TileIte
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, rp.alg == HEAT_BATH ? k_sweep_ising_resident<1> : k_sweep_ising_resident<0>, kThreads, smem));
   if (!coop || (int64_t)per_sm * n_sm < (int64_t)tiles.size()) return GPUMC_OK;
+  rp.dims = 2;
+  rp.smem = smem;
   rp.xstride = 2 * 4 * wmax;
   CUDA_TRY(cudaMallocAsync(&rp.d_nbr, sizeof(int2) * nbr.size(), st));
   CUDA_TRY(cudaMemcpyAsync(rp.d_nbr, nbr.data(), sizeof(int2) * nbr.size(), cudaMemcpyHostToDevice, st));
@@ -977,24 +1054,106 @@ int gpumc::build_resident(int device, cudaStream_t st, const std::vector<TileIte
   return GPUMC_OK;
 }
 
+// Zeroes the per-sweep accumulators of every lattice of a tile list (after a
+// resident launch gave up, its partial sums must not reach a later epilogue).
+__global__ void k_reset_accumulators(const TileItem* __restrict__ tiles, int n_tiles, LatDesc* __restrict__ lats) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_tiles; i += gridDim.x * blockDim.x) {
+    LatDesc* L = &lats[tiles[i].lat];
+    L->acc = Accum{};
+    L->acc2 = Accum{};
+  }
+}
+
 int gpumc::launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
                            GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
-                           int n_sweeps) {
+                           int n_sweeps, long long spin_limit) {
   // bar, err and epi are adjacent: one memset clears them
   CUDA_TRY(cudaMemsetAsync(&ctl->bar, 0, 2 * sizeof(unsigned int) + sizeof(int32_t), st));
   const int2* nbr = rp.d_nbr;
   uint2* xchg = rp.d_xchg;
   int xstride = rp.xstride;
   void* args[] = {(void*)&tiles, (void*)&lats, (void*)&groups, (void*)&ctl,
-                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps};
-  const void* kern = rp.alg == HEAT_BATH ? (const void*)k_sweep_ising_resident<1>
-                                          : (const void*)k_sweep_ising_resident<0>;
+                  (void*)&nbr, (void*)&xchg, (void*)&xstride, (void*)&n_sweeps, (void*)&spin_limit};
+  const void* kern = rp.dims == 3 ? (rp.alg == HEAT_BATH ? (const void*)k_sweep_ising_resident3<1>
+                                                         : (const void*)k_sweep_ising_resident3<0>)
+                                  : (rp.alg == HEAT_BATH ? (const void*)k_sweep_ising_resident<1>
+                                                         : (const void*)k_sweep_ising_resident<0>);
   CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(n_tiles), dim3(kThreads),
-                                       args, smem, st));
+                                       args, rp.smem ? rp.smem : smem, st));
   int32_t err = 0;
   CUDA_TRY(cudaMemcpyAsync(&err, &ctl->err, sizeof(err), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
-  if (err) return fail(GPUMC_ECUDA, "resident sweep: a grid-barrier wait timed out");
+  if (err) {
+    // the CTAs left at their next wait: no state was stored by the CTAs that
+    // gave up, and the launch's sweep counters and caches are not a
+    // trajectory; clear the partial sums so the handle can be restored
+    k_reset_accumulators<<<(n_tiles + 255) / 256, 256, 0, st>>>(tiles, n_tiles, lats);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return fail(GPUMC_ECUDA,
+                "resident sweep: a grid-barrier wait gave up after " + std::to_string(spin_limit) +
+                    " polls; the handle's spins, sweep count and energy cache must be restored "
+                    "(gpumc_set_spins / gpumc_set_sweep_count or a snapshot)");
+  }
+  return GPUMC_OK;
+}
+
+namespace gpumc {
+int bounds_read_sweep_o3(unsigned long long*, unsigned int*);
+int bounds_read_sweep_ising_bits(unsigned long long*, unsigned int*);
+int bounds_read_sweep_potts_bits(unsigned long long*, unsigned int*);
+int bounds_read_sweep_discrete(unsigned long long*, unsigned int*);
+int bounds_read_sweep_msc(unsigned long long*, unsigned int*);
+int bounds_read_cluster(unsigned long long*, unsigned int*);
+int bounds_read_lattice_ops(unsigned long long*, unsigned int*);
+}  // namespace gpumc
+
+int gpumc_debug_bounds(uint64_t* hits, int32_t* first_module, int32_t* first_line, int32_t* compiled) {
+  if (!hits || !first_module || !first_line || !compiled) return fail(GPUMC_EINVAL, "null argument");
+  int (*const readers[])(unsigned long long*, unsigned int*) = {
+      bounds_read_sweep_o3,   bounds_read_sweep_ising_bits, bounds_read_sweep_potts_bits,
+      bounds_read_sweep_discrete, bounds_read_sweep_msc,    bounds_read_cluster,
+      bounds_read_lattice_ops};
+  *hits = 0;
+  *first_module = -1;
+  *first_line = 0;
+  *compiled = 1;
+  for (int m = 0; m < (int)(sizeof(readers) / sizeof(readers[0])); ++m) {
+    unsigned long long h = 0;
+    unsigned int line = 0;
+    const int rc = readers[m](&h, &line);
+    if (rc < 0) return fail(GPUMC_ECUDA, "bounds counters: symbol copy failed");
+    if (rc > 0) *compiled = 0;  // release build: no checks compiled in
+    if (h && *first_module < 0) {
+      *first_module = m;
+      *first_line = (int32_t)line;
+    }
+    *hits += h;
+  }
+  return GPUMC_OK;
+}
+
+int gpumc_set_tile_knobs(const gpumc_tile_knobs* knobs) {
+  if (!knobs) return fail(GPUMC_EINVAL, "knobs: null");
+  const int32_t v[6] = {knobs->ising2d_rows, knobs->ising3d_planes, knobs->potts_segments,
+                        knobs->potts3d_planes, knobs->o3_rows, knobs->o3_planes};
+  for (int32_t x : v)
+    if (x < 0 || x > 4096) return fail(GPUMC_EINVAL, "knobs: each value must be in 0..4096 (0 = analytic)");
+  std::lock_guard<std::mutex> lock(g_knobs_mu);
+  g_knobs = *knobs;
+  return GPUMC_OK;
+}
+
+int gpumc_get_tile_knobs(gpumc_tile_knobs* knobs) {
+  if (!knobs) return fail(GPUMC_EINVAL, "knobs: null");
+  *knobs = current_knobs();
+  return GPUMC_OK;
+}
+
+int gpumc_engine_set_wait_limit(gpumc_engine* eng, int64_t polls) {
+  if (!eng) return fail(GPUMC_EINVAL, "engine: null");
+  if (polls < 0) return fail(GPUMC_EINVAL, "polls: must be >= 0");
+  eng->wait_limit = polls;
   return GPUMC_OK;
 }
 
@@ -1050,7 +1209,7 @@ int gpumc_engine::rebuild_batch() {
     c.group_ids = p.d_gids;
     c.n_tiles = p.n_tiles;
     CUDA_TRY(cudaMemcpyAsync(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
-    if (is_ising2d_bits_kind(p.kind)) {
+    if (is_ising_bits_kind(p.kind)) {
       int rc = build_resident(device, stream, tv, layout_of_lat, p.smem, p.res);
       if (rc) {
         p.release(stream);
@@ -1107,7 +1266,9 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
       rc = s->measure_room(room);
       if (rc) return rc;
     }
-    const uint32_t chunk = std::min<uint32_t>(room, 64);
+    uint32_t chunk = std::min<uint32_t>(room, 64);
+    for (gpumc_sim* s : eng->sims)
+      if (const uint32_t to_audit = s->sweeps_to_audit()) chunk = std::min(chunk, to_audit);
     if (eng->has_per_sweep_work()) {
       rc = eng->use_graphs ? eng->run_graph(chunk) : eng->launch_batch_sweeps(chunk);
       eng->launches += (uint64_t)chunk * eng->launches_per_batch_sweep();
@@ -1115,7 +1276,7 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
     for (auto& p : eng->batch_plans)
       if (rc == GPUMC_OK && p.res.on && eng->blocking) {
         rc = launch_resident(eng->stream, p.d_tiles, p.n_tiles, eng->d_lats, eng->d_groups, p.d_ctl, p.res,
-                             p.smem, (int)chunk);
+                             p.smem, (int)chunk, eng->wait_limit);
         eng->launches += 1;
       }
     if (rc) return rc;
@@ -1123,6 +1284,8 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
       s->sweeps = std::min<uint64_t>(s->sweeps + chunk, s->target);
       s->note_measured(chunk);
     }
+    for (gpumc_sim* s : eng->sims)
+      if (s->audit_interval && s->sweeps % s->audit_interval == 0 && (rc = s->audit()) != GPUMC_OK) return rc;
     left -= chunk;
   }
   return GPUMC_OK;

@@ -98,11 +98,17 @@ __device__ __forceinline__ void cluster_neighbour(const LatDesc* L, const Cluste
   addr = ((size_t)z * L->ly + y) * (size_t)L->pitch + x;
 }
 
+// Elements of one spin buffer of a lattice (bounds checks).
+__device__ __forceinline__ long long cl_elems(const LatDesc* L) {
+  return (long long)L->pitch * L->ly * (L->dims == 3 ? L->lz : 1);
+}
+
 // Active + bonds of a site (bit d), from the old configuration.
 template <int DIM>
 __device__ __forceinline__ uint32_t cluster_bonds(const LatDesc* L, const ClusterSite& c, const int8_t* cur,
                                                   unsigned long long thr, uint64_t sweep) {
-  const int8_t s = cur[c.addr];
+  const long long ne = cl_elems(L);
+  const int8_t s = ld_chk(cur, (long long)c.addr, ne);
   const uint4 o = draw(L->key, c.site, 0u, TAG_SW, 0u, sweep);
   uint32_t b = 0;
 #pragma unroll
@@ -117,7 +123,7 @@ __device__ __forceinline__ uint32_t cluster_bonds(const LatDesc* L, const Cluste
       const uint4 o2 = draw(L->key, c.site, 0u, TAG_SW, 1u, sweep);
       u = (unsigned long long)o2.x | ((unsigned long long)o2.y << 32);
     }
-    if (cur[na] == s && u < thr) b |= 1u << d;
+    if (ld_chk(cur, (long long)na, ne) == s && u < thr) b |= 1u << d;
   }
   return b;
 }
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(kThreads)
     const int lx = L->lx, ly = L->ly;
     const int sx = (int)(seed % (uint32_t)lx), sy = (int)((seed / (uint32_t)lx) % (uint32_t)ly);
     const int sz = (int)(seed / ((uint32_t)lx * (uint32_t)ly));
-    const int8_t ss = cur[((size_t)sz * ly + sy) * (size_t)L->pitch + sx];
+    const int8_t ss = ld_chk(cur, (long long)(((size_t)sz * ly + sy) * (size_t)L->pitch + sx), cl_elems(L));
     if (MODEL == ISING) {
       rule.target = (int8_t)-ss;
     } else {
@@ -328,8 +334,8 @@ __global__ void __launch_bounds__(kThreads)
   const ClusterSite c = cluster_site<DIM>(t, L);
   if (!c.in) return;
   const uint32_t r = global_find(lab, c.site);
-  __stcg(lab + c.site, r);
-  nxt[c.addr] = rule.apply(r, cur[c.addr]);
+  if (GPUMC_IN(c.site, L->n_sites)) __stcg(lab + c.site, r);
+  st_chk(nxt, (long long)c.addr, cl_elems(L), rule.apply(r, ld_chk(cur, (long long)c.addr, cl_elems(L))));
 }
 
 // Accounting of a lattice's sums: one block reduction, then one atomic per
@@ -395,13 +401,14 @@ __global__ void __launch_bounds__(kThreads)
     const int8_t* nxt = (const int8_t*)L->buf[(sweep & 1) ^ 1];
     const ClusterSite c = cluster_site<DIM>(t, L);
     if (c.in) {
-      const int8_t s = cur[c.addr], sn = nxt[c.addr];
+      const long long ne = cl_elems(L);
+      const int8_t s = ld_chk(cur, (long long)c.addr, ne), sn = ld_chk(nxt, (long long)c.addr, ne);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
         uint32_t ns;
         size_t na;
         cluster_neighbour<DIM>(L, c, d, ns, na);
-        dE += bond_energy<MODEL>(sn, nxt[na]) - bond_energy<MODEL>(s, cur[na]);
+        dE += bond_energy<MODEL>(sn, ld_chk(nxt, (long long)na, ne)) - bond_energy<MODEL>(s, ld_chk(cur, (long long)na, ne));
       }
       nch += sn != s;
       if (MODEL == ISING) mag += sn;
@@ -439,7 +446,8 @@ struct O3Spin {
 };
 
 __device__ __forceinline__ O3Spin o3_get(const float* S, size_t cs, size_t i) {
-  return O3Spin{S[i], S[cs + i], S[2 * cs + i]};
+  return O3Spin{ld_chk(S, (long long)i, (long long)cs), ld_chk(S + cs, (long long)i, (long long)cs),
+                ld_chk(S + 2 * cs, (long long)i, (long long)cs)};
 }
 
 __device__ __forceinline__ float o3_sigma(const O3Spin& v, const O3Axis& a) {
@@ -703,5 +711,7 @@ CLUSTER_INSTANTIATE(2, ISING, 1)
 CLUSTER_INSTANTIATE(3, ISING, 1)
 CLUSTER_INSTANTIATE(2, POTTS, 1)
 CLUSTER_INSTANTIATE(3, POTTS, 1)
+
+GPUMC_BOUNDS_MODULE(cluster)
 
 }  // namespace gpumc

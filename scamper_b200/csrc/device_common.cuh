@@ -9,6 +9,50 @@
 
 namespace gpumc {
 
+// Bounds-checked builds (compiled with -DGPUMC_DEBUG_BOUNDS; the stand-in for
+// a memory sanitizer): GPUMC_IN(i, n) is true when 0 <= i < n; otherwise it
+// counts the violation in this module's counters, keeps the first failing
+// source line, and is false, so the guarded load or store is skipped instead
+// of touching memory outside its buffer.  In release builds it is the
+// constant true and compiles away.  Each compiled module has its own
+// counters; bounds_read_<module>() (GPUMC_BOUNDS_MODULE) reads and clears them.
+#ifdef GPUMC_DEBUG_BOUNDS
+static __device__ unsigned long long g_bounds_hits;
+static __device__ unsigned int g_bounds_line;
+static __device__ __noinline__ bool bounds_fail(unsigned int line) {
+  if (atomicAdd(&g_bounds_hits, 1ull) == 0ull) g_bounds_line = line;
+  return false;
+}
+#define GPUMC_IN(i, n) \
+  (((unsigned long long)(long long)(i) < (unsigned long long)(long long)(n)) || ::gpumc::bounds_fail(__LINE__))
+#define GPUMC_BOUNDS_MODULE(name)                                                                   \
+  int bounds_read_##name(unsigned long long* hits, unsigned int* line) {                           \
+    const unsigned long long zero = 0;                                                              \
+    if (cudaMemcpyFromSymbol(hits, g_bounds_hits, sizeof(*hits)) != cudaSuccess) return -1;         \
+    if (cudaMemcpyFromSymbol(line, g_bounds_line, sizeof(*line)) != cudaSuccess) return -1;         \
+    return cudaMemcpyToSymbol(g_bounds_hits, &zero, sizeof(zero)) == cudaSuccess ? 0 : -1;          \
+  }
+#else
+#define GPUMC_IN(i, n) true
+#define GPUMC_BOUNDS_MODULE(name)                                       \
+  int bounds_read_##name(unsigned long long* hits, unsigned int* line) { \
+    *hits = 0;                                                         \
+    *line = 0;                                                         \
+    return 1;                                                          \
+  }
+#endif
+
+// Loads and stores of element i of a buffer of n elements, checked in
+// bounds-checked builds (an out-of-range load returns zero).
+template <typename T>
+__device__ __forceinline__ T ld_chk(const T* p, long long i, long long n) {
+  return GPUMC_IN(i, n) ? p[i] : T{};
+}
+template <typename T>
+__device__ __forceinline__ void st_chk(T* p, long long i, long long n, T v) {
+  if (GPUMC_IN(i, n)) p[i] = v;
+}
+
 __device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {

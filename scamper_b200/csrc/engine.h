@@ -50,9 +50,10 @@ struct Accum {
   unsigned long long accepted;  // accepted moves
   unsigned long long counts[kMaxPottsCounts];
   double dEf;                   // O(3) cluster updates: accumulated energy change
-  double mx, my, mz;            // O(3): magnetisation components
-  double ebond;                 // O(3) sweeps: sum over colour-1 sites of s . h (fp64)
-  int32_t fresh;                // set when ebond holds the full bond sum of a sweep
+  double mx, my, mz;            // O(3) cluster updates: magnetisation components
+  unsigned long long ebq;       // O(3) sweeps: int64 sum over colour-1 sites of rint(2^19 s . h)
+  unsigned long long mq[3];     // O(3) sweeps: int64 sums of rint(2^21 s_c) over all sites
+  int32_t fresh;                // set when ebq holds the full bond sum of a sweep
   int32_t pad;
 };
 

@@ -103,16 +103,21 @@ static __device__ void finish_replica(LatDesc* lats, GroupDesc* G, int r, int32_
     const double dEf = take_f64(&A->dEf);
     if (A->fresh) {
       // sweeps: every bond has exactly one colour-1 end, so the energy after
-      // the sweep is -J times the colour-1 pass's sum of s . h
+      // the sweep is -J times the colour-1 pass's sum of s . h, accumulated
+      // in fixed point (2^-19) from the fp32 dot products; the magnetisation
+      // components likewise at 2^-21 (integer sums: independent of order)
       A->fresh = 0;
-      L->e_f = -G->J * take_f64(&A->ebond);
+      L->e_f = -G->J * ((double)take_i64(&A->ebq) * 0x1p-19);
+      R.m[0] = (double)take_i64(&A->mq[0]) * 0x1p-21;
+      R.m[1] = (double)take_i64(&A->mq[1]) * 0x1p-21;
+      R.m[2] = (double)take_i64(&A->mq[2]) * 0x1p-21;
     } else {
       L->e_f += dEf;  // cluster updates: exact change of the flipped clusters
+      R.m[0] = take_f64(&A->mx);
+      R.m[1] = take_f64(&A->my);
+      R.m[2] = take_f64(&A->mz);
     }
     R.energy = L->e_f;
-    R.m[0] = take_f64(&A->mx);
-    R.m[1] = take_f64(&A->my);
-    R.m[2] = take_f64(&A->mz);
     if (L->adapt && L->sweep < G->adapt_until)
       L->omc = L->prop == 2 ? opss_adapt(L->omc, nacc, L->n_sites) : o3_adapt(L->omc, nacc, L->n_sites);
   } else {

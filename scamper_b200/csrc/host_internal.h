@@ -50,6 +50,9 @@ constexpr int kKindO3Uniform = 48, kKindO3Opss = 64;
 // 2D Ising on the bit-sliced kernel (either single-site algorithm): the kinds
 // the resident multi-sweep launch can take
 inline bool is_ising2d_bits_kind(int kind) { return kind == 0 || kind == kKindHeatBath; }
+inline bool is_ising_bits_kind(int kind) {
+  return kind == 0 || kind == 1 || kind == kKindHeatBath || kind == kKindHeatBath + 1;
+}
 int validate_spec(const gpumc_spec* s);
 // CTA slots of one B200 (148 SMs x 4 resident sweep CTAs); the engine
 // passes its device's own count.
@@ -83,6 +86,8 @@ int launch_msc_record(cudaStream_t st, LatDesc* lats, GroupDesc* groups, int gro
 struct ResidentPlan {
   bool on = false;
   int alg = METROPOLIS;  // kernel variant (all tiles of a plan share it)
+  int dims = 2;          // 2: whole-row square tiles; 3: whole-plane cubic slabs
+  size_t smem = 0;       // dynamic shared memory of the resident launch
   int2* d_nbr = nullptr;
   uint2* d_xchg = nullptr;
   int xstride = 0;  // uint2 words of exchange space per tile
@@ -101,17 +106,20 @@ struct BatchPlan {
   void release(cudaStream_t st);
 };
 
-// Qualifies a tile list for the resident Ising kernel (every tile a
-// whole-row 2D Ising tile of at least two rows, all tiles co-resident on the
-// device) and allocates its neighbour table and exchange buffer; leaves
-// rp.on false when the list does not qualify.
+// Qualifies a tile list for the resident Ising kernels (every tile a
+// whole-row 2D Ising tile of at least two rows, or every tile a whole-plane
+// 3D Ising slab of at least two planes; all tiles co-resident on the device)
+// and allocates its neighbour table and exchange buffer; leaves rp.on false
+// when the list does not qualify.
 int build_resident(int device, cudaStream_t st, const std::vector<TileItem>& tiles,
                    const std::map<int, const Layout*>& layout_of_lat, size_t smem, ResidentPlan& rp);
-// n_sweeps sweeps of every tile in one cooperative launch; waits for it and
-// reports a barrier timeout as an error.
+// n_sweeps sweeps of every tile in one cooperative launch whose inter-CTA
+// waits give up after spin_limit polls; waits for it and reports a wait that
+// gave up as an error.
 int launch_resident(cudaStream_t st, const TileItem* tiles, int n_tiles, LatDesc* lats,
                     GroupDesc* groups, LaunchCtl* ctl, const ResidentPlan& rp, size_t smem,
-                    int n_sweeps);
+                    int n_sweeps, long long spin_limit);
+constexpr long long kDefaultWaitLimit = 1ll << 22;  // polls of 128 ns, about half a second
 
 }  // namespace gpumc
 
@@ -135,6 +143,7 @@ struct gpumc_engine {
   std::vector<cudaEvent_t> side_done; // per-plan join events
   cudaEvent_t fork = nullptr;         // fork point on the engine stream
   uint64_t launches = 0;      // kernel launches issued by gpumc_engine_sweep
+  long long wait_limit = gpumc::kDefaultWaitLimit;  // polls before an inter-CTA wait gives up
   int slots = gpumc::kDefaultSlots;  // resident sweep CTAs of the device (tile planning)
   int slots3 = gpumc::kDefaultSlots3;  // the same for the 3D Ising kernel
   std::vector<gpumc::BatchPlan> batch_plans;
@@ -185,6 +194,7 @@ struct gpumc_sim {
   uint64_t launches = 0;     // kernel launches issued by gpumc_sweep
   std::map<uint32_t, cudaGraphExec_t> graphs;
   uint64_t sweeps = 0;  // host mirror of the device sweep counter
+  uint64_t audit_interval = 0;  // cache audit every this many sweeps (0 = off)
   uint64_t target = ~0ull;        // sweep target (serving)
   bool device_schedule = false;   // phases driven by measure_from / target on the device
   int phase = GPUMC_PHASE_THERMALIZATION;
@@ -210,6 +220,8 @@ struct gpumc_sim {
   int upload_own_tiles(std::vector<gpumc::TileItem>& tiles);
   void drop_graphs();
   int recompute(std::vector<double>& out, bool store);
+  int audit();
+  uint32_t sweeps_to_audit() const;
   int launch_energy(const void* buf, unsigned long long* d_e, unsigned int* d_bad);
   template <class T>
   int set_lat_field(int r, size_t offset, const T& v) {

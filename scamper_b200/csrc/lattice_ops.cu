@@ -249,4 +249,6 @@ __global__ void k_philox_probe(const uint4* ctr, const uint2* key, uint4* out, i
   if (i < n) out[i] = philox10(ctr[i], key[i].x, key[i].y);
 }
 
+GPUMC_BOUNDS_MODULE(lattice_ops)
+
 }  // namespace gpumc

@@ -294,6 +294,39 @@ int gpumc_sim::recompute(std::vector<double>& out, bool store) {
   return GPUMC_OK;
 }
 
+// Cache audit (audit_lattice_cache, CMC.rs/src/audit.rs:41-52): the cached
+// energy of every replica against an exact recomputation from the spins,
+// with the reference's tolerance 1e-10 (1 + |exact|).
+int gpumc_sim::audit() {
+  std::vector<LatDesc> d(n_rep);
+  CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  CUDA_TRY(cudaMemcpy(d.data(), eng->d_lats + lat0, sizeof(LatDesc) * n_rep, cudaMemcpyDeviceToHost));
+  std::vector<double> exact;
+  RC_TRY(recompute(exact, false));
+  for (int r = 0; r < n_rep; ++r) {
+    const double cached = lay.model == O3 ? d[r].e_f : spec.J * (double)d[r].e_int;
+    // O(3) sweeps record the energy as a fixed-point sum of fp32 bond
+    // products (each within 4e-6 of exact on a colour-1 site: the fp32
+    // neighbour sum, the fused dot and the 2^-19 rounding), so the audit
+    // allows that rounding on top of the reference's tolerance
+    const double fp32_bound = lay.model == O3 && !lay.cluster ? 2e-6 * std::fabs(spec.J) * (double)lay.n_sites : 0.0;
+    if (std::fabs(cached - exact[r]) > 1e-10 * (1.0 + std::fabs(exact[r])) + fp32_bound) {
+      char msg[256];
+      std::snprintf(msg, sizeof(msg),
+                    "lattice energy cache mismatch: replica %d after sweep %llu: cached=%.17g, exact=%.17g", r,
+                    (unsigned long long)sweeps, cached, exact[r]);
+      return fail(GPUMC_ESTATE, msg);
+    }
+  }
+  return GPUMC_OK;
+}
+
+// Sweeps a chunk may run before the next audit point (0 = no audit due).
+uint32_t gpumc_sim::sweeps_to_audit() const {
+  if (!audit_interval) return 0;
+  return (uint32_t)std::min<uint64_t>(audit_interval - sweeps % audit_interval, 1u << 30);
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -411,7 +444,7 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   c.group_ids = s->d_gid;
   c.n_tiles = s->n_tiles;
   CUDA_CLEAN(cudaMemcpyAsync(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, eng->stream));
-  if (is_ising2d_bits_kind(kernel_kind(s->lay))) {
+  if (is_ising_bits_kind(kernel_kind(s->lay))) {
     std::map<int, const Layout*> lay_of;
     for (int r = 0; r < s->n_rep; ++r) lay_of[s->lat0 + r] = &s->lay;
     rc = build_resident(eng->device, eng->stream, tiles, lay_of, s->lay.smem, s->res);
@@ -569,10 +602,11 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
   while (left > 0) {
     uint32_t room = left;
     RC_TRY(sim->measure_room(room));
-    const uint32_t chunk = std::min<uint32_t>(room, 64);
+    uint32_t chunk = std::min<uint32_t>(room, 64);
+    if (const uint32_t to_audit = sim->sweeps_to_audit()) chunk = std::min(chunk, to_audit);
     if (sim->res.on && sim->blocking) {
       RC_TRY(launch_resident(sim->eng->stream, sim->d_tiles, sim->n_tiles, sim->eng->d_lats, sim->eng->d_groups,
-                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk));
+                             sim->d_ctl, sim->res, sim->lay.smem, (int)chunk, sim->eng->wait_limit));
       sim->launches += 1;
     } else {
       RC_TRY(sim->run_graph(chunk));
@@ -583,7 +617,33 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
     sim->sweeps += chunk;
     sim->note_measured(chunk);
     left -= chunk;
+    if (sim->audit_interval && sim->sweeps % sim->audit_interval == 0) RC_TRY(sim->audit());
   }
+  return GPUMC_OK;
+}
+
+int gpumc_set_audit_interval(gpumc_sim* sim, uint64_t interval) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (interval && sim->device_schedule) return fail(GPUMC_ESTATE, "audit: not available for server jobs");
+  sim->audit_interval = interval;
+  return GPUMC_OK;
+}
+
+int gpumc_perturb_energy_cache(gpumc_sim* sim, int32_t replica, double delta) {
+  if (!sim) return fail(GPUMC_EINVAL, "sim: null");
+  if (replica < 0 || replica >= sim->n_rep) return fail(GPUMC_EINVAL, "replica: out of range");
+  if (!std::isfinite(delta)) return fail(GPUMC_EINVAL, "delta: must be finite");
+  CUDA_TRY(cudaSetDevice(sim->eng->device));
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
+  LatDesc d;
+  CUDA_TRY(cudaMemcpy(&d, sim->eng->d_lats + sim->lat0 + replica, sizeof(d), cudaMemcpyDeviceToHost));
+  if (sim->lay.model == O3) {
+    RC_TRY(sim->set_lat_field(replica, offsetof(LatDesc, e_f), d.e_f + delta));
+  } else {
+    if (delta != std::floor(delta)) return fail(GPUMC_EINVAL, "delta: integer models take a whole number of J");
+    RC_TRY(sim->set_lat_field(replica, offsetof(LatDesc, e_int), d.e_int + (long long)delta));
+  }
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
   return GPUMC_OK;
 }
 

@@ -372,6 +372,7 @@ __device__ __forceinline__ uint32_t owned_bytes(int remaining) {
 struct TileGeom {
   int x0, y0, W, S, Wv, ncv, hv, R;
   int lx, ly, pitch, pc;
+  long long gbytes;  // bytes of one int8 buffer of the lattice (bounds checks)
   // thread mapping of the vector passes: fixed chunk column, rows strided
   int col, row0, rstep;
   bool active;
@@ -390,7 +391,9 @@ __device__ __forceinline__ void stage_plane(uint8_t* plane, const int8_t* src, i
   const int c = g.col;
   for (int r = g.row0; r < g.R; r += g.rstep) {
     const int y = wrap_row(g.y0 - 2 + r, g.ly);
-    cp_async16(plane + r * g.S + 16 + 16 * c, src + (zoff + y) * (size_t)g.pitch + g.x0 + 16 * c);
+    const size_t so = (zoff + y) * (size_t)g.pitch + g.x0 + 16 * c;
+    if (GPUMC_IN(so + 15, g.gbytes) && GPUMC_IN(r * g.S + 31 + 16 * c, (long long)g.R * g.S))
+      cp_async16(plane + r * g.S + 16 + 16 * c, src + so);
   }
 }
 struct HaloBytes {
@@ -411,16 +414,16 @@ __device__ __forceinline__ HaloBytes fetch_halo(const int8_t* src, int z, const 
     for (int j = 0; j < 2; ++j) {
       int xr = p0 + j;
       xr = xr < 0 ? xr + g.lx : (xr >= g.lx ? xr - g.lx : xr);
-      h.v[j] = src[row + xr];
+      h.v[j] = ld_chk(src, (long long)(row + xr), g.gbytes);
       h.off[j] = r * g.S + 16 + (p0 + j - g.x0);
     }
   }
   return h;
 }
-__device__ __forceinline__ void store_halo(uint8_t* plane, const HaloBytes& h) {
+__device__ __forceinline__ void store_halo(uint8_t* plane, const HaloBytes& h, const TileGeom& g) {
   if (h.off[0] >= 0) {
-    plane[h.off[0]] = (uint8_t)h.v[0];
-    plane[h.off[1]] = (uint8_t)h.v[1];
+    st_chk(plane, h.off[0], (long long)g.R * g.S, (uint8_t)h.v[0]);
+    st_chk(plane, h.off[1], (long long)g.R * g.S, (uint8_t)h.v[1]);
   }
 }
 
@@ -526,7 +529,8 @@ __device__ __forceinline__ void white_pass(const uint8_t* B, const uint8_t* Bzm,
                                      rho * (uint32_t)g.lx + (uint32_t)(g.x0 + 16 * c), 1u, sweep, owned,
                                      nacc, acc2);
     }
-    *(uint4*)(dst + (size_t)rho * (size_t)g.pitch + g.x0 + 16 * c) = res;
+    const size_t doff = (size_t)rho * (size_t)g.pitch + g.x0 + 16 * c;
+    if (GPUMC_IN(doff + 15, g.gbytes)) *(uint4*)(dst + doff) = res;
     const uint32_t w[4] = {res.x, res.y, res.z, res.w};
     if (owned == 0xFFFFu) {
       if (MODEL == ISING) {
@@ -623,6 +627,7 @@ __device__ __forceinline__ TileGeom make_geom(const TileItem& t, const LatDesc* 
   g.col = threadIdx.x % g.ncv;
   g.row0 = threadIdx.x / g.ncv;
   g.active = g.row0 < g.rstep;
+  g.gbytes = (long long)L->pitch * L->ly * (L->dims == 3 ? L->lz : 1);
   return g;
 }
 
@@ -653,7 +658,7 @@ __global__ void __launch_bounds__(kThreads)
   const PhiloxCtx P = make_philox(key, sweep);
   cp_async_wait_all();
   __syncthreads();
-  store_halo(A, hb);
+  store_halo(A, hb, g);
   __syncthreads();
   int nacc = 0, acc2 = 0, mag = 0;
   int cnt[kMaxPottsCounts] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -707,7 +712,7 @@ __global__ void __launch_bounds__(kThreads)
     const HaloBytes hb = fetch_halo(cur, zlw, g);
     cp_async_wait_all();
     __syncthreads();
-    store_halo(Al, hb);
+    store_halo(Al, hb, g);
     __syncthreads();
     if (s >= 2) {
       const int zb = zl - 1;
@@ -737,5 +742,7 @@ template __global__ void k_sweep_discrete_2d<POTTS, 0>(const TileItem*, LatDesc*
 template __global__ void k_sweep_discrete_3d<POTTS, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_discrete_2d<POTTS, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_discrete_3d<POTTS, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+
+GPUMC_BOUNDS_MODULE(sweep_discrete)
 
 }  // namespace gpumc

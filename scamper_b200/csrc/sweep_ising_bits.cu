@@ -107,17 +107,19 @@ __device__ __forceinline__ void load_bits_plane(uint2* pl, const int8_t* src, in
     uint4 a[4], b[4];
     const bool ok0 = r0 < g.R, ok1 = r1 < g.R && it + 1 < g.iters_load;
     if (ok0) {
-      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - g.yo + r0, g.ly)) * g.pitch + 64 * gs);
+      const size_t off = (zrow + wrap_i(g.y0 - g.yo + r0, g.ly)) * g.pitch + 64 * gs;
+      const uint4* p = (const uint4*)(src + off);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) a[k] = __ldg(p + k);
+      for (int k = 0; k < 4; ++k) a[k] = GPUMC_IN(off + 63, g.gbytes) ? __ldg(p + k) : make_uint4(0, 0, 0, 0);
     }
     if (ok1) {
-      const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - g.yo + r1, g.ly)) * g.pitch + 64 * gs);
+      const size_t off = (zrow + wrap_i(g.y0 - g.yo + r1, g.ly)) * g.pitch + 64 * gs;
+      const uint4* p = (const uint4*)(src + off);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) b[k] = __ldg(p + k);
+      for (int k = 0; k < 4; ++k) b[k] = GPUMC_IN(off + 63, g.gbytes) ? __ldg(p + k) : make_uint4(0, 0, 0, 0);
     }
-    if (ok0) pl[r0 * g.NC + g.col] = pack_segment(a[0], a[1], a[2], a[3]);
-    if (ok1) pl[r1 * g.NC + g.col] = pack_segment(b[0], b[1], b[2], b[3]);
+    if (ok0) st_chk(pl, r0 * g.NC + g.col, g.pw, pack_segment(a[0], a[1], a[2], a[3]));
+    if (ok1) st_chk(pl, r1 * g.NC + g.col, g.pw, pack_segment(b[0], b[1], b[2], b[3]));
   }
 }
 
@@ -171,11 +173,11 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
     if (active) {
       const int y = wrap_i(g.y0 - g.yo + r, g.ly);
       P_ = (colour + y + z) & 1;  // x parity of this colour's sites in the row
-      const uint2 me = pl[r * g.NC + cc];
+      const uint2 me = ld_chk(pl, r * g.NC + cc, g.pw);
       const int ru = g.yw && r == 0 ? g.R - 1 : r - 1;
       const int rd = g.yw && r == g.R - 1 ? 0 : r + 1;
-      const uint2 up = pl[ru * g.NC + cc];
-      const uint2 dn = pl[rd * g.NC + cc];
+      const uint2 up = ld_chk(pl, ru * g.NC + cc, g.pw);
+      const uint2 dn = ld_chk(pl, rd * g.NC + cc, g.pw);
       own = P_ ? me.y : me.x;
       const uint32_t other = P_ ? me.x : me.y;
       uint32_t lft, rgt;
@@ -183,7 +185,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
         // even x = 2i: left = odd 2i-1 (index i-1), right = odd 2i+1 (index i)
         uint32_t carry = 0;
         if (has_prev) {
-          const uint32_t po = pl[r * g.NC + cprev].y;
+          const uint32_t po = ld_chk(pl, r * g.NC + cprev, g.pw).y;
           carry = first_seg ? (po >> (g.hlast - 1)) & 1u : po >> 31;
         }
         lft = (other << 1) | carry;
@@ -191,7 +193,7 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       } else {
         // odd x = 2i+1: left = even 2i (index i), right = even 2i+2 (index i+1)
         lft = other;
-        const uint32_t ne = has_next ? pl[r * g.NC + cnext].x & 1u : 0u;
+        const uint32_t ne = has_next ? ld_chk(pl, r * g.NC + cnext, g.pw).x & 1u : 0u;
         const int hb = last_seg ? g.hlast - 1 : 31;
         rgt = ((other >> 1) & ~(1u << hb)) | (ne << hb);
       }
@@ -271,9 +273,12 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
       // heat bath: the new spin is down iff (lt == neg), i.e. ~(lt ^ neg)
       flip = ALG ? (own ^ ~(lt ^ negm)) & valid : (always | lt) & valid;
       const uint32_t nw = own ^ flip;
-      uint2& me = pl[r * g.NC + cc];
-      if (P_) me.y = nw;
-      else me.x = nw;
+      const int mi = GPUMC_IN(r * g.NC + cc, g.pw) ? r * g.NC + cc : 0;
+      uint2& me = pl[mi];
+      if (GPUMC_IN(r * g.NC + cc, g.pw)) {
+        if (P_) me.y = nw;
+        else me.x = nw;
+      }
       const bool owned = owned_plane && owned_col && r >= g.yo && r < g.yo + g.hv;
       if (owned) {
         acc.nacc += __popc(flip);
@@ -294,11 +299,14 @@ __device__ __forceinline__ void bits_pass(uint2* pl, const uint2* pm, const uint
           const int y = wrap_i(g.y0 - g.yo + r, g.ly);
           uint4 v0, v1, v2, v3;
           unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
-          uint4* out = (uint4*)(dst + ((size_t)z * g.ly + y) * g.pitch + 64 * gs);
-          out[0] = v0;
-          out[1] = v1;
-          out[2] = v2;
-          out[3] = v3;
+          const size_t off = ((size_t)z * g.ly + y) * g.pitch + 64 * gs;
+          uint4* out = (uint4*)(dst + off);
+          if (GPUMC_IN(off + 63, g.gbytes)) {
+            out[0] = v0;
+            out[1] = v1;
+            out[2] = v2;
+            out[3] = v3;
+          }
         }
         acc.down += __popc(fin.x & valid) + __popc(fin.y & valid);
         acc.owned_sites += 2 * __popc(valid);
@@ -437,12 +445,12 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
 //   * the next sweep refreshes the tile's four halo rows from the two
 //     neighbours' slots (tile above: its last two rows; tile below: its first
 //     two) and recomputes the black halo rows as usual.
-// Every barrier wait is bounded: a CTA that waits too long (or sees another
-// CTA's error) sets ctl->err and returns, every other CTA then leaves at its
-// next barrier, and the host reports the error.  The cooperative launch
-// guarantees that all CTAs are co-resident.
+// Every barrier wait is bounded by `spin_limit` polls (128 ns sleeps; the
+// host's default is 2^22, about half a second): a CTA that waits too long (or
+// sees another CTA's error) sets ctl->err and returns, every other CTA then
+// leaves at its next barrier, and the host reports the error.  The
+// cooperative launch guarantees that all CTAs are co-resident.
 // ---------------------------------------------------------------------------
-constexpr long long kGridSpinLimit = 1ll << 22;  // polls (128 ns sleeps) per barrier wait
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
   unsigned int v;
@@ -454,7 +462,7 @@ __device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t* p) {
   return *(const volatile uint64_t*)p;
 }
 
-__device__ bool resident_grid_sync(LaunchCtl* ctl, unsigned int target) {
+__device__ bool resident_grid_sync(LaunchCtl* ctl, unsigned int target, long long spin_limit) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -463,7 +471,7 @@ __device__ bool resident_grid_sync(LaunchCtl* ctl, unsigned int target) {
     int good = 1;
     long long it = 0;
     while (ld_acquire_u32(&ctl->bar) < target) {
-      if (*(volatile int32_t*)&ctl->err != 0 || ++it > kGridSpinLimit) {
+      if (*(volatile int32_t*)&ctl->err != 0 || ++it > spin_limit) {
         atomicExch(&ctl->err, 1);
         good = 0;
         break;
@@ -479,13 +487,13 @@ __device__ bool resident_grid_sync(LaunchCtl* ctl, unsigned int target) {
 
 // Bounded wait until block 0 has finished the epilogue of launch-local sweep
 // `k1 - 1` (ctl->epi >= k1); on giving up, flags the error like a barrier.
-__device__ bool resident_wait_epilogue(LaunchCtl* ctl, unsigned int k1) {
+__device__ bool resident_wait_epilogue(LaunchCtl* ctl, unsigned int k1, long long spin_limit) {
   __shared__ int ok;
   if (threadIdx.x == 0) {
     int good = 1;
     long long it = 0;
     while (ld_acquire_u32(&ctl->epi) < k1) {
-      if (*(volatile int32_t*)&ctl->err != 0 || ++it > kGridSpinLimit) {
+      if (*(volatile int32_t*)&ctl->err != 0 || ++it > spin_limit) {
         atomicExch(&ctl->err, 1);
         good = 0;
         break;
@@ -505,15 +513,18 @@ __device__ __forceinline__ void store_owned_rows(const uint2* pl, const BitsGeom
   for (int it = 0; it < g.iters_white; ++it) {
     const int r = 2 + g.row0 + it * g.rstep;
     if (r >= 2 + g.hv) break;
-    const uint2 fin = pl[r * g.NC + g.col];
+    const uint2 fin = ld_chk(pl, r * g.NC + g.col, g.pw);
     const int y = wrap_i(g.y0 - 2 + r, g.ly);
     uint4 v0, v1, v2, v3;
     unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
-    uint4* out = (uint4*)(dst + (size_t)y * g.pitch + 64 * gs);
-    out[0] = v0;
-    out[1] = v1;
-    out[2] = v2;
-    out[3] = v3;
+    const size_t off = (size_t)y * g.pitch + 64 * gs;
+    uint4* out = (uint4*)(dst + off);
+    if (GPUMC_IN(off + 63, g.gbytes)) {
+      out[0] = v0;
+      out[1] = v1;
+      out[2] = v2;
+      out[3] = v3;
+    }
   }
 }
 
@@ -522,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_ising_resident(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                            GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl,
                            const int2* __restrict__ nbr, uint2* __restrict__ xchg, int xstride,
-                           int n_sweeps) {
+                           int n_sweeps, long long spin_limit) {
   extern __shared__ __align__(16) uint2 bsm[];
   __shared__ BitsTab tab;
   const TileItem t = tiles[blockIdx.x];
@@ -548,8 +559,12 @@ __global__ void __launch_bounds__(kThreads, 4)
         for (int i = threadIdx.x; i < 4 * W; i += kThreads) {
           const int sl = i / W, c = i - sl * W;
           const int row = sl < 2 ? sl : g.hv + sl;  // local rows 0, 1, hv+2, hv+3
-          bsm[(size_t)row * W + c] = sl < 2 ? __ldcg(up + (size_t)(2 + sl) * W + c)
-                                            : __ldcg(dn + (size_t)(sl - 2) * W + c);
+          const long long xn = (long long)gridDim.x * xstride;  // exchange buffer words
+          const long long iu = (long long)(up - xchg) + (long long)(2 + sl) * W + c;
+          const long long id = (long long)(dn - xchg) + (long long)(sl - 2) * W + c;
+          const uint2 v = sl < 2 ? (GPUMC_IN(iu, xn) ? __ldcg(xchg + iu) : make_uint2(0, 0))
+                                 : (GPUMC_IN(id, xn) ? __ldcg(xchg + id) : make_uint2(0, 0));
+          st_chk(bsm, (long long)row * W + c, (long long)g.pw, v);
         }
       }
       // the acceptance table depends only on the label, which within a
@@ -570,10 +585,11 @@ __global__ void __launch_bounds__(kThreads, 4)
       for (int i = threadIdx.x; i < 4 * W; i += kThreads) {
         const int sl = i / W, c = i - sl * W;
         const int row = sl < 2 ? 2 + sl : g.hv + sl - 2;  // local rows 2, 3, hv, hv+1
-        __stcg(out + (size_t)sl * W + c, bsm[(size_t)row * W + c]);
+        const long long io = (long long)(out - xchg) + (long long)sl * W + c;
+        if (GPUMC_IN(io, (long long)gridDim.x * xstride)) __stcg(xchg + io, ld_chk(bsm, (long long)row * W + c, (long long)g.pw));
       }
     }
-    if (!resident_grid_sync(ctl, ++phase * gridDim.x)) return;
+    if (!resident_grid_sync(ctl, ++phase * gridDim.x, spin_limit)) return;
     if (blockIdx.x == 0) {
       // the epilogue of sweep k drains accumulator slot k & 1, which no CTA
       // touches again before the next barrier (its next use is sweep k + 2)
@@ -586,11 +602,124 @@ __global__ void __launch_bounds__(kThreads, 4)
     } else if (G->pt_interval > 0 && sweep < target && ((sweep + 1) % (uint64_t)G->pt_interval) == 0) {
       // a PT exchange after this sweep changes this group's labels (its
       // acceptance tables for the next sweep): wait for the epilogue
-      if (!resident_wait_epilogue(ctl, (unsigned int)(k + 1))) return;
+      if (!resident_wait_epilogue(ctl, (unsigned int)(k + 1), spin_limit)) return;
     }
   }
   const uint64_t s_end = s0 + (uint64_t)n_sweeps < target ? s0 + (uint64_t)n_sweeps : (s0 > target ? s0 : target);
   store_owned_rows(bsm, g, (int8_t*)L->buf[s_end & 1]);
+}
+
+// ---------------------------------------------------------------------------
+// Resident 3D tiles: the same temporal blocking for cubic lattices.  A tile is
+// a slab of whole planes z0 .. z0+dz-1 (dz >= 2; rows wrap inside a plane, no
+// y halo), held with two halo planes on each side: local planes 0 .. dz+3,
+// plane p at z0 - 2 + p.  A sweep runs the black pass on planes 1 .. dz+2
+// (the halo planes next to the slab too, so the white pass of the slab's end
+// planes sees final black neighbours) and the white pass on the owned planes
+// 2 .. dz+1, the same passes and stream as the streaming 3D kernel, so the
+// trajectory is bit-identical to it.  After the white pass a tile publishes
+// its first two and last two owned planes to its exchange slot (parity k & 1)
+// and, after the grid barrier, refreshes halo planes 0, 1 from the slab below
+// (its last two owned planes) and dz+2, dz+3 from the slab above (its first
+// two).  The epilogue, the PT exchange and the bounded waits are those of the
+// 2D resident kernel.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_plane(const uint2* pl, const BitsGeom& g, int z, int8_t* dst) {
+  if (g.row0 >= g.rstep) return;
+  const int gs = wrap_i(g.s0 + g.col - g.xh, g.nseg);
+  for (int it = 0; it < g.iters_load; ++it) {
+    const int r = g.row0 + it * g.rstep;
+    if (r >= g.R) break;
+    const uint2 fin = ld_chk(pl, r * g.NC + g.col, g.pw);
+    uint4 v0, v1, v2, v3;
+    unpack_segment(fin.x, fin.y, v0, v1, v2, v3);
+    const size_t off = ((size_t)z * g.ly + r) * g.pitch + 64 * gs;
+    uint4* out = (uint4*)(dst + off);
+    if (GPUMC_IN(off + 63, g.gbytes)) {
+      out[0] = v0;
+      out[1] = v1;
+      out[2] = v2;
+      out[3] = v3;
+    }
+  }
+}
+
+template <int ALG>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_sweep_ising_resident3(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
+                            GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl,
+                            const int2* __restrict__ nbr, uint2* __restrict__ xchg, int xstride,
+                            int n_sweeps, long long spin_limit) {
+  extern __shared__ __align__(16) uint2 bsm[];
+  __shared__ BitsTab tab;
+  const TileItem t = tiles[blockIdx.x];
+  LatDesc* L = &lats[t.lat];
+  const GroupDesc* G = &groups[L->group];
+  const BitsGeom g = make_bits_geom(t, L);  // whole planes: yw, R = hv = ly
+  const int lz = L->lz;
+  const int dz = min(t.tz, lz - t.z0);
+  const int pw = g.pw;
+  const long long np = (long long)(dz + 4) * pw;  // words of the resident slab
+  const size_t slot = (size_t)4 * pw;
+  const long long xn = (long long)gridDim.x * xstride;  // words of the exchange buffer
+  uint2* mine = xchg + (size_t)blockIdx.x * xstride;  // [parity][4 planes][pw]
+  const int2 nb = nbr[blockIdx.x];  // (slab below, slab above)
+  const uint64_t s0 = ld_volatile_u64(&L->sweep);
+  const uint64_t target = L->target;
+  auto zof = [&](int p) { return wrap_i(t.z0 - 2 + p, lz); };
+  for (int p = 0; p < dz + 4; ++p) load_bits_plane(bsm + (size_t)p * pw, (const int8_t*)L->buf[s0 & 1], zof(p), g);
+  unsigned int phase = 0;
+  for (int k = 0; k < n_sweeps; ++k) {
+    const uint64_t sweep = s0 + (uint64_t)k;
+    if (sweep < target) {
+      if (k > 0) {
+        const long long dn = (long long)nb.x * xstride + (long long)((k - 1) & 1) * slot;
+        const long long up = (long long)nb.y * xstride + (long long)((k - 1) & 1) * slot;
+        for (int i = threadIdx.x; i < 4 * pw; i += kThreads) {
+          const int sl = i / pw, w = i - sl * pw;
+          const int p = sl < 2 ? sl : dz + sl;  // local planes 0, 1, dz+2, dz+3
+          const long long src = sl < 2 ? dn + (long long)(2 + sl) * pw + w : up + (long long)(sl - 2) * pw + w;
+          const uint2 v = GPUMC_IN(src, xn) ? __ldcg(xchg + src) : make_uint2(0, 0);
+          st_chk(bsm, (long long)p * pw + w, np, v);
+        }
+      }
+      if (k == 0 || (G->pt_interval > 0 && sweep % (uint64_t)G->pt_interval == 0))
+        load_bits_table<ALG>(tab, L, G);
+      __syncthreads();
+      const BitsPhilox P = make_bits_philox(L->key, sweep);
+      PassAcc acc = {0, 0, 0, 0};
+      for (int p = 1; p <= dz + 2; ++p)
+        bits_pass<3, ALG>(bsm + (size_t)p * pw, bsm + (size_t)(p - 1) * pw, bsm + (size_t)(p + 1) * pw, g, zof(p),
+                          0, 0, g.R, g.iters_black, p >= 2 && p <= dz + 1, 0, nullptr, tab, P, acc);
+      __syncthreads();
+      for (int p = 2; p <= dz + 1; ++p)
+        bits_pass<3, ALG>(bsm + (size_t)p * pw, bsm + (size_t)(p - 1) * pw, bsm + (size_t)(p + 1) * pw, g, zof(p),
+                          1, 0, g.hv, g.iters_white, true, 2, nullptr, tab, P, acc);
+      flush_bits((k & 1) ? &L->acc2 : &L->acc, acc, 6);
+      __syncthreads();
+      const long long out = (long long)blockIdx.x * xstride + (long long)(k & 1) * slot;
+      for (int i = threadIdx.x; i < 4 * pw; i += kThreads) {
+        const int sl = i / pw, w = i - sl * pw;
+        const int p = sl < 2 ? 2 + sl : dz + sl - 2;  // local planes 2, 3, dz, dz+1
+        if (GPUMC_IN(out + (long long)sl * pw + w, xn))
+          __stcg(xchg + out + (long long)sl * pw + w, ld_chk(bsm, (long long)p * pw + w, np));
+      }
+    }
+    if (!resident_grid_sync(ctl, ++phase * gridDim.x, spin_limit)) return;
+    if (blockIdx.x == 0) {
+      finish_groups(lats, groups, ctl->group_ids, ctl->n_groups, k & 1);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicExch(&ctl->epi, (unsigned int)(k + 1));
+      }
+    } else if (G->pt_interval > 0 && sweep < target && ((sweep + 1) % (uint64_t)G->pt_interval) == 0) {
+      if (!resident_wait_epilogue(ctl, (unsigned int)(k + 1), spin_limit)) return;
+    }
+  }
+  (void)mine;
+  const uint64_t s_end = s0 + (uint64_t)n_sweeps < target ? s0 + (uint64_t)n_sweeps : (s0 > target ? s0 : target);
+  for (int p = 2; p <= dz + 1; ++p) store_plane(bsm + (size_t)p * pw, g, zof(p), (int8_t*)L->buf[s_end & 1]);
 }
 
 template __global__ void k_sweep_ising_bits<2, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
@@ -598,8 +727,14 @@ template __global__ void k_sweep_ising_bits<3, 0>(const TileItem*, LatDesc*, Gro
 template __global__ void k_sweep_ising_bits<2, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_ising_bits<3, 1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_ising_resident<0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*,
-                                                   const int2*, uint2*, int, int);
+                                                   const int2*, uint2*, int, int, long long);
 template __global__ void k_sweep_ising_resident<1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*,
-                                                   const int2*, uint2*, int, int);
+                                                   const int2*, uint2*, int, int, long long);
+template __global__ void k_sweep_ising_resident3<0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*,
+                                                    const int2*, uint2*, int, int, long long);
+template __global__ void k_sweep_ising_resident3<1>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*,
+                                                    const int2*, uint2*, int, int, long long);
+
+GPUMC_BOUNDS_MODULE(sweep_ising_bits)
 
 }  // namespace gpumc

@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
   const int hv = min(t.ty, ly - t.y0);
   const int S = Wv + 4, R = hv + 4;
   const int plane = R * S;
+  const long long gwords = (long long)pitch * ly * lz;  // words of one buffer (bounds checks)
   long long dE = 0;
   // words k, k + kThreads, ... of the R x S staged rows, walked by a
   // division-free (row, column) cursor
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
     while (r < R) {
       const int y = wrap1(t.y0 - 2 + r, ly);
       const int x = wrap1(t.x0 - 2 + c, lx);
-      pl[r * S + c] = cur[((size_t)z * ly + y) * (size_t)pitch + x];
+      st_chk(pl, r * S + c, plane, ld_chk(cur, (long long)(((size_t)z * ly + y) * (size_t)pitch + x), gwords));
       c += lstep_c;
       r += lstep_r;
       if (c >= S) {
@@ -198,28 +199,29 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
         const int y = wrap1(t.y0 - 2 + r, ly);
         const int pos = xlo + 2 * k + ((xlo + y + z + colour) & 1);
         const int off = r * S + (pos - t.x0 + 2);
-        unsigned long long nb[6] = {pl[off - 1], pl[off + 1], pl[off - S], pl[off + S], 0, 0};
+        unsigned long long nb[6] = {ld_chk(pl, off - 1, plane), ld_chk(pl, off + 1, plane),
+                                    ld_chk(pl, off - S, plane), ld_chk(pl, off + S, plane), 0, 0};
         if (DIM == 3) {
-          nb[4] = pm[off];
-          nb[5] = pp[off];
+          nb[4] = ld_chk(pm, off, plane);
+          nb[5] = ld_chk(pp, off, plane);
         }
         const int xr = wrap1(pos, lx);
         const uint64_t site = ((uint64_t)z * ly + y) * (uint64_t)lx + (uint64_t)xr;
         const bool owned = owned_plane && r >= 2 && r < 2 + hv && pos >= t.x0 && pos < t.x0 + Wv;
         long long de = 0;
-        const unsigned long long nw = msc_site<DIM>(pl[off], nb, tab, P, site, (uint32_t)colour, de);
+        const unsigned long long nw = msc_site<DIM>(ld_chk(pl, off, plane), nb, tab, P, site, (uint32_t)colour, de);
         res[it] = nw;
         roff[it] = off;
         if (owned) {
           dE += de;
-          nxt[((size_t)z * ly + y) * (size_t)pitch + xr] = nw;
+          st_chk(nxt, (long long)(((size_t)z * ly + y) * (size_t)pitch + xr), gwords, nw);
         }
       }
     }
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kMscMaxItems; ++it)
-      if (roff[it] >= 0) pl[roff[it]] = res[it];
+      if (roff[it] >= 0) st_chk(pl, roff[it], plane, res[it]);
     __syncthreads();
   };
   if (DIM == 2) {
@@ -372,5 +374,7 @@ template __global__ void k_sweep_msc<2>(const TileItem*, LatDesc*, GroupDesc*, L
 template __global__ void k_sweep_msc<3>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_msc_measure<2>(const LatDesc*, int, unsigned long long*);
 template __global__ void k_msc_measure<3>(const LatDesc*, int, unsigned long long*);
+
+GPUMC_BOUNDS_MODULE(sweep_msc)
 
 }  // namespace gpumc

@@ -9,12 +9,18 @@
 // and neighbour reads are served by L1/L2.  The colour-1 launch ends with the
 // sweep epilogue.
 //
-// Energy: on the bipartite periodic lattice every bond has exactly one
+// Observables: on the bipartite periodic lattice every bond has exactly one
 // colour-1 end, so the colour-1 pass sums s . h over its sites with their
-// final spins (fp64 neighbour sums of the fp32 components, exact products)
-// and the epilogue sets E = -J times that sum: the energy after each sweep is
-// computed afresh rather than carried by a cache of per-move changes, so it
-// cannot drift, and the colour-0 pass does no fp64 work.
+// final spins and the epilogue sets E = -J times that sum: the energy after
+// each sweep is computed afresh rather than carried by a cache of per-move
+// changes, so it cannot drift.  The sum is taken in fixed point: each site
+// adds rint(2^19 s . h) (the fp32 dot with its fp32 neighbour sum h, the
+// decision's h) to an integer accumulator, and the magnetisation components
+// add rint(2^21 s_c); integer sums do not depend on the order in which
+// threads and CTAs combine them, so the records are bit-identical to the CPU
+// replay.  Accuracy: a few 1e-7 per bond from the fp32 products, i.e. the
+// precision of the fp32 spins themselves (relative 1e-9 on the total energy
+// of a 64^3 lattice).
 //
 // Proposal: a uniform point on the spherical cap of half-angle alpha around
 // the current spin (w = 1 - cos(alpha) stored per lattice, adapted toward 50 %
@@ -47,9 +53,16 @@
 // the cap proposal.  Draws come from tag TAG_O3HB (word 0: v, word 1: phi);
 // there is no cone to adapt, and "accepted" counts the sites that changed.
 //
-// Every fp32 operation is an explicitly rounded intrinsic and exp / log /
-// sin / cos are the engine's own polynomials, so a CPU replay in the same
-// operation order reproduces the device trajectory bit for bit.
+// Arithmetic of the Metropolis step (ALG 0, 2, 3): two sites per thread
+// evaluated together with Blackwell's packed fp32 pair instructions
+// (fma/add/mul.rn.f32x2: one instruction, two IEEE-rounded lane results),
+// uniforms built from Philox bits (1.m - 1 with 23 bits of the word, no
+// integer-to-float conversion), products fused where the CPU replay fuses
+// them (fmaf), square root and division IEEE-rounded, and exp / sin / cos the
+// engine's own polynomials; the CPU replay (oracle/oracle.c,
+// orc_o3_propose / orc_o3_accept) performs the same operations per site and
+// reproduces the device trajectory bit for bit.  The heat bath (ALG 1) keeps
+// its scalar per-site arithmetic.
 #include "device_common.cuh"
 #include "epilogue.cuh"
 
@@ -95,64 +108,6 @@ __device__ __forceinline__ void o3_renorm(float& px, float& py, float& pz) {
   pz = fmul(pz, f);
 }
 
-// Metropolis step: PROP 0 cap proposal (w = 1 - cos(alpha) in omc), 1
-// uniform unit vector, 2 OPSS plane rotation (sigma in omc).  Returns the
-// decision and the proposed spin and its fp32 dE.
-template <int PROP>
-__device__ __forceinline__ bool o3_update(float ax, float ay, float az, float hx, float hy,
-                                          float hz, uint4 o, float omc, float mJ, float beta,
-                                          float& nx, float& ny, float& nz, float& dE) {
-  float px, py, pz;
-  if (PROP == 0) {
-    const float w = fmul(fmul((float)(o.x >> 8), 0x1p-24f), omc);
-    const float ct = fsub(1.0f, w);
-    const float st = fsqrt(fmul(w, fsub(2.0f, w)));
-    float cp, sp;
-    sincos_turn(o.y, cp, sp);
-    o3_place(ax, ay, az, ct, st, cp, sp, px, py, pz);
-  } else if (PROP == 1) {
-    pz = fsub(1.0f, fmul(2.0f, fmul((float)(o.x >> 8), 0x1p-24f)));
-    const float rho = fsqrt(fmul(fsub(1.0f, pz), fadd(1.0f, pz)));
-    float cp, sp;
-    sincos_turn(o.y, cp, sp);
-    px = fmul(rho, cp);
-    py = fmul(rho, sp);
-    o3_renorm(px, py, pz);
-  } else {
-    const uint32_t plane = __umulhi(o.x, 3u);
-    const float u = fmul(fadd((float)(o.y >> 8), 0.5f), 0x1p-24f);
-    const float theta = fmul(omc, fsub(fmul(2.0f, u), 1.0f));
-    // theta as a signed fraction of a turn, 32-bit fixed point
-    const float turns = fmul(theta, 0x1.45f306p-3f);  // 1 / (2 pi)
-    const uint32_t tu = (uint32_t)(long long)__float2ll_rn(fmul(turns, 0x1p32f));
-    float c, s;
-    sincos_turn(tu, c, s);
-    const float a0 = plane == 0 ? ax : (plane == 1 ? ay : az);
-    const float a1 = plane == 0 ? ay : (plane == 1 ? az : ax);
-    const float r0 = fsub(fmul(c, a0), fmul(s, a1)), r1 = fadd(fmul(s, a0), fmul(c, a1));
-    px = plane == 0 ? r0 : (plane == 1 ? ax : r1);
-    py = plane == 0 ? r1 : (plane == 1 ? r0 : ay);
-    pz = plane == 0 ? az : (plane == 1 ? r1 : r0);
-    o3_renorm(px, py, pz);
-  }
-  const float dot =
-      fadd(fadd(fmul(fsub(px, ax), hx), fmul(fsub(py, ay), hy)), fmul(fsub(pz, az), hz));
-  const float de = fmul(mJ, dot);
-  bool ok;
-  if (de <= 0.0f) {
-    ok = true;
-  } else {
-    const float p = exp_neg(-fmul(beta, de));
-    const float u = fmul(fadd((float)(o.z >> 8), 0.5f), 0x1p-24f);
-    ok = u < p;
-  }
-  nx = px;
-  ny = py;
-  nz = pz;
-  dE = de;
-  return ok;
-}
-
 // Heat-bath draw of a site with neighbour sum h (fp32) under coupling Jf.
 __device__ __forceinline__ void o3_heat_bath(float hx, float hy, float hz, uint4 o, float Jf, float beta,
                                              float& nx, float& ny, float& nz) {
@@ -176,6 +131,200 @@ __device__ __forceinline__ void o3_heat_bath(float hx, float hy, float hz, uint4
   float cp, sp;
   sincos_turn(o.y, cp, sp);
   o3_place(ax, ay, az, ct, st, cp, sp, nx, ny, nz);
+}
+
+// ---- packed fp32 pairs (lane 0: the thread's first site, lane 1: its second)
+struct f2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ f2 F2(float a, float b) {
+  return f2{((unsigned long long)__float_as_uint(b) << 32) | __float_as_uint(a)};
+}
+__device__ __forceinline__ f2 F2s(float a) { return F2(a, a); }
+__device__ __forceinline__ float lo(f2 x) { return __uint_as_float((uint32_t)x.v); }
+__device__ __forceinline__ float hi(f2 x) { return __uint_as_float((uint32_t)(x.v >> 32)); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return d;
+}
+
+// Uniforms from Philox bits without an integer-to-float conversion:
+// unit23 = 1.m - 1 with the top 23 bits of u as m (multiples of 2^-23 in
+// [0, 1)); half23 = unit23 + 2^-24 (in (0, 1)).  Both subtractions are exact.
+__device__ __forceinline__ float bits23(uint32_t u) { return __uint_as_float(0x3F800000u | (u >> 9)); }
+__device__ __forceinline__ f2 unit23_2(uint32_t a, uint32_t b) { return sub2(F2(bits23(a), bits23(b)), F2s(1.0f)); }
+__device__ __forceinline__ f2 half23_2(uint32_t a, uint32_t b) {
+  return sub2(F2(bits23(a), bits23(b)), F2s(0x1.fffffep-1f));
+}
+
+// (cos, sin) of 2 pi u / 2^32 for both lanes: octant from the top 3 bits, the
+// next 23 bits as the fraction t of the octant (1.m - 1), Taylor polynomials
+// of degree 9 / 10 on [0, pi/4] (fused Horner, packed), swaps and signs per
+// lane by octant.
+__device__ __forceinline__ void sincos23_2(uint32_t ua, uint32_t ub, f2& c, f2& s) {
+  const uint32_t oa = ua >> 29, ob = ub >> 29;
+  f2 t = sub2(F2(__uint_as_float(0x3F800000u | ((ua >> 6) & 0x7FFFFFu)),
+                 __uint_as_float(0x3F800000u | ((ub >> 6) & 0x7FFFFFu))),
+              F2s(1.0f));
+  const f2 t1 = sub2(F2s(1.0f), t);
+  t = F2((oa & 1u) ? lo(t1) : lo(t), (ob & 1u) ? hi(t1) : hi(t));
+  const f2 th = mul2(t, F2s(0x1.921fb6p-1f));
+  const f2 t2 = mul2(th, th);
+  f2 sp = fma2(F2s(0x1.71de3ap-19f), t2, F2s(-0x1.a01a02p-13f));
+  sp = fma2(sp, t2, F2s(0x1.111112p-7f));
+  sp = fma2(sp, t2, F2s(-0x1.555556p-3f));
+  sp = fma2(sp, t2, F2s(1.0f));
+  const f2 sn = mul2(th, sp);
+  f2 cp = fma2(F2s(-0x1.27e4fcp-22f), t2, F2s(0x1.a01a02p-16f));
+  cp = fma2(cp, t2, F2s(-0x1.6c16c2p-10f));
+  cp = fma2(cp, t2, F2s(0x1.555556p-5f));
+  cp = fma2(cp, t2, F2s(-0.5f));
+  const f2 cs = fma2(cp, t2, F2s(1.0f));
+  // octants 1, 2, 5, 6 swap; cos < 0 in octants 2..5, sin < 0 in 4..7
+  const bool swa = ((oa + 1u) & 2u) != 0u, swb = ((ob + 1u) & 2u) != 0u;
+  const float aa = swa ? lo(sn) : lo(cs), ba = swa ? lo(cs) : lo(sn);
+  const float ab = swb ? hi(sn) : hi(cs), bb = swb ? hi(cs) : hi(sn);
+  c = F2(((oa + 2u) & 4u) ? -aa : aa, ((ob + 2u) & 4u) ? -ab : ab);
+  s = F2((oa & 4u) ? -ba : ba, (ob & 4u) ? -bb : bb);
+}
+
+// exp(x) for -87 <= x <= 0, both lanes (lanes below -87 are clamped there,
+// where the result is below every acceptance draw; lanes above 0 are not
+// used): x log2(e) = n + f, n = rint by the 1.5 2^23 shifter, f in
+// [-1/2, 1/2], e^(f ln 2) by the degree-7 Taylor polynomial, times 2^n.
+__device__ __forceinline__ f2 exp_neg2_2(f2 x) {
+  x = F2(fmaxf(lo(x), -87.0f), fmaxf(hi(x), -87.0f));
+  const f2 y = mul2(x, F2s(0x1.715476p+0f));
+  const f2 r = add2(y, F2s(0x1.8p23f));
+  const f2 n = sub2(r, F2s(0x1.8p23f));
+  const f2 t = mul2(sub2(y, n), F2s(0x1.62e430p-1f));
+  f2 p = fma2(F2s(0x1.a01a02p-13f), t, F2s(0x1.6c16c2p-10f));
+  p = fma2(p, t, F2s(0x1.111112p-7f));
+  p = fma2(p, t, F2s(0x1.555556p-5f));
+  p = fma2(p, t, F2s(0x1.555556p-3f));
+  p = fma2(p, t, F2s(0.5f));
+  p = fma2(p, t, F2s(1.0f));
+  p = fma2(p, t, F2s(1.0f));
+  // 2^n: (bits(r) - 0x4B400000 + 127) << 23
+  const f2 sc = F2(__uint_as_float((__float_as_uint(lo(r)) - 0x4B3FFF81u) << 23),
+                   __uint_as_float((__float_as_uint(hi(r)) - 0x4B3FFF81u) << 23));
+  return mul2(p, sc);
+}
+
+// Metropolis step of two sites (PROP 0 cap of 1 - cos(alpha) = omc, 1
+// uniform unit vector, 2 OPSS rotation with bound omc): proposals n and the
+// decisions.  Per lane the operations of orc_o3_propose / orc_o3_accept.
+template <int PROP>
+__device__ __forceinline__ void o3_metropolis_2(f2 ax, f2 ay, f2 az, f2 hx, f2 hy, f2 hz, const uint4& oa,
+                                                const uint4& ob, float omc, float mJ, float beta, f2& nx,
+                                                f2& ny, f2& nz, bool& ok_a, bool& ok_b) {
+  f2 px, py, pz;
+  if (PROP == 0) {
+    const f2 w = mul2(unit23_2(oa.x, ob.x), F2s(omc));
+    const f2 ct = sub2(F2s(1.0f), w);
+    const f2 s2 = fma2(mul2(w, F2s(-1.0f)), w, add2(w, w));
+    const f2 st = F2(__fsqrt_rn(lo(s2)), __fsqrt_rn(hi(s2)));
+    f2 cp, sp;
+    sincos23_2(oa.y, ob.y, cp, sp);
+    const f2 vx = mul2(st, cp), vy = mul2(st, sp);
+    // Duff et al. (JCGT 2017) basis {e1, e2, a}: sg = sign(az), k = -1/(sg + az)
+    const f2 sg = F2(lo(az) >= 0.0f ? 1.0f : -1.0f, hi(az) >= 0.0f ? 1.0f : -1.0f);
+    const f2 d = add2(sg, az);
+    const f2 k = F2(__fdiv_rn(-1.0f, lo(d)), __fdiv_rn(-1.0f, hi(d)));
+    const f2 axk = mul2(ax, k);
+    const f2 b = mul2(ay, axk);
+    const f2 sax = mul2(sg, ax);
+    const f2 e1x = fma2(sax, axk, F2s(1.0f)), e1y = mul2(sg, b), e1z = mul2(sax, F2s(-1.0f));
+    const f2 e2x = b, e2y = fma2(mul2(ay, k), ay, sg), e2z = mul2(ay, F2s(-1.0f));
+    px = fma2(ct, ax, fma2(vy, e2x, mul2(vx, e1x)));
+    py = fma2(ct, ay, fma2(vy, e2y, mul2(vx, e1y)));
+    pz = fma2(ct, az, fma2(vy, e2z, mul2(vx, e1z)));
+  } else if (PROP == 1) {
+    pz = fma2(F2s(-2.0f), unit23_2(oa.x, ob.x), F2s(1.0f));
+    const f2 r2 = fma2(mul2(pz, F2s(-1.0f)), pz, F2s(1.0f));
+    const f2 rho = F2(__fsqrt_rn(lo(r2)), __fsqrt_rn(hi(r2)));
+    f2 cp, sp;
+    sincos23_2(oa.y, ob.y, cp, sp);
+    px = mul2(rho, cp);
+    py = mul2(rho, sp);
+  } else {
+    const f2 theta = mul2(F2s(omc), fma2(F2s(2.0f), half23_2(oa.y, ob.y), F2s(-1.0f)));
+    const f2 turns = mul2(mul2(theta, F2s(0x1.45f306p-3f)), F2s(0x1p32f));
+    const uint32_t ta = (uint32_t)(long long)__float2ll_rn(lo(turns));
+    const uint32_t tb = (uint32_t)(long long)__float2ll_rn(hi(turns));
+    f2 c, sn;
+    sincos23_2(ta, tb, c, sn);
+    const uint32_t pa = __umulhi(oa.x, 3u), pb = __umulhi(ob.x, 3u);
+    const f2 a0 = F2(pa == 0 ? lo(ax) : (pa == 1 ? lo(ay) : lo(az)), pb == 0 ? hi(ax) : (pb == 1 ? hi(ay) : hi(az)));
+    const f2 a1 = F2(pa == 0 ? lo(ay) : (pa == 1 ? lo(az) : lo(ax)), pb == 0 ? hi(ay) : (pb == 1 ? hi(az) : hi(ax)));
+    const f2 r0 = fma2(c, a0, mul2(mul2(sn, a1), F2s(-1.0f))), r1 = fma2(sn, a0, mul2(c, a1));
+    px = F2(pa == 0 ? lo(r0) : (pa == 1 ? lo(ax) : lo(r1)), pb == 0 ? hi(r0) : (pb == 1 ? hi(ax) : hi(r1)));
+    py = F2(pa == 0 ? lo(r1) : (pa == 1 ? lo(r0) : lo(ay)), pb == 0 ? hi(r1) : (pb == 1 ? hi(r0) : hi(ay)));
+    pz = F2(pa == 0 ? lo(az) : (pa == 1 ? lo(r1) : lo(r0)), pb == 0 ? hi(az) : (pb == 1 ? hi(r1) : hi(r0)));
+  }
+  // one Newton step of 1/sqrt(n2) from 1
+  const f2 n2 = fma2(pz, pz, fma2(py, py, mul2(px, px)));
+  const f2 f = fma2(F2s(-0.5f), n2, F2s(1.5f));
+  px = mul2(px, f);
+  py = mul2(py, f);
+  pz = mul2(pz, f);
+  const f2 dot = fma2(sub2(pz, az), hz, fma2(sub2(py, ay), hy, mul2(sub2(px, ax), hx)));
+  const f2 de = mul2(F2s(mJ), dot);
+  const f2 p = exp_neg2_2(mul2(F2s(-beta), de));
+  const f2 u = half23_2(oa.z, ob.z);
+  ok_a = lo(de) <= 0.0f || lo(u) < lo(p);
+  ok_b = hi(de) <= 0.0f || hi(u) < hi(p);
+  nx = px;
+  ny = py;
+  nz = pz;
+}
+
+// Fixed-point observables of a site's final spin (s) and, in the colour-1
+// pass, its bond sum with the fp32 neighbour sum h: rint(2^21 s_c) and
+// rint(2^19 s . h) by the 1.5 2^23 shifter (|2^21 s_c| <= 2^21,
+// |2^19 s . h| <= 6 2^19 < 2^22), summed in 32-bit integers.
+struct O3Fix {
+  int32_t m[3], e;
+};
+__device__ __forceinline__ int32_t fix_shift(float v) { return (int32_t)(__float_as_uint(v) - 0x4B400000u); }
+template <bool BOND>
+__device__ __forceinline__ void o3_fix_add_2(O3Fix& q, f2 sx, f2 sy, f2 sz, f2 hx, f2 hy, f2 hz, bool use_b) {
+  const f2 X = F2s(0x1.8p23f);
+  const f2 mx = fma2(sx, F2s(0x1p21f), X), my = fma2(sy, F2s(0x1p21f), X), mz = fma2(sz, F2s(0x1p21f), X);
+  q.m[0] += fix_shift(lo(mx)) + (use_b ? fix_shift(hi(mx)) : 0);
+  q.m[1] += fix_shift(lo(my)) + (use_b ? fix_shift(hi(my)) : 0);
+  q.m[2] += fix_shift(lo(mz)) + (use_b ? fix_shift(hi(mz)) : 0);
+  if (BOND) {
+    const f2 e = fma2(fma2(sz, hz, fma2(sy, hy, mul2(sx, hx))), F2s(0x1p19f), X);
+    q.e += fix_shift(lo(e)) + (use_b ? fix_shift(hi(e)) : 0);
+  }
+}
+// Scalar form (heat-bath sites).
+template <bool BOND>
+__device__ __forceinline__ void o3_fix_add(O3Fix& q, float sx, float sy, float sz, float hx, float hy, float hz) {
+  q.m[0] += fix_shift(__fmaf_rn(sx, 0x1p21f, 0x1.8p23f));
+  q.m[1] += fix_shift(__fmaf_rn(sy, 0x1p21f, 0x1.8p23f));
+  q.m[2] += fix_shift(__fmaf_rn(sz, 0x1p21f, 0x1.8p23f));
+  if (BOND) {
+    const float e = __fmaf_rn(sz, hz, __fmaf_rn(sy, hy, __fmul_rn(sx, hx)));
+    q.e += fix_shift(__fmaf_rn(e, 0x1p19f, 0x1.8p23f));
+  }
 }
 
 // Philox4x32-10 of counter (site, colour | TAG_O3 << 1, sweep) with the
@@ -212,18 +361,16 @@ __device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
 }
 
 // One site of a colour pass: its own spin and the fp32 sum of its
-// neighbours (the decision), plus, in the colour-1 pass, their exact fp64 sum
-// (the sweep's bond sum), loaded before any update of the thread's sites so
-// that the loads of two sites overlap.
+// neighbours (in the fixed order x-1, x+1, y-1, y+1, z-1, z+1).
 struct O3Site {
   uint32_t me, site;
   float ax, ay, az, hx, hy, hz;
-  double hxd, hyd, hzd;
 };
 
-template <int DIM, bool EXACT>
+template <int DIM>
 __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const float* S1, const float* S2,
-                                             int x, int y, int z, int lx, int ly, int lz, int pitch) {
+                                             int x, int y, int z, int lx, int ly, int lz, int pitch,
+                                             uint32_t cs) {
   const uint32_t rowoff = ((uint32_t)z * ly + y) * (uint32_t)pitch;
   const int ym = y ? y - 1 : ly - 1, yp = y + 1 < ly ? y + 1 : 0;
   const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
@@ -233,43 +380,100 @@ __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const fl
     zmo = ((uint32_t)zm * ly + y) * (uint32_t)pitch + x;
     zpo = ((uint32_t)zp * ly + y) * (uint32_t)pitch + x;
   }
-  // neighbour sum in the fixed order x-1, x+1, y-1, y+1, z-1, z+1
   const uint32_t nb[6] = {rowoff + xm, rowoff + xp, ((uint32_t)z * ly + ym) * (uint32_t)pitch + x,
                           ((uint32_t)z * ly + yp) * (uint32_t)pitch + x, zmo, zpo};
-  float hx = __ldg(S + nb[0]), hy = __ldg(S1 + nb[0]), hz = __ldg(S2 + nb[0]);
-  double hxd = 0.0, hyd = 0.0, hzd = 0.0;
-  if (EXACT) {
-    hxd = (double)hx;
-    hyd = (double)hy;
-    hzd = (double)hz;
-  }
+  float hx = ld_chk(S, nb[0], cs), hy = ld_chk(S1, nb[0], cs), hz = ld_chk(S2, nb[0], cs);
 #pragma unroll
   for (int i = 1; i < 2 * DIM; ++i) {
-    const float vx = __ldg(S + nb[i]), vy = __ldg(S1 + nb[i]), vz = __ldg(S2 + nb[i]);
-    hx = fadd(hx, vx);
-    hy = fadd(hy, vy);
-    hz = fadd(hz, vz);
-    if (EXACT) {
-      hxd += (double)vx;
-      hyd += (double)vy;
-      hzd += (double)vz;
-    }
+    hx = fadd(hx, ld_chk(S, nb[i], cs));
+    hy = fadd(hy, ld_chk(S1, nb[i], cs));
+    hz = fadd(hz, ld_chk(S2, nb[i], cs));
   }
   q.me = rowoff + x;
-  q.ax = S[q.me];
-  q.ay = S1[q.me];
-  q.az = S2[q.me];
+  q.ax = ld_chk(S, q.me, cs);
+  q.ay = ld_chk(S1, q.me, cs);
+  q.az = ld_chk(S2, q.me, cs);
   q.hx = hx;
   q.hy = hy;
   q.hz = hz;
-  q.hxd = hxd;
-  q.hyd = hyd;
-  q.hzd = hzd;
   q.site = (uint32_t)((size_t)(z * ly + y) * lx + x);
 }
 
+// Updates the pair (qa, qb) of a colour pass (qb only when `two`): writes
+// accepted spins in place, counts acceptances and adds the fixed-point
+// observables of the final spins.
+template <int COLOUR, int ALG>
+__device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& qb, bool two, const O3Philox& P,
+                                               float omc, float mJ, float beta, float* S, float* S1, float* S2,
+                                               uint32_t cs, O3Fix& fx, int& nacc) {
+  const uint4 oa = o3_philox(P, qa.site);
+  const uint4 ob = o3_philox(P, two ? qb.site : qa.site);
+  f2 fx2 = F2(qa.ax, qb.ax), fy2 = F2(qa.ay, qb.ay), fz2 = F2(qa.az, qb.az);
+  const f2 hx = F2(qa.hx, qb.hx), hy = F2(qa.hy, qb.hy), hz = F2(qa.hz, qb.hz);
+  bool ok_a, ok_b;
+  if (ALG == 1) {
+    float nx, ny, nz, mx, my, mz;
+    o3_heat_bath(qa.hx, qa.hy, qa.hz, oa, -mJ, beta, nx, ny, nz);
+    o3_heat_bath(qb.hx, qb.hy, qb.hz, ob, -mJ, beta, mx, my, mz);
+    ok_a = (nx != qa.ax) | (ny != qa.ay) | (nz != qa.az);
+    ok_b = (mx != qb.ax) | (my != qb.ay) | (mz != qb.az);
+    fx2 = F2(nx, mx);
+    fy2 = F2(ny, my);
+    fz2 = F2(nz, mz);
+  } else {
+    f2 nx, ny, nz;
+    o3_metropolis_2<ALG == 2 ? 1 : (ALG == 3 ? 2 : 0)>(fx2, fy2, fz2, hx, hy, hz, oa, ob, omc, mJ, beta, nx, ny, nz,
+                                                        ok_a, ok_b);
+    fx2 = F2(ok_a ? lo(nx) : qa.ax, ok_b ? hi(nx) : qb.ax);
+    fy2 = F2(ok_a ? lo(ny) : qa.ay, ok_b ? hi(ny) : qb.ay);
+    fz2 = F2(ok_a ? lo(nz) : qa.az, ok_b ? hi(nz) : qb.az);
+  }
+  ok_b = ok_b && two;
+  if (ok_a) {
+    st_chk(S, qa.me, cs, lo(fx2));
+    st_chk(S1, qa.me, cs, lo(fy2));
+    st_chk(S2, qa.me, cs, lo(fz2));
+  }
+  if (ok_b) {
+    st_chk(S, qb.me, cs, hi(fx2));
+    st_chk(S1, qb.me, cs, hi(fy2));
+    st_chk(S2, qb.me, cs, hi(fz2));
+  }
+  nacc += (int)ok_a + (int)ok_b;
+  // every bond has one colour-1 end: the colour-1 pass also sums s . h
+  o3_fix_add_2<COLOUR == 1>(fx, fx2, fy2, fz2, hx, hy, hz, two);
+}
+
+// Per-thread fixed-point sums into 64-bit totals (flushed often enough that
+// the 32-bit partial sums cannot overflow), then CTA sums and one atomic each.
+struct O3Totals {
+  long long m[3], e;
+};
+__device__ __forceinline__ void o3_flush(O3Totals& t, O3Fix& q) {
+  t.m[0] += q.m[0];
+  t.m[1] += q.m[1];
+  t.m[2] += q.m[2];
+  t.e += q.e;
+  q = O3Fix{{0, 0, 0}, 0};
+}
+template <int COLOUR>
+__device__ __forceinline__ void o3_commit(LatDesc* L, O3Totals& t, int nacc) {
+  long long v[5] = {t.m[0], t.m[1], t.m[2], t.e, (long long)nacc};
+  cta_sum(v);
+  if (threadIdx.x == 0) {
+    atomic_add_i64(&L->acc.mq[0], v[0]);
+    atomic_add_i64(&L->acc.mq[1], v[1]);
+    atomic_add_i64(&L->acc.mq[2], v[2]);
+    if (COLOUR == 1) {
+      atomic_add_i64(&L->acc.ebq, v[3]);
+      L->acc.fresh = 1;
+    }
+    if (v[4]) atomic_add_i64(&L->acc.accepted, v[4]);
+  }
+}
+
 // One colour pass over a tile of full rows (y0 .. y0+hv-1, planes z0 ..
-// z0+dv-1), one thread per site of the colour.
+// z0+dv-1), one thread per site of the colour, two sites at a time.
 template <int DIM, int COLOUR, int ALG>
 __global__ void __launch_bounds__(kThreads, 4)
     k_sweep_o3(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
@@ -287,9 +491,6 @@ __global__ void __launch_bounds__(kThreads, 4)
   float* S = (float*)L->buf[0];  // in place; component planes S, S1, S2
   float* S1 = S + (size_t)cs;
   float* S2 = S + 2 * (size_t)cs;
-  const float* Sr = S;
-  const float* Sr1 = S1;
-  const float* Sr2 = S2;
   const int label = G->label[L->replica];
   const float beta = G->betas_f[label];
   const float mJ = -G->Jf;
@@ -312,7 +513,8 @@ __global__ void __launch_bounds__(kThreads, 4)
     r0 = threadIdx.x / half;
     rstep = kThreads / half;
   }
-  double eb = 0.0, mx = 0.0, my = 0.0, mz = 0.0;  // eb: colour 1's sum of s . h
+  O3Fix fx = {{0, 0, 0}, 0};
+  O3Totals tot = {{0, 0, 0}, 0};
   int nacc = 0;
   // this thread's sites, row-major: rows r0, r0 + rstep, ... of the tile's
   // rows (y fastest, then z), columns col0, col0 + cstep, ...; taken two at a
@@ -336,61 +538,23 @@ __global__ void __launch_bounds__(kThreads, 4)
       }
     }
   };
-  auto update = [&](const O3Site& q) {
-    float nx, ny, nz, de;
-    bool ok;
-    if (ALG == 1) {
-      o3_heat_bath(q.hx, q.hy, q.hz, o3_philox(P, q.site), -mJ, beta, nx, ny, nz);
-      ok = (nx != q.ax) | (ny != q.ay) | (nz != q.az);
-    } else {
-      ok = o3_update<ALG == 2 ? 1 : (ALG == 3 ? 2 : 0)>(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site),
-                                                         omc, mJ, beta, nx, ny, nz, de);
-    }
-    float fx = q.ax, fy = q.ay, fz = q.az;
-    if (ok) {
-      ++nacc;
-      fx = nx;
-      fy = ny;
-      fz = nz;
-      S[q.me] = fx;
-      S1[q.me] = fy;
-      S2[q.me] = fz;
-    }
-    mx += (double)fx;
-    my += (double)fy;
-    mz += (double)fz;
-    // every bond has one colour-1 end: the sweep's energy is -J times the
-    // colour-1 pass's sum of s . h over the final spins (exact products of
-    // fp32 components and fp64 neighbour sums)
-    if (COLOUR == 1) eb += ((double)fx * q.hxd + (double)fy * q.hyd) + (double)fz * q.hzd;
-  };
   for (int k = 0; k < n_items; k += 2) {
     int x, y, z;
     O3Site qa, qb;
     next_site(x, y, z);
-    o3_load_site<DIM, COLOUR == 1>(qa, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
+    o3_load_site<DIM>(qa, S, S1, S2, x, y, z, lx, ly, lz, pitch, cs);
     const bool two = k + 1 < n_items;
     if (two) {
       next_site(x, y, z);
-      o3_load_site<DIM, COLOUR == 1>(qb, Sr, Sr1, Sr2, x, y, z, lx, ly, lz, pitch);
+      o3_load_site<DIM>(qb, S, S1, S2, x, y, z, lx, ly, lz, pitch, cs);
+    } else {
+      qb = qa;
     }
-    update(qa);
-    if (two) update(qb);
+    o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, S1, S2, cs, fx, nacc);
+    if ((k & 62) == 62) o3_flush(tot, fx);  // every 64 sites: 32-bit partials stay far from overflow
   }
-  double v[4] = {eb, mx, my, mz};
-  long long n[1] = {nacc};
-  cta_sum(v);
-  cta_sum(n);
-  if (threadIdx.x == 0) {
-    if (COLOUR == 1) {
-      atomicAdd(&L->acc.ebond, v[0]);
-      L->acc.fresh = 1;
-    }
-    atomicAdd(&L->acc.mx, v[1]);
-    atomicAdd(&L->acc.my, v[2]);
-    atomicAdd(&L->acc.mz, v[3]);
-    if (n[0]) atomic_add_i64(&L->acc.accepted, n[0]);
-  }
+  o3_flush(tot, fx);
+  o3_commit<COLOUR>(L, tot, nacc);
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
 
@@ -429,7 +593,7 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     return;
   }
   const int lx = L->lx, ly = L->ly, lz = L->lz, pitch = L->pitch;
-  const size_t cs = (size_t)pitch * ly * lz;  // component plane stride
+  const uint32_t cs = (uint32_t)pitch * ly * lz;  // component plane stride (< 2^32 elements)
   float* S = (float*)L->buf[0];
   const int label = G->label[L->replica];
   const float beta = G->betas_f[label];
@@ -448,8 +612,8 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
   const int cv0 = threadIdx.x % nvec, ccr0 = threadIdx.x / nvec;
   const int cc0 = ccr0 / RW, cr0 = ccr0 - cc0 * RW;
   const int step_v = kThreads % nvec, step_r = kThreads / nvec;
-  float* S1 = S + cs;
-  float* S2 = S + 2 * cs;
+  float* S1 = S + (size_t)cs;
+  float* S2 = S + 2 * (size_t)cs;
   auto copy_plane = [&](int sl, int z) {
     const int zz = z < 0 ? z + lz : (z >= lz ? z - lz : z);
     float* dst = osm + sl * slot;
@@ -458,7 +622,10 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     while (c < 3) {
       int y = t.y0 - 1 + r;
       y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
-      o3_cp_async16(dst + c * cstr + r * pitch + 4 * v, src + c * cs + y * pitch + 4 * v);
+      const long long so = (long long)(src - S) + (long long)c * cs + (long long)y * pitch + 4 * v;
+      const long long dof = (long long)(dst - osm) + (long long)c * cstr + (long long)r * pitch + 4 * v;
+      if (GPUMC_IN(so + 3, 3ll * cs) && GPUMC_IN(dof + 3, 4ll * slot))
+        o3_cp_async16(dst + c * cstr + r * pitch + 4 * v, src + (size_t)c * cs + y * pitch + 4 * v);
       v += step_v;
       r += step_r;
       if (v >= nvec) {
@@ -472,36 +639,12 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  double eb = 0.0, mx = 0.0, my = 0.0, mz = 0.0;  // eb: colour 1's sum of s . h
+  O3Fix fx = {{0, 0, 0}, 0};
+  O3Totals tot = {{0, 0, 0}, 0};
   int nacc = 0;
   const int half = lx >> 1;
   const int n_items = hv * half;  // colour sites of the tile's rows in one plane
   const int dr = kThreads / half, dj = kThreads - dr * half;  // cursor step of kThreads items
-  auto update = [&](const O3Site& q) {
-    float nx, ny, nz, de;
-    bool ok;
-    if (ALG == 1) {
-      o3_heat_bath(q.hx, q.hy, q.hz, o3_philox(P, q.site), -mJ, beta, nx, ny, nz);
-      ok = (nx != q.ax) | (ny != q.ay) | (nz != q.az);
-    } else {
-      ok = o3_update<ALG == 2 ? 1 : (ALG == 3 ? 2 : 0)>(q.ax, q.ay, q.az, q.hx, q.hy, q.hz, o3_philox(P, q.site),
-                                                         omc, mJ, beta, nx, ny, nz, de);
-    }
-    float fx = q.ax, fy = q.ay, fz = q.az;
-    if (ok) {
-      ++nacc;
-      fx = nx;
-      fy = ny;
-      fz = nz;
-      S[q.me] = fx;
-      S1[q.me] = fy;
-      S2[q.me] = fz;
-    }
-    mx += (double)fx;
-    my += (double)fy;
-    mz += (double)fz;
-    if (COLOUR == 1) eb += ((double)fx * q.hxd + (double)fy * q.hyd) + (double)fz * q.hzd;
-  };
   copy_plane(0, t.z0 - 1);
   copy_plane(1, t.z0);
   copy_plane(2, t.z0 + 1);
@@ -526,35 +669,28 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
       const int oc = (rl + 1) * pitch;  // slot row of y
       // neighbour order x-1, x+1, y-1, y+1, z-1, z+1 (as k_sweep_o3)
       float h[3];
-      double hd[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float* P = pc + c * cstr;
-        const float v0 = P[oc + xm], v1 = P[oc + xp];
-        const float v2 = P[oc - pitch + x];
-        const float v3 = P[oc + pitch + x];
-        const float v4 = pm[c * cstr + oc + x];
-        const float v5 = pp[c * cstr + oc + x];
-        h[c] = fadd(fadd(fadd(fadd(fadd(v0, v1), v2), v3), v4), v5);
-        hd[c] = COLOUR == 1
-                    ? (((((double)v0 + (double)v1) + (double)v2) + (double)v3) + (double)v4) + (double)v5
-                    : 0.0;
+        h[c] = fadd(fadd(fadd(fadd(fadd(ld_chk(P, oc + xm, cstr), ld_chk(P, oc + xp, cstr)),
+                                   ld_chk(P, oc - pitch + x, cstr)),
+                              ld_chk(P, oc + pitch + x, cstr)),
+                         ld_chk(pm + c * cstr, oc + x, cstr)),
+                    ld_chk(pp + c * cstr, oc + x, cstr));
       }
-      q.ax = pc[oc + x];
-      q.ay = pc[cstr + oc + x];
-      q.az = pc[2 * cstr + oc + x];
+      q.ax = ld_chk(pc, oc + x, cstr);
+      q.ay = ld_chk(pc + cstr, oc + x, cstr);
+      q.az = ld_chk(pc + 2 * cstr, oc + x, cstr);
       q.hx = h[0];
       q.hy = h[1];
       q.hz = h[2];
-      q.hxd = hd[0];
-      q.hyd = hd[1];
-      q.hzd = hd[2];
       // 32-bit index arithmetic: the same values as the 64-bit products
       // truncated to the 32-bit fields
       q.me = ((uint32_t)z * (uint32_t)ly + (uint32_t)y) * (uint32_t)pitch + (uint32_t)x;
       q.site = ((uint32_t)z * (uint32_t)ly + (uint32_t)y) * (uint32_t)lx + (uint32_t)x;
     };
-    // items i = threadIdx.x, + kThreads, ... as (row, column) cursors
+    // items i = threadIdx.x, + kThreads, ... as (row, column) cursors, two
+    // at a time
     int ra = threadIdx.x / half, ja = threadIdx.x - ra * half;
     for (int i = threadIdx.x; i < n_items; i += 2 * kThreads) {
       O3Site qa, qb;
@@ -566,8 +702,8 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
       }
       const bool two = i + kThreads < n_items;
       if (two) load_site(qb, rb, jb);
-      update(qa);
-      if (two) update(qb);
+      else qb = qa;
+      o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, S1, S2, cs, fx, nacc);
       ra = rb + dr;
       ja = jb + dj;
       if (ja >= half) {
@@ -575,23 +711,11 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
         ra += 1;
       }
     }
+    o3_flush(tot, fx);  // per plane: at most hv * lx / 512 sites per thread since the last flush
     __syncthreads();  // the next copy overwrites the z-1 slot read above
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  double v[4] = {eb, mx, my, mz};
-  long long n[1] = {nacc};
-  cta_sum(v);
-  cta_sum(n);
-  if (threadIdx.x == 0) {
-    if (COLOUR == 1) {
-      atomicAdd(&L->acc.ebond, v[0]);
-      L->acc.fresh = 1;
-    }
-    atomicAdd(&L->acc.mx, v[1]);
-    atomicAdd(&L->acc.my, v[2]);
-    atomicAdd(&L->acc.mz, v[3]);
-    if (n[0]) atomic_add_i64(&L->acc.accepted, n[0]);
-  }
+  o3_commit<COLOUR>(L, tot, nacc);
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
 
@@ -606,5 +730,7 @@ O3_INSTANTIATE(0)
 O3_INSTANTIATE(1)
 O3_INSTANTIATE(2)
 O3_INSTANTIATE(3)
+
+GPUMC_BOUNDS_MODULE(sweep_o3)
 
 }  // namespace gpumc

@@ -121,9 +121,13 @@ __device__ __forceinline__ void load_potts_plane(uint4* pl, const int8_t* src, i
   for (int it = 0; it < g.iters_load; ++it) {
     const int r = g.row0 + it * g.rstep;
     if (r >= g.R) break;
-    const uint4* p = (const uint4*)(src + (zrow + wrap_i(g.y0 - g.yo + r, g.ly)) * g.pitch + 64 * gs);
-    const uint4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
-    pl[r * g.NC + g.col] = pack_potts(a, b, c, d);
+    const size_t off = (zrow + wrap_i(g.y0 - g.yo + r, g.ly)) * g.pitch + 64 * gs;
+    const uint4* p = (const uint4*)(src + off);
+    const bool in = GPUMC_IN(off + 63, g.gbytes);
+    const uint4 z4 = make_uint4(0, 0, 0, 0);
+    const uint4 a = in ? __ldg(p) : z4, b = in ? __ldg(p + 1) : z4, c = in ? __ldg(p + 2) : z4,
+                d = in ? __ldg(p + 3) : z4;
+    st_chk(pl, r * g.NC + g.col, g.pw, pack_potts(a, b, c, d));
   }
 }
 
@@ -204,11 +208,11 @@ __device__ __forceinline__ void potts_pass(uint4* pl, const uint4* pm, const uin
     if (active) {
       const int y = wrap_i(g.y0 - g.yo + r, g.ly);
       P_ = (colour + y + z) & 1;  // x parity of this colour's sites in the row
-      const uint4 me = pl[r * g.NC + cc];
+      const uint4 me = ld_chk(pl, r * g.NC + cc, g.pw);
       const int ru = g.yw && r == 0 ? g.R - 1 : r - 1;
       const int rd = g.yw && r == g.R - 1 ? 0 : r + 1;
-      const uint4 up = pl[ru * g.NC + cc];
-      const uint4 dn = pl[rd * g.NC + cc];
+      const uint4 up = ld_chk(pl, ru * g.NC + cc, g.pw);
+      const uint4 dn = ld_chk(pl, rd * g.NC + cc, g.pw);
       own0 = P_ ? me.z : me.x;
       own1 = P_ ? me.w : me.y;
       const uint32_t ot0 = P_ ? me.x : me.z, ot1 = P_ ? me.y : me.w;
@@ -216,7 +220,7 @@ __device__ __forceinline__ void potts_pass(uint4* pl, const uint4* pm, const uin
         // even x = 2i: left = odd 2i-1 (index i-1), right = odd 2i+1 (index i)
         uint32_t c0 = 0, c1 = 0;
         if (has_prev) {
-          const uint4 po = pl[r * g.NC + cprev];
+          const uint4 po = ld_chk(pl, r * g.NC + cprev, g.pw);
           const int sh = first_seg ? g.hlast - 1 : 31;
           c0 = (po.z >> sh) & 1u;
           c1 = (po.w >> sh) & 1u;
@@ -231,7 +235,7 @@ __device__ __forceinline__ void potts_pass(uint4* pl, const uint4* pm, const uin
         n1[0] = ot1;
         uint32_t e0 = 0, e1 = 0;
         if (has_next) {
-          const uint4 ne = pl[r * g.NC + cnext];
+          const uint4 ne = ld_chk(pl, r * g.NC + cnext, g.pw);
           e0 = ne.x & 1u;
           e1 = ne.y & 1u;
         }
@@ -321,13 +325,16 @@ __device__ __forceinline__ void potts_pass(uint4* pl, const uint4* pm, const uin
       const uint32_t acc_m = (always | lt) & valid;
       const uint32_t f0 = (own0 & ~acc_m) | (new0 & acc_m);
       const uint32_t f1 = (own1 & ~acc_m) | (new1 & acc_m);
-      uint4& me = pl[r * g.NC + cc];
-      if (P_) {
-        me.z = f0;
-        me.w = f1;
-      } else {
-        me.x = f0;
-        me.y = f1;
+      const bool in_me = GPUMC_IN(r * g.NC + cc, g.pw);
+      uint4& me = pl[in_me ? r * g.NC + cc : 0];
+      if (in_me) {
+        if (P_) {
+          me.z = f0;
+          me.w = f1;
+        } else {
+          me.x = f0;
+          me.y = f1;
+        }
       }
       const bool owned = owned_plane && owned_col && r >= g.yo && r < g.yo + g.hv;
       if (owned) {
@@ -348,11 +355,14 @@ __device__ __forceinline__ void potts_pass(uint4* pl, const uint4* pm, const uin
           const int y = wrap_i(g.y0 - g.yo + r, g.ly);
           uint4 o0, o1, o2, o3;
           unpack_potts(fin, o0, o1, o2, o3);
-          uint4* out = (uint4*)(dst + ((size_t)z * g.ly + y) * g.pitch + 64 * gs);
-          out[0] = o0;
-          out[1] = o1;
-          out[2] = o2;
-          out[3] = o3;
+          const size_t off = ((size_t)z * g.ly + y) * g.pitch + 64 * gs;
+          uint4* out = (uint4*)(dst + off);
+          if (GPUMC_IN(off + 63, g.gbytes)) {
+            out[0] = o0;
+            out[1] = o1;
+            out[2] = o2;
+            out[3] = o3;
+          }
         }
       }
     }
@@ -432,5 +442,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2)
 
 template __global__ void k_sweep_potts_bits<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template __global__ void k_sweep_potts_bits<3>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+
+GPUMC_BOUNDS_MODULE(sweep_potts_bits)
 
 }  // namespace gpumc

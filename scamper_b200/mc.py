@@ -190,6 +190,11 @@ class Engine:
         keep every lattice's full-launch tiles; results identical."""
         _lib.call("gpumc_engine_set_tile_refinement", self.h, 1 if enable else 0)
 
+    def set_wait_limit(self, polls=None):
+        """Polls after which an inter-CTA wait of the resident kernel gives up
+        (None = the default, about half a second)."""
+        _lib.call("gpumc_engine_set_wait_limit", self.h, (1 << 22) if polls is None else int(polls))
+
     def set_concurrent_kinds(self, enable):
         """Run each kernel kind's sweeps on a stream of its own (default) or
         all kinds in sequence on the engine stream; results identical."""
@@ -430,6 +435,23 @@ class ClassicalMC:
         v = ctypes.c_void_p()
         _lib.call("gpumc_engine_stream", e, ctypes.byref(v))
         return v.value
+
+    def set_audit_interval(self, interval):
+        """Compare cached and recomputed energies after every `interval`-th
+        sweep (0 = off); a mismatch raises GpumcError (ESTATE)."""
+        _lib.call("gpumc_set_audit_interval", self.h, int(interval))
+
+    def perturb_energy_cache(self, replica, delta):
+        """Adds `delta` to a replica's cached energy, spins untouched (a
+        host-made cache fault for audit tests)."""
+        _lib.call("gpumc_perturb_energy_cache", self.h, replica, float(delta))
+
+    def set_wait_limit(self, polls=None):
+        """Polls after which an inter-CTA wait of the resident kernel gives up
+        (None = the default, about half a second), for the handle's engine."""
+        e = ctypes.c_void_p()
+        _lib.call("gpumc_sim_engine", self.h, ctypes.byref(e))
+        _lib.call("gpumc_engine_set_wait_limit", e, (1 << 22) if polls is None else int(polls))
 
     def launches_per_sweep(self):
         v = ctypes.c_int32()

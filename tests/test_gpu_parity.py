@@ -49,7 +49,10 @@ def _run_parity(gpumc, oracle, model_name, shape, beta, seed, sweeps, q=3, J=1.0
         if model_name in ("ising", "potts"):
             assert mc.energy()[0] == orc.cached_energy() == orc.energy()
         elif model_name == "o3":
-            assert mc.energy()[0] == pytest.approx(orc.energy(), rel=1e-9, abs=1e-9)
+            # the kernels' fixed-point bond sum of the fp32 configuration,
+            # exactly; within fp32 rounding of the exact fp64 energy
+            assert mc.energy()[0] == orc.fixed_observables()[0]
+            assert mc.energy()[0] == pytest.approx(orc.energy(), rel=1e-6, abs=1e-4)
         else:
             e64, m64 = mc.replica_observables(0)
             oe, om = orc.msc_observables()
@@ -240,7 +243,8 @@ def test_device_matches_committed_golden_fingerprints(gpumc, case):
     st = np.ascontiguousarray(_gpu_state(mc))
     assert hashlib.sha256(st.tobytes()).hexdigest() == case["sha256"]
     if case["model"] == "o3":
-        assert mc.energy()[0] == pytest.approx(case["energy"], rel=1e-9, abs=1e-9)
+        # fixture: exact fp64 energy; device: fixed-point sum of fp32 bonds
+        assert mc.energy()[0] == pytest.approx(case["energy"], rel=1e-6, abs=1e-4)
     elif case["model"] == "msc":
         e64, _ = mc.replica_observables(0)
         assert float(e64.sum()) == case["energy"]

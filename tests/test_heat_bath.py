@@ -222,7 +222,10 @@ def test_gpu_o3_heat_bath_matches_oracle(gpumc, oracle, shape, J):
         mc.sweep(2)
         ch = ref.sweep() + ref.sweep()
         np.testing.assert_array_equal(mc.spins(), ref.state().reshape(mc.spins().shape))
-        assert mc.energy()[0] == pytest.approx(ref.cached_energy(), rel=1e-12, abs=1e-9)
+        # the kernels' fixed-point bond sum, exactly; within fp32 rounding of
+        # the reference's exact energy cache
+        assert mc.energy()[0] == ref.fixed_observables()[0]
+        assert mc.energy()[0] == pytest.approx(ref.cached_energy(), rel=1e-6, abs=1e-4)
     obs = mc.observables()
     assert obs[-1]["acceptance"] == pytest.approx(ch / 2 / ref.n) or obs[-1]["acceptance"] > 0.99
     mc.close()
