@@ -545,40 +545,58 @@ def bench_mixed(gpumc, torch, args):
     return out
 
 
+SERVE_TC = {"ising2": 2.0 / math.log(1 + math.sqrt(2)), "potts2": 1.0 / math.log(1 + math.sqrt(3)),
+            "ising3": 4.5115, "o33": 1.443}
+
+
+def serving_jobs(rng, lam, n_jobs, sweep_scale):
+    """The serving workload: Poisson arrivals at rate lam; each job uniformly
+    one of 2D Ising, 2D Potts (q=3), 3D Ising, 3D O(3); L log-uniform in
+    32..2048 (2D) or 16..192 (3D), rounded to even; T ~ U[0.6, 1.4] T_c;
+    sweep count log-uniform in 10^2..10^4 (times sweep_scale)."""
+    jobs = []
+    t = 0.0
+    for _ in range(n_jobs):
+        t += rng.exponential(1.0 / lam)
+        kind = ["ising2", "potts2", "ising3", "o33"][int(rng.integers(4))]
+        if kind.endswith("2"):
+            L = int(round(math.exp(rng.uniform(math.log(32), math.log(2048)))))
+            lt = "square"
+        else:
+            L = int(round(math.exp(rng.uniform(math.log(16), math.log(192)))))
+            lt = "cubic"
+        L = max(4, L + (L & 1))
+        T = rng.uniform(0.6, 1.4) * SERVE_TC[kind]
+        sweeps = max(1, int(round(math.exp(rng.uniform(math.log(100), math.log(10000))) * sweep_scale)))
+        model = {"ising2": "ising", "potts2": "potts", "ising3": "ising", "o33": "o3"}[kind]
+        p = {"lattice_type": lt, "L": L, "beta": 1.0 / T, "q": 3}
+        att = float(L ** (2 if lt == "square" else 3)) * sweeps
+        jobs.append((t, model, p, sweeps, att))
+    return jobs
+
+
 def bench_serving(gpumc, torch, args):
-    """Poisson arrivals of jobs (2D Ising, 2D Potts q=3, 3D Ising, 3D O(3);
-    L log-uniform 32..2048 (2D) / 16..192 (3D); T ~ U[0.6, 1.4] T_c; sweeps
-    log-uniform 1e2..1e4), scaled to `serve_jobs` jobs per rate."""
+    """Continuous batching of Poisson job arrivals (serving_jobs) at each rate
+    of --serve-rates: jobs are submitted at their arrival time, admitted by
+    HBM footprint, advanced `chunk` sweeps per server step together with
+    every running job, and retired with their observables.  Reports per rate
+    p50 / p99 time to completion, aggregate attempts/ns over the wall time and
+    over the busy time, and the time the server needed after the last
+    arrival; the saturation rate is the busy throughput divided by the mean
+    attempts of a job."""
     rng = np.random.default_rng(99)
-    tc = {"ising2": 2.0 / math.log(1 + math.sqrt(2)), "potts2": 1.0 / math.log(1 + math.sqrt(3)),
-          "ising3": 4.5115, "o33": 1.443}
     out = []
+    busy_rates = []
+    mean_att = None
     for lam in args.serve_rates:
-        jobs = []
-        t = 0.0
-        for j in range(args.serve_jobs):
-            t += rng.exponential(1.0 / lam)
-            kind = ["ising2", "potts2", "ising3", "o33"][int(rng.integers(4))]
-            if kind.endswith("2"):
-                L = int(round(math.exp(rng.uniform(math.log(32), math.log(2048)))))
-                lt = "square"
-            else:
-                L = int(round(math.exp(rng.uniform(math.log(16), math.log(192)))))
-                lt = "cubic"
-            L = max(4, L + (L & 1))
-            T = rng.uniform(0.6, 1.4) * tc[kind]
-            sweeps = int(round(math.exp(rng.uniform(math.log(100), math.log(10000)))) * args.serve_sweep_scale)
-            sweeps = max(1, sweeps)
-            model = {"ising2": "ising", "potts2": "potts", "ising3": "ising", "o33": "o3"}[kind]
-            p = {"lattice_type": lt, "L": L, "beta": 1.0 / T, "q": 3}
-            att = float(L ** (2 if lt == "square" else 3)) * sweeps
-            jobs.append((t, model, p, sweeps, att))
+        jobs = serving_jobs(rng, lam, args.serve_jobs, args.serve_sweep_scale)
         srv = gpumc.Server(hbm_budget=int(args.serve_budget_gb * (1 << 30)), chunk=args.serve_chunk)
         srv.set_keep_spins(0)  # a job's product is its observables (the reference's task results)
         t0 = time.perf_counter()
         pending = list(jobs)
         done = {}
         ids = {}
+        max_active = 0
         while len(done) < len(jobs):
             now = time.perf_counter() - t0
             while pending and pending[0][0] <= now:
@@ -586,6 +604,7 @@ def bench_serving(gpumc, torch, args):
                 jid = srv.submit(p, 10_000 + len(ids), sw, 0, model=model)
                 ids[jid] = (t_arr, att)
             active = srv.step()
+            max_active = max(max_active, active)
             for r in srv.poll():
                 done[r["job_id"]] = r
             if active == 0 and pending:
@@ -595,25 +614,24 @@ def bench_serving(gpumc, torch, args):
         srv.close()
         lat = np.array([r["finish_s"] - r["submit_s"] for r in done.values()])
         total_att = sum(a for _, a in ids.values())
+        mean_att = total_att / len(jobs)
+        busy = st["attempts"] / (st["busy_s"] * 1e9)
+        busy_rates.append(busy)
+        last_arrival = jobs[-1][0]
         out.append({"lambda_per_s": lam, "jobs": len(jobs), "sweep_scale": args.serve_sweep_scale,
-                    "p50_s": float(np.percentile(lat, 50)),
-                    "p99_s": float(np.percentile(lat, 99)), "wall_s": wall,
+                    "mean_job_attempts": mean_att,
+                    "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                    "max_s": float(lat.max()), "wall_s": wall, "arrival_span_s": last_arrival,
+                    "drain_s": wall - last_arrival, "max_jobs_in_system": max_active,
                     "attempts_per_ns": total_att / (wall * 1e9),
-                    "busy_attempts_per_ns": st["attempts"] / (st["busy_s"] * 1e9),
+                    "busy_attempts_per_ns": busy,
                     "host_s": {"admit": round(st["admit_s"], 4), "sweep": round(st["sweep_s"], 4),
                                "retire": round(st["retire_s"], 4)}})
-    return out
-
-
-def headline_config(world, args):
-    """The workload description both arms print (same dict, so the two lines
-    name the same configuration)."""
-    return {"workload": f"2D square Ising L={HEADLINE_L}, J=1, one lattice per beta in "
-                        f"{HEADLINE_BETAS}, single-site Metropolis sweeps, observables recorded every sweep",
-            "global_batch": len(HEADLINE_BETAS) * world, "sites_per_lattice": HEADLINE_L ** 2,
-            "sweeps_per_step": args.sweeps_per_step,
-            "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (2 x 3 x 64 MiB resident)"}
+    return {"config": "Poisson stream of jobs: 2D Ising, 2D Potts q=3, 3D Ising, 3D O(3); L log-uniform 32..2048 "
+                      "(2D) / 16..192 (3D); T ~ U[0.6,1.4] T_c; sweeps log-uniform 1e2..1e4",
+            "jobs_per_rate": args.serve_jobs, "sweep_scale": args.serve_sweep_scale, "chunk": args.serve_chunk,
+            "rates": out,
+            "saturation_lambda_per_s": max(busy_rates) * 1e9 / mean_att if mean_att else None}
 
 
 # ---------------------------------------------------------------------------
@@ -731,8 +749,8 @@ def main():
                     default=None,
                     help="run one extra workload alone (profiling)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 30.0, 100.0, 300.0, 1000.0])
-    ap.add_argument("--serve-jobs", type=int, default=64)
-    ap.add_argument("--serve-sweep-scale", type=float, default=0.1)
+    ap.add_argument("--serve-jobs", type=int, default=300)
+    ap.add_argument("--serve-sweep-scale", type=float, default=1.0)
     ap.add_argument("--serve-chunk", type=int, default=20)
     ap.add_argument("--serve-budget-gb", type=float, default=64.0)
     args = ap.parse_args()
