@@ -586,6 +586,15 @@ int gpumc_set_tile_refinement(gpumc_sim* sim, int32_t enable) {
     return rc;
   }
   sim->drop_graphs();
+  // the resident plan follows the new tiles (whole-row or whole-plane Ising
+  // tiles may qualify now, or no longer)
+  sim->res.release(sim->eng->stream);
+  if (is_ising_bits_kind(kernel_kind(sim->lay))) {
+    std::map<int, const Layout*> lay_of;
+    for (int r = 0; r < sim->n_rep; ++r) lay_of[sim->lat0 + r] = &sim->lay;
+    RC_TRY(build_resident(sim->eng->device, sim->eng->stream, tiles, lay_of, sim->lay.smem, sim->res));
+  }
+  CUDA_TRY(cudaStreamSynchronize(sim->eng->stream));
   return GPUMC_OK;
 }
 
