@@ -1150,6 +1150,17 @@ int gpumc_get_tile_knobs(gpumc_tile_knobs* knobs) {
   return GPUMC_OK;
 }
 
+int gpumc::check_launch_flag(cudaStream_t st, LaunchCtl* ctl) {
+  int32_t err = 0;
+  CUDA_TRY(cudaMemcpyAsync(&err, &ctl->err, sizeof(err), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (!err) return GPUMC_OK;
+  CUDA_TRY(cudaMemsetAsync(&ctl->err, 0, sizeof(int32_t), st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return fail(GPUMC_ECUDA, "O(3) sweep: a shared-memory plane copy did not complete in time; the launch's "
+                           "spins, energies and records are not a trajectory and must be restored");
+}
+
 int gpumc_engine_set_wait_limit(gpumc_engine* eng, int64_t polls) {
   if (!eng) return fail(GPUMC_EINVAL, "engine: null");
   if (polls < 0) return fail(GPUMC_EINVAL, "polls: must be >= 0");
@@ -1288,6 +1299,8 @@ int gpumc_engine_sweep(gpumc_engine* eng, uint32_t n_sweeps) {
       if (s->audit_interval && s->sweeps % s->audit_interval == 0 && (rc = s->audit()) != GPUMC_OK) return rc;
     left -= chunk;
   }
+  for (auto& p : eng->batch_plans)
+    if (is_o3_march_kind(p.kind) && (rc = check_launch_flag(eng->stream, p.d_ctl)) != GPUMC_OK) return rc;
   return GPUMC_OK;
 }
 

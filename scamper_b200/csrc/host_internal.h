@@ -50,6 +50,12 @@ constexpr int kKindO3Uniform = 48, kKindO3Opss = 64;
 // 2D Ising on the bit-sliced kernel (either single-site algorithm): the kinds
 // the resident multi-sweep launch can take
 inline bool is_ising2d_bits_kind(int kind) { return kind == 0 || kind == kKindHeatBath; }
+// O(3) z-march kernels (any proposal or the heat bath): their ring copies
+// flag a wait that gave up in LaunchCtl::err
+inline bool is_o3_march_kind(int kind) { return !is_cluster_kind(kind) && kind % 16 == 10; }
+// Reads and clears LaunchCtl::err after the stream's work; a set flag (a
+// ring copy that did not land in time) becomes GPUMC_ECUDA.
+int check_launch_flag(cudaStream_t st, LaunchCtl* ctl);
 inline bool is_ising_bits_kind(int kind) {
   return kind == 0 || kind == 1 || kind == kKindHeatBath || kind == kKindHeatBath + 1;
 }

@@ -628,6 +628,7 @@ int gpumc_sweep(gpumc_sim* sim, uint32_t n_sweeps) {
     left -= chunk;
     if (sim->audit_interval && sim->sweeps % sim->audit_interval == 0) RC_TRY(sim->audit());
   }
+  if (is_o3_march_kind(kernel_kind(sim->lay))) RC_TRY(check_launch_flag(sim->eng->stream, sim->d_ctl));
   return GPUMC_OK;
 }
 

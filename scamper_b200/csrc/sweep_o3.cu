@@ -563,17 +563,52 @@ __global__ void __launch_bounds__(kThreads, 4)
 //
 // A tile is whole rows y0 .. y0+hv-1 of planes z0 .. z0+dv-1.  Each plane the
 // tile touches (z0-1 .. z0+dv) is copied once, rows y0-1 .. y0+hv with all
-// three components, by 16-byte cp.async into a ring slot, and serves as the
-// z-1, z and z+1 plane of three consecutive steps; the copy of plane z+2 is in
-// flight while plane z is computed.  Every neighbour read is then a
-// shared-memory read.  The pass reads only the other colour's values (and its
-// own sites' old values, which only this tile writes), so copying planes that
-// other tiles update in place is race-free.  The site arithmetic and its
-// operation order are those of k_sweep_o3.
+// three components, into a ring slot and serves as the z-1, z and z+1 plane
+// of three consecutive steps; the copy of plane z+2 is in flight while plane
+// z is computed.  The copies are bulk asynchronous copies (cp.async.bulk, no
+// multicast) issued by one thread: per component the slot's rows are at most
+// three contiguous runs of the plane (split where the rows wrap), and each
+// slot's mbarrier counts the bytes in (expect_tx / complete_tx).  Plane p of
+// the march (p = 0 for z0-1) goes to slot p & 3 as that slot's (p >> 2)-th
+// fill, so a step waits for phase parity (p >> 2) & 1 of its three slots.
+// Every wait is bounded; one that gives up flags the launch (ctl->err), waits
+// (bounded again) for the copies in flight and leaves the tile.  Every
+// neighbour read is a shared-memory read.  The pass reads only the other
+// colour's values (and its own sites' old values, which only this tile
+// writes), so copying planes that other tiles update in place is race-free.
+// The site arithmetic and its operation order are those of k_sweep_o3.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void o3_cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+constexpr long long kRingWaitPolls = 1ll << 20;  // try_wait polls per ring wait
+
+__device__ __forceinline__ void ring_init(unsigned long long* bar) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void ring_expect(unsigned long long* bar, uint32_t bytes) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(a),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void ring_bulk_copy(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
+               "l"(src), "r"(bytes), "r"(a)
+               : "memory");
+}
+// Bounded wait for the completion of phase `parity` of a slot's mbarrier.
+__device__ __forceinline__ bool ring_wait(unsigned long long* bar, uint32_t parity) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  for (long long it = 0; it < kRingWaitPolls; ++it) {
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(a), "r"(parity)
+                 : "memory");
+    if (done) return true;
+  }
+  return false;
 }
 
 // Colour 1 also carries the sweep epilogue's shared memory, so three CTAs
@@ -605,39 +640,34 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
   const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
   const int cstr = RW * pitch;              // floats per component in a slot
   const int slot = 3 * cstr;                // floats per ring slot
-  const int nvec = pitch >> 2;              // 16-byte chunks per row
-  // Plane copies: thread k copies chunks k, k + kThreads, ... of the
-  // 3 x RW x nvec chunks (component c, slot row r, chunk v), walked by a
-  // division-free cursor that advances kThreads chunks per step.
-  const int cv0 = threadIdx.x % nvec, ccr0 = threadIdx.x / nvec;
-  const int cc0 = ccr0 / RW, cr0 = ccr0 - cc0 * RW;
-  const int step_v = kThreads % nvec, step_r = kThreads / nvec;
   float* S1 = S + (size_t)cs;
   float* S2 = S + 2 * (size_t)cs;
-  auto copy_plane = [&](int sl, int z) {
-    const int zz = z < 0 ? z + lz : (z >= lz ? z - lz : z);
-    float* dst = osm + sl * slot;
-    const float* src = S + (size_t)zz * ly * pitch;
-    int v = cv0, r = cr0, c = cc0;
-    while (c < 3) {
-      int y = t.y0 - 1 + r;
-      y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
-      const long long so = (long long)(src - S) + (long long)c * cs + (long long)y * pitch + 4 * v;
-      const long long dof = (long long)(dst - osm) + (long long)c * cstr + (long long)r * pitch + 4 * v;
-      if (GPUMC_IN(so + 3, 3ll * cs) && GPUMC_IN(dof + 3, 4ll * slot))
-        o3_cp_async16(dst + c * cstr + r * pitch + 4 * v, src + (size_t)c * cs + y * pitch + 4 * v);
-      v += step_v;
-      r += step_r;
-      if (v >= nvec) {
-        v -= nvec;
-        ++r;
-      }
-      while (r >= RW) {
-        r -= RW;
-        ++c;
+  __shared__ __align__(8) unsigned long long ring_bar[4];
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 4; ++i) ring_init(&ring_bar[i]);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the inits, visible to the copy engine
+  }
+  __syncthreads();
+  // plane p of the march (z0 - 1 + p) into slot p & 3, by thread 0
+  auto copy_plane = [&](int p) {
+    if (threadIdx.x != 0) return;
+    const int sl = p & 3;
+    int zz = t.z0 - 1 + p;
+    zz = zz < 0 ? zz + lz : (zz >= lz ? zz - lz : zz);
+    ring_expect(&ring_bar[sl], (uint32_t)(3 * cstr) * 4u);
+    for (int c = 0; c < 3; ++c) {
+      int r = 0;
+      while (r < RW) {
+        int y = t.y0 - 1 + r;
+        y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
+        const int n = min(RW - r, ly - y);  // rows contiguous up to the plane's last row
+        const long long so = (long long)c * cs + ((long long)zz * ly + y) * pitch;
+        const long long dof = (long long)sl * slot + (long long)c * cstr + (long long)r * pitch;
+        if (GPUMC_IN(so + (long long)n * pitch - 1, 3ll * cs) && GPUMC_IN(dof + (long long)n * pitch - 1, 4ll * slot))
+          ring_bulk_copy(osm + dof, S + so, (uint32_t)(n * pitch) * 4u, &ring_bar[sl]);
+        r += n;
       }
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
   O3Fix fx = {{0, 0, 0}, 0};
   O3Totals tot = {{0, 0, 0}, 0};
@@ -645,20 +675,24 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
   const int half = lx >> 1;
   const int n_items = hv * half;  // colour sites of the tile's rows in one plane
   const int dr = kThreads / half, dj = kThreads - dr * half;  // cursor step of kThreads items
-  copy_plane(0, t.z0 - 1);
-  copy_plane(1, t.z0);
-  copy_plane(2, t.z0 + 1);
-  for (int k = 0; k < dv; ++k) {
+  copy_plane(0);
+  copy_plane(1);
+  copy_plane(2);
+  bool ok_ring = true;
+  int issued = 3;  // planes whose copies were issued
+  for (int k = 0; k < dv && ok_ring; ++k) {
     const int z = t.z0 + k;
     // plane z+2 (needed as z+1 of the next step) into the slot freed by the
-    // previous step; an empty group keeps the count when it is not needed
+    // previous step
     if (k + 1 < dv) {
-      copy_plane((k + 3) & 3, z + 2);
-    } else {
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      copy_plane(k + 3);
+      issued = k + 4;
     }
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // planes z-1, z, z+1 landed
-    __syncthreads();
+    // planes z-1, z, z+1 = march planes k, k+1, k+2
+    for (int i = 0; i < 3 && ok_ring; ++i)
+      ok_ring = ring_wait(&ring_bar[(k + i) & 3], (uint32_t)((k + i) >> 2) & 1u);
+    ok_ring = __syncthreads_and(ok_ring) != 0;  // one decision for the whole CTA
+    if (!ok_ring) break;
     const float* pm = osm + (k & 3) * slot;
     const float* pc = osm + ((k + 1) & 3) * slot;
     const float* pp = osm + ((k + 2) & 3) * slot;
@@ -714,7 +748,12 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     o3_flush(tot, fx);  // per plane: at most hv * lx / 512 sites per thread since the last flush
     __syncthreads();  // the next copy overwrites the z-1 slot read above
   }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  if (!ok_ring) {
+    // a copy did not land in time: flag the launch, wait (bounded) for every
+    // copy still in flight into this CTA's ring, and leave the tile
+    atomicExch(&ctl->err, 2);
+    for (int p = max(0, issued - 4); p < issued; ++p) ring_wait(&ring_bar[p & 3], (uint32_t)(p >> 2) & 1u);
+  }
   o3_commit<COLOUR>(L, tot, nacc);
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
