@@ -69,10 +69,11 @@ class TileCache:
         os.replace(tmp, self.path)
 
 
-def time_workload(build, knobs, sweeps, warm, torch):
+def time_workload(build, knobs, sweeps, warm, torch, repeats=3):
     """ms per engine sweep of the workload planned with `knobs`: a fresh
-    engine, `warm` untimed sweeps (graph capture included), then `sweeps`
-    sweeps between CUDA events on the engine's stream."""
+    engine, `warm` untimed sweeps (graph capture included), then the fastest
+    of `repeats` windows of `sweeps` sweeps between CUDA events on the
+    engine's stream (the minimum filters other work on a shared device)."""
     from .mc import Engine
     prev = set_knobs(knobs)
     try:
@@ -82,13 +83,16 @@ def time_workload(build, knobs, sweeps, warm, torch):
             eng.sweep(warm)
             eng.synchronize()
             st = torch.cuda.ExternalStream(eng.stream_ptr())
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(st)
-            eng.sweep(sweeps)
-            b.record(st)
-            b.synchronize()
-            return a.elapsed_time(b) / sweeps
+            best = float("inf")
+            for _ in range(max(1, repeats)):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                eng.sweep(sweeps)
+                b.record(st)
+                b.synchronize()
+                best = min(best, a.elapsed_time(b) / sweeps)
+            return best
         finally:
             for s in sims:
                 s.close()
@@ -97,7 +101,7 @@ def time_workload(build, knobs, sweeps, warm, torch):
         set_knobs(prev)
 
 
-def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None):
+def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None, repeats=3):
     """Coordinate descent over `space` ({knob: [candidates]}, 0 = analytic)
     for the workload that build(engine) creates.  Returns {"knobs",
     "ms_per_sweep", "analytic_ms_per_sweep", "table"} with every timed
@@ -108,7 +112,7 @@ def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None):
         if name not in KNOBS:
             raise ValueError(f"unknown tile knob: {name}")
     best = {name: 0 for name in KNOBS}
-    analytic = time_workload(build, best, sweeps, warm, torch)
+    analytic = time_workload(build, best, sweeps, warm, torch, repeats)
     best_t = analytic
     table = [{"knobs": dict(best), "ms_per_sweep": analytic}]
     for _ in range(rounds):
@@ -117,7 +121,7 @@ def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None):
                 if v == best[name]:
                     continue
                 trial = dict(best, **{name: int(v)})
-                t = time_workload(build, trial, sweeps, warm, torch)
+                t = time_workload(build, trial, sweeps, warm, torch, repeats)
                 table.append({"knobs": trial, "ms_per_sweep": t})
                 if t < best_t:
                     best, best_t = trial, t
