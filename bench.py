@@ -637,6 +637,17 @@ def bench_serving(gpumc, torch, args):
             "saturation_lambda_per_s": max(busy_rates) * 1e9 / mean_att if mean_att else None}
 
 
+def headline_config(world, args):
+    """The workload description both arms print (same dict, so the two lines
+    name the same configuration)."""
+    return {"workload": f"2D square Ising L={HEADLINE_L}, J=1, one lattice per beta in "
+                        f"{HEADLINE_BETAS}, single-site Metropolis sweeps, observables recorded every sweep",
+            "global_batch": len(HEADLINE_BETAS) * world, "sites_per_lattice": HEADLINE_L ** 2,
+            "sweeps_per_step": args.sweeps_per_step,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (2 x 3 x 64 MiB resident)"}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline (the reference's algorithm restated in C; bounded sample)
 # ---------------------------------------------------------------------------
