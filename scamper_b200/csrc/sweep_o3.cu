@@ -299,62 +299,63 @@ __device__ __forceinline__ void o3_metropolis_2(f2 ax, f2 ay, f2 az, f2 hx, f2 h
 // pass, its bond sum with the fp32 neighbour sum h: rint(2^21 s_c) and
 // rint(2^19 s . h) by the 1.5 2^23 shifter (|2^21 s_c| <= 2^21,
 // |2^19 s . h| <= 6 2^19 < 2^22), summed in 32-bit integers.
+// The shifter's bit patterns are summed as they are (modulo 2^32) and the
+// shifter's own pattern, once per term, is taken off at the flush: one
+// three-input add per value and pair.  A pair with one site scales its second
+// lane by zero, so that lane adds exactly the shifter.
 struct O3Fix {
-  int32_t m[3], e;
+  uint32_t m[3], e;
+  uint32_t n;  // terms per value since the last flush
 };
 __device__ __forceinline__ int32_t fix_shift(float v) { return (int32_t)(__float_as_uint(v) - 0x4B400000u); }
 template <bool BOND>
 __device__ __forceinline__ void o3_fix_add_2(O3Fix& q, f2 sx, f2 sy, f2 sz, f2 hx, f2 hy, f2 hz, bool use_b) {
   const f2 X = F2s(0x1.8p23f);
-  const f2 mx = fma2(sx, F2s(0x1p21f), X), my = fma2(sy, F2s(0x1p21f), X), mz = fma2(sz, F2s(0x1p21f), X);
-  q.m[0] += fix_shift(lo(mx)) + (use_b ? fix_shift(hi(mx)) : 0);
-  q.m[1] += fix_shift(lo(my)) + (use_b ? fix_shift(hi(my)) : 0);
-  q.m[2] += fix_shift(lo(mz)) + (use_b ? fix_shift(hi(mz)) : 0);
+  const f2 sm = F2(0x1p21f, use_b ? 0x1p21f : 0.0f);
+  const f2 mx = fma2(sx, sm, X), my = fma2(sy, sm, X), mz = fma2(sz, sm, X);
+  q.m[0] += __float_as_uint(lo(mx)) + __float_as_uint(hi(mx));
+  q.m[1] += __float_as_uint(lo(my)) + __float_as_uint(hi(my));
+  q.m[2] += __float_as_uint(lo(mz)) + __float_as_uint(hi(mz));
   if (BOND) {
-    const f2 e = fma2(fma2(sz, hz, fma2(sy, hy, mul2(sx, hx))), F2s(0x1p19f), X);
-    q.e += fix_shift(lo(e)) + (use_b ? fix_shift(hi(e)) : 0);
+    const f2 se = F2(0x1p19f, use_b ? 0x1p19f : 0.0f);
+    const f2 e = fma2(fma2(sz, hz, fma2(sy, hy, mul2(sx, hx))), se, X);
+    q.e += __float_as_uint(lo(e)) + __float_as_uint(hi(e));
   }
-}
-// Scalar form (heat-bath sites).
-template <bool BOND>
-__device__ __forceinline__ void o3_fix_add(O3Fix& q, float sx, float sy, float sz, float hx, float hy, float hz) {
-  q.m[0] += fix_shift(__fmaf_rn(sx, 0x1p21f, 0x1.8p23f));
-  q.m[1] += fix_shift(__fmaf_rn(sy, 0x1p21f, 0x1.8p23f));
-  q.m[2] += fix_shift(__fmaf_rn(sz, 0x1p21f, 0x1.8p23f));
-  if (BOND) {
-    const float e = __fmaf_rn(sz, hz, __fmaf_rn(sy, hy, __fmul_rn(sx, hx)));
-    q.e += fix_shift(__fmaf_rn(e, 0x1p19f, 0x1.8p23f));
-  }
+  q.n += 2;
 }
 
 // Philox4x32-10 of counter (site, colour | TAG_O3 << 1, sweep) with the
-// sweep-uniform part of round 1 precomputed; the round keys are bumped on the
-// fly (two adds per round instead of twenty live registers: resident warps
-// matter more here), and each round multiply is one 32x32->64 wide product.
+// sweep-uniform part of round 1 and the ten round keys precomputed once per
+// tile (the key is the lattice's, the same for the whole CTA, so the compiler
+// holds the schedule in uniform registers: measured 15 fewer instructions per
+// site than bumping the keys every round, at the same 64 registers), and each
+// round multiply one 32x32->64 wide product.
 struct O3Philox {
-  uint32_t a, b, c, k0, k1;
+  uint32_t a, b, c;
+  uint32_t k0[10], k1[10];
 };
 __device__ __forceinline__ O3Philox make_o3_philox(uint64_t key, uint64_t sweep, uint32_t ctrl) {
   O3Philox P;
-  P.k0 = (uint32_t)key;
-  P.k1 = (uint32_t)(key >> 32);
+  const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
   const uint32_t c2 = (uint32_t)sweep, c3 = (uint32_t)(sweep >> 32);
-  P.a = __umulhi(0xCD9E8D57u, c2) ^ P.k0 ^ ctrl;
+  P.a = __umulhi(0xCD9E8D57u, c2) ^ k0 ^ ctrl;
   P.b = 0xCD9E8D57u * c2;
-  P.c = c3 ^ P.k1;
+  P.c = c3 ^ k1;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    P.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
+    P.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
+  }
   return P;
 }
 __device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
   const uint64_t p00 = (uint64_t)0xD2511F53u * index;
   uint4 c = make_uint4(P.a, P.b, (uint32_t)(p00 >> 32) ^ P.c, (uint32_t)p00);
-  uint32_t k0 = P.k0, k1 = P.k1;
 #pragma unroll
   for (int r = 1; r < 10; ++r) {
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
     const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
     const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
-    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1,
+    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ P.k0[r], (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ P.k1[r],
                    (uint32_t)p0);
   }
   return c;
@@ -449,12 +450,14 @@ __device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& q
 struct O3Totals {
   long long m[3], e;
 };
+template <bool BOND>
 __device__ __forceinline__ void o3_flush(O3Totals& t, O3Fix& q) {
-  t.m[0] += q.m[0];
-  t.m[1] += q.m[1];
-  t.m[2] += q.m[2];
-  t.e += q.e;
-  q = O3Fix{{0, 0, 0}, 0};
+  const uint32_t off = q.n * 0x4B400000u;  // the shifter's pattern, once per term (mod 2^32)
+  t.m[0] += (int32_t)(q.m[0] - off);
+  t.m[1] += (int32_t)(q.m[1] - off);
+  t.m[2] += (int32_t)(q.m[2] - off);
+  if (BOND) t.e += (int32_t)(q.e - off);
+  q = O3Fix{{0, 0, 0}, 0, 0};
 }
 template <int COLOUR>
 __device__ __forceinline__ void o3_commit(LatDesc* L, O3Totals& t, int nacc) {
@@ -513,7 +516,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     r0 = threadIdx.x / half;
     rstep = kThreads / half;
   }
-  O3Fix fx = {{0, 0, 0}, 0};
+  O3Fix fx = {{0, 0, 0}, 0, 0};
   O3Totals tot = {{0, 0, 0}, 0};
   int nacc = 0;
   // this thread's sites, row-major: rows r0, r0 + rstep, ... of the tile's
@@ -551,9 +554,9 @@ __global__ void __launch_bounds__(kThreads, 4)
       qb = qa;
     }
     o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, S1, S2, cs, fx, nacc);
-    if ((k & 62) == 62) o3_flush(tot, fx);  // every 64 sites: 32-bit partials stay far from overflow
+    if ((k & 62) == 62) o3_flush<COLOUR == 1>(tot, fx);  // every 64 sites: 32-bit partials stay far from overflow
   }
-  o3_flush(tot, fx);
+  o3_flush<COLOUR == 1>(tot, fx);
   o3_commit<COLOUR>(L, tot, nacc);
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
 }
@@ -669,12 +672,18 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
       }
     }
   };
-  O3Fix fx = {{0, 0, 0}, 0};
+  O3Fix fx = {{0, 0, 0}, 0, 0};
   O3Totals tot = {{0, 0, 0}, 0};
   int nacc = 0;
-  const int half = lx >> 1;
-  const int n_items = hv * half;  // colour sites of the tile's rows in one plane
-  const int dr = kThreads / half, dj = kThreads - dr * half;  // cursor step of kThreads items
+  // Work items are pairs of horizontally adjacent sites of the colour in one
+  // row (x and x + 2, x = 4m + parity): both sites' neighbours then sit at
+  // fixed offsets from one row position (the x + 1 site is shared), and a
+  // thread's pair is found once per tile, not per plane.
+  const int half = lx >> 1;             // sites of the colour per row
+  const int np = (half + 1) >> 1;       // pairs per row (the last may be single)
+  const int n_pairs = hv * np;          // pairs of the tile's rows in one plane
+  const int r0 = threadIdx.x / np, m0 = threadIdx.x - r0 * np;
+  const int dr = kThreads / np, dm = kThreads - dr * np;  // cursor step of kThreads pairs
   copy_plane(0);
   copy_plane(1);
   copy_plane(2);
@@ -696,56 +705,74 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     const float* pm = osm + (k & 3) * slot;
     const float* pc = osm + ((k + 1) & 3) * slot;
     const float* pp = osm + ((k + 2) & 3) * slot;
-    auto load_site = [&](O3Site& q, int rl, int j) {  // local owned row, colour column
+    int rl = r0, m = m0;
+    for (int i = threadIdx.x; i < n_pairs; i += kThreads) {
       const int y = t.y0 + rl;
-      const int x = 2 * j + ((y + z + COLOUR) & 1);
-      const int xm = x ? x - 1 : lx - 1, xp = x + 1 < lx ? x + 1 : 0;
+      const int xa = 4 * m + ((y + z + COLOUR) & 1), xb = xa + 2;
+      const bool two = 2 * m + 1 < half;
       const int oc = (rl + 1) * pitch;  // slot row of y
-      // neighbour order x-1, x+1, y-1, y+1, z-1, z+1 (as k_sweep_o3)
-      float h[3];
+      // x-1 of a and x+1 of b wrap at the row's ends; x+1 of a = x-1 of b
+      // (x+1 of a wraps only for a single last site, x = lx - 1)
+      const int xam = xa ? xa - 1 : lx - 1;
+      const int xap = xa + 1 < lx ? xa + 1 : 0;
+      const int xbp = xb + 1 < lx ? xb + 1 : 0;
+      O3Site qa, qb;
+      float ha[3], hb[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float* P = pc + c * cstr;
-        h[c] = fadd(fadd(fadd(fadd(fadd(ld_chk(P, oc + xm, cstr), ld_chk(P, oc + xp, cstr)),
-                                   ld_chk(P, oc - pitch + x, cstr)),
-                              ld_chk(P, oc + pitch + x, cstr)),
-                         ld_chk(pm + c * cstr, oc + x, cstr)),
-                    ld_chk(pp + c * cstr, oc + x, cstr));
+        const float* M = pm + c * cstr;
+        const float* Q = pp + c * cstr;
+        const float mid = ld_chk(P, oc + xap, cstr);
+        // neighbour order x-1, x+1, y-1, y+1, z-1, z+1 (as k_sweep_o3)
+        ha[c] = fadd(fadd(fadd(fadd(fadd(ld_chk(P, oc + xam, cstr), mid), ld_chk(P, oc - pitch + xa, cstr)),
+                                ld_chk(P, oc + pitch + xa, cstr)),
+                           ld_chk(M, oc + xa, cstr)),
+                      ld_chk(Q, oc + xa, cstr));
+        if (two)
+          hb[c] = fadd(fadd(fadd(fadd(fadd(mid, ld_chk(P, oc + xbp, cstr)), ld_chk(P, oc - pitch + xb, cstr)),
+                                  ld_chk(P, oc + pitch + xb, cstr)),
+                             ld_chk(M, oc + xb, cstr)),
+                        ld_chk(Q, oc + xb, cstr));
+        else
+          hb[c] = ha[c];
       }
-      q.ax = ld_chk(pc, oc + x, cstr);
-      q.ay = ld_chk(pc + cstr, oc + x, cstr);
-      q.az = ld_chk(pc + 2 * cstr, oc + x, cstr);
-      q.hx = h[0];
-      q.hy = h[1];
-      q.hz = h[2];
+      qa.ax = ld_chk(pc, oc + xa, cstr);
+      qa.ay = ld_chk(pc + cstr, oc + xa, cstr);
+      qa.az = ld_chk(pc + 2 * cstr, oc + xa, cstr);
+      qa.hx = ha[0];
+      qa.hy = ha[1];
+      qa.hz = ha[2];
       // 32-bit index arithmetic: the same values as the 64-bit products
       // truncated to the 32-bit fields
-      q.me = ((uint32_t)z * (uint32_t)ly + (uint32_t)y) * (uint32_t)pitch + (uint32_t)x;
-      q.site = ((uint32_t)z * (uint32_t)ly + (uint32_t)y) * (uint32_t)lx + (uint32_t)x;
-    };
-    // items i = threadIdx.x, + kThreads, ... as (row, column) cursors, two
-    // at a time
-    int ra = threadIdx.x / half, ja = threadIdx.x - ra * half;
-    for (int i = threadIdx.x; i < n_items; i += 2 * kThreads) {
-      O3Site qa, qb;
-      load_site(qa, ra, ja);
-      int rb = ra + dr, jb = ja + dj;
-      if (jb >= half) {
-        jb -= half;
-        rb += 1;
+      const uint32_t row = (uint32_t)z * (uint32_t)ly + (uint32_t)y;
+      qa.me = row * (uint32_t)pitch + (uint32_t)xa;
+      qa.site = row * (uint32_t)lx + (uint32_t)xa;
+      if (two) {
+        qb.ax = ld_chk(pc, oc + xb, cstr);
+        qb.ay = ld_chk(pc + cstr, oc + xb, cstr);
+        qb.az = ld_chk(pc + 2 * cstr, oc + xb, cstr);
+        qb.me = qa.me + 2;
+        qb.site = qa.site + 2;
+      } else {
+        qb.ax = qa.ax;
+        qb.ay = qa.ay;
+        qb.az = qa.az;
+        qb.me = qa.me;
+        qb.site = qa.site;
       }
-      const bool two = i + kThreads < n_items;
-      if (two) load_site(qb, rb, jb);
-      else qb = qa;
+      qb.hx = hb[0];
+      qb.hy = hb[1];
+      qb.hz = hb[2];
       o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, S1, S2, cs, fx, nacc);
-      ra = rb + dr;
-      ja = jb + dj;
-      if (ja >= half) {
-        ja -= half;
-        ra += 1;
+      rl += dr;
+      m += dm;
+      if (m >= np) {
+        m -= np;
+        rl += 1;
       }
     }
-    o3_flush(tot, fx);  // per plane: at most hv * lx / 512 sites per thread since the last flush
+    o3_flush<COLOUR == 1>(tot, fx);  // per plane: at most one pair per thread per 256 pairs since the last flush
     __syncthreads();  // the next copy overwrites the z-1 slot read above
   }
   if (!ok_ring) {
