@@ -466,7 +466,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     // tiles re-read fewer halo planes but leave the last wave ragged: on
     // that mix 22 planes ran at 41.2 attempts/ns, 11 at 42.7, 8 at 47.5,
     // 6 at 44.1 and 4 at 45.2.
-    const int ty_max = (int)(kO3MarchSmem / (48 * (size_t)L.pitch)) - 2;
+    const int ty_max = (int)(kO3MarchSmem / (12 * (size_t)kO3RingSlots * L.pitch)) - 2;
     if (L.dims == 3 && ty_max >= 1) {
       L.march = true;
       const int rows = std::min(kn.o3_rows > 0 ? kn.o3_rows : 16, ty_max);
@@ -475,7 +475,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
       const int planes = kn.o3_planes > 0 ? kn.o3_planes : 8;
       const int ntz = (lz + planes - 1) / planes;
       L.tile_z = (lz + ntz - 1) / ntz;
-      L.smem = 48 * (size_t)(L.tile_y + 2) * L.pitch;
+      L.smem = 12 * (size_t)kO3RingSlots * (L.tile_y + 2) * L.pitch;
     } else {
       L.tile_y = std::max(1, std::min(ly, 4096 / lx));
       L.tile_z = L.dims == 3 ? std::max(1, std::min(lz, 4096 / (lx * L.tile_y))) : 1;

@@ -64,7 +64,8 @@ int validate_spec(const gpumc_spec* s);
 // passes its device's own count.
 constexpr int kDefaultSlots = 148 * 4;
 constexpr size_t kIsingTileSmem = 48 * 1024;  // whole-row Ising tile budget
-constexpr size_t kO3MarchSmem = 56 * 1024;   // ring of four O(3) planes per tile
+// O(3) z-march ring: the shared-memory budget that bounds a tile's rows
+constexpr size_t kO3MarchSmem = kO3RingSlots == 4 ? 56 * 1024 : 72 * 1024;
 constexpr int kDefaultSlots3 = 148 * 2;  // resident 3D Ising sweep CTAs of one B200
 Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots, int slots3 = kDefaultSlots3);
 int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);

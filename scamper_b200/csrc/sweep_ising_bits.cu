@@ -560,6 +560,7 @@ __global__ void __launch_bounds__(kThreads, 4)
           const int sl = i / W, c = i - sl * W;
           const int row = sl < 2 ? sl : g.hv + sl;  // local rows 0, 1, hv+2, hv+3
           const long long xn = (long long)gridDim.x * xstride;  // exchange buffer words
+          (void)xn;
           const long long iu = (long long)(up - xchg) + (long long)(2 + sl) * W + c;
           const long long id = (long long)(dn - xchg) + (long long)(sl - 2) * W + c;
           const uint2 v = sl < 2 ? (GPUMC_IN(iu, xn) ? __ldcg(xchg + iu) : make_uint2(0, 0))
@@ -662,6 +663,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   const long long np = (long long)(dz + 4) * pw;  // words of the resident slab
   const size_t slot = (size_t)4 * pw;
   const long long xn = (long long)gridDim.x * xstride;  // words of the exchange buffer
+  (void)xn;
   uint2* mine = xchg + (size_t)blockIdx.x * xstride;  // [parity][4 planes][pw]
   const int2 nb = nbr[blockIdx.x];  // (slab below, slab above)
   const uint64_t s0 = ld_volatile_u64(&L->sweep);

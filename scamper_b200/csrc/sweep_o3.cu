@@ -572,8 +572,9 @@ __global__ void __launch_bounds__(kThreads, 4)
 // multicast) issued by one thread: per component the slot's rows are at most
 // three contiguous runs of the plane (split where the rows wrap), and each
 // slot's mbarrier counts the bytes in (expect_tx / complete_tx).  Plane p of
-// the march (p = 0 for z0-1) goes to slot p & 3 as that slot's (p >> 2)-th
-// fill, so a step waits for phase parity (p >> 2) & 1 of its three slots.
+// the march (p = 0 for z0-1) goes to slot p % S as that slot's (p / S)-th
+// fill (S = kO3RingSlots), so a step waits for phase parity (p / S) & 1 of its
+// three slots; the copy of a plane is issued S - 3 steps before its first use.
 // Every wait is bounded; one that gives up flags the launch (ctl->err), waits
 // (bounded again) for the copies in flight and leaves the tile.  Every
 // neighbour read is a shared-memory read.  The pass reads only the other
@@ -618,7 +619,7 @@ __device__ __forceinline__ bool ring_wait(unsigned long long* bar, uint32_t pari
 // fit an SM: its register budget is that of three CTAs (no spills of the fp64
 // neighbour sums).
 template <int COLOUR, int ALG>
-__global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
+__global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 : 4)
     k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                      GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
   extern __shared__ __align__(16) float osm[];
@@ -645,16 +646,17 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
   const int slot = 3 * cstr;                // floats per ring slot
   float* S1 = S + (size_t)cs;
   float* S2 = S + 2 * (size_t)cs;
-  __shared__ __align__(8) unsigned long long ring_bar[4];
+  constexpr int NS = kO3RingSlots;
+  __shared__ __align__(8) unsigned long long ring_bar[NS];
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 4; ++i) ring_init(&ring_bar[i]);
+    for (int i = 0; i < NS; ++i) ring_init(&ring_bar[i]);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the inits, visible to the copy engine
   }
   __syncthreads();
-  // plane p of the march (z0 - 1 + p) into slot p & 3, by thread 0
+  // plane p of the march (z0 - 1 + p) into slot p % NS, by thread 0
   auto copy_plane = [&](int p) {
     if (threadIdx.x != 0) return;
-    const int sl = p & 3;
+    const int sl = p % NS;
     int zz = t.z0 - 1 + p;
     zz = zz < 0 ? zz + lz : (zz >= lz ? zz - lz : zz);
     ring_expect(&ring_bar[sl], (uint32_t)(3 * cstr) * 4u);
@@ -666,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
         const int n = min(RW - r, ly - y);  // rows contiguous up to the plane's last row
         const long long so = (long long)c * cs + ((long long)zz * ly + y) * pitch;
         const long long dof = (long long)sl * slot + (long long)c * cstr + (long long)r * pitch;
-        if (GPUMC_IN(so + (long long)n * pitch - 1, 3ll * cs) && GPUMC_IN(dof + (long long)n * pitch - 1, 4ll * slot))
+        if (GPUMC_IN(so + (long long)n * pitch - 1, 3ll * cs) && GPUMC_IN(dof + (long long)n * pitch - 1, (long long)NS * slot))
           ring_bulk_copy(osm + dof, S + so, (uint32_t)(n * pitch) * 4u, &ring_bar[sl]);
         r += n;
       }
@@ -684,27 +686,25 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
   const int n_pairs = hv * np;          // pairs of the tile's rows in one plane
   const int r0 = threadIdx.x / np, m0 = threadIdx.x - r0 * np;
   const int dr = kThreads / np, dm = kThreads - dr * np;  // cursor step of kThreads pairs
-  copy_plane(0);
-  copy_plane(1);
-  copy_plane(2);
+  int issued = 0;  // planes whose copies were issued: march planes 0 .. dv + 1 in all
+  for (; issued <= NS - 2 && issued <= dv + 1; ++issued) copy_plane(issued);
   bool ok_ring = true;
-  int issued = 3;  // planes whose copies were issued
   for (int k = 0; k < dv && ok_ring; ++k) {
     const int z = t.z0 + k;
     // plane z+2 (needed as z+1 of the next step) into the slot freed by the
     // previous step
-    if (k + 1 < dv) {
-      copy_plane(k + 3);
-      issued = k + 4;
+    if (k + NS - 1 <= dv + 1) {
+      copy_plane(k + NS - 1);
+      issued = k + NS;
     }
     // planes z-1, z, z+1 = march planes k, k+1, k+2
     for (int i = 0; i < 3 && ok_ring; ++i)
-      ok_ring = ring_wait(&ring_bar[(k + i) & 3], (uint32_t)((k + i) >> 2) & 1u);
+      ok_ring = ring_wait(&ring_bar[(k + i) % NS], (uint32_t)((k + i) / NS) & 1u);
     ok_ring = __syncthreads_and(ok_ring) != 0;  // one decision for the whole CTA
     if (!ok_ring) break;
-    const float* pm = osm + (k & 3) * slot;
-    const float* pc = osm + ((k + 1) & 3) * slot;
-    const float* pp = osm + ((k + 2) & 3) * slot;
+    const float* pm = osm + (k % NS) * slot;
+    const float* pc = osm + ((k + 1) % NS) * slot;
+    const float* pp = osm + ((k + 2) % NS) * slot;
     int rl = r0, m = m0;
     for (int i = threadIdx.x; i < n_pairs; i += kThreads) {
       const int y = t.y0 + rl;
@@ -779,7 +779,7 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 ? 3 : 4)
     // a copy did not land in time: flag the launch, wait (bounded) for every
     // copy still in flight into this CTA's ring, and leave the tile
     atomicExch(&ctl->err, 2);
-    for (int p = max(0, issued - 4); p < issued; ++p) ring_wait(&ring_bar[p & 3], (uint32_t)(p >> 2) & 1u);
+    for (int p = max(0, issued - NS); p < issued; ++p) ring_wait(&ring_bar[p % NS], (uint32_t)(p / NS) & 1u);
   }
   o3_commit<COLOUR>(L, tot, nacc);
   if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
