@@ -648,6 +648,49 @@ def headline_config(world, args):
             "l2": "inputs larger than L2 (2 x 3 x 64 MiB resident)"}
 
 
+def capture_workload(gpumc, torch, name):
+    """A few launches of one workload for ncu captures (no timing):
+    headline = the headline handle (3 x 8192^2 Ising) as a 64-sweep and a
+    16-sweep resident launch; pt = the PT ensembles (2D L=512 x64 + 3D L=128
+    x32, exchange every 10) as a 64-sweep and a 16-sweep chunk; o3 = 48 3D
+    O(3) lattices of 64^3 (cap proposal) batched, 6 sweeps (12 launches)."""
+    from scamper_b200 import _lib
+    if name == "headline":
+        mc = gpumc.ClassicalMC.from_params({"lattice_type": "square", "L": HEADLINE_L}, 1000, n_replicas=3,
+                                           betas=HEADLINE_BETAS, record_capacity=128)
+        mc.on_phase_start(_lib.PHASE_MEASUREMENT)
+        mc.sweep(64)
+        mc.observables()
+        mc.sweep(16)
+        mc.observables()
+        n = mc.launch_count()
+        mc.close()
+        return {"launches": n}
+    eng = gpumc.Engine()
+    if name == "pt":
+        sims = [gpumc.ClassicalMC.from_params({"lattice_type": "square", "L": 512}, 11, n_replicas=64,
+                                              betas=gpumc.geometric_ladder_betas(1.5, 3.5, 64), engine=eng),
+                gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 128}, 12, n_replicas=32,
+                                              betas=gpumc.geometric_ladder_betas(3.5, 5.5, 32), engine=eng)]
+        for m in sims:
+            m.pt_configure(10)
+        eng.sweep(64)
+        eng.sweep(16)
+    else:
+        rng = np.random.default_rng(5)
+        sims = [gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 64,
+                                               "beta": 1.0 / float(rng.uniform(1.2, 1.6)), "cone_half_angle": 1.0},
+                                              300 + i, model="o3", engine=eng, record_capacity=8)
+                for i in range(48)]
+        eng.sweep(6)
+    eng.synchronize()
+    n = eng.launch_count()
+    for m in sims:
+        m.close()
+    eng.close()
+    return {"launches": n}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline (the reference's algorithm restated in C; bounded sample)
 # ---------------------------------------------------------------------------
@@ -756,6 +799,8 @@ def main():
     ap.add_argument("--cpu1-meas", type=int, default=10000)
     ap.add_argument("--cpu1-msc-sweeps", type=int, default=300)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--capture", choices=["headline", "pt", "o3"], default=None,
+                    help="run a few launches of one workload for an ncu capture, no timing")
     ap.add_argument("--tune", action="store_true",
                     help="tune the tile knobs of the mixed and PT workloads live instead of using the cache")
     ap.add_argument("--only-headline", action="store_true")
@@ -780,6 +825,9 @@ def main():
     torch.cuda.set_device(local)
     import scamper_b200 as gpumc
 
+    if args.capture:
+        print(json.dumps({"capture": args.capture, "result": capture_workload(gpumc, torch, args.capture)}), flush=True)
+        return 0
     if args.only:
         fn = {"msc": bench_msc, "pt": bench_pt, "mixed": bench_mixed, "serving": bench_serving,
               "heat_bath": bench_heat_bath, "cluster": bench_cluster, "o3_proposals": bench_o3_proposals}[args.only]
