@@ -74,7 +74,13 @@ def max_over_ranks(dist, v):
 # clocks
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during a timed region."""
+    """Samples nvidia-smi clocks and throttle reasons during a timed region.
+    The sampler starts before the warm-up (nvidia-smi needs a few hundred ms
+    to print its first line); `mark(True)` / `mark(False)` bracket the timed
+    region on the host clock, and the summary keeps the samples inside it.
+    A timed region shorter than the 20 ms poll period falls back to the
+    samples nearest to it (taken under the same load, during the warm-up and
+    just after), and says so (`window`)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -82,9 +88,17 @@ class ClockSampler:
 
     def __init__(self, device):
         self.device = device
-        self.samples = []
+        self.samples = []  # (host time, fields)
         self.proc = None
         self.thread = None
+        self.t0 = self.t1 = None
+
+    def mark(self, start):
+        if start:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
+            time.sleep(0.05)  # one more poll after the region
 
     def __enter__(self):
         try:
@@ -102,7 +116,7 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.samples.append(parts)
+                self.samples.append((time.perf_counter(), parts))
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -114,19 +128,29 @@ class ClockSampler:
         return False
 
     def summary(self):
-        if not self.samples:
+        window = "timed region"
+        picked = self.samples
+        if self.t0 is not None and self.t1 is not None:
+            picked = [p for t, p in self.samples if self.t0 <= t <= self.t1]
+            if not picked:  # region shorter than the poll period
+                near = sorted(self.samples, key=lambda tp: min(abs(tp[0] - self.t0), abs(tp[0] - self.t1)))
+                picked = [p for _, p in near[:3]]
+                window = "nearest samples (timed region shorter than the 20 ms poll)"
+        else:
+            picked = [p for _, p in self.samples]
+        if not picked:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        sm = [float(s[1]) for s in picked if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in picked if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for s in self.samples:
+        for s in picked:
             for i, n in enumerate(names):
                 if s[5 + i].lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "reasons": sorted(reasons), "samples": len(picked), "window": window}
 
 
 # ---------------------------------------------------------------------------
@@ -206,12 +230,14 @@ def headline(gpumc, torch, args, dist, rank, world):
                                        record_capacity=max(64, n_sweeps, args.warmup * spp))
     mc.on_phase_start(_lib.PHASE_MEASUREMENT)  # observables recorded every sweep
     sp = mc.stream_ptr()
-    mc.sweep(args.warmup * spp)
-    mc.observables()
-    barrier(dist)
-    n0 = mc.launch_count()
     with ClockSampler(torch.cuda.current_device()) as clk:
+        mc.sweep(args.warmup * spp)
+        mc.observables()
+        barrier(dist)
+        n0 = mc.launch_count()
+        clk.mark(True)
         ms = time_sweeps(torch, mc, sp, n_sweeps, mc.sweep, warm=False)
+        clk.mark(False)
     launches = mc.launch_count() - n0
     barrier(dist)
     ms_max = max_over_ranks(dist, ms)
@@ -653,7 +679,8 @@ def capture_workload(gpumc, torch, name):
     headline = the headline handle (3 x 8192^2 Ising) as a 64-sweep and a
     16-sweep resident launch; pt = the PT ensembles (2D L=512 x64 + 3D L=128
     x32, exchange every 10) as a 64-sweep and a 16-sweep chunk; o3 = 48 3D
-    O(3) lattices of 64^3 (cap proposal) batched, 6 sweeps (12 launches)."""
+    O(3) lattices of 64^3 (cap proposal) batched, 6 sweeps (12 launches);
+    mixed = the uneven mix (256 2D Potts + 32 3D O(3)) batched, 6 sweeps."""
     from scamper_b200 import _lib
     if name == "headline":
         mc = gpumc.ClassicalMC.from_params({"lattice_type": "square", "L": HEADLINE_L}, 1000, n_replicas=3,
@@ -676,6 +703,10 @@ def capture_workload(gpumc, torch, name):
             m.pt_configure(10)
         eng.sweep(64)
         eng.sweep(16)
+    elif name == "mixed":
+        sims = [gpumc.ClassicalMC.from_params(p, 300 + i, model=m, engine=eng, record_capacity=8)
+                for i, (m, p, _) in enumerate(mixed_specs())]
+        eng.sweep(6)
     else:
         rng = np.random.default_rng(5)
         sims = [gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 64,
@@ -799,7 +830,7 @@ def main():
     ap.add_argument("--cpu1-meas", type=int, default=10000)
     ap.add_argument("--cpu1-msc-sweeps", type=int, default=300)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--capture", choices=["headline", "pt", "o3"], default=None,
+    ap.add_argument("--capture", choices=["headline", "pt", "o3", "mixed"], default=None,
                     help="run a few launches of one workload for an ncu capture, no timing")
     ap.add_argument("--tune", action="store_true",
                     help="tune the tile knobs of the mixed and PT workloads live instead of using the cache")
@@ -808,7 +839,7 @@ def main():
                     default=None,
                     help="run one extra workload alone (profiling)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[10.0, 30.0, 100.0, 300.0, 1000.0])
-    ap.add_argument("--serve-jobs", type=int, default=300)
+    ap.add_argument("--serve-jobs", type=int, default=1000)
     ap.add_argument("--serve-sweep-scale", type=float, default=1.0)
     ap.add_argument("--serve-chunk", type=int, default=20)
     ap.add_argument("--serve-budget-gb", type=float, default=64.0)

@@ -816,6 +816,29 @@ static inline uint32_t f_bits(float f) { uint32_t b; memcpy(&b, &f, 4); return b
 float orc_unit23(uint32_t u) { return bits_f(0x3F800000u | (u >> 9)) - 1.0f; }
 float orc_half23(uint32_t u) { return bits_f(0x3F800000u | (u >> 9)) - 0x1.fffffep-1f; }
 
+/* The three draw words of one O(3) site from two Philox words u, v: the top
+ * 21 bits of u and of v (low bits zero), and the two low 11-bit fields
+ * joined into the top 22 bits of the third word. */
+void orc_o3_split(uint32_t u, uint32_t v, uint32_t o[4]) {
+    o[0] = u & ~0x7FFu;
+    o[1] = v & ~0x7FFu;
+    o[2] = (u << 21) | ((v & 0x7FFu) << 10);
+    o[3] = 0;
+}
+
+/* The draw of an O(3) site update: one Philox call per pair of sites of the
+ * colour adjacent in a row (x0 = 4m + parity and x0 + 2, the sweep kernels'
+ * unit of work), counter (x0's site, colour | tag << 1, sweep); the pair's
+ * first site takes words 0-1, the second words 2-3 (orc_o3_split). */
+static void o3_site_draw(const geom* g, int64_t x, int64_t y, int64_t z, uint32_t colour, uint32_t tag,
+                         const uint32_t key[2], uint64_t sweep, uint32_t o[4]) {
+    int64_t lane = (x >> 1) & 1;
+    uint32_t ctr[4], w[4];
+    make_ctr(ctr, (uint64_t)site_of(g, x - 2 * lane, y, z), colour, tag, 0, sweep);
+    orc_philox4x32_10(ctr, key, w);
+    orc_o3_split(w[2 * lane], w[2 * lane + 1], o);
+}
+
 /* (cos, sin) of 2 pi u / 2^32: octant from the top 3 bits, the next 23 bits
  * as the fraction t of the octant, Taylor polynomials of degree 9 / 10 on
  * [0, pi/4] (Horner, fused), swaps and signs by octant. */
@@ -987,9 +1010,8 @@ double orc_sweep_o3_prop(int dims, int64_t lx, int64_t ly, int64_t lz, float J, 
                         hz = hz + sz[nb[i]];
                     }
                     float ax = sx[site], ay = sy[site], az = sz[site];
-                    uint32_t ctr[4], o[4];
-                    make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_O3, 0, sweep);
-                    orc_philox4x32_10(ctr, key, o);
+                    uint32_t o[4];
+                    o3_site_draw(&g, x, y, z, colour, ORC_TAG_O3, key, sweep, o);
                     float nx, ny, nz;
                     orc_o3_propose(prop, ax, ay, az, o, omc, &nx, &ny, &nz);
                     if (orc_o3_accept(ax, ay, az, nx, ny, nz, hx, hy, hz, mJ, beta, o[2])) {
@@ -1084,9 +1106,8 @@ double orc_sweep_o3_hb(int dims, int64_t lx, int64_t ly, int64_t lz, float J, fl
                         hy = hy + sy[nb[i]];
                         hz = hz + sz[nb[i]];
                     }
-                    uint32_t ctr[4], o[4];
-                    make_ctr(ctr, (uint64_t)site, colour, ORC_TAG_O3HB, 0, sweep);
-                    orc_philox4x32_10(ctr, key, o);
+                    uint32_t o[4];
+                    o3_site_draw(&g, x, y, z, colour, ORC_TAG_O3HB, key, sweep, o);
                     /* w = 1 - cos(theta) by the inverse CDF of exp(kappa cos) */
                     float fx = J * hx, fy = J * hy, fz = J * hz;
                     float nrm = sqrtf((fx * fx + fy * fy) + fz * fz);

@@ -148,6 +148,10 @@ float orc_log_one_minus(float y);
  * colour-1 bond sums at 2^-19, magnetisation components at 2^-21). */
 float orc_unit23(uint32_t u);
 float orc_half23(uint32_t u);
+/* The three draw words of an O(3) site from two Philox words (one Philox
+ * call per pair of adjacent sites of a colour in a row, keyed by the pair's
+ * first site; the first site takes words 0-1, the second words 2-3). */
+void orc_o3_split(uint32_t u, uint32_t v, uint32_t o[4]);
 void orc_sincos23(uint32_t u, float* c, float* s);
 float orc_exp_neg2(float x);
 void orc_o3_propose(int prop, float ax, float ay, float az, const uint32_t o[4], float omc,

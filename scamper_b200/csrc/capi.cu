@@ -37,7 +37,7 @@ template <int DIM>
 __global__ void k_sweep_msc(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM>
 __global__ void k_sweep_potts_bits(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
-template <int COLOUR, int ALG>
+template <int COLOUR, int ALG, int CLS>
 __global__ void k_sweep_o3_march(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 template <int DIM, int MODEL, int WOLFF>
 __global__ void k_cluster_local(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
@@ -460,7 +460,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     L.inplace = true;
     L.tile_cx = (lx + 3) / 4;
     // 3D: tiles of whole rows marched along z through a ring of four shared
-    // planes (3 components x (rows + 2 halo rows) x pitch floats each) of at
+    // planes (3 components x (rows + 2 halo rows) x pitch floats) of at
     // most 56 KB (three CTAs per SM), up to 16 rows x 8 planes per tile (for
     // 32 lattices of 64^3: 1024 tiles, 2.3 waves of 148 x 3 CTAs).  Deeper
     // tiles re-read fewer halo planes but leave the last wave ragged: on
@@ -475,7 +475,8 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
       const int planes = kn.o3_planes > 0 ? kn.o3_planes : 8;
       const int ntz = (lz + planes - 1) / planes;
       L.tile_z = (lz + ntz - 1) / ntz;
-      L.smem = 12 * (size_t)kO3RingSlots * (L.tile_y + 2) * L.pitch;
+      const int cls = o3_row_class(L.pitch);
+      L.smem = 12 * (size_t)kO3RingSlots * L.pitch * (cls ? o3_class_rows(cls) : L.tile_y + 2);
     } else {
       L.tile_y = std::max(1, std::min(ly, 4096 / lx));
       L.tile_z = L.dims == 3 ? std::max(1, std::min(lz, 4096 / (lx * L.tile_y))) : 1;
@@ -536,7 +537,7 @@ int kernel_kind(const Layout& L) {
                  : L.prop == GPUMC_O3_UNIFORM ? kKindO3Uniform
                  : L.prop == GPUMC_O3_OPSS ? kKindO3Opss : 0;
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
-  if (L.model == O3 && L.march) return 10 + hb;
+  if (L.model == O3 && L.march) return 10 + o3_row_class(L.pitch) + hb;
   return L.model * 2 + (L.dims - 2) + hb;
 }
 
@@ -655,7 +656,21 @@ size_t footprint_bytes(const gpumc_spec* s) {
 // kernel launch table
 // ---------------------------------------------------------------------------
 typedef void (*SweepKernel)(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
+// The O(3) z-march kernel of a colour for kind 10..13 (+ algorithm offset).
+#define O3_MARCH_ROW(C, A) \
+  {k_sweep_o3_march<C, A, 0>, k_sweep_o3_march<C, A, 1>, k_sweep_o3_march<C, A, 2>, k_sweep_o3_march<C, A, 3>}
+static const SweepKernel kO3March[2][4][4] = {
+    {O3_MARCH_ROW(0, 0), O3_MARCH_ROW(0, 1), O3_MARCH_ROW(0, 2), O3_MARCH_ROW(0, 3)},
+    {O3_MARCH_ROW(1, 0), O3_MARCH_ROW(1, 1), O3_MARCH_ROW(1, 2), O3_MARCH_ROW(1, 3)}};
+#undef O3_MARCH_ROW
+static SweepKernel o3_march_kernel(int colour, int kind) {
+  if (!is_o3_march_kind(kind)) return nullptr;
+  const int off = kind - kind % 16;
+  const int alg = off == kKindHeatBath ? 1 : off == kKindO3Uniform ? 2 : off == kKindO3Opss ? 3 : 0;
+  return kO3March[colour][alg][kind % 16 - 10];
+}
 static SweepKernel kernel_for(int kind) {
+  if (is_o3_march_kind(kind)) return o3_march_kernel(1, kind);
   switch (kind) {
     case 0: return k_sweep_ising_bits<2, 0>;
     case 1: return k_sweep_ising_bits<3, 0>;
@@ -667,20 +682,16 @@ static SweepKernel kernel_for(int kind) {
     case 7: return k_sweep_msc<3>;
     case 8: return k_sweep_potts_bits<2>;
     case 9: return k_sweep_potts_bits<3>;
-    case 10: return k_sweep_o3_march<1, 0>;
     case kKindHeatBath + 0: return k_sweep_ising_bits<2, 1>;
     case kKindHeatBath + 1: return k_sweep_ising_bits<3, 1>;
     case kKindHeatBath + 2: return k_sweep_discrete_2d<POTTS, 1>;
     case kKindHeatBath + 3: return k_sweep_discrete_3d<POTTS, 1>;
     case kKindHeatBath + 4: return k_sweep_o3<2, 1, 1>;
     case kKindHeatBath + 5: return k_sweep_o3<3, 1, 1>;
-    case kKindHeatBath + 10: return k_sweep_o3_march<1, 1>;
     case kKindO3Uniform + 4: return k_sweep_o3<2, 1, 2>;
     case kKindO3Uniform + 5: return k_sweep_o3<3, 1, 2>;
-    case kKindO3Uniform + 10: return k_sweep_o3_march<1, 2>;
     case kKindO3Opss + 4: return k_sweep_o3<2, 1, 3>;
     case kKindO3Opss + 5: return k_sweep_o3<3, 1, 3>;
-    case kKindO3Opss + 10: return k_sweep_o3_march<1, 3>;
     default: return nullptr;
   }
 }
@@ -707,12 +718,12 @@ static int prepare_kernels() {
       cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
     }
-    const void* colour0[] = {(const void*)k_sweep_o3_march<0, 0>, (const void*)k_sweep_o3_march<0, 1>,
-                             (const void*)k_sweep_o3_march<0, 2>, (const void*)k_sweep_o3_march<0, 3>};
-    for (const void* f : colour0) {
-      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
-      if (e != cudaSuccess) status = e;
-    }
+    for (int a = 0; a < 4; ++a)
+      for (int c = 0; c < 4; ++c) {
+        cudaError_t e = cudaFuncSetAttribute(kO3March[0][a][c], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kMaxDynSmem);
+        if (e != cudaSuccess) status = e;
+      }
   });
   if (status != cudaSuccess)
     return fail(GPUMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(status));
@@ -749,19 +760,13 @@ int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_
   // O(3) sweeps in place: colour 0, then colour 1 (which runs the epilogue)
   if (kind == 4) k_sweep_o3<2, 0, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == 5) k_sweep_o3<3, 0, 0><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
-  if (kind == 10) k_sweep_o3_march<0, 0><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindHeatBath + 4) k_sweep_o3<2, 0, 1><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindHeatBath + 5) k_sweep_o3<3, 0, 1><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
-  if (kind == kKindHeatBath + 10)
-    k_sweep_o3_march<0, 1><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindO3Uniform + 4) k_sweep_o3<2, 0, 2><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindO3Uniform + 5) k_sweep_o3<3, 0, 2><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
-  if (kind == kKindO3Uniform + 10)
-    k_sweep_o3_march<0, 2><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindO3Opss + 4) k_sweep_o3<2, 0, 3><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindO3Opss + 5) k_sweep_o3<3, 0, 3><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
-  if (kind == kKindO3Opss + 10)
-    k_sweep_o3_march<0, 3><<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
+  if (is_o3_march_kind(kind)) o3_march_kernel(0, kind)<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   k<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   CUDA_TRY(cudaGetLastError());
   return GPUMC_OK;
@@ -1241,7 +1246,7 @@ uint64_t gpumc_engine::launches_per_batch_sweep() const {
   for (const auto& p : batch_plans)
     if (!(p.res.on && blocking)) {
       const int base = p.kind % kKindHeatBath;  // O(3) sweeps are two colour launches
-      n += is_cluster_kind(p.kind) ? 4 : (base == 4 || base == 5 || base == 10) ? 2 : 1;
+      n += is_cluster_kind(p.kind) ? 4 : (base == 4 || base == 5 || is_o3_march_kind(p.kind)) ? 2 : 1;
     }
   for (gpumc_sim* s : sims)
     if (s->lay.model == MSC && s->phase == GPUMC_PHASE_MEASUREMENT) n += (uint64_t)s->n_rep + 1;

@@ -44,6 +44,22 @@ constexpr int kThreads = 256;      // CTA size of the sweep kernels
 #define GPUMC_O3_RING_SLOTS 4
 #endif
 constexpr int kO3RingSlots = GPUMC_O3_RING_SLOTS;
+// O(3) z-march ring slots: a slot holds the three component planes of the
+// tile's rows (y0-1 .. y0+hv) one after another, rows at the lattice's
+// pitch, so each component's rows are one contiguous copy (split only where
+// the rows wrap).  For the row pitches 32, 64 and 128 (row classes 1, 2, 3)
+// the kernel is compiled with the pitch and a component stride of
+// o3_class_rows(class) rows (the most rows a ring of kO3RingSlots slots of
+// kO3MarchSmem bytes holds), so every neighbour offset is a compile-time constant;
+// class 0 takes both at run time.
+__host__ __device__ constexpr int o3_row_class(int pitch) {
+  return pitch == 32 ? 1 : pitch == 64 ? 2 : pitch == 128 ? 3 : 0;
+}
+__host__ __device__ constexpr int o3_class_row(int cls) { return cls == 1 ? 32 : cls == 2 ? 64 : cls == 3 ? 128 : 0; }
+constexpr int kO3MarchSmem = kO3RingSlots == 4 ? 56 * 1024 : 72 * 1024;  // ring bytes per CTA at most
+__host__ __device__ constexpr int o3_class_rows(int cls) {
+  return cls == 0 ? 0 : kO3MarchSmem / (12 * kO3RingSlots * o3_class_row(cls));
+}
 // observables binned on the device, in this order: Energy, E2, Magnetization,
 // M2, M4 (DefaultObservableSet, CMC.rs/src/observables/common.rs:81-95)
 constexpr int kBinObs = 5;

@@ -52,7 +52,8 @@ constexpr int kKindO3Uniform = 48, kKindO3Opss = 64;
 inline bool is_ising2d_bits_kind(int kind) { return kind == 0 || kind == kKindHeatBath; }
 // O(3) z-march kernels (any proposal or the heat bath): their ring copies
 // flag a wait that gave up in LaunchCtl::err
-inline bool is_o3_march_kind(int kind) { return !is_cluster_kind(kind) && kind % 16 == 10; }
+// O(3) z-march kinds: 10 + the row class (o3_row_class) of the lattices
+inline bool is_o3_march_kind(int kind) { return !is_cluster_kind(kind) && kind % 16 >= 10 && kind % 16 <= 13; }
 // Reads and clears LaunchCtl::err after the stream's work; a set flag (a
 // ring copy that did not land in time) becomes GPUMC_ECUDA.
 int check_launch_flag(cudaStream_t st, LaunchCtl* ctl);
@@ -65,7 +66,7 @@ int validate_spec(const gpumc_spec* s);
 constexpr int kDefaultSlots = 148 * 4;
 constexpr size_t kIsingTileSmem = 48 * 1024;  // whole-row Ising tile budget
 // O(3) z-march ring: the shared-memory budget that bounds a tile's rows
-constexpr size_t kO3MarchSmem = kO3RingSlots == 4 ? 56 * 1024 : 72 * 1024;
+
 constexpr int kDefaultSlots3 = 148 * 2;  // resident 3D Ising sweep CTAs of one B200
 Layout plan_layout(const gpumc_spec* s, int slots = kDefaultSlots, int slots3 = kDefaultSlots3);
 int ising_tile_rows(int ly, int n_rep, int nseg, int hv_max, int slots);

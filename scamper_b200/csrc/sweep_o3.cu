@@ -52,11 +52,18 @@
 // branch.  The sample is placed with the same basis and renormalisation as
 // the cap proposal.  Draws come from tag TAG_O3HB (word 0: v, word 1: phi);
 // there is no cone to adapt, and "accepted" counts the sites that changed.
+// (Word 0 and word 1 here are a site's first and second draw.)
+//
+// Random draws: one Philox4x32-10 call per pair of sites of the colour that
+// are adjacent in a row (x0 = 4m + parity and x0 + 2: the kernels' unit of
+// work), counter (x0's site, colour | tag << 1, sweep); the first site takes
+// words 0-1 and the second words 2-3, each site's two words split into its
+// three draws (o3_split: 21, 21 and 22 bits).
 //
 // Arithmetic of the Metropolis step (ALG 0, 2, 3): two sites per thread
 // evaluated together with Blackwell's packed fp32 pair instructions
 // (fma/add/mul.rn.f32x2: one instruction, two IEEE-rounded lane results),
-// uniforms built from Philox bits (1.m - 1 with 23 bits of the word, no
+// uniforms built from Philox bits (1.m - 1 with the draw's top bits as m, no
 // integer-to-float conversion), products fused where the CPU replay fuses
 // them (fmaf), square root and division IEEE-rounded, and exp / sin / cos the
 // engine's own polynomials; the CPU replay (oracle/oracle.c,
@@ -361,6 +368,13 @@ __device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
   return c;
 }
 
+// The three draw words of a site from two Philox words u, v: the top 21
+// bits of u and of v (low bits zero), and the two low 11-bit fields joined
+// into the top 22 bits of the third word (orc_o3_split).
+__device__ __forceinline__ uint4 o3_split(uint32_t u, uint32_t v) {
+  return make_uint4(u & ~0x7FFu, v & ~0x7FFu, (u << 21) | ((v & 0x7FFu) << 10), 0u);
+}
+
 // One site of a colour pass: its own spin and the fp32 sum of its
 // neighbours (in the fixed order x-1, x+1, y-1, y+1, z-1, z+1).
 struct O3Site {
@@ -403,12 +417,25 @@ __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const fl
 // Updates the pair (qa, qb) of a colour pass (qb only when `two`): writes
 // accepted spins in place, counts acceptances and adds the fixed-point
 // observables of the final spins.
+// Stores spin (x, y, z) at element `me` of the three component planes of S
+// (plane stride cs).
+__device__ __forceinline__ void o3_store3(float* S, uint32_t cs, uint32_t me, float x, float y, float z) {
+  if (GPUMC_IN(me, cs)) {
+    float* p = S + me;
+    p[0] = x;
+    p[cs] = y;
+    p[2 * (size_t)cs] = z;
+  }
+}
+
 template <int COLOUR, int ALG>
 __device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& qb, bool two, const O3Philox& P,
-                                               float omc, float mJ, float beta, float* S, float* S1, float* S2,
-                                               uint32_t cs, O3Fix& fx, int& nacc) {
-  const uint4 oa = o3_philox(P, qa.site);
-  const uint4 ob = o3_philox(P, two ? qb.site : qa.site);
+                                               float omc, float mJ, float beta, float* S, uint32_t cs, O3Fix& fx,
+                                               int& nacc) {
+  // one draw per pair (keyed by its first site, qa): words 0-1 for qa,
+  // 2-3 for qb
+  const uint4 w = o3_philox(P, qa.site);
+  const uint4 oa = o3_split(w.x, w.y), ob = o3_split(w.z, w.w);
   f2 fx2 = F2(qa.ax, qb.ax), fy2 = F2(qa.ay, qb.ay), fz2 = F2(qa.az, qb.az);
   const f2 hx = F2(qa.hx, qb.hx), hy = F2(qa.hy, qb.hy), hz = F2(qa.hz, qb.hz);
   bool ok_a, ok_b;
@@ -430,16 +457,8 @@ __device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& q
     fz2 = F2(ok_a ? lo(nz) : qa.az, ok_b ? hi(nz) : qb.az);
   }
   ok_b = ok_b && two;
-  if (ok_a) {
-    st_chk(S, qa.me, cs, lo(fx2));
-    st_chk(S1, qa.me, cs, lo(fy2));
-    st_chk(S2, qa.me, cs, lo(fz2));
-  }
-  if (ok_b) {
-    st_chk(S, qb.me, cs, hi(fx2));
-    st_chk(S1, qb.me, cs, hi(fy2));
-    st_chk(S2, qb.me, cs, hi(fz2));
-  }
+  if (ok_a) o3_store3(S, cs, qa.me, lo(fx2), lo(fy2), lo(fz2));
+  if (ok_b) o3_store3(S, cs, qb.me, hi(fx2), hi(fy2), hi(fz2));
   nacc += (int)ok_a + (int)ok_b;
   // every bond has one colour-1 end: the colour-1 pass also sums s . h
   o3_fix_add_2<COLOUR == 1>(fx, fx2, fy2, fz2, hx, hy, hz, two);
@@ -501,36 +520,38 @@ __global__ void __launch_bounds__(kThreads, 4)
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
   const int hv = min(t.ty, ly - t.y0);
   const int dv = DIM == 3 ? min(t.tz, lz - t.z0) : 1;
-  const int half = lx >> 1;
+  const int half = lx >> 1;        // sites of the colour per row
+  const int np = (half + 1) >> 1;  // pairs per row (the last may be single)
   const int rows = hv * dv;
-  // thread mapping: fixed column (or column stride) per thread, rows strided
+  // Work items are pairs of horizontally adjacent sites of the colour in one
+  // row (x and x + 2, x = 4m + parity), one draw per pair, as in the z-march
+  // kernel.  Thread mapping: fixed pair column (or column stride) per thread,
+  // rows strided.
   int col0, cstep, r0, rstep;
-  if (half >= kThreads) {
+  if (np >= kThreads) {
     col0 = threadIdx.x;
     cstep = kThreads;
     r0 = 0;
     rstep = 1;
   } else {
-    col0 = threadIdx.x % half;
-    cstep = half;
-    r0 = threadIdx.x / half;
-    rstep = kThreads / half;
+    col0 = threadIdx.x % np;
+    cstep = np;
+    r0 = threadIdx.x / np;
+    rstep = kThreads / np;
   }
   O3Fix fx = {{0, 0, 0}, 0, 0};
   O3Totals tot = {{0, 0, 0}, 0};
   int nacc = 0;
-  // this thread's sites, row-major: rows r0, r0 + rstep, ... of the tile's
-  // rows (y fastest, then z), columns col0, col0 + cstep, ...; taken two at a
-  // time, with the (row, column) cursor advanced without divisions
-  const int nc = (r0 < rstep && col0 < half) ? (half - col0 + cstep - 1) / cstep : 0;
+  // this thread's pairs, row-major: rows r0, r0 + rstep, ... of the tile's
+  // rows (y fastest, then z), pair columns col0, col0 + cstep, ...; the
+  // (row, column) cursor advances without divisions
+  const int nc = (r0 < rstep && col0 < np) ? (np - col0 + cstep - 1) / cstep : 0;
   const int nr = r0 < rstep ? (rows - r0 + rstep - 1) / rstep : 0;
   const int n_items = nc * nr;
   int cy = t.y0 + (DIM == 3 ? r0 % hv : r0), cz = DIM == 3 ? t.z0 + r0 / hv : 0, cc = 0;
   const int ry = DIM == 3 ? rstep % hv : rstep, rz = DIM == 3 ? rstep / hv : 0;
-  auto next_site = [&](int& x, int& y, int& z) {
-    y = cy;
-    z = cz;
-    x = 2 * (col0 + cc * cstep) + ((y + z + COLOUR) & 1);
+  for (int k = 0; k < n_items; ++k) {
+    const int y = cy, z = cz, m = col0 + cc * cstep;
     if (++cc == nc) {
       cc = 0;
       cy += ry;
@@ -540,21 +561,16 @@ __global__ void __launch_bounds__(kThreads, 4)
         cz += 1;
       }
     }
-  };
-  for (int k = 0; k < n_items; k += 2) {
-    int x, y, z;
+    const int xa = 4 * m + ((y + z + COLOUR) & 1);
+    const bool two = 2 * m + 1 < half;
     O3Site qa, qb;
-    next_site(x, y, z);
-    o3_load_site<DIM>(qa, S, S1, S2, x, y, z, lx, ly, lz, pitch, cs);
-    const bool two = k + 1 < n_items;
-    if (two) {
-      next_site(x, y, z);
-      o3_load_site<DIM>(qb, S, S1, S2, x, y, z, lx, ly, lz, pitch, cs);
-    } else {
+    o3_load_site<DIM>(qa, S, S1, S2, xa, y, z, lx, ly, lz, pitch, cs);
+    if (two)
+      o3_load_site<DIM>(qb, S, S1, S2, xa + 2, y, z, lx, ly, lz, pitch, cs);
+    else
       qb = qa;
-    }
-    o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, S1, S2, cs, fx, nacc);
-    if ((k & 62) == 62) o3_flush<COLOUR == 1>(tot, fx);  // every 64 sites: 32-bit partials stay far from overflow
+    o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, cs, fx, nacc);
+    if ((k & 31) == 31) o3_flush<COLOUR == 1>(tot, fx);  // every 64 sites: 32-bit partials stay far from overflow
   }
   o3_flush<COLOUR == 1>(tot, fx);
   o3_commit<COLOUR>(L, tot, nacc);
@@ -562,27 +578,39 @@ __global__ void __launch_bounds__(kThreads, 4)
 }
 
 // ---------------------------------------------------------------------------
-// 3D colour pass marched along z through a ring of four shared-memory planes.
+// 3D colour pass marched along z through a ring of shared-memory planes.
 //
 // A tile is whole rows y0 .. y0+hv-1 of planes z0 .. z0+dv-1.  Each plane the
 // tile touches (z0-1 .. z0+dv) is copied once, rows y0-1 .. y0+hv with all
 // three components, into a ring slot and serves as the z-1, z and z+1 plane
-// of three consecutive steps; the copy of plane z+2 is in flight while plane
-// z is computed.  The copies are bulk asynchronous copies (cp.async.bulk, no
-// multicast) issued by one thread: per component the slot's rows are at most
-// three contiguous runs of the plane (split where the rows wrap), and each
-// slot's mbarrier counts the bytes in (expect_tx / complete_tx).  Plane p of
-// the march (p = 0 for z0-1) goes to slot p % S as that slot's (p / S)-th
-// fill (S = kO3RingSlots), so a step waits for phase parity (p / S) & 1 of its
-// three slots; the copy of a plane is issued S - 3 steps before its first use.
-// Every wait is bounded; one that gives up flags the launch (ctl->err), waits
-// (bounded again) for the copies in flight and leaves the tile.  Every
-// neighbour read is a shared-memory read.  The pass reads only the other
-// colour's values (and its own sites' old values, which only this tile
-// writes), so copying planes that other tiles update in place is race-free.
-// The site arithmetic and its operation order are those of k_sweep_o3.
+// of three consecutive steps.  A slot holds the three components one after
+// another, each as the tile's rows at the lattice's pitch; for pitches 32, 64
+// and 128 the pitch and the component stride are compiled in
+// (o3_row_class), so every neighbour of a thread's sites is a fixed offset
+// from one index per plane and the loads take the offsets as immediates.
+//
+// The copies are bulk asynchronous copies (cp.async.bulk, no multicast), one
+// per component and contiguous run of rows (at most three: split where the
+// rows wrap), issued by three lanes of one warp; each slot's mbarrier counts
+// the bytes in (expect_tx / complete_tx).  (One copy per row and component
+// measured 1.65x slower: many small copies queue in the copy engine.)  Plane p of a
+// tile's march (p = 0 for z0-1) goes to slot p % S (S = kO3RingSlots) as that
+// slot's (p / S)-th fill, so a step waits for phase parity (p / S) & 1 of its
+// three slots.  The warps are not synchronised per plane: each warp waits for
+// the planes of its step, computes its pairs and then releases the plane it
+// no longer needs (a per-slot arrival counter in shared memory); the warp
+// whose arrival completes a slot's count refills the slot with plane p + S.
+// A warp can thus run up to S - 3 steps ahead of the slowest one, and no
+// step ends in a CTA-wide barrier.  Every wait is bounded; one that gives up
+// flags the launch (ctl->err), stops the other warps' waits, waits (bounded
+// again) for the copies in flight and leaves the tile.  The pass reads only
+// the other colour's values (and its own sites' old values, which only this
+// tile writes), so copying planes that other tiles update in place is
+// race-free.  The site arithmetic and its operation order are those of
+// k_sweep_o3.
 // ---------------------------------------------------------------------------
 constexpr long long kRingWaitPolls = 1ll << 20;  // try_wait polls per ring wait
+constexpr int kWarps = kThreads / 32;
 
 __device__ __forceinline__ void ring_init(unsigned long long* bar) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
@@ -601,170 +629,207 @@ __device__ __forceinline__ void ring_bulk_copy(void* dst, const void* src, uint3
                "l"(src), "r"(bytes), "r"(a)
                : "memory");
 }
-// Bounded wait for the completion of phase `parity` of a slot's mbarrier.
-__device__ __forceinline__ bool ring_wait(unsigned long long* bar, uint32_t parity) {
+__device__ __forceinline__ bool ring_test(unsigned long long* bar, uint32_t parity) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  uint32_t done;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(done)
+               : "r"(a), "r"(parity)
+               : "memory");
+  return done != 0;
+}
+// Bounded wait for the completion of phase `parity` of a slot's mbarrier;
+// gives up early when another warp has flagged the ring (`abort`).
+__device__ __forceinline__ bool ring_wait(unsigned long long* bar, uint32_t parity, const volatile int* abort) {
   for (long long it = 0; it < kRingWaitPolls; ++it) {
-    uint32_t done;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(done)
-                 : "r"(a), "r"(parity)
-                 : "memory");
-    if (done) return true;
+    if (ring_test(bar, parity)) return true;
+    if ((it & 63) == 63 && *abort) return false;
   }
   return false;
 }
 
-// Colour 1 also carries the sweep epilogue's shared memory, so three CTAs
-// fit an SM: its register budget is that of three CTAs (no spills of the fp64
-// neighbour sums).
-template <int COLOUR, int ALG>
-__global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 : 4)
-    k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
-                     GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
-  extern __shared__ __align__(16) float osm[];
-  const TileItem t = tiles[blockIdx.x];
-  LatDesc* L = &lats[t.lat];
-  const GroupDesc* G = &groups[L->group];
-  const uint64_t sweep = L->sweep;
-  if (sweep >= L->target) {
-    if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
-    return;
+// Ring state of a CTA: per-slot fill barriers and arrival counters, and the
+// tile's observable totals (kept here rather than in registers).
+struct O3Ring {
+  unsigned long long full[kO3RingSlots];
+  unsigned int freed[kO3RingSlots];
+  int abort;
+  int issued;        // march planes whose copies were issued (this tile)
+  long long tot[5];  // magnetisation x, y, z, bond sum, accepted
+};
+
+// Adds the warp's fixed-point partial sums (and acceptances) to the CTA
+// totals: 64-bit butterfly over the lanes, one shared atomic per value.  All
+// 32 lanes call.  The 32-bit partials are exact modulo 2^32 and their true
+// values stay below 2^31 in magnitude (fewer than 512 terms of at most
+// 6 2^19 each), so each lane's value is recovered exactly.
+template <bool BOND>
+__device__ __forceinline__ void o3_flush_warp(O3Ring& R, O3Fix& q, int& nacc) {
+  const uint32_t off = q.n * 0x4B400000u;
+  long long v[5] = {(int32_t)(q.m[0] - off), (int32_t)(q.m[1] - off), (int32_t)(q.m[2] - off),
+                    BOND ? (long long)(int32_t)(q.e - off) : 0ll, (long long)nacc};
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xFFFFFFFFu, v[i], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+      if (v[i]) atomicAdd((unsigned long long*)&R.tot[i], (unsigned long long)v[i]);
+  q = O3Fix{{0, 0, 0}, 0, 0};
+  nacc = 0;
+}
+
+// Issues the copy of march plane p of tile t into its slot: per component,
+// the tile's rows y0-1 .. y0+hv as one contiguous run of the plane (split
+// where the rows wrap), by lanes 0..2 of the calling warp (all 32 lanes
+// call).  `crows` is the slot's rows per component.  The geometry is read
+// again from the lattice descriptor (cached), so none of it stays live in
+// registers across the march.
+__device__ __forceinline__ void o3_issue_plane(const TileItem& t, const LatDesc* L, O3Ring& R, float* osm, int p,
+                                               int crows, int lane) {
+  const int ly = L->ly, lz = L->lz, pitch = L->pitch;
+  const long long cs = (long long)pitch * ly * lz;
+  const int hv = min(t.ty, ly - t.y0);
+  const int RW = hv + 2;
+  const long long cstr = (long long)crows * pitch;
+  const long long slot = 3 * cstr;
+  const int sl = p % kO3RingSlots;
+  if (lane == 0) {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // generic reads of the slot before the refill
+    ring_expect(&R.full[sl], (uint32_t)(RW * 3 * pitch) * 4u);
   }
+  __syncwarp();
+  if (lane < 3) {
+    const int c = lane;
+    const float* S = (const float*)L->buf[0];
+    int zz = t.z0 - 1 + p;
+    zz = zz < 0 ? zz + lz : (zz >= lz ? zz - lz : zz);
+    int r = 0;
+    while (r < RW) {
+      int y = t.y0 - 1 + r;
+      y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
+      const int n = min(RW - r, ly - y);  // rows contiguous up to the plane's last row
+      const long long so = (long long)c * cs + ((long long)zz * ly + y) * pitch;
+      const long long dof = (long long)sl * slot + (long long)c * cstr + (long long)r * pitch;
+      if (GPUMC_IN(so + (long long)n * pitch - 1, 3 * cs) && GPUMC_IN(dof + (long long)n * pitch - 1, kO3RingSlots * slot))
+        ring_bulk_copy(osm + dof, S + so, (uint32_t)(n * pitch) * 4u, &R.full[sl]);
+      r += n;
+    }
+  }
+}
+
+// Shared-memory load of slot element i (checked in bounds-checked builds).
+__device__ __forceinline__ float o3_lds(const float* base, int i, int lim) {
+#ifdef GPUMC_DEBUG_BOUNDS
+  return GPUMC_IN(i, lim) ? base[i] : 0.0f;
+#else
+  (void)lim;
+  return base[i];
+#endif
+}
+
+// One tile of a colour pass; RP_ is the compiled row pitch and CROWS_ the
+// compiled rows per component of a slot (0: the lattice's pitch and the
+// tile's rows at run time).
+template <int COLOUR, int ALG, int RP_, int CROWS_>
+__device__ __forceinline__ void o3_march_tile(const TileItem& t, LatDesc* L, const GroupDesc* G, LaunchCtl* ctl,
+                                              float* osm, O3Ring& R) {
+  O3Fix fx = {{0, 0, 0}, 0, 0};
+  int nacc = 0;
   const int lx = L->lx, ly = L->ly, lz = L->lz, pitch = L->pitch;
-  const uint32_t cs = (uint32_t)pitch * ly * lz;  // component plane stride (< 2^32 elements)
+  const long long csl = (long long)pitch * ly * lz;
   float* S = (float*)L->buf[0];
+  const int hv = min(t.ty, ly - t.y0);
+  const int dv = min(t.tz, lz - t.z0);
+  const int RP = RP_ > 0 ? RP_ : pitch;               // floats per slot row (= pitch)
+  const int crows = CROWS_ > 0 ? CROWS_ : hv + 2;     // slot rows per component
+  const int cstr = crows * RP;                        // floats per component in a slot
+  const int slot = 3 * cstr;                          // floats per slot
+  const int lim = slot;                  // every index below is within its plane's slot
+  const uint32_t cs = (uint32_t)csl;     // < 2^32 elements
+  const uint64_t sweep = L->sweep;
   const int label = G->label[L->replica];
   const float beta = G->betas_f[label];
   const float mJ = -G->Jf;
   const float omc = L->omc;
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
-  const int hv = min(t.ty, ly - t.y0);
-  const int dv = min(t.tz, lz - t.z0);
-  const int RW = hv + 2;                    // slot rows: y0-1 .. y0+hv
-  const int cstr = RW * pitch;              // floats per component in a slot
-  const int slot = 3 * cstr;                // floats per ring slot
-  float* S1 = S + (size_t)cs;
-  float* S2 = S + 2 * (size_t)cs;
-  constexpr int NS = kO3RingSlots;
-  __shared__ __align__(8) unsigned long long ring_bar[NS];
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < NS; ++i) ring_init(&ring_bar[i]);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the inits, visible to the copy engine
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    for (int p = 0; p < kO3RingSlots && p <= dv + 1; ++p) o3_issue_plane(t, L, R, osm, p, crows, lane);
+    if (lane == 0) R.issued = min(kO3RingSlots, dv + 2);
   }
-  __syncthreads();
-  // plane p of the march (z0 - 1 + p) into slot p % NS, by thread 0
-  auto copy_plane = [&](int p) {
-    if (threadIdx.x != 0) return;
-    const int sl = p % NS;
-    int zz = t.z0 - 1 + p;
-    zz = zz < 0 ? zz + lz : (zz >= lz ? zz - lz : zz);
-    ring_expect(&ring_bar[sl], (uint32_t)(3 * cstr) * 4u);
-    for (int c = 0; c < 3; ++c) {
-      int r = 0;
-      while (r < RW) {
-        int y = t.y0 - 1 + r;
-        y = y < 0 ? y + ly : (y >= ly ? y - ly : y);
-        const int n = min(RW - r, ly - y);  // rows contiguous up to the plane's last row
-        const long long so = (long long)c * cs + ((long long)zz * ly + y) * pitch;
-        const long long dof = (long long)sl * slot + (long long)c * cstr + (long long)r * pitch;
-        if (GPUMC_IN(so + (long long)n * pitch - 1, 3ll * cs) && GPUMC_IN(dof + (long long)n * pitch - 1, (long long)NS * slot))
-          ring_bulk_copy(osm + dof, S + so, (uint32_t)(n * pitch) * 4u, &ring_bar[sl]);
-        r += n;
-      }
-    }
-  };
-  O3Fix fx = {{0, 0, 0}, 0, 0};
-  O3Totals tot = {{0, 0, 0}, 0};
-  int nacc = 0;
   // Work items are pairs of horizontally adjacent sites of the colour in one
   // row (x and x + 2, x = 4m + parity): both sites' neighbours then sit at
   // fixed offsets from one row position (the x + 1 site is shared), and a
-  // thread's pair is found once per tile, not per plane.
-  const int half = lx >> 1;             // sites of the colour per row
-  const int np = (half + 1) >> 1;       // pairs per row (the last may be single)
-  const int n_pairs = hv * np;          // pairs of the tile's rows in one plane
+  // thread's pairs are found once per tile, not per plane.
+  const int half = lx >> 1;        // sites of the colour per row
+  const int np = (half + 1) >> 1;  // pairs per row (the last may be single)
+  const int n_pairs = hv * np;     // pairs of the tile's rows in one plane
+  const int rs = RP;               // floats per slot row
   const int r0 = threadIdx.x / np, m0 = threadIdx.x - r0 * np;
   const int dr = kThreads / np, dm = kThreads - dr * np;  // cursor step of kThreads pairs
-  int issued = 0;  // planes whose copies were issued: march planes 0 .. dv + 1 in all
-  for (; issued <= NS - 2 && issued <= dv + 1; ++issued) copy_plane(issued);
-  bool ok_ring = true;
-  for (int k = 0; k < dv && ok_ring; ++k) {
+  bool ok = true;
+  for (int k = 0; k < dv && ok; ++k) {
     const int z = t.z0 + k;
-    // plane z+2 (needed as z+1 of the next step) into the slot freed by the
-    // previous step
-    if (k + NS - 1 <= dv + 1) {
-      copy_plane(k + NS - 1);
-      issued = k + NS;
-    }
     // planes z-1, z, z+1 = march planes k, k+1, k+2
-    for (int i = 0; i < 3 && ok_ring; ++i)
-      ok_ring = ring_wait(&ring_bar[(k + i) % NS], (uint32_t)((k + i) / NS) & 1u);
-    ok_ring = __syncthreads_and(ok_ring) != 0;  // one decision for the whole CTA
-    if (!ok_ring) break;
-    const float* pm = osm + (k % NS) * slot;
-    const float* pc = osm + ((k + 1) % NS) * slot;
-    const float* pp = osm + ((k + 2) % NS) * slot;
+    for (int i = 0; i < 3 && ok; ++i)
+      ok = ring_wait(&R.full[(k + i) % kO3RingSlots], (uint32_t)((k + i) / kO3RingSlots) & 1u, &R.abort);
+    ok = __all_sync(0xFFFFFFFFu, ok);  // one decision per warp
+    if (!ok) break;
+    const float* pm = osm + (k % kO3RingSlots) * slot;
+    const float* pc = osm + ((k + 1) % kO3RingSlots) * slot;
+    const float* pp = osm + ((k + 2) % kO3RingSlots) * slot;
     int rl = r0, m = m0;
     for (int i = threadIdx.x; i < n_pairs; i += kThreads) {
       const int y = t.y0 + rl;
       const int xa = 4 * m + ((y + z + COLOUR) & 1), xb = xa + 2;
       const bool two = 2 * m + 1 < half;
-      const int oc = (rl + 1) * pitch;  // slot row of y
+      const int row = (rl + 1) * rs;  // slot row of y (component 0; component c at + c cstr)
+      const int ia = row + xa;
+      const int ib = two ? ia + 2 : ia;
       // x-1 of a and x+1 of b wrap at the row's ends; x+1 of a = x-1 of b
       // (x+1 of a wraps only for a single last site, x = lx - 1)
-      const int xam = xa ? xa - 1 : lx - 1;
-      const int xap = xa + 1 < lx ? xa + 1 : 0;
-      const int xbp = xb + 1 < lx ? xb + 1 : 0;
+      const int iam = xa ? ia - 1 : row + lx - 1;
+      const int iap = xa + 1 < lx ? ia + 1 : row;
+      const int ibp = two ? (xb + 1 < lx ? ia + 3 : row) : iap;
+      const int ibm = two ? iap : iam;
       O3Site qa, qb;
       float ha[3], hb[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float* P = pc + c * cstr;
-        const float* M = pm + c * cstr;
-        const float* Q = pp + c * cstr;
-        const float mid = ld_chk(P, oc + xap, cstr);
-        // neighbour order x-1, x+1, y-1, y+1, z-1, z+1 (as k_sweep_o3)
-        ha[c] = fadd(fadd(fadd(fadd(fadd(ld_chk(P, oc + xam, cstr), mid), ld_chk(P, oc - pitch + xa, cstr)),
-                                ld_chk(P, oc + pitch + xa, cstr)),
-                           ld_chk(M, oc + xa, cstr)),
-                      ld_chk(Q, oc + xa, cstr));
-        if (two)
-          hb[c] = fadd(fadd(fadd(fadd(fadd(mid, ld_chk(P, oc + xbp, cstr)), ld_chk(P, oc - pitch + xb, cstr)),
-                                  ld_chk(P, oc + pitch + xb, cstr)),
-                             ld_chk(M, oc + xb, cstr)),
-                        ld_chk(Q, oc + xb, cstr));
-        else
-          hb[c] = ha[c];
+        const int o = c * cstr;
+        // both sites' sums in one packed chain, neighbour order x-1, x+1,
+        // y-1, y+1, z-1, z+1 per lane (as k_sweep_o3); a single site's
+        // second lane repeats the first
+        const f2 h2 = add2(add2(add2(add2(add2(F2(o3_lds(pc, iam + o, lim), o3_lds(pc, ibm + o, lim)),
+                                               F2(o3_lds(pc, iap + o, lim), o3_lds(pc, ibp + o, lim))),
+                                          F2(o3_lds(pc, ia - rs + o, lim), o3_lds(pc, ib - rs + o, lim))),
+                                     F2(o3_lds(pc, ia + rs + o, lim), o3_lds(pc, ib + rs + o, lim))),
+                                F2(o3_lds(pm, ia + o, lim), o3_lds(pm, ib + o, lim))),
+                           F2(o3_lds(pp, ia + o, lim), o3_lds(pp, ib + o, lim)));
+        ha[c] = lo(h2);
+        hb[c] = hi(h2);
       }
-      qa.ax = ld_chk(pc, oc + xa, cstr);
-      qa.ay = ld_chk(pc + cstr, oc + xa, cstr);
-      qa.az = ld_chk(pc + 2 * cstr, oc + xa, cstr);
+      qa.ax = o3_lds(pc, ia, lim);
+      qa.ay = o3_lds(pc, ia + cstr, lim);
+      qa.az = o3_lds(pc, ia + 2 * cstr, lim);
+      qb.ax = o3_lds(pc, ib, lim);
+      qb.ay = o3_lds(pc, ib + cstr, lim);
+      qb.az = o3_lds(pc, ib + 2 * cstr, lim);
       qa.hx = ha[0];
       qa.hy = ha[1];
       qa.hz = ha[2];
-      // 32-bit index arithmetic: the same values as the 64-bit products
-      // truncated to the 32-bit fields
-      const uint32_t row = (uint32_t)z * (uint32_t)ly + (uint32_t)y;
-      qa.me = row * (uint32_t)pitch + (uint32_t)xa;
-      qa.site = row * (uint32_t)lx + (uint32_t)xa;
-      if (two) {
-        qb.ax = ld_chk(pc, oc + xb, cstr);
-        qb.ay = ld_chk(pc + cstr, oc + xb, cstr);
-        qb.az = ld_chk(pc + 2 * cstr, oc + xb, cstr);
-        qb.me = qa.me + 2;
-        qb.site = qa.site + 2;
-      } else {
-        qb.ax = qa.ax;
-        qb.ay = qa.ay;
-        qb.az = qa.az;
-        qb.me = qa.me;
-        qb.site = qa.site;
-      }
       qb.hx = hb[0];
       qb.hy = hb[1];
       qb.hz = hb[2];
-      o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, S1, S2, cs, fx, nacc);
+      // 32-bit index arithmetic: the same values as the 64-bit products
+      // truncated to the 32-bit fields
+      const uint32_t grow = (uint32_t)z * (uint32_t)ly + (uint32_t)y;
+      qa.me = grow * (uint32_t)pitch + (uint32_t)xa;
+      qa.site = grow * (uint32_t)lx + (uint32_t)xa;
+      qb.me = two ? qa.me + 2 : qa.me;
+      o3_update_pair<COLOUR, ALG>(qa, qb, two, P, omc, mJ, beta, S, cs, fx, nacc);
       rl += dr;
       m += dm;
       if (m >= np) {
@@ -772,22 +837,98 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 
         rl += 1;
       }
     }
-    o3_flush<COLOUR == 1>(tot, fx);  // per plane: at most one pair per thread per 256 pairs since the last flush
-    __syncthreads();  // the next copy overwrites the z-1 slot read above
+    // a thread adds at most 8 terms per plane (n_pairs <= 4 kThreads), so
+    // flushing at 256 keeps every 32-bit partial below 2^31
+    if (__any_sync(0xFFFFFFFFu, fx.n >= 256u)) o3_flush_warp<COLOUR == 1>(R, fx, nacc);
+    // release the planes this warp no longer needs: plane k after step k,
+    // and the last three after the last step
+    __syncwarp();
+    const int p_lo = k, p_hi = k + 1 < dv ? k : dv + 1;
+    for (int p = p_lo; p <= p_hi; ++p) {
+      const int sl = p % kO3RingSlots;
+      int last = 0;
+      if (lane == 0) {
+        __threadfence_block();
+        last = atomicAdd(&R.freed[sl], 1u) == (unsigned)(kWarps - 1);
+        if (last) {
+          atomicExch(&R.freed[sl], 0u);
+          __threadfence_block();
+        }
+      }
+      last = __shfl_sync(0xFFFFFFFFu, last, 0);
+      if (last && p + kO3RingSlots <= dv + 1) {
+        o3_issue_plane(t, L, R, osm, p + kO3RingSlots, crows, lane);
+        if (lane == 0) atomicMax(&R.issued, p + kO3RingSlots + 1);
+      }
+    }
   }
-  if (!ok_ring) {
-    // a copy did not land in time: flag the launch, wait (bounded) for every
-    // copy still in flight into this CTA's ring, and leave the tile
+  o3_flush_warp<COLOUR == 1>(R, fx, nacc);
+  if (!ok && lane == 0) {
     atomicExch(&ctl->err, 2);
-    for (int p = max(0, issued - NS); p < issued; ++p) ring_wait(&ring_bar[p % NS], (uint32_t)(p / NS) & 1u);
+    *(volatile int*)&R.abort = 1;
   }
-  o3_commit<COLOUR>(L, tot, nacc);
-  if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+  __syncthreads();
+  if (R.abort) {
+    // a copy did not land in time: wait (bounded) for the last copy issued
+    // into each slot, so none is in flight when the CTA leaves
+    if (threadIdx.x == 0)
+      for (int p = max(0, R.issued - kO3RingSlots); p < R.issued; ++p) {
+        for (long long it = 0; it < kRingWaitPolls; ++it)
+          if (ring_test(&R.full[p % kO3RingSlots], (uint32_t)(p / kO3RingSlots) & 1u)) break;
+      }
+    __syncthreads();
+  }
 }
 
+// Colour 1 also carries the sweep epilogue's shared memory, so three CTAs
+// fit an SM: its register budget is that of three CTAs (no spills of the fp64
+// neighbour sums).
+template <int COLOUR, int ALG, int CLS>
+__global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 : 4)
+    k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
+                     GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
+  extern __shared__ __align__(16) float osm[];
+  __shared__ O3Ring R;
+  const TileItem t = tiles[blockIdx.x];
+  LatDesc* L = &lats[t.lat];
+  const GroupDesc* G = &groups[L->group];
+  if (L->sweep >= L->target) {
+    if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kO3RingSlots; ++i) {
+      ring_init(&R.full[i]);
+      R.freed[i] = 0;
+    }
+    for (int i = 0; i < 5; ++i) R.tot[i] = 0;
+    R.abort = 0;
+    R.issued = 0;
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the inits, visible to the copy engine
+  }
+  __syncthreads();
+  o3_march_tile<COLOUR, ALG, o3_class_row(CLS), o3_class_rows(CLS)>(t, L, G, ctl, osm, R);
+  // the tile function ends with a CTA barrier after the last flush
+  if (threadIdx.x == 0) {
+    atomic_add_i64(&L->acc.mq[0], R.tot[0]);
+    atomic_add_i64(&L->acc.mq[1], R.tot[1]);
+    atomic_add_i64(&L->acc.mq[2], R.tot[2]);
+    if (COLOUR == 1) {
+      atomic_add_i64(&L->acc.ebq, R.tot[3]);
+      L->acc.fresh = 1;
+    }
+    if (R.tot[4]) atomic_add_i64(&L->acc.accepted, R.tot[4]);
+  }
+  if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+}
+#define O3_INSTANTIATE_MARCH(ALG, CLS)                                                                     \
+  template __global__ void k_sweep_o3_march<0, ALG, CLS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \
+  template __global__ void k_sweep_o3_march<1, ALG, CLS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 #define O3_INSTANTIATE(ALG)                                                                          \
-  template __global__ void k_sweep_o3_march<0, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \
-  template __global__ void k_sweep_o3_march<1, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \
+  O3_INSTANTIATE_MARCH(ALG, 0)                                                                       \
+  O3_INSTANTIATE_MARCH(ALG, 1)                                                                       \
+  O3_INSTANTIATE_MARCH(ALG, 2)                                                                       \
+  O3_INSTANTIATE_MARCH(ALG, 3)                                                                       \
   template __global__ void k_sweep_o3<2, 0, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);    \
   template __global__ void k_sweep_o3<2, 1, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);    \
   template __global__ void k_sweep_o3<3, 0, ALG>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);    \
