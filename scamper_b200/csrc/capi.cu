@@ -1182,6 +1182,7 @@ int gpumc_engine::rebuild_batch() {
   std::map<int, BatchPlan> plans;
   std::map<int, std::vector<TileItem>> tiles;
   std::map<int, std::vector<int32_t>> gids;
+  std::map<int, std::vector<int32_t>> gtiles;  // tiles of each group of a plan
   std::map<int, const Layout*> layout_of_lat;
   // tile shapes for this batch: the simulations of one kernel family (kind
   // of the creation-time plan) share its launch and are refined together
@@ -1202,11 +1203,15 @@ int gpumc_engine::rebuild_batch() {
     BatchPlan& p = plans[kind];
     p.kind = kind;
     p.smem = std::max(p.smem, s->blay.smem);
+    const size_t first = tiles[kind].size();
     for (int r = 0; r < s->n_rep; ++r) {
       enumerate_tiles(s->blay, s->lat0 + r, tiles[kind]);
       layout_of_lat[s->lat0 + r] = &s->blay;
     }
+    const int32_t pos = (int32_t)gids[kind].size();  // the group's position in the plan
+    for (size_t i = first; i < tiles[kind].size(); ++i) tiles[kind][i].pad = pos;
     gids[kind].push_back(s->group);
+    gtiles[kind].push_back((int32_t)(tiles[kind].size() - first));
   }
   for (auto& kv : plans) {
     BatchPlan p = kv.second;
@@ -1214,15 +1219,21 @@ int gpumc_engine::rebuild_batch() {
     auto& gv = gids[kv.first];
     p.n_tiles = (int)tv.size();
     p.n_groups = (int)gv.size();
+    // group ids, tiles per group, done counters (zero) in one buffer
+    std::vector<int32_t> gbuf(gv);
+    gbuf.insert(gbuf.end(), gtiles[kv.first].begin(), gtiles[kv.first].end());
+    gbuf.resize(3 * gv.size(), 0);
     CUDA_TRY(cudaMallocAsync(&p.d_tiles, sizeof(TileItem) * tv.size(), stream));
-    CUDA_TRY(cudaMallocAsync(&p.d_gids, sizeof(int32_t) * gv.size(), stream));
+    CUDA_TRY(cudaMallocAsync(&p.d_gids, sizeof(int32_t) * gbuf.size(), stream));
     CUDA_TRY(cudaMallocAsync(&p.d_ctl, sizeof(LaunchCtl), stream));
     CUDA_TRY(cudaMemcpyAsync(p.d_tiles, tv.data(), sizeof(TileItem) * tv.size(), cudaMemcpyHostToDevice, stream));
-    CUDA_TRY(cudaMemcpyAsync(p.d_gids, gv.data(), sizeof(int32_t) * gv.size(), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(p.d_gids, gbuf.data(), sizeof(int32_t) * gbuf.size(), cudaMemcpyHostToDevice, stream));
     LaunchCtl c;
     c.done = 0;
     c.n_groups = p.n_groups;
     c.group_ids = p.d_gids;
+    c.group_tiles = p.d_gids + gv.size();
+    c.group_done = (unsigned int*)(p.d_gids + 2 * gv.size());
     c.n_tiles = p.n_tiles;
     CUDA_TRY(cudaMemcpyAsync(p.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
     if (is_ising_bits_kind(p.kind)) {

@@ -151,7 +151,7 @@ struct GroupDesc {
 // leaves CTA slots idle splits its lattices into smaller tiles.
 struct TileItem {
   int32_t lat, x0, y0, z0;
-  int32_t cx, ty, tz, pad;
+  int32_t cx, ty, tz, pad;  // pad: position of the tile's group in the launch (LaunchCtl::group_ids)
 };
 
 // Device-side bookkeeping of one launch (last-CTA epilogue; grid barrier of
@@ -160,6 +160,11 @@ struct LaunchCtl {
   unsigned int done;
   int32_t n_groups;
   const int32_t* group_ids;  // [n_groups] indices into the group pool
+  // per-group epilogues (group_epilogue): the tiles of each group of the
+  // launch (TileItem::pad of a tile = its group's position) and how many of
+  // them are done; null: one epilogue for the whole launch
+  const int32_t* group_tiles = nullptr;  // [n_groups]
+  unsigned int* group_done = nullptr;    // [n_groups]
   unsigned int bar = 0;      // resident kernel: grid-barrier arrivals of this launch
   int32_t err = 0;           // resident kernel: 1 = a barrier wait gave up
   unsigned int epi = 0;      // resident kernel: launch-local sweeps whose epilogue is done

@@ -81,6 +81,7 @@ int gpumc_sim::upload_own_tiles(std::vector<TileItem>& tiles) {
   if (d_ctl) {
     const int32_t n = n_tiles;
     CUDA_TRY(cudaMemcpyAsync(&d_ctl->n_tiles, &n, sizeof(n), cudaMemcpyHostToDevice, eng->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_gid + 1, &n, sizeof(n), cudaMemcpyHostToDevice, eng->stream));  // the group's tiles
     CUDA_TRY(cudaStreamSynchronize(eng->stream));  // `n` lives on this stack frame
   }
   return GPUMC_OK;
@@ -435,13 +436,18 @@ int gpumc_create(gpumc_engine* eng, const gpumc_spec* spec, uint64_t base_seed, 
   std::vector<TileItem> tiles;
   rc = s->upload_own_tiles(tiles);
   if (rc) return cleanup(rc);
-  CUDA_CLEAN(cudaMallocAsync(&s->d_gid, sizeof(int32_t), eng->stream));
-  CUDA_CLEAN(cudaMemcpyAsync(s->d_gid, &s->group, sizeof(int32_t), cudaMemcpyHostToDevice, eng->stream));
+  // the group id, its tile count and its done counter (tiles are the group's
+  // only: TileItem::pad = 0)
+  const int32_t gbuf[3] = {s->group, s->n_tiles, 0};
+  CUDA_CLEAN(cudaMallocAsync(&s->d_gid, sizeof(gbuf), eng->stream));
+  CUDA_CLEAN(cudaMemcpyAsync(s->d_gid, gbuf, sizeof(gbuf), cudaMemcpyHostToDevice, eng->stream));
   CUDA_CLEAN(cudaMallocAsync(&s->d_ctl, sizeof(LaunchCtl), eng->stream));
   LaunchCtl c;
   c.done = 0;
   c.n_groups = 1;
   c.group_ids = s->d_gid;
+  c.group_tiles = s->d_gid + 1;
+  c.group_done = (unsigned int*)(s->d_gid + 2);
   c.n_tiles = s->n_tiles;
   CUDA_CLEAN(cudaMemcpyAsync(s->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, eng->stream));
   if (is_ising_bits_kind(kernel_kind(s->lay))) {

@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(kThreads)
   const GroupDesc* G = &groups[L->group];
   const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {  // finished lattice: nothing to do this launch
-    launch_epilogue(lats, groups, ctl);
+    group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   const uint64_t key = L->key;
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   white_pass<MODEL, 2, ALG>(B, B, B, g, 0, tab, q, key, sweep, P, nxt, nacc, acc2, mag, cnt);
   flush_accumulators<MODEL, 2>(L, nacc, acc2, mag, cnt, q);
-  launch_epilogue(lats, groups, ctl);
+  group_epilogue(t.pad, lats, groups, ctl);
 }
 
 // 3D: the tile is tile_cx chunks x tile_y rows in the xy plane, marched over
@@ -687,7 +687,7 @@ __global__ void __launch_bounds__(kThreads)
   const GroupDesc* G = &groups[L->group];
   const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {
-    launch_epilogue(lats, groups, ctl);
+    group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   const uint64_t key = L->key;
@@ -735,7 +735,7 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();  // the next stage overwrites A and B slots read in this step
   }
   flush_accumulators<MODEL, 3>(L, nacc, acc2, mag, cnt, q);
-  launch_epilogue(lats, groups, ctl);
+  group_epilogue(t.pad, lats, groups, ctl);
 }
 
 template __global__ void k_sweep_discrete_2d<POTTS, 0>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);

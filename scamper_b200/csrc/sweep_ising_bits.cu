@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
   const GroupDesc* G = &groups[L->group];
   const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {
-    launch_epilogue(lats, groups, ctl);
+    group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
     }
   }
   flush_bits(&L->acc, acc, 2 * DIM);
-  launch_epilogue(lats, groups, ctl);
+  group_epilogue(t.pad, lats, groups, ctl);
 }
 
 // ---------------------------------------------------------------------------

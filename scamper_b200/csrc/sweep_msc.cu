@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
   const GroupDesc* G = &groups[L->group];
   const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {
-    launch_epilogue(lats, groups, ctl);
+    group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   const int lx = L->lx, ly = L->ly, lz = DIM == 3 ? L->lz : 1, pitch = L->pitch;
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
   long long v[1] = {dE};
   cta_sum(v);
   if (threadIdx.x == 0 && v[0]) atomic_add_i64(&L->acc.dE, v[0]);
-  launch_epilogue(lats, groups, ctl);
+  group_epilogue(t.pad, lats, groups, ctl);
 }
 
 // Per-replica magnetisation and energy of a multi-spin lattice: positional

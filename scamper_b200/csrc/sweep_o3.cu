@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   const GroupDesc* G = &groups[L->group];
   const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {
-    if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+    if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   const int lx = L->lx, ly = L->ly, lz = DIM == 3 ? L->lz : 1, pitch = L->pitch;
@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   }
   o3_flush<COLOUR == 1>(tot, fx);
   o3_commit<COLOUR>(L, tot, nacc);
-  if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+  if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
 }
 
 // ---------------------------------------------------------------------------
@@ -893,7 +893,7 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 
   LatDesc* L = &lats[t.lat];
   const GroupDesc* G = &groups[L->group];
   if (L->sweep >= L->target) {
-    if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+    if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   if (threadIdx.x == 0) {
@@ -919,7 +919,7 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 
     }
     if (R.tot[4]) atomic_add_i64(&L->acc.accepted, R.tot[4]);
   }
-  if (COLOUR == 1) launch_epilogue(lats, groups, ctl);
+  if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
 }
 #define O3_INSTANTIATE_MARCH(ALG, CLS)                                                                     \
   template __global__ void k_sweep_o3_march<0, ALG, CLS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2)
   const GroupDesc* G = &groups[L->group];
   const uint64_t sweep = L->sweep;
   if (sweep >= L->target) {
-    launch_epilogue(lats, groups, ctl);
+    group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
   const int8_t* cur = (const int8_t*)L->buf[sweep & 1];
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 2)
     }
   }
   flush_potts(&L->acc, acc, 2 * DIM);
-  launch_epilogue(lats, groups, ctl);
+  group_epilogue(t.pad, lats, groups, ctl);
 }
 
 template __global__ void k_sweep_potts_bits<2>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
