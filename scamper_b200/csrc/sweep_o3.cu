@@ -754,11 +754,7 @@ __device__ __forceinline__ void o3_march_tile(const TileItem& t, LatDesc* L, con
   const float mJ = -G->Jf;
   const float omc = L->omc;
   const O3Philox P = make_o3_philox(L->key, sweep, (uint32_t)COLOUR | ((ALG == 1 ? TAG_O3HB : TAG_O3) << 1));
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp == 0) {
-    for (int p = 0; p < kO3RingSlots && p <= dv + 1; ++p) o3_issue_plane(t, L, R, osm, p, crows, lane);
-    if (lane == 0) R.issued = min(kO3RingSlots, dv + 2);
-  }
+  const int lane = threadIdx.x & 31;
   // Work items are pairs of horizontally adjacent sites of the colour in one
   // row (x and x + 2, x = 4m + parity): both sites' neighbours then sit at
   // fixed offsets from one row position (the x + 1 site is shared), and a
@@ -896,15 +892,25 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 
     if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
     return;
   }
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < kO3RingSlots; ++i) {
-      ring_init(&R.full[i]);
-      R.freed[i] = 0;
+  // warp 0 initialises the ring and issues the first planes' copies right
+  // away, before the rest of the tile's set-up (its loads of the group's
+  // labels and temperatures): a CTA's first planes are its longest wait
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    if (lane == 0) {
+      for (int i = 0; i < kO3RingSlots; ++i) {
+        ring_init(&R.full[i]);
+        R.freed[i] = 0;
+      }
+      for (int i = 0; i < 5; ++i) R.tot[i] = 0;
+      R.abort = 0;
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the inits, visible to the copy engine
     }
-    for (int i = 0; i < 5; ++i) R.tot[i] = 0;
-    R.abort = 0;
-    R.issued = 0;
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the inits, visible to the copy engine
+    __syncwarp();
+    const int dv = min(t.tz, L->lz - t.z0);
+    const int crows = o3_class_rows(CLS) > 0 ? o3_class_rows(CLS) : min(t.ty, L->ly - t.y0) + 2;
+    for (int p = 0; p < kO3RingSlots && p <= dv + 1; ++p) o3_issue_plane(t, L, R, osm, p, crows, lane);
+    if (lane == 0) R.issued = min(kO3RingSlots, dv + 2);
   }
   __syncthreads();
   o3_march_tile<COLOUR, ALG, o3_class_row(CLS), o3_class_rows(CLS)>(t, L, G, ctl, osm, R);
