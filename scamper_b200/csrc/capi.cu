@@ -477,6 +477,7 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
       L.tile_z = (lz + ntz - 1) / ntz;
       const int cls = o3_row_class(L.pitch);
       L.smem = 12 * (size_t)kO3RingSlots * L.pitch * (cls ? o3_class_rows(cls) : L.tile_y + 2);
+      L.smem = std::max(L.smem, sizeof(int) * (size_t)kEpiScratchInts);  // colour 1's epilogue scratch
     } else {
       L.tile_y = std::max(1, std::min(ly, 4096 / lx));
       L.tile_z = L.dims == 3 ? std::max(1, std::min(lz, 4096 / (lx * L.tile_y))) : 1;

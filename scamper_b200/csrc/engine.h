@@ -38,6 +38,7 @@ enum Algorithm : int32_t { METROPOLIS = 0, HEAT_BATH = 1, SWENDSEN_WANG = 2, WOL
 constexpr int kMaxClasses = 13;    // 2z+1 for z = 6 (Potts on the cubic lattice)
 constexpr int kMaxPottsCounts = 8; // fused order-parameter histogram (q <= 8)
 constexpr int kThreads = 256;      // CTA size of the sweep kernels
+constexpr int kEpiScratchInts = 3 * kThreads + 1;  // scratch of an epilogue in a kernel's dynamic shared memory
 // O(3) z-march ring slots per tile: the copy of a plane is issued
 // kO3RingSlots - 3 planes ahead of its first use
 #ifndef GPUMC_O3_RING_SLOTS

@@ -158,11 +158,28 @@ static __device__ void finish_replica(LatDesc* lats, GroupDesc* G, int r, int32_
 //      independent, so they run in parallel with the same outcome as a
 //      sequential loop over t = offset, offset + 2, ...
 // Multi-spin records (64 per word lattice) are written by k_msc_record.
-static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int32_t* ids, int ng,
-                                     int slot) {
-  __shared__ int s_off[kThreads + 1];
-  __shared__ int32_t s_f[kThreads];
-  __shared__ int s_due[kThreads];
+// EXT: the three per-group arrays live in `ext` (kEpiScratchInts ints of the
+// caller's shared memory, e.g. a kernel's dynamic shared memory that is free
+// by the time of the epilogue) instead of static shared memory of their own,
+// so the kernel needs no more shared memory than its own.
+template <bool EXT>
+static __device__ void finish_groups_in(LatDesc* lats, GroupDesc* groups, const int32_t* ids, int ng, int slot,
+                                        int* ext) {
+  int* s_off;
+  int32_t* s_f;
+  int* s_due;
+  if (EXT) {
+    s_off = ext;
+    s_f = ext + kThreads + 1;
+    s_due = ext + 2 * kThreads + 1;
+  } else {
+    __shared__ int own_off[kThreads + 1];
+    __shared__ int32_t own_f[kThreads];
+    __shared__ int own_due[kThreads];
+    s_off = own_off;
+    s_f = own_f;
+    s_due = own_due;
+  }
   __shared__ int s_ndue;
   __shared__ unsigned long long s_acc;
   const int t = threadIdx.x;
@@ -283,10 +300,18 @@ static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int
 // end of the launch (measured: ~11 us per launch of one last-CTA epilogue
 // over 32 to 256 groups, on the critical path of every sweep).  A launch
 // without per-group counts falls back to launch_epilogue.
-__device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl);
-__device__ __forceinline__ void group_epilogue(int pos, LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl) {
+static __device__ void finish_groups(LatDesc* lats, GroupDesc* groups, const int32_t* ids, int ng, int slot) {
+  finish_groups_in<false>(lats, groups, ids, ng, slot, nullptr);
+}
+
+template <bool EXT = false>
+__device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl,
+                                                int* ext = nullptr);
+template <bool EXT = false>
+__device__ __forceinline__ void group_epilogue(int pos, LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl,
+                                               int* ext = nullptr) {
   if (ctl->group_tiles == nullptr) {
-    launch_epilogue(lats, groups, ctl);
+    launch_epilogue<EXT>(lats, groups, ctl, ext);
     return;
   }
   __shared__ bool is_last_of_group;
@@ -299,12 +324,13 @@ __device__ __forceinline__ void group_epilogue(int pos, LatDesc* lats, GroupDesc
   __syncthreads();
   if (!is_last_of_group) return;
   __threadfence();
-  finish_groups(lats, groups, ctl->group_ids + pos, 1, 0);
+  finish_groups_in<EXT>(lats, groups, ctl->group_ids + pos, 1, 0, ext);
   __syncthreads();
   if (threadIdx.x == 0) ctl->group_done[pos] = 0;
 }
 
-__device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl) {
+template <bool EXT>
+__device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups, LaunchCtl* ctl, int* ext) {
   __shared__ bool is_last;
   __threadfence();
   __syncthreads();
@@ -315,7 +341,7 @@ __device__ __forceinline__ void launch_epilogue(LatDesc* lats, GroupDesc* groups
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  finish_groups(lats, groups, ctl->group_ids, ctl->n_groups, 0);
+  finish_groups_in<EXT>(lats, groups, ctl->group_ids, ctl->n_groups, 0, ext);
   __syncthreads();
   if (threadIdx.x == 0) ctl->done = 0;
 }

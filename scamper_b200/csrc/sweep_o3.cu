@@ -876,11 +876,10 @@ __device__ __forceinline__ void o3_march_tile(const TileItem& t, LatDesc* L, con
   }
 }
 
-// Colour 1 also carries the sweep epilogue's shared memory, so three CTAs
-// fit an SM: its register budget is that of three CTAs (no spills of the fp64
-// neighbour sums).
+// Four CTAs per SM for both colours (64 registers, 55 KB of ring each):
+// colour 1's sweep epilogue takes its scratch arrays from the ring.
 template <int COLOUR, int ALG, int CLS>
-__global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 : 4)
+__global__ void __launch_bounds__(kThreads, kO3RingSlots > 4 ? 3 : 4)
     k_sweep_o3_march(const TileItem* __restrict__ tiles, LatDesc* __restrict__ lats,
                      GroupDesc* __restrict__ groups, LaunchCtl* __restrict__ ctl) {
   extern __shared__ __align__(16) float osm[];
@@ -889,7 +888,7 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 
   LatDesc* L = &lats[t.lat];
   const GroupDesc* G = &groups[L->group];
   if (L->sweep >= L->target) {
-    if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
+    if (COLOUR == 1) group_epilogue<true>(t.pad, lats, groups, ctl, (int*)osm);
     return;
   }
   // warp 0 initialises the ring and issues the first planes' copies right
@@ -925,7 +924,8 @@ __global__ void __launch_bounds__(kThreads, COLOUR == 1 || kO3RingSlots > 4 ? 3 
     }
     if (R.tot[4]) atomic_add_i64(&L->acc.accepted, R.tot[4]);
   }
-  if (COLOUR == 1) group_epilogue(t.pad, lats, groups, ctl);
+  // the epilogue's scratch is the ring, whose copies have all landed
+  if (COLOUR == 1) group_epilogue<true>(t.pad, lats, groups, ctl, (int*)osm);
 }
 #define O3_INSTANTIATE_MARCH(ALG, CLS)                                                                     \
   template __global__ void k_sweep_o3_march<0, ALG, CLS>(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*); \
