@@ -768,8 +768,10 @@ __device__ __forceinline__ void o3_march_tile(const TileItem& t, LatDesc* L, con
   bool ok = true;
   for (int k = 0; k < dv && ok; ++k) {
     const int z = t.z0 + k;
-    // planes z-1, z, z+1 = march planes k, k+1, k+2
-    for (int i = 0; i < 3 && ok; ++i)
+    // planes z-1, z, z+1 = march planes k, k+1, k+2; after the first step
+    // only plane k+2 is new to this warp (a wait on a completed phase still
+    // costs some hundred cycles, so the others are not waited for again)
+    for (int i = k == 0 ? 0 : 2; i < 3 && ok; ++i)
       ok = ring_wait(&R.full[(k + i) % kO3RingSlots], (uint32_t)((k + i) / kO3RingSlots) & 1u, &R.abort);
     ok = __all_sync(0xFFFFFFFFu, ok);  // one decision per warp
     if (!ok) break;
