@@ -456,20 +456,33 @@ Layout plan_layout(const gpumc_spec* s, int slots, int slots3) {
     // in place, one thread per site of the colour, tiles of whole rows with
     // about 2048 sites of each colour
     L.pitch = (lx + 3) / 4 * 4;
+    // 3D rows within 15 % of a compiled z-march row class (32, 64, 128
+    // floats) are padded to it, for its compile-time neighbour offsets
+    // (measured on 12.6 M sites: L = 64 at 67.7 attempts/ns, L = 56 / 60 / 72
+    // at 53.9 / 54.5 / 57.5 with the offsets at run time)
+    if (L.dims == 3)
+      for (int c : {32, 64, 128})
+        if (L.pitch <= c && 100 * c <= 115 * L.pitch) {
+          L.pitch = c;
+          break;
+        }
     L.buf_bytes = 3 * sizeof(float) * (size_t)L.pitch * rows;
     L.inplace = true;
     L.tile_cx = (lx + 3) / 4;
     // 3D: tiles of whole rows marched along z through a ring of four shared
     // planes (3 components x (rows + 2 halo rows) x pitch floats) of at
-    // most 56 KB (three CTAs per SM), up to 16 rows x 8 planes per tile (for
-    // 32 lattices of 64^3: 1024 tiles, 2.3 waves of 148 x 3 CTAs).  Deeper
+    // most 56 KB (four CTAs per SM), rows x 8 planes per tile (for 32
+    // lattices of 64^3: 16 rows, 1024 tiles, 1.7 waves of 148 x 4 CTAs).  Deeper
     // tiles re-read fewer halo planes but leave the last wave ragged: on
     // that mix 22 planes ran at 41.2 attempts/ns, 11 at 42.7, 8 at 47.5,
     // 6 at 44.1 and 4 at 45.2.
     const int ty_max = (int)(kO3MarchSmem / (12 * (size_t)kO3RingSlots * L.pitch)) - 2;
     if (L.dims == 3 && ty_max >= 1) {
       L.march = true;
-      const int rows = std::min(kn.o3_rows > 0 ? kn.o3_rows : 16, ty_max);
+      // rows per tile: about one site pair per thread per plane (16 rows
+      // at L = 64; fewer pairs per row, more rows)
+      const int np = std::max(1, ((lx >> 1) + 1) >> 1);
+      const int rows = std::min(kn.o3_rows > 0 ? kn.o3_rows : std::max(1, kThreads / np), ty_max);
       const int nty = (ly + rows - 1) / rows;
       L.tile_y = (ly + nty - 1) / nty;
       const int planes = kn.o3_planes > 0 ? kn.o3_planes : 8;
