@@ -1,13 +1,15 @@
 // Checkerboard sweep for O(3) Heisenberg spins (float32 unit vectors, three
 // component planes) on periodic square and cubic lattices.
 //
-// The O(3) update costs ~200 arithmetic instructions per attempt against 24 B
-// of compulsory traffic, so it is bound by instruction throughput, not HBM.
-// It therefore runs in place as two launches per sweep (colour 0, then colour
-// 1), one thread per site: a colour pass reads only the other colour, whose
-// values stay fixed during the pass, so no tiles, halos or barriers are needed
-// and neighbour reads are served by L1/L2.  The colour-1 launch ends with the
-// sweep epilogue.
+// The O(3) update costs some 270 instructions per site against 24 B of
+// compulsory traffic, so it is bound by instruction issue and dependency
+// latency, not HBM.  It runs in place as two launches per sweep (colour 0,
+// then colour 1): a colour pass reads only the other colour, whose values
+// stay fixed during the pass, so tiles need no coordination.  3D lattices are
+// marched along z through shared-memory planes (k_sweep_o3_march); 2D
+// lattices and 3D lattices too small for the march use k_sweep_o3, whose
+// neighbour reads are served by L1/L2.  Both take the sites of a colour in
+// pairs.  The colour-1 launch ends with the sweep epilogue.
 //
 // Observables: on the bipartite periodic lattice every bond has exactly one
 // colour-1 end, so the colour-1 pass sums s . h over its sites with their
