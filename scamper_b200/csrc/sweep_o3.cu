@@ -90,7 +90,7 @@ __device__ __forceinline__ void o3_place(float ax, float ay, float az, float ct,
                                          float sp, float& px, float& py, float& pz) {
   const float vx = fmul(st, cp), vy = fmul(st, sp);
   const float sg = az >= 0.0f ? 1.0f : -1.0f;
-  const float k = fdiv(-1.0f, fadd(sg, az));
+  const float k = -__frcp_rn(fadd(sg, az));  // = fdiv(-1, sg + az) bit for bit (|sg + az| >= 1)
   const float b = fmul(fmul(ax, ay), k);
   const float e1x = fadd(1.0f, fmul(fmul(sg, fmul(ax, ax)), k));
   const float e1y = fmul(sg, b);
@@ -255,7 +255,9 @@ __device__ __forceinline__ void o3_metropolis_2(f2 ax, f2 ay, f2 az, f2 hx, f2 h
     // Duff et al. (JCGT 2017) basis {e1, e2, a}: sg = sign(az), k = -1/(sg + az)
     const f2 sg = F2(lo(az) >= 0.0f ? 1.0f : -1.0f, hi(az) >= 0.0f ? 1.0f : -1.0f);
     const f2 d = add2(sg, az);
-    const f2 k = F2(__fdiv_rn(-1.0f, lo(d)), __fdiv_rn(-1.0f, hi(d)));
+    // -1 / d as the negated correctly rounded reciprocal: round-to-nearest
+    // is symmetric in sign, so this is the IEEE quotient bit for bit (|d| >= 1)
+    const f2 k = F2(-__frcp_rn(lo(d)), -__frcp_rn(hi(d)));
     const f2 axk = mul2(ax, k);
     const f2 b = mul2(ay, axk);
     const f2 sax = mul2(sg, ax);
