@@ -339,8 +339,7 @@ __device__ __forceinline__ void o3_fix_add_2(O3Fix& q, f2 sx, f2 sy, f2 sz, f2 h
 // sweep-uniform part of round 1 and the ten round keys precomputed once per
 // tile (the key is the lattice's, the same for the whole CTA, so the compiler
 // holds the schedule in uniform registers: measured 15 fewer instructions per
-// site than bumping the keys every round, at the same 64 registers), and each
-// round multiply one 32x32->64 wide product.
+// site than bumping the keys every round, at the same 64 registers).
 struct O3Philox {
   uint32_t a, b, c;
   uint32_t k0[10], k1[10];
@@ -364,10 +363,11 @@ __device__ __forceinline__ uint4 o3_philox(const O3Philox& P, uint32_t index) {
   uint4 c = make_uint4(P.a, P.b, (uint32_t)(p00 >> 32) ^ P.c, (uint32_t)p00);
 #pragma unroll
   for (int r = 1; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
-    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
-    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ P.k0[r], (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ P.k1[r],
-                   (uint32_t)p0);
+    // separate high and low products: 10 fewer instructions per site here
+    // than one 32x32->64 wide product (which the bit-sliced kernels keep)
+    const uint32_t h0 = __umulhi(0xD2511F53u, c.x), l0 = 0xD2511F53u * c.x;
+    const uint32_t h1 = __umulhi(0xCD9E8D57u, c.z), l1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(h1 ^ c.y ^ P.k0[r], l1, h0 ^ c.w ^ P.k1[r], l0);
   }
   return c;
 }
