@@ -81,8 +81,8 @@ __device__ __forceinline__ uint4 draw(uint64_t key, uint64_t index, uint32_t col
 // of round 1 precomputed and the round keys bumped on the fly: five
 // registers, for kernels where resident warps matter more than two adds per
 // round.  ctrl0 (given once) and ctrl (per call) are XORed into word 1, so a
-// call equals draw() with word 1 = ctrl0 ^ ctrl.  Each round multiply is one
-// 32x32->64 wide product.
+// call equals draw() with word 1 = ctrl0 ^ ctrl.  Each round multiply is a
+// separate high and low product.
 struct RunPhilox {
   uint32_t a, b, c, k0, k1;
 };
@@ -104,10 +104,11 @@ __device__ __forceinline__ uint4 run_philox(const RunPhilox& P, uint32_t index, 
   for (int r = 1; r < 10; ++r) {
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
-    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
-    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
-    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1,
-                   (uint32_t)p0);
+    // separate high and low products (the multi-spin kernel measured 10 %
+    // faster than with one 32x32->64 wide product per multiply)
+    const uint32_t h0 = __umulhi(0xD2511F53u, c.x), l0 = 0xD2511F53u * c.x;
+    const uint32_t h1 = __umulhi(0xCD9E8D57u, c.z), l1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(h1 ^ c.y ^ k0, l1, h0 ^ c.w ^ k1, l0);
   }
   return c;
 }
