@@ -440,8 +440,10 @@ __global__ void __launch_bounds__(kThreads, DIM == 2 ? 4 : 3)
 //   * after its white pass a tile publishes its first two and last two owned
 //     rows (packed) to its exchange slot for that sweep's parity;
 //   * a grid barrier ends the sweep; block 0 then runs the sweep epilogue of
-//     every group (records, energy caches, sweep counters, PT exchange), and a
-//     second grid barrier publishes it;
+//     every group (records, energy caches, sweep counters, PT exchange) and
+//     publishes its completion in ctl->epi, which the other CTAs wait for
+//     only before a sweep that follows a PT exchange (the labels, and so the
+//     acceptance tables, change there);
 //   * the next sweep refreshes the tile's four halo rows from the two
 //     neighbours' slots (tile above: its last two rows; tile below: its first
 //     two) and recomputes the black halo rows as usual.
