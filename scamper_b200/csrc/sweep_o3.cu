@@ -1,7 +1,7 @@
 // Checkerboard sweep for O(3) Heisenberg spins (float32 unit vectors, three
 // component planes) on periodic square and cubic lattices.
 //
-// The O(3) update costs some 270 instructions per site against 24 B of
+// The O(3) update costs some 250-270 instructions per site against 24 B of
 // compulsory traffic, so it is bound by instruction issue and dependency
 // latency, not HBM.  It runs in place as two launches per sweep (colour 0,
 // then colour 1): a colour pass reads only the other colour, whose values
@@ -418,9 +418,6 @@ __device__ __forceinline__ void o3_load_site(O3Site& q, const float* S, const fl
   q.site = (uint32_t)((size_t)(z * ly + y) * lx + x);
 }
 
-// Updates the pair (qa, qb) of a colour pass (qb only when `two`): writes
-// accepted spins in place, counts acceptances and adds the fixed-point
-// observables of the final spins.
 // Stores spin (x, y, z) at element `me` of the three component planes of S
 // (plane stride cs).
 __device__ __forceinline__ void o3_store3(float* S, uint32_t cs, uint32_t me, float x, float y, float z) {
@@ -432,6 +429,9 @@ __device__ __forceinline__ void o3_store3(float* S, uint32_t cs, uint32_t me, fl
   }
 }
 
+// Updates the pair (qa, qb) of a colour pass (qb only when `two`): writes
+// the final spins in place, counts acceptances and adds the fixed-point
+// observables of the final spins.
 template <int COLOUR, int ALG>
 __device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& qb, bool two, const O3Philox& P,
                                                float omc, float mJ, float beta, float* S, uint32_t cs, O3Fix& fx,
@@ -461,8 +461,13 @@ __device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& q
     fz2 = F2(ok_a ? lo(nz) : qa.az, ok_b ? hi(nz) : qb.az);
   }
   ok_b = ok_b && two;
-  if (ok_a) o3_store3(S, cs, qa.me, lo(fx2), lo(fy2), lo(fz2));
-  if (ok_b) o3_store3(S, cs, qb.me, hi(fx2), hi(fy2), hi(fz2));
+  // every site of the pair is stored, rejected ones with their old spin: a
+  // colour pass reads only the other colour, so the rewrite is invisible,
+  // and the stores no longer branch on the decisions (measured 1-2 % faster;
+  // the DRAM writes barely change, as a sector of four colour sites almost
+  // always holds an accepted one)
+  o3_store3(S, cs, qa.me, lo(fx2), lo(fy2), lo(fz2));
+  if (two) o3_store3(S, cs, qb.me, hi(fx2), hi(fy2), hi(fz2));
   nacc += (int)ok_a + (int)ok_b;
   // every bond has one colour-1 end: the colour-1 pass also sums s . h
   o3_fix_add_2<COLOUR == 1>(fx, fx2, fy2, fz2, hx, hy, hz, two);
