@@ -20,6 +20,10 @@ from . import _lib
 
 KNOBS = ("ising2d_rows", "ising3d_planes", "potts_segments", "potts3d_planes", "o3_rows", "o3_planes")
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_tiles.json")
+# A candidate plan must beat the best so far by this fraction to replace it.
+# Two tuning runs of the uneven mix on B200 boxes ordered the Potts segment
+# candidates differently by up to 2.4 %, so smaller gains are not resolved.
+MIN_GAIN = 0.02
 
 
 def get_knobs():
@@ -101,9 +105,12 @@ def time_workload(build, knobs, sweeps, warm, torch, repeats=3):
         set_knobs(prev)
 
 
-def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None, repeats=3):
+def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None, repeats=3, min_gain=MIN_GAIN):
     """Coordinate descent over `space` ({knob: [candidates]}, 0 = analytic)
-    for the workload that build(engine) creates.  Returns {"knobs",
+    for the workload that build(engine) creates.  A candidate replaces the
+    best plan so far only when it is faster by more than `min_gain` (a
+    fraction): differences inside the run-to-run spread of the timings keep
+    the analytic plan.  Returns {"knobs",
     "ms_per_sweep", "analytic_ms_per_sweep", "table"} with every timed
     candidate in the table."""
     if torch is None:
@@ -123,6 +130,6 @@ def tune(build, space, sweeps=20, warm=3, rounds=1, torch=None, repeats=3):
                 trial = dict(best, **{name: int(v)})
                 t = time_workload(build, trial, sweeps, warm, torch, repeats)
                 table.append({"knobs": trial, "ms_per_sweep": t})
-                if t < best_t:
+                if t < best_t * (1.0 - min_gain):
                     best, best_t = trial, t
     return {"knobs": best, "ms_per_sweep": best_t, "analytic_ms_per_sweep": analytic, "table": table}

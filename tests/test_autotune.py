@@ -49,6 +49,34 @@ def test_tile_cache_round_trip(tmp_path):
         assert json.load(f)["NVIDIA B200|mix"]["analytic_ms_per_sweep"] == 2.0
 
 
+def test_tuner_keeps_the_analytic_plan_within_the_noise_margin(monkeypatch):
+    from scamper_b200 import autotune
+    assert autotune.MIN_GAIN == 0.02
+    # fake timings (ms per sweep) by knob setting, relative to the analytic 1.0
+    times = {(): 1.0,
+             (("potts_segments", 768),): 0.995,                       # 0.5 % faster: inside the margin
+             (("o3_planes", 16),): 0.996,
+             (("potts_segments", 3072),): 0.95,                       # 5 % faster: taken
+             (("o3_planes", 16), ("potts_segments", 3072)): 0.945,    # a further 0.5 %: not taken
+             (("o3_planes", 4), ("potts_segments", 3072)): 0.92,      # a further 3 %: taken
+             (("o3_planes", 16), ("potts_segments", 768)): 0.999}
+
+    def fake_time(build, knobs, sweeps, warm, torch, repeats=3):
+        return times[tuple(sorted((k, v) for k, v in knobs.items() if v))]
+
+    monkeypatch.setattr(autotune, "time_workload", fake_time)
+    res = autotune.tune(lambda eng: [], {"potts_segments": [768], "o3_planes": [16]}, torch=object())
+    assert res["knobs"]["potts_segments"] == 0 and res["knobs"]["o3_planes"] == 0
+    assert res["ms_per_sweep"] == res["analytic_ms_per_sweep"] == 1.0
+    assert [e["ms_per_sweep"] for e in res["table"]] == [1.0, 0.995, 0.996]
+    res = autotune.tune(lambda eng: [], {"potts_segments": [768, 3072], "o3_planes": [16, 4]}, torch=object())
+    assert res["knobs"]["potts_segments"] == 3072 and res["knobs"]["o3_planes"] == 4
+    assert res["ms_per_sweep"] == 0.92 and res["analytic_ms_per_sweep"] == 1.0
+    # with no margin any improvement is kept
+    res = autotune.tune(lambda eng: [], {"potts_segments": [768], "o3_planes": [16]}, torch=object(), min_gain=0.0)
+    assert res["knobs"]["potts_segments"] == 768 and res["ms_per_sweep"] == 0.995
+
+
 def _mix(gpumc, eng):
     sims = []
     for i, L in enumerate((34, 130, 258)):
@@ -99,7 +127,11 @@ def test_tuner_times_candidates_and_keeps_the_fastest(gpumc):
     from scamper_b200 import autotune
     res = autotune.tune(lambda eng: _mix(gpumc, eng), {"o3_planes": [4, 16], "potts_segments": [768]},
                         sweeps=5, warm=2, torch=torch)
-    assert len(res["table"]) == 4
-    assert res["ms_per_sweep"] == min(r["ms_per_sweep"] for r in res["table"])
+    times = [r["ms_per_sweep"] for r in res["table"]]
+    assert len(times) == 4
+    # the kept plan is a timed one, and no candidate beat it by more than the
+    # tuner's margin
+    assert res["ms_per_sweep"] in times
+    assert res["ms_per_sweep"] <= min(times) / (1.0 - autotune.MIN_GAIN) * (1.0 + 1e-12)
     assert res["ms_per_sweep"] <= res["analytic_ms_per_sweep"]
     assert autotune.get_knobs() == {k: 0 for k in autotune.KNOBS}
