@@ -1,7 +1,7 @@
 // Checkerboard sweep for O(3) Heisenberg spins (float32 unit vectors, three
 // component planes) on periodic square and cubic lattices.
 //
-// The O(3) update costs some 250-270 instructions per site against 24 B of
+// The O(3) update costs some 245-255 instructions per site against 24 B of
 // compulsory traffic, so it is bound by instruction issue and dependency
 // latency, not HBM.  It runs in place as two launches per sweep (colour 0,
 // then colour 1): a colour pass reads only the other colour, whose values
