@@ -410,11 +410,12 @@ def bench_heat_bath(gpumc, torch, args):
 def bench_o3_proposals(gpumc, torch, args):
     """O(3) Metropolis proposals on 3D L=64 x 8 replicas at beta=0.7: the
     engine's adapted cap, the reference's StandardStrategy (uniform unit
-    vector) and OPSSStrategy (plane rotation, sigma adapted), measured in the
-    measurement phase after 20 adapting sweeps."""
+    vector) and OPSSStrategy (plane rotation, sigma adapted), and the cap
+    with the hardware approximations (float32-tolerance parity), measured in
+    the measurement phase after 20 adapting sweeps."""
     from scamper_b200 import _lib
     out = {}
-    for prop in ("cap", "standard", "opss"):
+    for prop in ("cap", "standard", "opss", "cap_fast"):
         mc = gpumc.ClassicalMC.from_params({"lattice_type": "cubic", "L": 64}, 37, model="o3", n_replicas=8,
                                            betas=[0.7], o3_proposal=prop, record_capacity=64)
         mc.sweep(20)

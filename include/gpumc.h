@@ -62,10 +62,15 @@ extern "C" {
 /* O(3) Metropolis proposals: the engine's cap around the current spin
  * (adapted half-angle), the reference's StandardStrategy (independent uniform
  * unit vector, CMC.rs/src/lattice/proposal.rs:45-63) and OPSSStrategy (random
- * plane rotation with adapted bound, proposal.rs:72-167) */
+ * plane rotation with adapted bound, proposal.rs:72-167).  GPUMC_O3_CAP_FAST
+ * is the cap on the same random stream with the hardware approximations of
+ * sqrt, reciprocal, sin / cos and exp: float32-tolerance parity (spins within
+ * a few 1e-7 of the exact cap's, decisions equal except within about 1e-6 of
+ * a threshold), not bit-identical to the CPU replay. */
 #define GPUMC_O3_CAP 0
 #define GPUMC_O3_UNIFORM 1
 #define GPUMC_O3_OPSS 2
+#define GPUMC_O3_CAP_FAST 3
 
 #define GPUMC_INIT_HOT 0  /* "hot" / "random" initial_state */
 #define GPUMC_INIT_COLD 1 /* "cold" / "ordered" */
@@ -99,7 +104,7 @@ typedef struct {
                             /* sigma (radians), (0, pi]                        */
   int32_t record_capacity;  /* measured sweeps buffered on the device (>= 1)   */
   int32_t algorithm;        /* GPUMC_METROPOLIS / HEAT_BATH / SWENDSEN_WANG / WOLFF */
-  int32_t o3_proposal;      /* GPUMC_O3_CAP / UNIFORM / OPSS (O(3) Metropolis) */
+  int32_t o3_proposal;      /* GPUMC_O3_CAP / UNIFORM / OPSS / CAP_FAST        */
 } gpumc_spec;
 
 /* One measured sweep of one replica (Context::measure of Energy, E2,

@@ -38,6 +38,7 @@ WOLFF = 3
 O3_CAP = 0
 O3_UNIFORM = 1
 O3_OPSS = 2
+O3_CAP_FAST = 3
 PHASE_THERMALIZATION = 1
 PHASE_MEASUREMENT = 2
 

@@ -233,8 +233,8 @@ int validate_spec(const gpumc_spec* s) {
     return fail(GPUMC_EINVAL, "initial_state: expected hot/random or cold/ordered");
   if (s->model == GPUMC_O3 && !(s->cone_half_angle > 0.0 && s->cone_half_angle <= M_PI))
     return fail(GPUMC_EINVAL, "cone_half_angle: must be in (0, pi]");
-  if (s->o3_proposal < GPUMC_O3_CAP || s->o3_proposal > GPUMC_O3_OPSS)
-    return fail(GPUMC_EINVAL, "o3_proposal: expected cap, uniform (standard) or opss");
+  if (s->o3_proposal < GPUMC_O3_CAP || s->o3_proposal > GPUMC_O3_CAP_FAST)
+    return fail(GPUMC_EINVAL, "o3_proposal: expected cap, uniform (standard), opss or cap_fast");
   if (s->record_capacity < 1) return fail(GPUMC_EINVAL, "record_capacity: must be >= 1");
   if (s->algorithm < GPUMC_METROPOLIS || s->algorithm > GPUMC_WOLFF)
     return fail(GPUMC_EINVAL, "algorithm: expected metropolis, heat_bath, swendsen_wang or wolff");
@@ -549,7 +549,8 @@ int kernel_kind(const Layout& L) {
   if (L.cluster) return kKindCluster + (L.model == POTTS ? 2 : 0) + (L.dims - 2) + (L.alg == WOLFF ? 4 : 0);
   const int hb = L.alg == HEAT_BATH ? kKindHeatBath
                  : L.prop == GPUMC_O3_UNIFORM ? kKindO3Uniform
-                 : L.prop == GPUMC_O3_OPSS ? kKindO3Opss : 0;
+                 : L.prop == GPUMC_O3_OPSS ? kKindO3Opss
+                 : L.prop == GPUMC_O3_CAP_FAST ? kKindO3Fast : 0;
   if (L.model == POTTS && L.bits) return 8 + (L.dims - 2);
   if (L.model == O3 && L.march) return 10 + o3_row_class(L.pitch) + hb;
   return L.model * 2 + (L.dims - 2) + hb;
@@ -673,14 +674,15 @@ typedef void (*SweepKernel)(const TileItem*, LatDesc*, GroupDesc*, LaunchCtl*);
 // The O(3) z-march kernel of a colour for kind 10..13 (+ algorithm offset).
 #define O3_MARCH_ROW(C, A) \
   {k_sweep_o3_march<C, A, 0>, k_sweep_o3_march<C, A, 1>, k_sweep_o3_march<C, A, 2>, k_sweep_o3_march<C, A, 3>}
-static const SweepKernel kO3March[2][4][4] = {
-    {O3_MARCH_ROW(0, 0), O3_MARCH_ROW(0, 1), O3_MARCH_ROW(0, 2), O3_MARCH_ROW(0, 3)},
-    {O3_MARCH_ROW(1, 0), O3_MARCH_ROW(1, 1), O3_MARCH_ROW(1, 2), O3_MARCH_ROW(1, 3)}};
+static const SweepKernel kO3March[2][5][4] = {
+    {O3_MARCH_ROW(0, 0), O3_MARCH_ROW(0, 1), O3_MARCH_ROW(0, 2), O3_MARCH_ROW(0, 3), O3_MARCH_ROW(0, 4)},
+    {O3_MARCH_ROW(1, 0), O3_MARCH_ROW(1, 1), O3_MARCH_ROW(1, 2), O3_MARCH_ROW(1, 3), O3_MARCH_ROW(1, 4)}};
 #undef O3_MARCH_ROW
 static SweepKernel o3_march_kernel(int colour, int kind) {
   if (!is_o3_march_kind(kind)) return nullptr;
   const int off = kind - kind % 16;
-  const int alg = off == kKindHeatBath ? 1 : off == kKindO3Uniform ? 2 : off == kKindO3Opss ? 3 : 0;
+  const int alg = off == kKindHeatBath ? 1 : off == kKindO3Uniform ? 2 : off == kKindO3Opss ? 3
+                  : off == kKindO3Fast ? 4 : 0;
   return kO3March[colour][alg][kind % 16 - 10];
 }
 static SweepKernel kernel_for(int kind) {
@@ -706,6 +708,8 @@ static SweepKernel kernel_for(int kind) {
     case kKindO3Uniform + 5: return k_sweep_o3<3, 1, 2>;
     case kKindO3Opss + 4: return k_sweep_o3<2, 1, 3>;
     case kKindO3Opss + 5: return k_sweep_o3<3, 1, 3>;
+    case kKindO3Fast + 4: return k_sweep_o3<2, 1, 4>;
+    case kKindO3Fast + 5: return k_sweep_o3<3, 1, 4>;
     default: return nullptr;
   }
 }
@@ -716,7 +720,7 @@ static int prepare_kernels() {
   static std::once_flag once;
   static cudaError_t status = cudaSuccess;
   std::call_once(once, [] {
-    for (int k = 0; k < kKindO3Opss + 16; ++k) {
+    for (int k = 0; k < kKindO3Fast + 16; ++k) {
       if (!kernel_for(k)) continue;
       cudaError_t e = cudaFuncSetAttribute(kernel_for(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kMaxDynSmem);
@@ -732,7 +736,7 @@ static int prepare_kernels() {
       cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
       if (e != cudaSuccess) status = e;
     }
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 5; ++a)
       for (int c = 0; c < 4; ++c) {
         cudaError_t e = cudaFuncSetAttribute(kO3March[0][a][c], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kMaxDynSmem);
@@ -780,6 +784,8 @@ int launch_sweep_kernel(cudaStream_t st, int kind, const TileItem* tiles, int n_
   if (kind == kKindO3Uniform + 5) k_sweep_o3<3, 0, 2><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindO3Opss + 4) k_sweep_o3<2, 0, 3><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (kind == kKindO3Opss + 5) k_sweep_o3<3, 0, 3><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Fast + 4) k_sweep_o3<2, 0, 4><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
+  if (kind == kKindO3Fast + 5) k_sweep_o3<3, 0, 4><<<n_tiles, kThreads, 0, st>>>(tiles, lats, groups, ctl);
   if (is_o3_march_kind(kind)) o3_march_kernel(0, kind)<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   k<<<n_tiles, kThreads, smem, st>>>(tiles, lats, groups, ctl);
   CUDA_TRY(cudaGetLastError());

@@ -96,7 +96,7 @@ struct LatDesc {
   int32_t tile_cx, tile_y, tile_z;  // creation-time tile shape (kernels read TileItem's)
   int32_t group;                    // index into the group array (PT / records)
   int32_t replica;                  // replica index within its group
-  int32_t prop;                     // O(3) Metropolis proposal: 0 cap, 1 uniform, 2 OPSS
+  int32_t prop;                     // O(3) Metropolis proposal: 0 cap, 1 uniform, 2 OPSS, 3 fast cap
   int64_t n_sites;
   void* buf[2];
   void* aux;                        // cluster updates: uint32 label per site

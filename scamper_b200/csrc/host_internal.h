@@ -45,8 +45,9 @@ constexpr int kKindHeatBath = 16;
 // O(3): kKindCluster + 8 + (dims - 2) + 2 (Wolff)
 constexpr int kKindCluster = 32;
 inline bool is_cluster_kind(int kind) { return kind >= kKindCluster && kind < kKindCluster + 16; }
-// O(3) Metropolis with the uniform / OPSS proposal: the cap kind plus these
-constexpr int kKindO3Uniform = 48, kKindO3Opss = 64;
+// O(3) Metropolis with the uniform / OPSS / fast-cap proposal: the cap kind
+// plus these
+constexpr int kKindO3Uniform = 48, kKindO3Opss = 64, kKindO3Fast = 80;
 // 2D Ising on the bit-sliced kernel (either single-site algorithm): the kinds
 // the resident multi-sweep launch can take
 inline bool is_ising2d_bits_kind(int kind) { return kind == 0 || kind == kKindHeatBath; }

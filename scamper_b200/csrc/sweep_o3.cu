@@ -44,6 +44,14 @@
 // ordered pairs) and theta = sigma (2u - 1), u from word 1, its sine and
 // cosine by the engine's own turn polynomials; sigma is the lattice's `omc`.
 //
+// ALG = 4, the fast cap: the cap proposal on the same draws with the
+// hardware approximations of sqrt, reciprocal, sin / cos and exp in place of
+// the exactly rounded operations and the engine's polynomials (about 40
+// instructions per site fewer).  Its spins follow the exact cap's to a few
+// 1e-7 and its decisions differ only where a uniform falls within about 1e-6
+// of its acceptance probability, so its parity is float32 tolerance and
+// statistics, not bit identity with the CPU replay.
+//
 // Heat bath (ALG = 1; ContinuousHeatBathCore, CMC.rs/src/algorithms/
 // heat_bath.rs:75-134, with ContinuousHeatBathable for ONModel<3>,
 // CMC.rs/src/lattice/models.rs:617-663): the new spin is drawn from
@@ -236,28 +244,55 @@ __device__ __forceinline__ f2 exp_neg2_2(f2 x) {
   return mul2(p, sc);
 }
 
+// Hardware approximations (PTX sqrt.approx / rcp.approx, the sin / cos / exp
+// intrinsics) for the fast cap proposal.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Metropolis step of two sites (PROP 0 cap of 1 - cos(alpha) = omc, 1
-// uniform unit vector, 2 OPSS rotation with bound omc): proposals n and the
-// decisions.  Per lane the operations of orc_o3_propose / orc_o3_accept.
+// uniform unit vector, 2 OPSS rotation with bound omc, 3 the cap with the
+// hardware approximations of sqrt, reciprocal, sin / cos and exp): proposals
+// n and the decisions.  Per lane (PROP 0-2) the operations of
+// orc_o3_propose / orc_o3_accept; PROP 3 takes the same draws and differs from
+// PROP 0 only by the approximations' rounding (float32-tolerance parity).
 template <int PROP>
 __device__ __forceinline__ void o3_metropolis_2(f2 ax, f2 ay, f2 az, f2 hx, f2 hy, f2 hz, const uint4& oa,
                                                 const uint4& ob, float omc, float mJ, float beta, f2& nx,
                                                 f2& ny, f2& nz, bool& ok_a, bool& ok_b) {
   f2 px, py, pz;
-  if (PROP == 0) {
+  if (PROP == 0 || PROP == 3) {
     const f2 w = mul2(unit23_2(oa.x, ob.x), F2s(omc));
     const f2 ct = sub2(F2s(1.0f), w);
     const f2 s2 = fma2(mul2(w, F2s(-1.0f)), w, add2(w, w));
-    const f2 st = F2(__fsqrt_rn(lo(s2)), __fsqrt_rn(hi(s2)));
-    f2 cp, sp;
-    sincos23_2(oa.y, ob.y, cp, sp);
+    f2 st, cp, sp;
+    if (PROP == 0) {
+      st = F2(__fsqrt_rn(lo(s2)), __fsqrt_rn(hi(s2)));
+      sincos23_2(oa.y, ob.y, cp, sp);
+    } else {
+      st = F2(sqrt_approx(lo(s2)), sqrt_approx(hi(s2)));
+      // phi = 2 pi u / 2^32 taken in [-pi, pi) (u as a signed word): the
+      // same angle modulo 2 pi, where the intrinsics are most accurate
+      float sa, ca, sb, cb;
+      __sincosf((float)(int32_t)oa.y * 0x1.921fb6p-30f, &sa, &ca);
+      __sincosf((float)(int32_t)ob.y * 0x1.921fb6p-30f, &sb, &cb);
+      cp = F2(ca, cb);
+      sp = F2(sa, sb);
+    }
     const f2 vx = mul2(st, cp), vy = mul2(st, sp);
     // Duff et al. (JCGT 2017) basis {e1, e2, a}: sg = sign(az), k = -1/(sg + az)
     const f2 sg = F2(lo(az) >= 0.0f ? 1.0f : -1.0f, hi(az) >= 0.0f ? 1.0f : -1.0f);
     const f2 d = add2(sg, az);
     // -1 / d as the negated correctly rounded reciprocal: round-to-nearest
     // is symmetric in sign, so this is the IEEE quotient bit for bit (|d| >= 1)
-    const f2 k = F2(-__frcp_rn(lo(d)), -__frcp_rn(hi(d)));
+    const f2 k = PROP == 0 ? F2(-__frcp_rn(lo(d)), -__frcp_rn(hi(d))) : F2(-rcp_approx(lo(d)), -rcp_approx(hi(d)));
     const f2 axk = mul2(ax, k);
     const f2 b = mul2(ay, axk);
     const f2 sax = mul2(sg, ax);
@@ -297,7 +332,8 @@ __device__ __forceinline__ void o3_metropolis_2(f2 ax, f2 ay, f2 az, f2 hx, f2 h
   pz = mul2(pz, f);
   const f2 dot = fma2(sub2(pz, az), hz, fma2(sub2(py, ay), hy, mul2(sub2(px, ax), hx)));
   const f2 de = mul2(F2s(mJ), dot);
-  const f2 p = exp_neg2_2(mul2(F2s(-beta), de));
+  const f2 bde = mul2(F2s(-beta), de);
+  const f2 p = PROP == 3 ? F2(__expf(fmaxf(lo(bde), -87.0f)), __expf(fmaxf(hi(bde), -87.0f))) : exp_neg2_2(bde);
   const f2 u = half23_2(oa.z, ob.z);
   ok_a = lo(de) <= 0.0f || lo(u) < lo(p);
   ok_b = hi(de) <= 0.0f || hi(u) < hi(p);
@@ -454,8 +490,8 @@ __device__ __forceinline__ void o3_update_pair(const O3Site& qa, const O3Site& q
     fz2 = F2(nz, mz);
   } else {
     f2 nx, ny, nz;
-    o3_metropolis_2<ALG == 2 ? 1 : (ALG == 3 ? 2 : 0)>(fx2, fy2, fz2, hx, hy, hz, oa, ob, omc, mJ, beta, nx, ny, nz,
-                                                        ok_a, ok_b);
+    constexpr int PROP = ALG == 2 ? 1 : (ALG == 3 ? 2 : (ALG == 4 ? 3 : 0));
+    o3_metropolis_2<PROP>(fx2, fy2, fz2, hx, hy, hz, oa, ob, omc, mJ, beta, nx, ny, nz, ok_a, ok_b);
     fx2 = F2(ok_a ? lo(nx) : qa.ax, ok_b ? hi(nx) : qb.ax);
     fy2 = F2(ok_a ? lo(ny) : qa.ay, ok_b ? hi(ny) : qb.ay);
     fz2 = F2(ok_a ? lo(nz) : qa.az, ok_b ? hi(nz) : qb.az);
@@ -954,6 +990,7 @@ O3_INSTANTIATE(0)
 O3_INSTANTIATE(1)
 O3_INSTANTIATE(2)
 O3_INSTANTIATE(3)
+O3_INSTANTIATE(4)
 
 GPUMC_BOUNDS_MODULE(sweep_o3)
 

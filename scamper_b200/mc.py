@@ -108,9 +108,11 @@ def lattice_from_params(params):
 
 # O(3) Metropolis proposals: the engine's adapted cap, the reference's
 # StandardStrategy (uniform unit vector) and OPSSStrategy (plane rotation),
-# CMC.rs/src/lattice/proposal.rs:45-167
+# CMC.rs/src/lattice/proposal.rs:45-167, and the cap with the hardware
+# approximations of sqrt, reciprocal, sin / cos and exp ("cap_fast":
+# float32-tolerance parity, not bit-identical)
 O3_PROPOSALS = {"cap": _lib.O3_CAP, "cone": _lib.O3_CAP, "standard": _lib.O3_UNIFORM,
-                "uniform": _lib.O3_UNIFORM, "opss": _lib.O3_OPSS}
+                "uniform": _lib.O3_UNIFORM, "opss": _lib.O3_OPSS, "cap_fast": _lib.O3_CAP_FAST}
 
 
 def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capacity=1024, algorithm=None,
@@ -138,7 +140,7 @@ def spec_from_params(params, model=None, n_replicas=1, betas=None, record_capaci
     prop = "cap" if o3_proposal is None else str(o3_proposal).lower()
     if prop not in O3_PROPOSALS:
         raise InvalidConfig(_lib.EINVAL, f"o3_proposal: unknown proposal `{o3_proposal}` "
-                                         "(expected cap, standard or opss)")
+                                         "(expected cap, standard, opss or cap_fast)")
     # the OPSS bound starts at OPSSStrategy's default sigma = 0.5 unless given
     step = params.get_as("opss_sigma", float, 0.5) if O3_PROPOSALS[prop] == _lib.O3_OPSS else \
         params.get_as("cone_half_angle", float, 1.0)
@@ -248,8 +250,11 @@ class ClassicalMC:
         per sweep), the cluster updates for Ising / Potts / O(3) with J >= 0.
         `o3_proposal` (O(3) Metropolis): "cap" (default: a cap around the
         current spin, half-angle adapted), "standard" (StandardStrategy:
-        uniform unit vector) or "opss" (OPSSStrategy: plane rotation, bound
-        from params["opss_sigma"], default 0.5, adapted)."""
+        uniform unit vector), "opss" (OPSSStrategy: plane rotation, bound
+        from params["opss_sigma"], default 0.5, adapted) or "cap_fast" (the
+        cap on the same draws with the hardware approximations of sqrt,
+        reciprocal, sin / cos and exp: spins within float32 tolerance of the
+        cap's, not bit-identical)."""
         spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas,
                                       record_capacity=record_capacity, algorithm=algorithm,
                                       o3_proposal=o3_proposal)

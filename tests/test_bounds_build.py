@@ -52,6 +52,7 @@ CHILD = textwrap.dedent('''
         ("o3", (66, 10), {}, None), ("o3", (8, 6, 20), {}, None), ("o3", (64, 64, 8), {}, None),
         ("o3", (70, 4, 6), {}, "heat_bath"), ("o3", (16, 8, 12), {"o3_proposal": "opss"}, None),
         ("o3", (10, 6), {"o3_proposal": "standard"}, None), ("o3", (8, 8, 8), {}, "wolff"),
+        ("o3", (16, 8, 12), {"o3_proposal": "cap_fast"}, None), ("o3", (10, 6), {"o3_proposal": "cap_fast"}, None),
         ("msc", (66, 10), {}, None), ("msc", (34, 6, 20), {}, None),
     ]
     oracle.build()
