@@ -18,6 +18,7 @@ bit identity:
   (random-permutation Metropolis, oracle/refsampler.c) within |z| < 3, as
   the exact cap does (CMC.rs/tests/physics/zscore_extended.rs:175-245).
 """
+import ctypes
 import math
 
 import numpy as np
@@ -40,6 +41,10 @@ def test_fast_cap_is_a_named_proposal(gpumc):
     spec, _keep = gpumc.mc.spec_from_params(_params((8, 8), beta=0.5), model="o3", o3_proposal="cap_fast")
     assert spec.o3_proposal == _lib.O3_CAP_FAST == 3
     gpumc.ClassicalMC.validate_params(_params((8, 8, 8), beta=0.5), model="o3", o3_proposal="cap_fast")
+    # the C ABI rejects proposal codes past the last one
+    spec.o3_proposal = 4
+    with pytest.raises(gpumc.InvalidConfig):
+        _lib.call("gpumc_validate", ctypes.byref(spec))
 
 
 @pytest.mark.gpu
