@@ -306,7 +306,10 @@ typedef struct {
 /* hbm_budget: bytes of device memory the server may hold for resident
  * lattices; chunk: sweeps per batched launch group (admission granularity). */
 int gpumc_server_create(int32_t device, size_t hbm_budget, uint32_t chunk, gpumc_server** out);
-/* Admits the job if its footprint fits the free budget, else GPUMC_EAGAIN. */
+/* Queues the job; gpumc_server_step admits queued jobs in arrival order as
+ * their footprint fits the free budget.  The spec (its betas included) is
+ * copied.  GPUMC_EAGAIN when the admission queue is full, GPUMC_EINVAL when
+ * the footprint exceeds the whole budget. */
 int gpumc_submit(gpumc_server* srv, const gpumc_job* job, uint64_t* job_id);
 /* Runs one scheduling round: packs admitted jobs into the running batch,
  * launches `chunk` sweeps, retires finished jobs.  Returns the number of

@@ -641,19 +641,21 @@ class Server:
         self.h = ctypes.c_void_p()
         _lib.call("gpumc_server_create", device, ctypes.c_size_t(int(hbm_budget)), chunk,
                   ctypes.byref(self.h))
-        self._keep = {}
 
     def submit(self, params, seed, n_sweeps, n_therm=0, model=None, n_replicas=1, betas=None,
-               algorithm=None):
+               algorithm=None, o3_proposal=None):
+        """Queues a job (ClassicalMC.from_params's model / algorithm /
+        o3_proposal arguments); returns its id, or None when the queue is
+        full (GPUMC_EAGAIN)."""
         spec, keep = spec_from_params(params, model=model, n_replicas=n_replicas, betas=betas,
-                                      algorithm=algorithm)
+                                      algorithm=algorithm, o3_proposal=o3_proposal)
         job = _lib.Job(spec=spec, base_seed=seed, n_sweeps=n_sweeps, n_therm=n_therm)
         jid = ctypes.c_uint64()
         rc = _lib.load().gpumc_submit(self.h, ctypes.byref(job), ctypes.byref(jid))
         if rc == _lib.EAGAIN:
             return None
         _lib.check(rc)
-        self._keep[jid.value] = keep
+        del keep  # gpumc_submit copied the spec and its betas
         return jid.value
 
     def step(self):

@@ -164,11 +164,15 @@ def test_server_results_identical_alone_and_in_mix(gpumc):
         ("o3", (8, 8, 8), dict(beta=0.7), 30, 12),
         ("ising", (16, 16, 16), dict(beta=0.22), 17, 3),
         ("potts", (66, 18), dict(q=4, beta=1.1), 50, 0),
+        ("o3", (8, 8, 6), dict(beta=0.7, o3_proposal="opss"), 20, 6),
+        ("o3", (6, 6, 6), dict(beta=0.7, o3_proposal="cap_fast"), 15, 4),
     ]
     srv = gpumc.Server(hbm_budget=1 << 30, chunk=7)
     ids = []
     for i, (model, shape, kw, nmeas, ntherm) in enumerate(jobs):
-        ids.append(srv.submit(_params(shape, **kw), 500 + i, nmeas, ntherm, model=model))
+        kw = dict(kw)
+        prop = kw.pop("o3_proposal", None)
+        ids.append(srv.submit(_params(shape, **kw), 500 + i, nmeas, ntherm, model=model, o3_proposal=prop))
         srv.step()  # later jobs arrive while earlier ones are running
     done = {}
     for _ in range(200):
@@ -182,7 +186,10 @@ def test_server_results_identical_alone_and_in_mix(gpumc):
     assert len(done) == len(jobs)
     for jid, (model, shape, kw, nmeas, ntherm) in zip(ids, jobs):
         assert done[jid]["status"] == 0
-        alone = gpumc.ClassicalMC.from_params(_params(shape, **kw), 500 + ids.index(jid), model=model)
+        kw = dict(kw)
+        prop = kw.pop("o3_proposal", None)
+        alone = gpumc.ClassicalMC.from_params(_params(shape, **kw), 500 + ids.index(jid), model=model,
+                                              o3_proposal=prop)
         from scamper_b200 import _lib
         alone.sweep(ntherm)
         alone.on_phase_start(_lib.PHASE_MEASUREMENT)
