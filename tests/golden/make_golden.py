@@ -47,13 +47,21 @@ CASES = [
     ("potts", [10, 8, 6], 0.55, 134, 4, {"q": 4, "algorithm": "wolff"}),
     ("o3", [34, 18], 0.8, 135, 3, {"algorithm": "swendsen_wang"}),
     ("o3", [10, 8, 6], 0.6, 136, 4, {"algorithm": "wolff"}),
+    # the reference's O(3) proposals (StandardStrategy, OPSSStrategy at a
+    # fixed sigma)
+    ("o3", [34, 18], 0.8, 137, 3, {"proposal": "standard"}),
+    ("o3", [16, 8, 12], 0.7, 138, 3, {"proposal": "opss", "sigma": 0.7}),
 ]
 
 _ALGS = {"heat_bath": "-hb", "swendsen_wang": "-sw", "wolff": "-wolff"}
+# O(3) Metropolis proposal codes of the oracle (0 = the engine's cap)
+PROPOSALS = {"standard": 1, "opss": 2}
 
 
 def case_id(c):
     suffix = _ALGS.get(c["extra"].get("algorithm"), "")
+    if "proposal" in c["extra"]:
+        suffix += "-" + c["extra"]["proposal"]
     return f"{c['model']}-{'x'.join(map(str, c['shape']))}{suffix}"
 
 
@@ -69,8 +77,11 @@ def run_case(oracle, model, shape, beta, seed, sweeps, extra):
     mid = {"ising": oracle.ISING, "potts": oracle.POTTS, "o3": oracle.O3, "msc": oracle.MSC}[model]
     alg = {"heat_bath": oracle.HEAT_BATH, "swendsen_wang": oracle.SWENDSEN_WANG,
            "wolff": oracle.WOLFF}.get(extra.get("algorithm"), oracle.METROPOLIS)
+    prop = PROPOSALS.get(extra.get("proposal"), 0)
+    # OPSS: the oracle's step parameter is sigma itself (float32)
+    step = float(np.float32(extra["sigma"])) if prop == 2 else omc(extra.get("alpha", 1.0))
     lat = oracle.Lattice(mid, tuple(shape), q=extra.get("q", 3), J=extra.get("J", 1.0), beta=beta,
-                         seed=seed, omc=omc(extra.get("alpha", 1.0)), algorithm=alg)
+                         seed=seed, omc=step, algorithm=alg, prop=prop)
     for _ in range(sweeps):
         lat.sweep(adapt=False)
     st = lat.state()

@@ -225,6 +225,7 @@ def _golden_cases():
                          ids=[f"{c['model']}-{'x'.join(map(str, c['shape']))}"
                               + {"heat_bath": "-hb", "swendsen_wang": "-sw", "wolff": "-wolff"}.get(
                                   c["extra"].get("algorithm"), "")
+                              + ("-" + c["extra"]["proposal"] if "proposal" in c["extra"] else "")
                               for c in _golden_cases()])
 def test_device_matches_committed_golden_fingerprints(gpumc, case):
     """The device against the committed fixtures, without the oracle."""
@@ -232,12 +233,12 @@ def test_device_matches_committed_golden_fingerprints(gpumc, case):
     from scamper_b200 import _lib
     shape, extra = tuple(case["shape"]), case["extra"]
     params = _params(shape, beta=case["beta"], q=extra.get("q", 3), J=extra.get("J", 1.0),
-                     cone_half_angle=extra.get("alpha", 1.0))
+                     cone_half_angle=extra.get("alpha", 1.0), opss_sigma=extra.get("sigma", 0.5))
     if case["model"] == "msc":
         mc = gpumc.MultiSpinIsing.from_params(params, case["seed"])
     else:
         mc = gpumc.ClassicalMC.from_params(params, case["seed"], model=case["model"],
-                                           algorithm=extra.get("algorithm"))
+                                           algorithm=extra.get("algorithm"), o3_proposal=extra.get("proposal"))
     mc.on_phase_start(_lib.PHASE_MEASUREMENT)  # no cone adaptation (O(3))
     mc.sweep(case["sweeps"])
     st = np.ascontiguousarray(_gpu_state(mc))
