@@ -307,3 +307,47 @@ def test_kaufman_energy_approaches_onsager():
     ons = exact.onsager_energy_per_site(b)
     assert ons == pytest.approx(-math.sqrt(2.0), abs=1e-9)
     assert abs(e512 - ons) < abs(e64 - ons) < 0.02
+
+
+def _abs_m_series(oracle, L, beta, seed, therm, meas, algorithm):
+    lat = oracle.Lattice(oracle.ISING, (L, L), beta=beta, seed=seed, algorithm=algorithm)
+    for _ in range(therm):
+        lat.sweep()
+    m = np.empty(meas)
+    for t in range(meas):
+        lat.sweep()
+        m[t] = abs(int(lat.spins.sum(dtype=np.int64))) / (L * L)
+    return m
+
+
+def _binned_mean(x, n_bins=20):
+    bins = np.array_split(x, n_bins)
+    means = np.array([b.mean() for b in bins])
+    return means.mean(), means.std(ddof=1) / math.sqrt(n_bins)
+
+
+def test_wolff_binder_cumulant_at_tc_matches_universal_value(oracle):
+    """U4 = 1 - <m^4> / (3 <m^2>^2) of the 2D Ising model at beta_c from the
+    oracle's Wolff update: within 0.04 of the universal 0.610 at L = 32 and
+    size-independent between L = 16 and 32 within 0.05, with the reference's
+    run lengths and criteria (10^4 + 8 10^4 single-cluster updates, seed 42;
+    CMC.rs/tests/physics/long_convergence.rs:16-61)."""
+    u = {}
+    for L in (16, 32):
+        m = _abs_m_series(oracle, L, exact.BETA_C_2D_ISING, 42, 10_000, 80_000, oracle.WOLFF)
+        u[L] = 1.0 - np.mean(m ** 4) / (3.0 * np.mean(m ** 2) ** 2)
+    assert abs(u[32] - 0.610) < 0.04, u
+    assert abs(u[16] - u[32]) < 0.05, u
+
+
+def test_checkerboard_magnetization_follows_onsager(oracle):
+    """The checkerboard Metropolis replay (the engine's method) on the 8 x 8
+    torus: |M| vanishes at beta = 0.1 (below 0.3 + 3 sigma) and matches
+    Onsager's spontaneous magnetisation (1 - sinh(2 beta)^-4)^(1/8) within
+    10 % + 3 sigma at beta = 1 (CMC.rs/tests/exact/onsager.rs:60-95)."""
+    m, err = _binned_mean(_abs_m_series(oracle, 8, 0.1, 7, 500, 2000, oracle.METROPOLIS))
+    assert m < 0.3 + 3.0 * err, (m, err)
+    m, err = _binned_mean(_abs_m_series(oracle, 8, 1.0, 8, 1000, 2000, oracle.METROPOLIS))
+    onsager = (1.0 - math.sinh(2.0) ** -4) ** 0.125
+    assert m > 0.5 - 3.0 * err, (m, err)
+    assert abs(m - onsager) < 0.10 * onsager + 3.0 * err, (m, err, onsager)
