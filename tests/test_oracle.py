@@ -351,3 +351,35 @@ def test_checkerboard_magnetization_follows_onsager(oracle):
     onsager = (1.0 - math.sinh(2.0) ** -4) ** 0.125
     assert m > 0.5 - 3.0 * err, (m, err)
     assert abs(m - onsager) < 0.10 * onsager + 3.0 * err, (m, err, onsager)
+
+
+def test_o3_energy_is_the_bond_dot_product(oracle):
+    """-J sum over bonds of s_i . s_j (CMC.rs/tests/physics/continuous_spins.rs:9-25,
+    there on a two-site chain; here on the 4 x 4 torus, 2N bonds): equal
+    spins give -J 2N, orthogonal spins on the two colours give 0, and a
+    random configuration equals the edge-list sum; the fixed-point energy the
+    kernels record agrees to its resolution."""
+    J, L = 1.7, 4
+    lat = oracle.Lattice(oracle.O3, (L, L), J=J, beta=0.5, seed=3)
+    n = L * L
+    lat.set_state(np.tile(np.float32([0.0, 0.6, 0.8]), (n, 1)))
+    assert lat.energy() == pytest.approx(-J * 2 * n, rel=1e-6)
+    y, x = np.divmod(np.arange(n), L)
+    cb = np.where(((x + y) % 2 == 0)[:, None], np.float32([1.0, 0.0, 0.0]), np.float32([0.0, 0.6, 0.8]))
+    lat.set_state(cb)
+    assert lat.energy() == pytest.approx(0.0, abs=1e-6)
+    v = np.random.default_rng(11).normal(size=(n, 3))
+    s = (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+    lat.set_state(s)
+    s64 = s.astype(np.float64).reshape(L, L, 3)
+    bonds = (s64 * np.roll(s64, -1, axis=0)).sum() + (s64 * np.roll(s64, -1, axis=1)).sum()
+    assert lat.energy() == pytest.approx(-J * bonds, rel=1e-6, abs=1e-9)
+    assert lat.fixed_observables()[0] == pytest.approx(-J * bonds, abs=1e-4)
+
+
+def test_potts_critical_coupling(gpumc):
+    """beta_c(q) = ln(1 + sqrt(q)) (CMC.rs/tests/physics/potts_exact.rs:480-485):
+    1.0051 for q = 3, and q = 2 is twice the Ising coupling (the Potts energy
+    counts equal neighbours, half the Ising bond's range)."""
+    assert gpumc.potts_beta_c(3) == pytest.approx(1.0051, abs=1e-4)
+    assert gpumc.potts_beta_c(2) == pytest.approx(2.0 * exact.BETA_C_2D_ISING, rel=1e-15)
