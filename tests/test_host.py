@@ -122,3 +122,35 @@ def test_every_geometry_has_a_tile_plan(gpumc, model):
                     p = {"lattice_type": "square", "Lx": shape[0], "Ly": shape[1], "beta": 0.4, "q": q}
                     spec, keep = spec_from_params(p, model=model)
                     assert lib.gpumc_validate(ctypes.byref(spec)) == 0, (model, q, shape, gpumc._lib.last_error())
+
+
+def test_random_geometries_validate_and_plan(gpumc):
+    """Seeded random lattices across models, algorithms and O(3) proposals:
+    every even extent >= 4 validates and gets a tile plan with and without
+    refinement; an odd extent is rejected with GPUMC_EINVAL (the checkerboard
+    needs even extents)."""
+    import random
+    from scamper_b200.mc import spec_from_params
+    lib = gpumc._lib.load()
+    rng = random.Random(5)
+    for _ in range(600):
+        model = rng.choice(["ising", "potts", "o3"])
+        q = rng.choice([2, 3, 4, 5, 6, 8]) if model == "potts" else 3
+        alg = rng.choice([None, "heat_bath"])
+        prop = rng.choice([None, "standard", "opss", "cap_fast"]) if model == "o3" and alg is None else None
+        if rng.random() < 0.5:
+            lx, ly = 2 * rng.randint(2, 6000), 2 * rng.randint(2, 3000)
+            if lx * ly > 300_000_000:
+                continue
+            p = {"lattice_type": "square", "Lx": lx, "Ly": ly, "beta": 0.4, "q": q}
+        else:
+            lx, ly, lz = (2 * rng.randint(2, 160) for _ in range(3))
+            p = {"lattice_type": "cubic", "Lx": lx, "Ly": ly, "Lz": lz, "beta": 0.4, "q": q}
+        spec, keep = spec_from_params(p, model=model, algorithm=alg, o3_proposal=prop)
+        assert lib.gpumc_validate(ctypes.byref(spec)) == 0, (p, model, alg, prop, gpumc._lib.last_error())
+        for refine in (True, False):
+            n, kind = gpumc.plan_tiles(p, model=model, algorithm=alg, refine=refine)
+            assert n > 0, (p, model, alg, refine)
+        odd = dict(p, Lx=lx + 1)
+        spec, keep = spec_from_params(odd, model=model, algorithm=alg, o3_proposal=prop)
+        assert lib.gpumc_validate(ctypes.byref(spec)) == gpumc._lib.EINVAL, odd
